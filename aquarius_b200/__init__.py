@@ -1,0 +1,335 @@
+"""aquarius_b200 — B200-native 3D FLIP step behind the Aquarius solver API.
+
+Python mirror of the reference's plugin surface (AmesingFlank/Aquarius):
+
+    FluidConfig, ConfigFLIP, InitializationVolume, ShapeType
+        Fluid/FluidConfig.cuh:16-97
+    Fluid.init(config) / simulationStep() / physicalTime / getCenter() /
+    getContainerSize() / draw(cmd)
+        Fluid/Fluid.h:4-12, Fluid/Fluid_3D.cuh:7-12, Fluid/Fluid_3D_FLIP.cu:316-505
+
+Everything runs in libaquarius_b200.so (hand-written sm_100a kernels behind
+the C ABI of include/aquarius_b200.h).  There is no CPU fallback: importing
+works without a GPU, but creating a Fluid without the library or a device
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import dataclasses
+import enum
+import os
+import pathlib
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+
+__all__ = [
+    "ShapeType", "InitializationVolume", "ConfigFLIP", "FluidConfig", "Fluid", "AquariusError",
+    "library_path", "load_library", "STAGES",
+]
+
+STAGES = _abi.STAGES
+_PKG = pathlib.Path(__file__).resolve().parent
+_LIB_NAME = "libaquarius_b200.so"
+_lib = None
+
+
+class AquariusError(RuntimeError):
+    """Raised when a C-ABI call returns a status other than AQ_OK."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{_abi.STATUS_NAMES.get(status, status)}: {message}")
+
+
+def library_path() -> pathlib.Path:
+    return _PKG / _LIB_NAME
+
+
+def load_library() -> ct.CDLL:
+    """Loads the in-tree library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = library_path()
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: build it with `python -m aquarius_b200.build`")
+    lib = ct.CDLL(str(p))
+    P = ct.c_void_p
+    sigs = {
+        "aq_abi_version": (ct.c_int32, []),
+        "aq_last_error": (ct.c_char_p, []),
+        "aq_config_default": (ct.c_int, [ct.POINTER(_abi.Config)]),
+        "aq_config_validate": (ct.c_int, [ct.POINTER(_abi.Config)]),
+        "aq_fluid_create": (ct.c_int, [ct.POINTER(_abi.Config), ct.POINTER(P)]),
+        "aq_fluid_step": (ct.c_int, [P, ct.c_int32]),
+        "aq_fluid_step_host": (ct.c_int, [P, ct.c_int32, P, P, P, P]),
+        "aq_fluid_run_stage": (ct.c_int, [P, ct.c_int32]),
+        "aq_fluid_synchronize": (ct.c_int, [P]),
+        "aq_fluid_time": (ct.c_int, [P, ct.POINTER(ct.c_double)]),
+        "aq_fluid_particle_count": (ct.c_int, [P, ct.POINTER(ct.c_int32)]),
+        "aq_fluid_container": (ct.c_int, [P, ct.POINTER(ct.c_float), ct.POINTER(ct.c_float)]),
+        "aq_fluid_stream": (ct.c_int, [P, ct.POINTER(P)]),
+        "aq_fluid_download_state": (ct.c_int, [P, ct.POINTER(_abi.HostState)]),
+        "aq_fluid_upload_state": (ct.c_int, [P, ct.POINTER(_abi.HostState)]),
+        "aq_fluid_solve_stats": (ct.c_int, [P, ct.POINTER(_abi.SolveStats)]),
+        "aq_fluid_pcg_reference": (ct.c_int, [P, ct.c_double, ct.c_int32, P, ct.POINTER(ct.c_double),
+                                              ct.POINTER(ct.c_int32), ct.POINTER(ct.c_double)]),
+        "aq_fluid_profile_step": (ct.c_int, [P, ct.POINTER(ct.c_float)]),
+        "aq_fluid_launches_per_step": (ct.c_int, [P, ct.POINTER(ct.c_int32)]),
+        "aq_fluid_launch_counts": (ct.c_int, [P, ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int32)]),
+        "aq_fluid_benchmark_pressure": (ct.c_int, [P, ct.c_int32, ct.POINTER(ct.c_float), ct.POINTER(ct.c_int32),
+                                                   ct.POINTER(ct.c_int64)]),
+        "aq_fluid_set_jacobi_plan": (ct.c_int, [P, ct.c_int32, ct.c_int32, ct.c_int32]),
+        "aq_fluid_get_jacobi_plan": (ct.c_int, [P, ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int32),
+                                                ct.POINTER(ct.c_int32)]),
+        "aq_fluid_destroy": (None, [P]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(status: int):
+    if status != _abi.AQ_OK:
+        msg = load_library().aq_last_error()
+        raise AquariusError(status, msg.decode() if msg else "")
+
+
+class ShapeType(enum.IntEnum):
+    """ShapeType {Sphere, Square} (Fluid/FluidConfig.cuh:16-18)."""
+    Sphere = _abi.SHAPE_SPHERE
+    Square = _abi.SHAPE_SQUARE
+
+
+@dataclasses.dataclass
+class InitializationVolume:
+    """InitializationVolume (Fluid/FluidConfig.cuh:20-38); [0,1] coordinates."""
+    shapeType: ShapeType = ShapeType.Square
+    boxMin: Sequence[float] = (0.0, 0.0, 0.0)
+    boxMax: Sequence[float] = (1.0, 0.1875, 1.0)
+    ballCenter: Sequence[float] = (0.5, 0.75, 0.5)
+    ballRadius: float = 0.125
+    phase: int = 0
+
+
+@dataclasses.dataclass
+class ConfigFLIP:
+    """ConfigFLIP (Fluid/FluidConfig.cuh:41-50)."""
+    sizeX: int = 50
+    sizeY: int = 50
+    sizeZ: int = 50
+    pressureIterations: int = 100
+    diffusionIterations: int = 100
+    timestep: float = 0.033
+    FLIPcoeff: float = 0.95
+    particleJitter: float = 0.05
+
+
+def _default_volumes():
+    return [InitializationVolume(ShapeType.Square), InitializationVolume(ShapeType.Sphere)]
+
+
+@dataclasses.dataclass
+class FluidConfig:
+    """FluidConfig (Fluid/FluidConfig.cuh:68-97) plus this library's solver options.
+
+    Extensions (no reference counterpart): gridPhysicalSize (the reference's
+    Fluid member, 10), seed (rand() seed; the reference's unseeded rand() is
+    seed 1), pressureInit ('carry' = reference, 'zero'), solveMode ('fixed' =
+    reference, 'residual'), relResidual, maxIterations, checkInterval,
+    device, stream (a cudaStream_t as int, or None).
+    """
+    method: str = "FLIP"
+    initialVolumes: list = dataclasses.field(default_factory=_default_volumes)
+    gravity: Sequence[float] = (0.0, -9.8, 0.0)
+    phaseCount: int = 2
+    phaseDensities: Sequence[float] = (1.0, 1.0, 1.0, 1.0)
+    diffusionCoeff: float = 0.001
+    FLIP: ConfigFLIP = dataclasses.field(default_factory=ConfigFLIP)
+    gridPhysicalSize: float = 10.0
+    seed: int = 1
+    pressureInit: str = "carry"
+    solveMode: str = "fixed"
+    relResidual: float = 1e-4
+    maxIterations: int = 2000
+    checkInterval: int = 40
+    device: int = 0
+    stream: Optional[int] = None
+
+    def to_c(self) -> _abi.Config:
+        if self.method != "FLIP":
+            raise ValueError(f"method {self.method!r}: this library implements the FLIP solver only")
+        vols = []
+        for v in self.initialVolumes:
+            vols.append(dict(shape="sphere" if ShapeType(v.shapeType) == ShapeType.Sphere else "box",
+                             min=tuple(v.boxMin), max=tuple(v.boxMax), center=tuple(v.ballCenter),
+                             radius=v.ballRadius, phase=v.phase))
+        f = self.FLIP
+        return _abi.make_config(
+            (f.sizeX, f.sizeY, f.sizeZ), vols, gravity=tuple(self.gravity), phase_count=self.phaseCount,
+            phase_densities=tuple(self.phaseDensities), diffusion_coeff=self.diffusionCoeff,
+            pressure_iterations=f.pressureIterations, diffusion_iterations=f.diffusionIterations,
+            timestep=f.timestep, flip_coeff=f.FLIPcoeff, particle_jitter=f.particleJitter,
+            domain_size=self.gridPhysicalSize, seed=self.seed,
+            pressure_init={"carry": _abi.PRESSURE_CARRY, "zero": _abi.PRESSURE_ZERO}[self.pressureInit],
+            solve_mode={"fixed": _abi.SOLVE_FIXED, "residual": _abi.SOLVE_RESIDUAL}[self.solveMode],
+            rel_residual=self.relResidual, max_iterations=self.maxIterations,
+            check_interval=self.checkInterval, device=self.device, stream=self.stream)
+
+
+class Fluid:
+    """Fluid_3D_FLIP::Fluid: init(config) then simulationStep() per frame."""
+
+    def __init__(self, config: Optional[FluidConfig] = None):
+        self._lib = load_library()
+        self._h = ct.c_void_p()
+        self.config: Optional[FluidConfig] = None
+        self._cfg_c: Optional[_abi.Config] = None
+        if config is not None:
+            self.init(config)
+
+    # -- reference surface ---------------------------------------------------
+    def init(self, config: FluidConfig):
+        """Fluid::init (Fluid/Fluid_3D_FLIP.cu:435-505)."""
+        self.close()
+        cfg_c = config.to_c() if isinstance(config, FluidConfig) else config
+        _check(self._lib.aq_fluid_create(ct.byref(cfg_c), ct.byref(self._h)))
+        self.config = config if isinstance(config, FluidConfig) else None
+        self._cfg_c = cfg_c
+        n = ct.c_int32()
+        _check(self._lib.aq_fluid_particle_count(self._h, ct.byref(n)))
+        self.particleCount = n.value
+        self.size = (cfg_c.size_x, cfg_c.size_y, cfg_c.size_z)
+
+    def simulationStep(self):
+        """Fluid::simulationStep (Fluid/Fluid_3D_FLIP.cu:316-352), asynchronous."""
+        _check(self._lib.aq_fluid_step(self._h, 1))
+
+    def draw(self, drawCommand=None):
+        """Rendering is not part of this library (headless)."""
+
+    @property
+    def physicalTime(self) -> float:
+        t = ct.c_double()
+        _check(self._lib.aq_fluid_time(self._h, ct.byref(t)))
+        return t.value
+
+    def getCenter(self):
+        c = (ct.c_float * 3)()
+        _check(self._lib.aq_fluid_container(self._h, c, None))
+        return tuple(c)
+
+    def getContainerSize(self) -> float:
+        s = ct.c_float()
+        _check(self._lib.aq_fluid_container(self._h, None, ct.byref(s)))
+        return s.value
+
+    # -- extensions -----------------------------------------------------------
+    def step(self, n: int = 1):
+        _check(self._lib.aq_fluid_step(self._h, n))
+
+    def step_host(self, n: int, position_in=None, velocity_in=None, position_out=None, velocity_out=None):
+        """Steps with particle state in host arrays ([3][N] float32)."""
+        def ptr(a):
+            return None if a is None else a.ctypes.data
+        _check(self._lib.aq_fluid_step_host(self._h, n, ptr(position_in), ptr(velocity_in), ptr(position_out),
+                                            ptr(velocity_out)))
+
+    def run_stage(self, stage):
+        k = STAGES[stage] if isinstance(stage, str) else int(stage)
+        _check(self._lib.aq_fluid_run_stage(self._h, k))
+
+    def synchronize(self):
+        _check(self._lib.aq_fluid_synchronize(self._h))
+
+    def stream(self) -> int:
+        s = ct.c_void_p()
+        _check(self._lib.aq_fluid_stream(self._h, ct.byref(s)))
+        return s.value or 0
+
+    def download_state(self, fields=None) -> dict:
+        sx, sy, sz = self.size
+        arrs = _abi.alloc_state(sx, sy, sz, self.particleCount, fields)
+        st = _abi.make_host_state(sx, sy, sz, self.particleCount, arrs)
+        _check(self._lib.aq_fluid_download_state(self._h, ct.byref(st)))
+        arrs["physical_time"] = st.physical_time
+        return arrs
+
+    def upload_state(self, state: dict):
+        sx, sy, sz = self.size
+        arrs = {k: np.ascontiguousarray(v) for k, v in state.items() if k in _abi.STATE_FIELDS}
+        st = _abi.make_host_state(sx, sy, sz, self.particleCount, arrs, float(state.get("physical_time", 0.0)))
+        _check(self._lib.aq_fluid_upload_state(self._h, ct.byref(st)))
+
+    def solve_stats(self) -> dict:
+        s = _abi.SolveStats()
+        _check(self._lib.aq_fluid_solve_stats(self._h, ct.byref(s)))
+        return {"iterations": s.iterations, "rel_residual": s.rel_residual, "b_norm": s.b_norm,
+                "fluid_cells": s.fluid_cells, "converged": bool(s.converged), "blocks": s.blocks,
+                "total_sweeps": s.total_sweeps, "total_blocks": s.total_blocks}
+
+    def pcg_reference(self, rel_tol: float = 1e-12, max_iter: int = 100000, want_pressure: bool = False):
+        """FP64 PCG solve of the current pressure system; returns the relative
+        L2 error of the fluid's pressure against it over fluid cells."""
+        out = np.zeros(self.size[0] * self.size[1] * self.size[2], np.float32) if want_pressure else None
+        err, res = ct.c_double(), ct.c_double()
+        it = ct.c_int32()
+        _check(self._lib.aq_fluid_pcg_reference(self._h, rel_tol, max_iter, None if out is None else out.ctypes.data,
+                                                ct.byref(err), ct.byref(it), ct.byref(res)))
+        d = {"rel_error": err.value, "iterations": it.value, "residual": res.value}
+        if out is not None:
+            d["pressure"] = out
+        return d
+
+    def profile_step(self) -> dict:
+        ms = (ct.c_float * 8)()
+        _check(self._lib.aq_fluid_profile_step(self._h, ms))
+        return {name: ms[k - 1] for name, k in STAGES.items()}
+
+    def launches_per_step(self) -> int:
+        n = ct.c_int32()
+        _check(self._lib.aq_fluid_launches_per_step(self._h, ct.byref(n)))
+        return n.value
+
+    def set_jacobi_plan(self, levels: int, rows: int, x_planes: int):
+        _check(self._lib.aq_fluid_set_jacobi_plan(self._h, levels, rows, x_planes))
+
+    def jacobi_plan(self) -> tuple:
+        a, b, c = ct.c_int32(), ct.c_int32(), ct.c_int32()
+        _check(self._lib.aq_fluid_get_jacobi_plan(self._h, ct.byref(a), ct.byref(b), ct.byref(c)))
+        return a.value, b.value, c.value
+
+    def launch_counts(self) -> tuple:
+        a, b = ct.c_int32(), ct.c_int32()
+        _check(self._lib.aq_fluid_launch_counts(self._h, ct.byref(a), ct.byref(b)))
+        return a.value, b.value
+
+    def benchmark_pressure(self, sweeps: int) -> dict:
+        """Times `sweeps` Jacobi sweeps of the current system (CUDA events)."""
+        ms, nl, cells = ct.c_float(), ct.c_int32(), ct.c_int64()
+        _check(self._lib.aq_fluid_benchmark_pressure(self._h, sweeps, ct.byref(ms), ct.byref(nl), ct.byref(cells)))
+        return {"ms": ms.value, "launches": nl.value, "cells_per_sweep": cells.value}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.aq_fluid_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,93 @@
+// Host launchers of the B200 FLIP kernels.  Each returns cudaGetLastError()
+// of its launch; all work is enqueued on `st`.
+#pragma once
+
+#include "aq_common.cuh"
+
+namespace aqb {
+
+// ---- particles (k_particles.cu) -------------------------------------------
+// Stage (d)+(a) front half: grid-to-particle FLIP/PIC blend and RK3 advection
+// (move=true) or a plain copy (move=false), written in the current order to
+// the temp arrays, plus the new cell key of every particle and its slot in a
+// per-cell atomic count.
+cudaError_t launch_particles_advance(cudaStream_t st, const Dims& d, const StepParams& sp, bool move,
+                                     Particles cur, Particles tmp, const float* u0, const float* v0,
+                                     const float* w0, const float* un, const float* vn, const float* wn,
+                                     const float4* nvf, int* key, int* slot, int* count, int n);
+// Exclusive scan of count[0..C] into off[0..C] (off[C] = N) and clears count.
+cudaError_t launch_cell_scan(cudaStream_t st, int C, int* count, int* off, int* tile_sums);
+size_t cell_scan_tiles(int C);
+// perm_u[off[key[i]] + slot[i]] = i
+cudaError_t launch_scatter(cudaStream_t st, const int* key, const int* slot, const int* off, int* perm_u, int n);
+// Stable placement: particle i goes to off[key]+#{j in its cell, j < i}.
+cudaError_t launch_rank_gather(cudaStream_t st, bool multiphase, const int* key, const int* off,
+                               const int* perm_u, Particles tmp, Particles cur, int* sort_index, int n);
+
+// ---- grid (k_grid.cu) -------------------------------------------------------
+// Stage (b): particle-to-grid gather onto the staggered faces, weight
+// normalisation, fluid marking, density/fractions and (forces=true) gravity
+// and the wall clamps of fixBoundary for nodes in [0,s)^3.
+cudaError_t launch_p2g(cudaStream_t st, const Dims& d, const StepParams& sp, bool forces, Particles cur,
+                       const int* off, int n, float* u0, float* v0, float* w0, float* un, float* vn,
+                       float* wn, int8_t* type, float* density, float4* vf, float4* nvf);
+// Gravity and wall clamps of the nodes with a coordinate equal to s (the
+// reference never resets them); reads `src` (persisted) and writes dst1/dst2.
+cudaError_t launch_slayer(cudaStream_t st, const Dims& d, const StepParams& sp, const int8_t* type,
+                          const float* su, const float* sv, const float* sw, float* u1, float* v1, float* w1,
+                          float* u2, float* v2, float* w2);
+// countParticlesInCells + computeDivergence; builds rhs = -div*rho, clears air
+// pressure in both buffers (all pressure when zero_init), flags active bricks
+// and writes per-block FP64 partial sums of ||b||^2 and fluid counts.
+cudaError_t launch_divergence(cudaStream_t st, const Dims& d, const int* off, const int8_t* type,
+                              const float* density, const float* un, const float* vn, const float* wn,
+                              int* pcount, float* div, float* rhs, float* pa, float* pb, bool zero_init,
+                              uint8_t* brick_active, double* part_b2, int* part_nf, int* nblocks_out);
+cudaError_t launch_b2_finalize(cudaStream_t st, const double* part_b2, const int* part_nf, int nblocks,
+                               SolveState* ss);
+// updateVelocityWithPressure on nodes in [0,s)^3: in place on u,v,w; writes has bits.
+cudaError_t launch_project(cudaStream_t st, const Dims& d, const int8_t* type, const float* p,
+                           const float* density, float* u, float* v, float* w, uint8_t* has);
+// One extrapolateVelocityByOne pass, reading (ui,hi) and writing (uo,ho).
+cudaError_t launch_extrapolate(cudaStream_t st, const Dims& d, const float* ui, const float* vi,
+                               const float* wi, const uint8_t* hi, float* uo, float* vo, float* wo,
+                               uint8_t* ho);
+// One diffusionJacobi sweep of the phase fractions (multiphase only).
+cudaError_t launch_diffuse(cudaStream_t st, const Dims& d, const int8_t* type, float lambda,
+                           const float4* fin, float4* fout);
+
+// ---- pressure (k_jacobi.cu) -------------------------------------------------
+struct JacobiPlan {
+  int levels;      // sweeps per launch (1,2,4,8)
+  int by;          // tile rows (y threads)
+  int xc;          // x planes per CTA
+};
+// Temporally blocked Jacobi: `levels` sweeps from pin to pout; with resid it
+// also writes per-CTA FP64 partial sums of ||b - A p_out||^2 to part.
+cudaError_t launch_jacobi(cudaStream_t st, const Dims& d, const JacobiPlan& plan, bool resid,
+                          const float* pin, float* pout, const float* rhs, const int8_t* type,
+                          const uint8_t* brick_active, double* part, int* nparts_out);
+int jacobi_parts(const Dims& d, const JacobiPlan& plan, bool resid);
+// Cells in the output regions of the tiles a sweep does not skip.
+long long jacobi_cells_updated(const Dims& d, const JacobiPlan& plan, const uint8_t* bact_host);
+// Sets the dynamic shared-memory limits of every Jacobi variant (call before capture).
+cudaError_t jacobi_prepare();
+// Sums residual partials; updates ss; in a conditional loop body it also
+// sets the loop's condition (continue while not converged and under cap).
+cudaError_t launch_resid_finalize(cudaStream_t st, const double* part, int nparts, SolveState* ss,
+                                  int sweeps_done_per_call, double tol, int max_iters,
+                                  bool set_cond, unsigned long long cond_handle);
+
+// ---- FP64 PCG (k_pcg.cu) ----------------------------------------------------
+cudaError_t launch_pcg_apply(cudaStream_t st, const Dims& d, const int8_t* type, const double* in,
+                             double* out);  // out = A in
+cudaError_t launch_pcg_dot(cudaStream_t st, int C, const double* a, const double* b, double* part,
+                           int nparts);
+cudaError_t launch_pcg_axpy(cudaStream_t st, int C, double alpha, const double* xv, double* yv);
+cudaError_t launch_pcg_precond(cudaStream_t st, const Dims& d, const int8_t* type, const double* r,
+                               double* z);
+cudaError_t launch_pcg_xpby(cudaStream_t st, int C, const double* xv, double beta, double* yv);
+cudaError_t launch_pcg_init(cudaStream_t st, const Dims& d, const int8_t* type, const float* rhs,
+                            double* b, double* x);
+
+}  // namespace aqb

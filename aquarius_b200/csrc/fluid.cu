@@ -1,0 +1,1388 @@
+// Host side of the B200 FLIP step: configuration, particle seeding, device
+// memory, stage sequencing, CUDA-graph capture and the C ABI declared in
+// include/aquarius_b200.h.
+//
+// Reference surface: Fluid_3D_FLIP::Fluid (Fluid/Fluid_3D_FLIP.cuh:53-156),
+// init (Fluid/Fluid_3D_FLIP.cu:435-505), simulationStep (:316-352).
+#include <cmath>
+#include <cstdlib>
+#include <algorithm>
+#include <cstring>
+#include <stdlib.h>
+#include <string>
+#include <vector>
+
+#include "../../include/aquarius_b200.h"
+#include "aq_kernels.cuh"
+
+using namespace aqb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+aq_status fail(aq_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+
+#define AQ_CUDA(call)                                                                            \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      return fail(e_ == cudaErrorMemoryAllocation ? AQ_ERR_OUT_OF_MEMORY : AQ_ERR_CUDA,          \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+  } while (0)
+
+#define AQ_TRY(expr)              \
+  do {                            \
+    aq_status s_ = (expr);        \
+    if (s_ != AQ_OK) return s_;   \
+  } while (0)
+
+__global__ void k_copy_f(const float* __restrict__ a, float* __restrict__ b, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = a[i];
+}
+
+int covered_faces(int s1, int s2) {  // fixBoundary launch coverage (Fluid/Fluid_3D_common.cu:13-41)
+  const int total = s1 * s2;
+  const int nt = total < 1024 ? total : 1024;
+  const int nb = nt == 0 ? 1 : (total % nt != 0 ? total / nt + 1 : total / nt);
+  const int t = nb * nt;
+  const int faces = (s1 + 1) * (s2 + 1);
+  return t < faces ? t : faces;
+}
+
+// ------------------------------------------------------------------ seeding
+// Fluid::createParticlesAt / createSquareFluid / createSphereFluid
+// (Fluid/Fluid_3D_FLIP.cu:508-594).  The jitter comes from glibc rand()
+// (Common/Commons.h:3-5); random_r with a 128-byte state replays
+// srand(seed); rand() exactly.  Jitter is drawn before the sphere filter, so
+// rejected sub-cells consume the sequence too.
+struct Seeder {
+  const aq_config& cfg;
+  int sx, sy, sz;
+  float h;
+  struct random_data rd;
+  char state[128];
+  std::vector<float> pos;  // xyz interleaved
+  std::vector<int> phase;
+
+  Seeder(const aq_config& c, float h_) : cfg(c), sx(c.size_x), sy(c.size_y), sz(c.size_z), h(h_) {
+    memset(&rd, 0, sizeof(rd));
+    memset(state, 0, sizeof(state));
+    initstate_r(c.seed, state, sizeof(state), &rd);
+  }
+  float random0to1() {
+    int32_t v;
+    random_r(&rd, &v);
+    return (float)v / (float)RAND_MAX;
+  }
+  void at(float cx, float cy, float cz, bool sphere, float scx, float scy, float scz, float rad, float spacing,
+          int ph) {
+    const float jit = cfg.particle_jitter;
+    for (float dx = 0; dx <= 1; ++dx)
+      for (float dy = 0; dy <= 1; ++dy)
+        for (float dz = 0; dz <= 1; ++dz) {
+          float px = (float)(dx - 0.5) * spacing + cx;
+          float py = (float)(dy - 0.5) * spacing + cy;
+          float pz = (float)(dz - 0.5) * spacing + cz;
+          const float xj = random0to1() - 0.5f, yj = random0to1() - 0.5f, zj = random0to1() - 0.5f;
+          px += xj * spacing * jit;
+          py += yj * spacing * jit;
+          pz += zj * spacing * jit;
+          const float md = spacing / 2;
+          px = fmaxf(md, fminf((float)sx * h - md, px));
+          py = fmaxf(md, fminf((float)sy * h - md, py));
+          pz = fmaxf(md, fminf((float)sz * h - md, pz));
+          bool keep = true;
+          if (sphere) {
+            const float ex = px - scx, ey = py - scy, ez = pz - scz;
+            const float len = sqrtf(ex * ex + ey * ey + ez * ez);
+            keep = len < rad * h * (float)sy;
+          }
+          if (keep) {
+            pos.push_back(px);
+            pos.push_back(py);
+            pos.push_back(pz);
+            phase.push_back(ph);
+          }
+        }
+  }
+  static bool valid01(const float* c) {
+    return !(c[0] < 0 || c[1] < 0 || c[2] < 0) && !(c[0] > 1 || c[1] > 1 || c[2] > 1);
+  }
+  void center(int x, int y, int z, float& cx, float& cy, float& cz) const {
+    cx = ((float)x + 0.5f) * h;
+    cy = ((float)y + 0.5f) * h;
+    cz = ((float)z + 0.5f) * h;
+  }
+  void square(const aq_volume& v) {
+    if (!valid01(v.box_min) || !valid01(v.box_max)) return;
+    float cx, cy, cz;
+    for (int z = (int)(v.box_min[2] * (float)sz); (float)z < v.box_max[2] * (float)sz; ++z)
+      for (int x = (int)(v.box_min[0] * (float)sx); (float)x < v.box_max[0] * (float)sx; ++x)
+        for (int y = (int)(v.box_min[1] * (float)sy); (float)y < v.box_max[1] * (float)sy; ++y) {
+          center(x, y, z, cx, cy, cz);
+          at(cx, cy, cz, false, 0, 0, 0, 0, h / 2, v.phase);
+        }
+  }
+  void sphere(const aq_volume& v) {
+    if (!valid01(v.ball_center)) return;
+    const float scx = (v.ball_center[0] * (float)sx * h);
+    const float scy = (v.ball_center[1] * (float)sy * h);
+    const float scz = (v.ball_center[2] * (float)sz * h);
+    float cx, cy, cz;
+    for (int y = 0; y < sy; ++y)
+      for (int x = 0; x < sx; ++x)
+        for (int z = 0; z < sz; ++z) {
+          center(x, y, z, cx, cy, cz);
+          at(cx, cy, cz, true, scx, scy, scz, v.ball_radius, h / 2, v.phase);
+        }
+  }
+};
+
+}  // namespace
+
+// =================================================================== fluid
+struct aq_fluid {
+  aq_config cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;  // body capture
+  bool own_stream = false;
+  Dims d{};
+  StepParams sp{};
+  int n = 0;
+  bool multiphase = false;
+  int phase = 0;
+  double time = 0.0;
+  int nv_cur = 2, has_cur = 2;  // which buffer holds newVelocity / has bits
+  // Stage 1 is fused with the sort; a following stage-2 call then has no work.
+  bool sorted_by_stage1 = false;
+
+  Particles cur{}, tmp{};
+  int *key = nullptr, *slot = nullptr, *perm_u = nullptr, *sort_index = nullptr;
+  int *count = nullptr, *off = nullptr, *tile_sums = nullptr;
+  float *u0 = nullptr, *v0 = nullptr, *w0 = nullptr;
+  float *un1 = nullptr, *vn1 = nullptr, *wn1 = nullptr;
+  float *un2 = nullptr, *vn2 = nullptr, *wn2 = nullptr;
+  uint8_t *h1 = nullptr, *h2 = nullptr;
+  int8_t* type = nullptr;
+  float *density = nullptr, *div = nullptr, *rhs = nullptr, *pa = nullptr, *pb = nullptr;
+  int* pcount = nullptr;
+  float4 *vf = nullptr, *nvf = nullptr, *nvf2 = nullptr;
+  uint8_t* bact = nullptr;
+  double* part_b2 = nullptr;
+  int* part_nf = nullptr;
+  int nbricks = 0;
+  double* jpart = nullptr;
+  int jpart_cap = 0;
+  SolveState* ss = nullptr;
+  SolveState* ss_host = nullptr;
+
+  JacobiPlan plan{4, 16, 32};
+  cudaGraphExec_t exec = nullptr;
+  int graph_launches = 0;  // launches outside the residual loop
+  int body_launches = 0;   // launches per residual-loop iteration
+
+  std::vector<void*> allocs;
+  // PCG scratch (lazily allocated)
+  double *pcg_b = nullptr, *pcg_x = nullptr, *pcg_r = nullptr, *pcg_z = nullptr, *pcg_p = nullptr,
+         *pcg_q = nullptr, *pcg_part = nullptr;
+
+  ~aq_fluid() {
+    if (device >= 0) cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    if (exec) cudaGraphExecDestroy(exec);
+    for (void* p : allocs) cudaFree(p);
+    if (ss_host) cudaFreeHost(ss_host);
+    if (side) cudaStreamDestroy(side);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+
+  template <typename T>
+  aq_status alloc(T** p, size_t count_) {
+    void* q = nullptr;
+    const size_t bytes = count_ * sizeof(T) > 0 ? count_ * sizeof(T) : 16;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess)
+      return fail(e == cudaErrorMemoryAllocation ? AQ_ERR_OUT_OF_MEMORY : AQ_ERR_CUDA,
+                  std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(q);
+    *p = (T*)q;
+    e = cudaMemsetAsync(q, 0, bytes, stream);
+    if (e != cudaSuccess) return fail(AQ_ERR_CUDA, cudaGetErrorString(e));
+    return AQ_OK;
+  }
+
+  float* nvx(int which) const { return which == 1 ? un1 : un2; }
+  float* nvy(int which) const { return which == 1 ? vn1 : vn2; }
+  float* nvz(int which) const { return which == 1 ? wn1 : wn2; }
+  uint8_t* hb(int which) const { return which == 1 ? h1 : h2; }
+
+  aq_status allocate();
+  aq_status seed_and_init();
+  // stage enqueues (eager or under capture)
+  aq_status enq_particles(bool move);
+  aq_status enq_p2g(bool forces);
+  aq_status enq_divergence();
+  aq_status enq_solve_fixed(int sweeps);
+  aq_status enq_solve_body(bool set_cond, unsigned long long handle, int* launches);
+  aq_status enq_solve_residual_eager();
+  aq_status enq_project();
+  aq_status enq_extrapolate();
+  aq_status enq_diffuse();
+  aq_status run_stage(int stage);
+  aq_status enq_pre_solve();
+  aq_status enq_post_solve();
+  aq_status build_graph();
+  aq_status step(int nsteps);
+  aq_status upload(const aq_host_state* s);
+  aq_status download(aq_host_state* s);
+  aq_status derive_from_state(const std::vector<int>& content, const std::vector<float>& divv,
+                              const std::vector<float>& dens);
+  int count_jacobi_launches(int sweeps) const;
+  void invalidate_graph() {
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+  }
+};
+
+// ------------------------------------------------------------- allocation
+aq_status aq_fluid::allocate() {
+  const size_t N = (size_t)n, C = (size_t)d.C, F = (size_t)d.F;
+  AQ_TRY(alloc(&cur.px, N)); AQ_TRY(alloc(&cur.py, N)); AQ_TRY(alloc(&cur.pz, N));
+  AQ_TRY(alloc(&cur.vx, N)); AQ_TRY(alloc(&cur.vy, N)); AQ_TRY(alloc(&cur.vz, N));
+  AQ_TRY(alloc(&tmp.px, N)); AQ_TRY(alloc(&tmp.py, N)); AQ_TRY(alloc(&tmp.pz, N));
+  AQ_TRY(alloc(&tmp.vx, N)); AQ_TRY(alloc(&tmp.vy, N)); AQ_TRY(alloc(&tmp.vz, N));
+  AQ_TRY(alloc(&cur.frac, N)); AQ_TRY(alloc(&tmp.frac, N));
+  AQ_TRY(alloc(&key, N)); AQ_TRY(alloc(&slot, N)); AQ_TRY(alloc(&perm_u, N)); AQ_TRY(alloc(&sort_index, N));
+  AQ_TRY(alloc(&count, C + 1)); AQ_TRY(alloc(&off, C + 1));
+  AQ_TRY(alloc(&tile_sums, cell_scan_tiles(d.C)));
+  AQ_TRY(alloc(&u0, F)); AQ_TRY(alloc(&v0, F)); AQ_TRY(alloc(&w0, F));
+  AQ_TRY(alloc(&un1, F)); AQ_TRY(alloc(&vn1, F)); AQ_TRY(alloc(&wn1, F));
+  AQ_TRY(alloc(&un2, F)); AQ_TRY(alloc(&vn2, F)); AQ_TRY(alloc(&wn2, F));
+  AQ_TRY(alloc(&h1, F)); AQ_TRY(alloc(&h2, F));
+  AQ_TRY(alloc(&type, C)); AQ_TRY(alloc(&density, C)); AQ_TRY(alloc(&div, C)); AQ_TRY(alloc(&rhs, C));
+  AQ_TRY(alloc(&pa, C)); AQ_TRY(alloc(&pb, C)); AQ_TRY(alloc(&pcount, C));
+  AQ_TRY(alloc(&vf, C)); AQ_TRY(alloc(&nvf, C)); AQ_TRY(alloc(&nvf2, C));
+  nbricks = d.bx * d.by * d.bz;
+  AQ_TRY(alloc(&bact, (size_t)nbricks)); AQ_TRY(alloc(&part_b2, (size_t)nbricks));
+  AQ_TRY(alloc(&part_nf, (size_t)nbricks));
+  jpart_cap = 0;
+  for (int lv : {1, 2, 4, 8})
+    for (int res = 0; res < 2; ++res) {
+      JacobiPlan p = plan;
+      p.levels = lv;
+      const int k = jacobi_parts(d, p, res != 0);
+      if (k > jpart_cap) jpart_cap = k;
+    }
+  if (jpart_cap < 1) jpart_cap = 1;
+  AQ_TRY(alloc(&jpart, (size_t)jpart_cap));
+  AQ_TRY(alloc(&ss, 1));
+  AQ_CUDA(cudaMallocHost(&ss_host, sizeof(SolveState)));
+  // default Jacobi plan: one vectorised sweep per launch where z allows it,
+  // otherwise the tiled kernel with two sweeps per launch
+  plan = d.sz % 4 == 0 ? JacobiPlan{1, 0, 1} : JacobiPlan{2, 16, 16};
+  if (jacobi_parts(d, JacobiPlan{1, 16, 16}, true) > jpart_cap) {
+    jpart_cap = jacobi_parts(d, JacobiPlan{1, 16, 16}, true);
+    AQ_TRY(alloc(&jpart, (size_t)jpart_cap));
+  }
+  memset(ss_host, 0, sizeof(SolveState));
+  return AQ_OK;
+}
+
+// ------------------------------------------------------------------ stages
+aq_status aq_fluid::enq_particles(bool move) {
+  AQ_CUDA(launch_particles_advance(stream, d, sp, move, cur, tmp, u0, v0, w0, un2, vn2, wn2, nvf, key, slot,
+                                   count, n));
+  AQ_CUDA(launch_cell_scan(stream, d.C, count, off, tile_sums));
+  AQ_CUDA(launch_scatter(stream, key, slot, off, perm_u, n));
+  AQ_CUDA(launch_rank_gather(stream, multiphase, key, off, perm_u, tmp, cur, sort_index, n));
+  return AQ_OK;
+}
+
+aq_status aq_fluid::enq_p2g(bool forces) {
+  AQ_CUDA(launch_p2g(stream, d, sp, forces, cur, off, n, u0, v0, w0, un1, vn1, wn1, type, density, vf, nvf));
+  if (forces) {
+    AQ_CUDA(launch_slayer(stream, d, sp, type, un2, vn2, wn2, un1, vn1, wn1, un2, vn2, wn2));
+  }
+  nv_cur = 1;
+  return AQ_OK;
+}
+
+aq_status aq_fluid::enq_divergence() {
+  int nb = 0;
+  AQ_CUDA(launch_divergence(stream, d, off, type, density, nvx(nv_cur), nvy(nv_cur), nvz(nv_cur), pcount, div,
+                            rhs, pa, pb, cfg.pressure_init == AQ_PRESSURE_ZERO, bact, part_b2, part_nf, &nb));
+  AQ_CUDA(launch_b2_finalize(stream, part_b2, part_nf, nb, ss));
+  return AQ_OK;
+}
+
+// Sweep counts per launch for `sweeps` sweeps with the plan's level count.
+static std::vector<int> split_sweeps(int sweeps, int levels) {
+  std::vector<int> out;
+  int left = sweeps;
+  while (left > 0) {
+    int l = levels;
+    while (l > left) l >>= 1;
+    out.push_back(l);
+    left -= l;
+  }
+  return out;
+}
+
+int aq_fluid::count_jacobi_launches(int sweeps) const {
+  const int k = (int)split_sweeps(sweeps, plan.levels).size();
+  return k + (k % 2) + 1;  // launches, parity copy, finalize
+}
+
+// `sweeps` Jacobi sweeps from pa; the last launch also writes the residual
+// partials of its output; the result ends in pa.
+static JacobiPlan resid_plan(const JacobiPlan& p, int levels) {
+  JacobiPlan q = p;
+  q.levels = levels;
+  if (q.by == 0) q = JacobiPlan{1, 16, 16};  // flat sweeps end with a tiled residual sweep
+  return q;
+}
+
+static aq_status enqueue_sweeps(aq_fluid* f, int sweeps) {
+  const std::vector<int> parts = split_sweeps(sweeps, f->plan.levels);
+  float* bufs[2] = {f->pa, f->pb};
+  for (size_t k = 0; k < parts.size(); ++k) {
+    const bool last = k + 1 == parts.size();
+    JacobiPlan p = last ? resid_plan(f->plan, parts[k]) : f->plan;
+    p.levels = parts[k];
+    int np = 0;
+    AQ_CUDA(launch_jacobi(f->stream, f->d, p, last, bufs[k % 2], bufs[(k + 1) % 2], f->rhs, f->type, f->bact,
+                          f->jpart, &np));
+  }
+  if (parts.size() % 2 == 1) {
+    k_copy_f<<<(f->d.C + 255) / 256, 256, 0, f->stream>>>(f->pb, f->pa, f->d.C);
+    AQ_CUDA(cudaGetLastError());
+  }
+  return AQ_OK;
+}
+
+static int last_parts(const aq_fluid* f, int sweeps) {
+  const std::vector<int> parts = split_sweeps(sweeps, f->plan.levels);
+  if (parts.empty()) return 0;
+  return jacobi_parts(f->d, resid_plan(f->plan, parts.back()), true);
+}
+
+aq_status aq_fluid::enq_solve_fixed(int sweeps) {
+  if (sweeps <= 0) return AQ_OK;
+  AQ_TRY(enqueue_sweeps(this, sweeps));
+  AQ_CUDA(launch_resid_finalize(stream, jpart, last_parts(this, sweeps), ss, sweeps, 0.0, 0, false, 0));
+  return AQ_OK;
+}
+
+aq_status aq_fluid::enq_solve_body(bool set_cond, unsigned long long handle, int* launches) {
+  const int m = cfg.check_interval;
+  AQ_TRY(enqueue_sweeps(this, m));
+  AQ_CUDA(launch_resid_finalize(stream, jpart, last_parts(this, m), ss, m, (double)cfg.rel_residual,
+                                cfg.max_iterations, set_cond, handle));
+  if (launches) *launches = count_jacobi_launches(m);
+  return AQ_OK;
+}
+
+// Residual mode without a graph: the host reads the solve state after each block.
+aq_status aq_fluid::enq_solve_residual_eager() {
+  for (int guard = 0; guard < 1000000; ++guard) {
+    AQ_TRY(enq_solve_body(false, 0, nullptr));
+    AQ_CUDA(cudaMemcpyAsync(ss_host, ss, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+    AQ_CUDA(cudaStreamSynchronize(stream));
+    const SolveState& s = *ss_host;
+    if (s.converged || s.nonfinite || s.iterations >= cfg.max_iterations) break;
+  }
+  return AQ_OK;
+}
+
+aq_status aq_fluid::enq_project() {
+  AQ_CUDA(launch_project(stream, d, type, pa, density, nvx(nv_cur), nvy(nv_cur), nvz(nv_cur), hb(nv_cur)));
+  has_cur = nv_cur;
+  return AQ_OK;
+}
+
+aq_status aq_fluid::enq_extrapolate() {
+  // extrapolateVelocity: 3 passes (Fluid/Fluid_3D_common.cu:65-82); ends in buffer 2.
+  int a = nv_cur, b = 3 - nv_cur;
+  if (has_cur != nv_cur) {
+    // has bits must sit beside the velocities they describe
+    AQ_CUDA(cudaMemcpyAsync(hb(nv_cur), hb(has_cur), (size_t)d.F, cudaMemcpyDeviceToDevice, stream));
+  }
+  for (int pass = 0; pass < 3; ++pass) {
+    AQ_CUDA(launch_extrapolate(stream, d, nvx(a), nvy(a), nvz(a), hb(a), nvx(b), nvy(b), nvz(b), hb(b)));
+    std::swap(a, b);
+  }
+  nv_cur = a;
+  has_cur = a;
+  if (nv_cur != 2) {
+    // keep the invariant that the step's final newVelocity lives in buffer 2
+    AQ_CUDA(cudaMemcpyAsync(un2, un1, sizeof(float) * d.F, cudaMemcpyDeviceToDevice, stream));
+    AQ_CUDA(cudaMemcpyAsync(vn2, vn1, sizeof(float) * d.F, cudaMemcpyDeviceToDevice, stream));
+    AQ_CUDA(cudaMemcpyAsync(wn2, wn1, sizeof(float) * d.F, cudaMemcpyDeviceToDevice, stream));
+    AQ_CUDA(cudaMemcpyAsync(h2, h1, (size_t)d.F, cudaMemcpyDeviceToDevice, stream));
+    nv_cur = has_cur = 2;
+  }
+  return AQ_OK;
+}
+
+aq_status aq_fluid::enq_diffuse() {
+  // solveDiffusionJacobi (Fluid/Fluid_3D_common.cu:85-91).  With every
+  // particle in one phase, each fluid cell holds the same one-hot vector and
+  // a sweep maps it to itself exactly (x/x = 1 in IEEE arithmetic), so the
+  // sweeps are skipped; air pressure is already 0 after the solve.
+  if (!multiphase || cfg.diffusion_iterations <= 0) return AQ_OK;
+  const float lambda = cfg.diffusion_coeff * cfg.timestep / (d.h * d.h);
+  float4* a = nvf;
+  float4* b = nvf2;
+  for (int i = 0; i < cfg.diffusion_iterations; ++i) {
+    AQ_CUDA(launch_diffuse(stream, d, type, lambda, a, b));
+    std::swap(a, b);
+  }
+  if (a != nvf) AQ_CUDA(cudaMemcpyAsync(nvf, a, sizeof(float4) * d.C, cudaMemcpyDeviceToDevice, stream));
+  return AQ_OK;
+}
+
+aq_status aq_fluid::run_stage(int stage) {
+  if (stage != AQ_STAGE_SORT) sorted_by_stage1 = false;
+  switch (stage) {
+    case AQ_STAGE_G2P_ADVECT:
+      // transferToParticles + moveParticles run fused with the spatial hash
+      // and sort, so the particles come out sorted already.
+      AQ_TRY(enq_particles(true));
+      sorted_by_stage1 = true;
+      return AQ_OK;
+    case AQ_STAGE_SORT:
+      if (!sorted_by_stage1) AQ_TRY(enq_particles(false));
+      sorted_by_stage1 = false;
+      return AQ_OK;
+    case AQ_STAGE_P2G: return enq_p2g(true);
+    case AQ_STAGE_DIVERGENCE: return enq_divergence();
+    case AQ_STAGE_PRESSURE:
+      if (cfg.pressure_init == AQ_PRESSURE_ZERO) {  // done by the divergence kernel inside a step
+        AQ_CUDA(cudaMemsetAsync(pa, 0, sizeof(float) * d.C, stream));
+        AQ_CUDA(cudaMemsetAsync(pb, 0, sizeof(float) * d.C, stream));
+      }
+      if (cfg.solve_mode == AQ_SOLVE_RESIDUAL) return enq_solve_residual_eager();
+      return enq_solve_fixed(cfg.pressure_iterations);
+    case AQ_STAGE_PROJECT: return enq_project();
+    case AQ_STAGE_EXTRAPOLATE: return enq_extrapolate();
+    case AQ_STAGE_DIFFUSE:
+      AQ_TRY(enq_diffuse());
+      time += (double)cfg.timestep;
+      return AQ_OK;
+    default: return fail(AQ_ERR_INVALID_ARGUMENT, "unknown stage");
+  }
+}
+
+aq_status aq_fluid::enq_pre_solve() {
+  nv_cur = 2;
+  AQ_TRY(enq_particles(true));
+  AQ_TRY(enq_p2g(true));
+  AQ_TRY(enq_divergence());
+  return AQ_OK;
+}
+
+aq_status aq_fluid::enq_post_solve() {
+  AQ_TRY(enq_project());
+  AQ_TRY(enq_extrapolate());
+  AQ_TRY(enq_diffuse());
+  return AQ_OK;
+}
+
+static aq_status leaves_of(cudaGraph_t g, std::vector<cudaGraphNode_t>& out) {
+  size_t nn = 0;
+  AQ_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  AQ_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+  out.clear();
+  for (cudaGraphNode_t nd : nodes) {
+    size_t k = 0;
+    AQ_CUDA(cudaGraphNodeGetDependentNodes(nd, nullptr, &k));
+    if (k == 0) out.push_back(nd);
+  }
+  return AQ_OK;
+}
+
+// The whole step as one CUDA graph.  RESIDUAL mode puts the sweeps in a
+// conditional WHILE node whose body ends with the residual check that sets
+// the loop condition, so a step needs no host round trip.
+aq_status aq_fluid::build_graph() {
+  invalidate_graph();
+  cudaGraph_t g = nullptr;
+  AQ_CUDA(cudaGraphCreate(&g, 0));
+  int launches = 0;
+  auto capture = [&](cudaGraph_t into, const cudaGraphNode_t* deps, size_t nd, auto&& body) -> aq_status {
+    AQ_CUDA(cudaStreamBeginCaptureToGraph(stream, into, deps, nullptr, nd, cudaStreamCaptureModeThreadLocal));
+    aq_status st = body();
+    cudaGraph_t got = nullptr;
+    cudaError_t e = cudaStreamEndCapture(stream, &got);
+    if (st != AQ_OK) return st;
+    if (e != cudaSuccess) return fail(AQ_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    return AQ_OK;
+  };
+  aq_status st = AQ_OK;
+  launches += (n > 0 ? 6 : 3) + 2 + 2;  // particles (+3 scan kernels), p2g, slayer, divergence, b2
+  if (cfg.solve_mode == AQ_SOLVE_RESIDUAL) {
+    st = capture(g, nullptr, 0, [&]() { return enq_pre_solve(); });
+    if (st != AQ_OK) { cudaGraphDestroy(g); return st; }
+    std::vector<cudaGraphNode_t> leaves;
+    st = leaves_of(g, leaves);
+    if (st != AQ_OK) { cudaGraphDestroy(g); return st; }
+    cudaGraphConditionalHandle handle;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return fail(AQ_ERR_CUDA, cudaGetErrorString(e)); }
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    e = cudaGraphAddNode(&cnode, g, leaves.data(), leaves.size(), &cp);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return fail(AQ_ERR_CUDA, std::string("conditional node: ") + cudaGetErrorString(e));
+    }
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    int bl = 0;
+    st = capture(body, nullptr, 0, [&]() { return enq_solve_body(true, (unsigned long long)handle, &bl); });
+    if (st != AQ_OK) { cudaGraphDestroy(g); return st; }
+    body_launches = bl;
+    st = capture(g, &cnode, 1, [&]() { return enq_post_solve(); });
+  } else {
+    st = capture(g, nullptr, 0, [&]() {
+      aq_status s2 = enq_pre_solve();
+      if (s2 != AQ_OK) return s2;
+      s2 = enq_solve_fixed(cfg.pressure_iterations);
+      if (s2 != AQ_OK) return s2;
+      return enq_post_solve();
+    });
+    launches += cfg.pressure_iterations > 0 ? count_jacobi_launches(cfg.pressure_iterations) : 0;
+    body_launches = 0;
+  }
+  if (st != AQ_OK) { cudaGraphDestroy(g); return st; }
+  launches += 1 + 3 + (multiphase ? cfg.diffusion_iterations : 0);
+  graph_launches = launches;
+  cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { exec = nullptr; return fail(AQ_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e)); }
+  return AQ_OK;
+}
+
+aq_status aq_fluid::step(int nsteps) {
+  if (!exec) AQ_TRY(build_graph());
+  for (int i = 0; i < nsteps; ++i) {
+    AQ_CUDA(cudaGraphLaunch(exec, stream));
+    time += (double)cfg.timestep;
+  }
+  nv_cur = has_cur = 2;
+  return AQ_OK;
+}
+
+// ------------------------------------------------------------------ init
+aq_status aq_fluid::seed_and_init() {
+  Seeder s(cfg, d.h);
+  for (int i = 0; i < cfg.volume_count; ++i) {
+    const aq_volume& v = cfg.volumes[i];
+    if (v.shape == AQ_SHAPE_SQUARE) s.square(v);
+    else if (v.shape == AQ_SHAPE_SPHERE) s.sphere(v);
+  }
+  n = (int)s.phase.size();
+  multiphase = false;
+  phase = n > 0 ? s.phase[0] : (cfg.volume_count > 0 ? cfg.volumes[0].phase : 0);
+  for (int i = 1; i < n; ++i)
+    if (s.phase[i] != phase) { multiphase = true; break; }
+  sp.multiphase = multiphase ? 1 : 0;
+  sp.phase = phase;
+  AQ_TRY(allocate());
+  if (n > 0) {
+    std::vector<float> comp((size_t)n);
+    float* dst[3] = {cur.px, cur.py, cur.pz};
+    for (int k = 0; k < 3; ++k) {
+      for (int i = 0; i < n; ++i) comp[i] = s.pos[3 * (size_t)i + k];
+      AQ_CUDA(cudaMemcpyAsync(dst[k], comp.data(), sizeof(float) * n, cudaMemcpyHostToDevice, stream));
+      AQ_CUDA(cudaStreamSynchronize(stream));
+    }
+    std::vector<float4> fr((size_t)n);
+    for (int i = 0; i < n; ++i) {
+      const int p = s.phase[i];
+      fr[i] = make_float4(p == 0, p == 1, p == 2, p == 3);
+    }
+    AQ_CUDA(cudaMemcpyAsync(cur.frac, fr.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream));
+    AQ_CUDA(cudaStreamSynchronize(stream));
+  }
+  // Fluid::init order: fixBoundary (zero velocities stay zero), seeding,
+  // transferToGrid (sort + P2G without forces); newVelocity = velocity.
+  AQ_TRY(enq_particles(false));
+  AQ_TRY(enq_p2g(false));
+  AQ_CUDA(cudaMemcpyAsync(un2, un1, sizeof(float) * d.F, cudaMemcpyDeviceToDevice, stream));
+  AQ_CUDA(cudaMemcpyAsync(vn2, vn1, sizeof(float) * d.F, cudaMemcpyDeviceToDevice, stream));
+  AQ_CUDA(cudaMemcpyAsync(wn2, wn1, sizeof(float) * d.F, cudaMemcpyDeviceToDevice, stream));
+  nv_cur = 2;
+  has_cur = 2;
+  AQ_CUDA(cudaStreamSynchronize(stream));
+  return AQ_OK;
+}
+
+// ----------------------------------------------------------- state exchange
+aq_status aq_fluid::download(aq_host_state* s) {
+  if (s->size_x != d.sx || s->size_y != d.sy || s->size_z != d.sz || s->particle_count != n)
+    return fail(AQ_ERR_INVALID_ARGUMENT, "state dimensions do not match the fluid");
+  AQ_CUDA(cudaStreamSynchronize(stream));
+  const size_t N = (size_t)n, C = (size_t)d.C, F = (size_t)d.F;
+  s->physical_time = time;
+  auto get = [&](void* dst, const void* src, size_t bytes) -> aq_status {
+    AQ_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    return AQ_OK;
+  };
+  if (s->position && N) {
+    AQ_TRY(get(s->position, cur.px, 4 * N)); AQ_TRY(get(s->position + N, cur.py, 4 * N));
+    AQ_TRY(get(s->position + 2 * N, cur.pz, 4 * N));
+  }
+  if (s->velocity_p && N) {
+    AQ_TRY(get(s->velocity_p, cur.vx, 4 * N)); AQ_TRY(get(s->velocity_p + N, cur.vy, 4 * N));
+    AQ_TRY(get(s->velocity_p + 2 * N, cur.vz, 4 * N));
+  }
+  std::vector<int8_t> ty(C);
+  AQ_TRY(get(ty.data(), type, C));
+  if (s->fractions && N) {
+    if (multiphase) {
+      std::vector<float4> fr(N);
+      AQ_TRY(get(fr.data(), cur.frac, sizeof(float4) * N));
+      for (size_t i = 0; i < N; ++i) {
+        s->fractions[i] = fr[i].x; s->fractions[N + i] = fr[i].y;
+        s->fractions[2 * N + i] = fr[i].z; s->fractions[3 * N + i] = fr[i].w;
+      }
+    } else {
+      for (int k = 0; k < 4; ++k)
+        for (size_t i = 0; i < N; ++i) s->fractions[k * N + i] = k == phase ? 1.f : 0.f;
+    }
+  }
+  if (s->content) {
+    for (int x = 0; x <= d.sx; ++x)
+      for (int y = 0; y <= d.sy; ++y)
+        for (int z = 0; z <= d.sz; ++z) {
+          int v;
+          if (x < d.sx && y < d.sy && z < d.sz) v = ty[cell_index(d, x, y, z)];
+          else
+            v = ((x == d.sx && covered_x(d, y, z)) || (y == d.sy && covered_y(d, x, z)) ||
+                 (z == d.sz && covered_z(d, x, y))) ? kSolid : kAir;
+          s->content[node_index(d, x, y, z)] = v;
+        }
+  }
+  if (s->velocity) {
+    AQ_TRY(get(s->velocity, u0, 4 * F)); AQ_TRY(get(s->velocity + F, v0, 4 * F));
+    AQ_TRY(get(s->velocity + 2 * F, w0, 4 * F));
+  }
+  if (s->new_velocity) {
+    AQ_TRY(get(s->new_velocity, nvx(nv_cur), 4 * F)); AQ_TRY(get(s->new_velocity + F, nvy(nv_cur), 4 * F));
+    AQ_TRY(get(s->new_velocity + 2 * F, nvz(nv_cur), 4 * F));
+  }
+  if (s->pressure) AQ_TRY(get(s->pressure, pa, 4 * C));
+  if (s->divergence) AQ_TRY(get(s->divergence, div, 4 * C));
+  if (s->particle_count_cell) AQ_TRY(get(s->particle_count_cell, pcount, 4 * C));
+  if (s->density) AQ_TRY(get(s->density, density, 4 * C));
+  if (s->has_velocity) {
+    std::vector<uint8_t> hbits(F);
+    AQ_TRY(get(hbits.data(), hb(has_cur), F));
+    for (int x = 0; x < d.sx; ++x)
+      for (int y = 0; y < d.sy; ++y)
+        for (int z = 0; z < d.sz; ++z) {
+          const uint8_t b = hbits[node_index(d, x, y, z)];
+          const size_t c = cell_index(d, x, y, z);
+          for (int k = 0; k < 3; ++k) s->has_velocity[k * C + c] = (b >> k) & 1;
+        }
+  }
+  if (s->volume_fractions || s->new_volume_fractions) {
+    if (multiphase) {
+      std::vector<float4> a(C);
+      if (s->volume_fractions) {
+        AQ_TRY(get(a.data(), vf, sizeof(float4) * C));
+        for (size_t c = 0; c < C; ++c) {
+          s->volume_fractions[c] = a[c].x; s->volume_fractions[C + c] = a[c].y;
+          s->volume_fractions[2 * C + c] = a[c].z; s->volume_fractions[3 * C + c] = a[c].w;
+        }
+      }
+      if (s->new_volume_fractions) {
+        AQ_TRY(get(a.data(), nvf, sizeof(float4) * C));
+        for (size_t c = 0; c < C; ++c) {
+          s->new_volume_fractions[c] = a[c].x; s->new_volume_fractions[C + c] = a[c].y;
+          s->new_volume_fractions[2 * C + c] = a[c].z; s->new_volume_fractions[3 * C + c] = a[c].w;
+        }
+      }
+    } else {
+      for (int k = 0; k < 4; ++k)
+        for (size_t c = 0; c < C; ++c) {
+          const float v = (ty[c] == kFluid && k == phase) ? 1.f : 0.f;
+          if (s->volume_fractions) s->volume_fractions[k * C + c] = v;
+          if (s->new_volume_fractions) s->new_volume_fractions[k * C + c] = v;
+        }
+    }
+  }
+  if (s->cell_start || s->cell_end || s->particle_hash) {
+    std::vector<int> o(C + 1);
+    AQ_TRY(get(o.data(), off, 4 * (C + 1)));
+    for (size_t c = 0; c < C; ++c) {
+      const bool occ = o[c + 1] > o[c];
+      if (s->cell_start) s->cell_start[c] = occ ? o[c] : -1;
+      if (s->cell_end) s->cell_end[c] = occ ? o[c + 1] - 1 : -1;
+      if (s->particle_hash)
+        for (int k = o[c]; k < o[c + 1]; ++k) s->particle_hash[k] = (int)c;
+    }
+  }
+  if (s->sort_index && N) AQ_TRY(get(s->sort_index, sort_index, 4 * N));
+  return AQ_OK;
+}
+
+// rhs, air pressure, active bricks and ||b||^2 from an injected state, as the
+// divergence stage would have left them.
+aq_status aq_fluid::derive_from_state(const std::vector<int>& content, const std::vector<float>& divv,
+                                      const std::vector<float>& dens) {
+  const size_t C = (size_t)d.C;
+  std::vector<int8_t> ty(C);
+  std::vector<float> r(C);
+  std::vector<uint8_t> act((size_t)nbricks, 0);
+  double b2 = 0.0;
+  int nf = 0;
+  for (int x = 0; x < d.sx; ++x)
+    for (int y = 0; y < d.sy; ++y)
+      for (int z = 0; z < d.sz; ++z) {
+        const int c = cell_index(d, x, y, z);
+        const bool fl = content[node_index(d, x, y, z)] == kFluid;
+        ty[c] = fl ? kFluid : kAir;
+        r[c] = fl ? (-divv[c]) * dens[c] : 0.f;
+        if (fl) {
+          b2 += (double)r[c] * (double)r[c];
+          nf++;
+          act[brick_index(d, x, y, z)] = 1;
+        }
+      }
+  AQ_CUDA(cudaMemcpy(type, ty.data(), C, cudaMemcpyHostToDevice));
+  AQ_CUDA(cudaMemcpy(rhs, r.data(), 4 * C, cudaMemcpyHostToDevice));
+  // air pressure is 0 before any sweep (the divergence stage clears it)
+  std::vector<float> p(C);
+  for (float* buf : {pa, pb}) {
+    AQ_CUDA(cudaMemcpy(p.data(), buf, 4 * C, cudaMemcpyDeviceToHost));
+    for (size_t c = 0; c < C; ++c)
+      if (ty[c] != kFluid) p[c] = 0.f;
+    AQ_CUDA(cudaMemcpy(buf, p.data(), 4 * C, cudaMemcpyHostToDevice));
+  }
+  AQ_CUDA(cudaMemcpy(bact, act.data(), (size_t)nbricks, cudaMemcpyHostToDevice));
+  SolveState s0;
+  memset(&s0, 0, sizeof(s0));
+  s0.b2 = b2;
+  s0.fluid_cells = nf;
+  s0.rel_residual = -1.0;
+  s0.r2 = -1.0;
+  AQ_CUDA(cudaMemcpy(ss, &s0, sizeof(s0), cudaMemcpyHostToDevice));
+  return AQ_OK;
+}
+
+aq_status aq_fluid::upload(const aq_host_state* s) {
+  if (s->size_x != d.sx || s->size_y != d.sy || s->size_z != d.sz || s->particle_count != n)
+    return fail(AQ_ERR_INVALID_ARGUMENT, "state dimensions do not match the fluid");
+  AQ_CUDA(cudaStreamSynchronize(stream));
+  const size_t N = (size_t)n, C = (size_t)d.C, F = (size_t)d.F;
+  if (s->position) {
+    const float lim[3] = {d.sx * d.h, d.sy * d.h, d.sz * d.h};
+    for (int k = 0; k < 3; ++k)
+      for (size_t i = 0; i < N; ++i) {
+        const float p = s->position[k * N + i];
+        if (!(p >= 0.f && p <= lim[k])) return fail(AQ_ERR_INVALID_ARGUMENT, "particle position outside the domain");
+      }
+  }
+  auto put = [&](void* dst, const void* src, size_t bytes) -> aq_status {
+    AQ_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    return AQ_OK;
+  };
+  time = s->physical_time;
+  if (s->position && N) {
+    AQ_TRY(put(cur.px, s->position, 4 * N)); AQ_TRY(put(cur.py, s->position + N, 4 * N));
+    AQ_TRY(put(cur.pz, s->position + 2 * N, 4 * N));
+  }
+  if (s->velocity_p && N) {
+    AQ_TRY(put(cur.vx, s->velocity_p, 4 * N)); AQ_TRY(put(cur.vy, s->velocity_p + N, 4 * N));
+    AQ_TRY(put(cur.vz, s->velocity_p + 2 * N, 4 * N));
+  }
+  bool mode_changed = false;
+  if (s->fractions && N) {
+    std::vector<float4> fr(N);
+    int ph = -1;
+    bool multi = false;
+    for (size_t i = 0; i < N; ++i) {
+      fr[i] = make_float4(s->fractions[i], s->fractions[N + i], s->fractions[2 * N + i], s->fractions[3 * N + i]);
+      const float e[4] = {fr[i].x, fr[i].y, fr[i].z, fr[i].w};
+      int hot = -1, nz = 0;
+      for (int k = 0; k < 4; ++k)
+        if (e[k] != 0.f) { nz++; hot = k; }
+      if (nz != 1 || e[hot] != 1.f) multi = true;
+      else if (ph < 0) ph = hot;
+      else if (ph != hot) multi = true;
+    }
+    if (!multi && ph >= 0) {
+      if (multiphase || phase != ph) mode_changed = true;
+      multiphase = false;
+      phase = ph;
+    } else if (multi) {
+      if (!multiphase) mode_changed = true;
+      multiphase = true;
+    }
+    AQ_TRY(put(cur.frac, fr.data(), sizeof(float4) * N));
+    sp.multiphase = multiphase ? 1 : 0;
+    sp.phase = phase;
+  }
+  std::vector<int> content;
+  if (s->content) content.assign(s->content, s->content + F);
+  if (s->velocity) {
+    AQ_TRY(put(u0, s->velocity, 4 * F)); AQ_TRY(put(v0, s->velocity + F, 4 * F));
+    AQ_TRY(put(w0, s->velocity + 2 * F, 4 * F));
+  }
+  if (s->new_velocity) {
+    for (int which = 1; which <= 2; ++which) {
+      AQ_TRY(put(nvx(which), s->new_velocity, 4 * F)); AQ_TRY(put(nvy(which), s->new_velocity + F, 4 * F));
+      AQ_TRY(put(nvz(which), s->new_velocity + 2 * F, 4 * F));
+    }
+  }
+  if (s->pressure) {
+    AQ_TRY(put(pa, s->pressure, 4 * C));
+    AQ_TRY(put(pb, s->pressure, 4 * C));
+  }
+  if (s->divergence) AQ_TRY(put(div, s->divergence, 4 * C));
+  if (s->particle_count_cell) AQ_TRY(put(pcount, s->particle_count_cell, 4 * C));
+  if (s->density) AQ_TRY(put(density, s->density, 4 * C));
+  if (s->has_velocity) {
+    std::vector<uint8_t> hbits(F, 0);
+    for (int x = 0; x < d.sx; ++x)
+      for (int y = 0; y < d.sy; ++y)
+        for (int z = 0; z < d.sz; ++z) {
+          const size_t c = cell_index(d, x, y, z);
+          uint8_t b = 0;
+          for (int k = 0; k < 3; ++k) b |= (s->has_velocity[k * C + c] ? 1 : 0) << k;
+          hbits[node_index(d, x, y, z)] = b;
+        }
+    AQ_TRY(put(h1, hbits.data(), F));
+    AQ_TRY(put(h2, hbits.data(), F));
+  }
+  if (s->volume_fractions || s->new_volume_fractions) {
+    std::vector<float4> a(C);
+    if (s->volume_fractions) {
+      for (size_t c = 0; c < C; ++c)
+        a[c] = make_float4(s->volume_fractions[c], s->volume_fractions[C + c], s->volume_fractions[2 * C + c],
+                           s->volume_fractions[3 * C + c]);
+      AQ_TRY(put(vf, a.data(), sizeof(float4) * C));
+    }
+    if (s->new_volume_fractions) {
+      for (size_t c = 0; c < C; ++c)
+        a[c] = make_float4(s->new_volume_fractions[c], s->new_volume_fractions[C + c],
+                           s->new_volume_fractions[2 * C + c], s->new_volume_fractions[3 * C + c]);
+      AQ_TRY(put(nvf, a.data(), sizeof(float4) * C));
+    }
+  }
+  if (s->cell_start && s->cell_end) {
+    std::vector<int> o(C + 1);
+    int run = 0;
+    for (size_t c = 0; c < C; ++c) {
+      o[c] = run;
+      if (s->cell_start[c] >= 0) {
+        if (s->cell_start[c] != run || s->cell_end[c] < s->cell_start[c])
+          return fail(AQ_ERR_INVALID_ARGUMENT, "cell tables are not a sorted partition of the particles");
+        run = s->cell_end[c] + 1;
+      }
+    }
+    if (run != n) return fail(AQ_ERR_INVALID_ARGUMENT, "cell tables do not cover every particle");
+    o[C] = run;
+    AQ_TRY(put(off, o.data(), 4 * (C + 1)));
+  }
+  if (s->sort_index && N) AQ_TRY(put(sort_index, s->sort_index, 4 * N));
+  // derived solver inputs
+  if (s->content || s->divergence || s->density) {
+    std::vector<int> ct = content;
+    if (ct.empty()) {
+      aq_host_state q;
+      memset(&q, 0, sizeof(q));
+      q.size_x = d.sx; q.size_y = d.sy; q.size_z = d.sz; q.particle_count = n;
+      ct.resize(F);
+      q.content = ct.data();
+      AQ_TRY(download(&q));
+    }
+    std::vector<float> dv(C), dn(C);
+    AQ_CUDA(cudaMemcpy(dv.data(), div, 4 * C, cudaMemcpyDeviceToHost));
+    AQ_CUDA(cudaMemcpy(dn.data(), density, 4 * C, cudaMemcpyDeviceToHost));
+    AQ_TRY(derive_from_state(ct, dv, dn));
+  }
+  nv_cur = has_cur = 2;
+  sorted_by_stage1 = false;
+  if (mode_changed) invalidate_graph();
+  return AQ_OK;
+}
+
+// ====================================================================== ABI
+namespace {
+
+aq_status validate(const aq_config* c) {
+  if (!c) return fail(AQ_ERR_INVALID_ARGUMENT, "config is NULL");
+  if (c->size_x < 4 || c->size_y < 4 || c->size_z < 4)
+    return fail(AQ_ERR_INVALID_CONFIG, "grid sizes must be >= 4 per axis");
+  if ((double)(c->size_x + 1) * (c->size_y + 1) * (c->size_z + 1) > 1.5e9)
+    return fail(AQ_ERR_INVALID_CONFIG, "grid too large");
+  if (c->phase_count > AQ_MAX_PHASES) return fail(AQ_ERR_INVALID_CONFIG, "Only supports up to 4 phases");
+  if (c->volume_count < 0 || c->volume_count > AQ_MAX_VOLUMES)
+    return fail(AQ_ERR_INVALID_CONFIG, "volume_count out of range");
+  for (int i = 0; i < c->volume_count; ++i) {
+    const aq_volume& v = c->volumes[i];
+    if (v.shape != AQ_SHAPE_SPHERE && v.shape != AQ_SHAPE_SQUARE)
+      return fail(AQ_ERR_INVALID_CONFIG, "unknown volume shape");
+    if (v.phase < 0 || v.phase >= AQ_MAX_PHASES)
+      return fail(AQ_ERR_INVALID_CONFIG, "volume phase must be in [0,4)");
+  }
+  if (!(c->domain_size > 0.f) || !std::isfinite(c->domain_size))
+    return fail(AQ_ERR_INVALID_CONFIG, "domain_size must be positive");
+  if (!std::isfinite(c->timestep) || c->timestep < 0.f) return fail(AQ_ERR_INVALID_CONFIG, "timestep must be >= 0");
+  if (c->pressure_iterations < 0 || c->diffusion_iterations < 0)
+    return fail(AQ_ERR_INVALID_CONFIG, "iteration counts must be >= 0");
+  if (c->pressure_init != AQ_PRESSURE_CARRY && c->pressure_init != AQ_PRESSURE_ZERO)
+    return fail(AQ_ERR_INVALID_CONFIG, "unknown pressure_init");
+  if (c->solve_mode != AQ_SOLVE_FIXED && c->solve_mode != AQ_SOLVE_RESIDUAL)
+    return fail(AQ_ERR_INVALID_CONFIG, "unknown solve_mode");
+  if (c->solve_mode == AQ_SOLVE_RESIDUAL) {
+    if (!(c->rel_residual > 0.f)) return fail(AQ_ERR_INVALID_CONFIG, "rel_residual must be > 0");
+    if (c->check_interval < 1 || c->max_iterations < c->check_interval)
+      return fail(AQ_ERR_INVALID_CONFIG, "need 1 <= check_interval <= max_iterations");
+  }
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(c->gravity[k])) return fail(AQ_ERR_INVALID_CONFIG, "gravity must be finite");
+  return AQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t aq_abi_version(void) { return AQ_ABI_VERSION; }
+
+const char* aq_last_error(void) { return g_last_error.c_str(); }
+
+aq_status aq_config_default(aq_config* c) {
+  if (!c) return fail(AQ_ERR_INVALID_ARGUMENT, "config is NULL");
+  memset(c, 0, sizeof(*c));
+  c->volume_count = 2;
+  c->volumes[0].shape = AQ_SHAPE_SQUARE;
+  c->volumes[1].shape = AQ_SHAPE_SPHERE;
+  for (int i = 0; i < 2; ++i) {
+    aq_volume& v = c->volumes[i];
+    v.box_min[0] = 0; v.box_min[1] = 0; v.box_min[2] = 0;
+    v.box_max[0] = 1; v.box_max[1] = 0.1875f; v.box_max[2] = 1;
+    v.ball_center[0] = 0.5f; v.ball_center[1] = 0.75f; v.ball_center[2] = 0.5f;
+    v.ball_radius = 0.125f;
+    v.phase = 0;
+  }
+  c->gravity[1] = -9.8f;
+  c->phase_count = 2;
+  for (int i = 0; i < 4; ++i) c->phase_densities[i] = 1.f;
+  c->diffusion_coeff = 0.001f;
+  c->size_x = c->size_y = c->size_z = 50;
+  c->pressure_iterations = 100;
+  c->diffusion_iterations = 100;
+  c->timestep = 0.033f;
+  c->flip_coeff = 0.95f;
+  c->particle_jitter = 0.05f;
+  c->domain_size = 10.f;
+  c->seed = 1;
+  c->pressure_init = AQ_PRESSURE_CARRY;
+  c->solve_mode = AQ_SOLVE_FIXED;
+  c->rel_residual = 1e-4f;
+  c->max_iterations = 2000;
+  c->check_interval = 40;
+  c->device = 0;
+  c->stream = nullptr;
+  g_last_error.clear();
+  return AQ_OK;
+}
+
+aq_status aq_config_validate(const aq_config* cfg) {
+  aq_status st = validate(cfg);
+  if (st == AQ_OK) g_last_error.clear();
+  return st;
+}
+
+aq_status aq_fluid_create(const aq_config* cfg, aq_fluid** out) {
+  if (!out) return fail(AQ_ERR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  AQ_TRY(validate(cfg));
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(AQ_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (cfg->device < 0 || cfg->device >= ndev) return fail(AQ_ERR_INVALID_CONFIG, "device ordinal out of range");
+  aq_fluid* f = new aq_fluid();
+  f->cfg = *cfg;
+  f->device = cfg->device;
+  cudaError_t e = cudaSetDevice(f->device);
+  if (e != cudaSuccess) { delete f; return fail(AQ_ERR_CUDA, cudaGetErrorString(e)); }
+  if (cfg->stream) {
+    f->stream = (cudaStream_t)cfg->stream;
+  } else {
+    e = cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete f; return fail(AQ_ERR_CUDA, cudaGetErrorString(e)); }
+    f->own_stream = true;
+  }
+  e = cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete f; return fail(AQ_ERR_CUDA, cudaGetErrorString(e)); }
+  Dims& d = f->d;
+  d.sx = cfg->size_x; d.sy = cfg->size_y; d.sz = cfg->size_z;
+  d.C = d.sx * d.sy * d.sz;
+  d.F = (d.sx + 1) * (d.sy + 1) * (d.sz + 1);
+  d.nz = d.sz + 1;
+  d.nyz = (d.sy + 1) * (d.sz + 1);
+  d.h = cfg->domain_size / (float)d.sy;  // cellPhysicalSize (Fluid/Fluid_3D_FLIP.cu:444)
+  d.inv_h = 1.0f / d.h;
+  d.bx = (d.sx + kBrick - 1) / kBrick; d.by = (d.sy + kBrick - 1) / kBrick; d.bz = (d.sz + kBrick - 1) / kBrick;
+  d.cov_x = covered_faces(d.sy, d.sz);
+  d.cov_y = covered_faces(d.sx, d.sz);
+  d.cov_z = covered_faces(d.sx, d.sy);
+  StepParams& sp = f->sp;
+  sp.dt = cfg->timestep;
+  sp.flip = cfg->flip_coeff;
+  sp.gdx = cfg->gravity[0] * cfg->timestep;
+  sp.gdy = cfg->gravity[1] * cfg->timestep;
+  sp.gdz = cfg->gravity[2] * cfg->timestep;
+  sp.gx_nz = cfg->gravity[0] != 0.f; sp.gy_nz = cfg->gravity[1] != 0.f; sp.gz_nz = cfg->gravity[2] != 0.f;
+  for (int k = 0; k < 4; ++k) sp.rho[k] = cfg->phase_densities[k];
+  e = jacobi_prepare();
+  if (e != cudaSuccess) { delete f; return fail(AQ_ERR_CUDA, std::string("jacobi_prepare: ") + cudaGetErrorString(e)); }
+  aq_status st = f->seed_and_init();
+  if (st != AQ_OK) { delete f; return st; }
+  *out = f;
+  g_last_error.clear();
+  return AQ_OK;
+}
+
+void aq_fluid_destroy(aq_fluid* f) { delete f; }
+
+aq_status aq_fluid_step(aq_fluid* f, int32_t n_steps) {
+  if (!f || n_steps < 0) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(f->device);
+  return f->step(n_steps);
+}
+
+aq_status aq_fluid_step_host(aq_fluid* f, int32_t n_steps, const float* pin, const float* vin, float* pout,
+                             float* vout) {
+  if (!f || n_steps < 0) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(f->device);
+  const size_t N = (size_t)f->n;
+  cudaStream_t s = f->stream;
+  if (N) {
+    if (pin) {
+      AQ_CUDA(cudaMemcpyAsync(f->cur.px, pin, 4 * N, cudaMemcpyHostToDevice, s));
+      AQ_CUDA(cudaMemcpyAsync(f->cur.py, pin + N, 4 * N, cudaMemcpyHostToDevice, s));
+      AQ_CUDA(cudaMemcpyAsync(f->cur.pz, pin + 2 * N, 4 * N, cudaMemcpyHostToDevice, s));
+    }
+    if (vin) {
+      AQ_CUDA(cudaMemcpyAsync(f->cur.vx, vin, 4 * N, cudaMemcpyHostToDevice, s));
+      AQ_CUDA(cudaMemcpyAsync(f->cur.vy, vin + N, 4 * N, cudaMemcpyHostToDevice, s));
+      AQ_CUDA(cudaMemcpyAsync(f->cur.vz, vin + 2 * N, 4 * N, cudaMemcpyHostToDevice, s));
+    }
+  }
+  AQ_TRY(f->step(n_steps));
+  if (N) {
+    if (pout) {
+      AQ_CUDA(cudaMemcpyAsync(pout, f->cur.px, 4 * N, cudaMemcpyDeviceToHost, s));
+      AQ_CUDA(cudaMemcpyAsync(pout + N, f->cur.py, 4 * N, cudaMemcpyDeviceToHost, s));
+      AQ_CUDA(cudaMemcpyAsync(pout + 2 * N, f->cur.pz, 4 * N, cudaMemcpyDeviceToHost, s));
+    }
+    if (vout) {
+      AQ_CUDA(cudaMemcpyAsync(vout, f->cur.vx, 4 * N, cudaMemcpyDeviceToHost, s));
+      AQ_CUDA(cudaMemcpyAsync(vout + N, f->cur.vy, 4 * N, cudaMemcpyDeviceToHost, s));
+      AQ_CUDA(cudaMemcpyAsync(vout + 2 * N, f->cur.vz, 4 * N, cudaMemcpyDeviceToHost, s));
+    }
+  }
+  AQ_CUDA(cudaStreamSynchronize(s));
+  return AQ_OK;
+}
+
+aq_status aq_fluid_run_stage(aq_fluid* f, int32_t stage) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  cudaSetDevice(f->device);
+  return f->run_stage(stage);
+}
+
+aq_status aq_fluid_synchronize(aq_fluid* f) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  AQ_CUDA(cudaStreamSynchronize(f->stream));
+  return AQ_OK;
+}
+
+aq_status aq_fluid_time(const aq_fluid* f, double* t) {
+  if (!f || !t) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  *t = f->time;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_particle_count(const aq_fluid* f, int32_t* n) {
+  if (!f || !n) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  *n = f->n;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_container(const aq_fluid* f, float center[3], float* size) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  // Fluid::getCenter / getContainerSize (Fluid/Fluid_3D_FLIP.cu:728-733)
+  const float g = f->cfg.domain_size;
+  if (center) center[0] = center[1] = center[2] = g / 2;
+  if (size) *size = g;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_stream(const aq_fluid* f, void** stream) {
+  if (!f || !stream) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  *stream = (void*)f->stream;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_download_state(aq_fluid* f, aq_host_state* s) {
+  if (!f || !s) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(f->device);
+  return f->download(s);
+}
+
+aq_status aq_fluid_upload_state(aq_fluid* f, const aq_host_state* s) {
+  if (!f || !s) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(f->device);
+  return f->upload(s);
+}
+
+aq_status aq_fluid_solve_stats(const aq_fluid* f, aq_solve_stats* st) {
+  if (!f || !st) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(f->device);
+  SolveState s;
+  AQ_CUDA(cudaMemcpyAsync(f->ss_host, f->ss, sizeof(SolveState), cudaMemcpyDeviceToHost, f->stream));
+  AQ_CUDA(cudaStreamSynchronize(f->stream));
+  s = *f->ss_host;
+  st->iterations = s.iterations;
+  st->rel_residual = s.rel_residual;
+  st->b_norm = s.b2 >= 0 ? sqrt(s.b2) : -1.0;
+  st->fluid_cells = s.fluid_cells;
+  st->converged = s.converged;
+  st->blocks = s.bodies;
+  st->total_sweeps = s.total_sweeps;
+  st->total_blocks = s.total_bodies;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_launches_per_step(const aq_fluid* f, int32_t* launches) {
+  if (!f || !launches) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  int32_t bodies = 0;
+  if (f->body_launches > 0) {
+    cudaSetDevice(f->device);
+    AQ_CUDA(cudaMemcpyAsync(f->ss_host, f->ss, sizeof(SolveState), cudaMemcpyDeviceToHost, f->stream));
+    AQ_CUDA(cudaStreamSynchronize(f->stream));
+    bodies = f->ss_host->bodies;
+  }
+  *launches = f->graph_launches + bodies * f->body_launches;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, int32_t x_planes) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  const bool flat = rows == 0;
+  if (flat ? (levels != 1 || f->d.sz % 4 != 0)
+           : (!(levels == 1 || levels == 2 || levels == 4 || levels == 8) || !(rows == 8 || rows == 16 || rows == 32) ||
+              x_planes < 1))
+    return fail(AQ_ERR_INVALID_ARGUMENT, "unsupported Jacobi plan");
+  JacobiPlan p{levels, rows, flat ? 1 : x_planes};
+  // every level count the sweeps split into must fit the tile with its halo,
+  // including the residual variant (one more level)
+  for (int l = levels; l >= 1; l >>= 1) {
+    const JacobiPlan q = resid_plan(p, l);
+    JacobiPlan q2 = p;
+    q2.levels = l;
+    if (jacobi_parts(f->d, q, true) <= 0 || jacobi_parts(f->d, q2, false) <= 0)
+      return fail(AQ_ERR_INVALID_ARGUMENT, "tile too small for the plan's halo");
+  }
+  cudaSetDevice(f->device);
+  AQ_CUDA(cudaStreamSynchronize(f->stream));
+  int need = 0;
+  for (int l = levels; l >= 1; l >>= 1)
+    need = std::max(need, jacobi_parts(f->d, resid_plan(p, l), true));
+  if (need > f->jpart_cap) {
+    double* np_ = nullptr;
+    AQ_TRY(f->alloc(&np_, (size_t)need));
+    f->jpart = np_;
+    f->jpart_cap = need;
+  }
+  f->plan = p;
+  f->invalidate_graph();
+  return AQ_OK;
+}
+
+aq_status aq_fluid_get_jacobi_plan(const aq_fluid* f, int32_t* levels, int32_t* rows, int32_t* x_planes) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  if (levels) *levels = f->plan.levels;
+  if (rows) *rows = f->plan.by;
+  if (x_planes) *x_planes = f->plan.xc;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_launch_counts(const aq_fluid* f, int32_t* per_step, int32_t* per_block) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  if (per_step) *per_step = f->graph_launches;
+  if (per_block) *per_block = f->body_launches;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, int32_t* launches,
+                                      int64_t* cells_per_sweep) {
+  if (!f || sweeps < 1) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(f->device);
+  // The sweeps are captured into a graph and replayed, as inside a step.
+  cudaGraph_t g = nullptr;
+  AQ_CUDA(cudaStreamBeginCapture(f->stream, cudaStreamCaptureModeThreadLocal));
+  aq_status st = enqueue_sweeps(f, sweeps);
+  cudaGraph_t got = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(f->stream, &got);
+  if (st != AQ_OK) { if (got) cudaGraphDestroy(got); return st; }
+  if (ce != cudaSuccess) return fail(AQ_ERR_CUDA, cudaGetErrorString(ce));
+  g = got;
+  cudaGraphExec_t ex = nullptr;
+  ce = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) return fail(AQ_ERR_CUDA, cudaGetErrorString(ce));
+  cudaEvent_t a, b;
+  AQ_CUDA(cudaEventCreate(&a));
+  AQ_CUDA(cudaEventCreate(&b));
+  AQ_CUDA(cudaGraphLaunch(ex, f->stream));  // warm
+  AQ_CUDA(cudaEventRecord(a, f->stream));
+  AQ_CUDA(cudaGraphLaunch(ex, f->stream));
+  AQ_CUDA(cudaEventRecord(b, f->stream));
+  AQ_CUDA(cudaEventSynchronize(b));
+  cudaGraphExecDestroy(ex);
+  float t = 0.f;
+  AQ_CUDA(cudaEventElapsedTime(&t, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  const std::vector<int> parts = split_sweeps(sweeps, f->plan.levels);
+  if (ms) *ms = t;
+  if (launches) *launches = (int32_t)(parts.size() + parts.size() % 2);
+  if (cells_per_sweep) {
+    std::vector<uint8_t> act((size_t)f->nbricks);
+    AQ_CUDA(cudaMemcpy(act.data(), f->bact, act.size(), cudaMemcpyDeviceToHost));
+    *cells_per_sweep = jacobi_cells_updated(f->d, f->plan, act.data());
+  }
+  return AQ_OK;
+}
+
+aq_status aq_fluid_pcg_reference(aq_fluid* f, double rel_tol, int32_t max_iter, float* pressure_out,
+                                 double* rel_error, int32_t* iterations, double* achieved) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  cudaSetDevice(f->device);
+  const Dims& d = f->d;
+  const size_t C = (size_t)d.C;
+  const int nparts = 1024;
+  if (!f->pcg_b) {
+    AQ_TRY(f->alloc(&f->pcg_b, C)); AQ_TRY(f->alloc(&f->pcg_x, C)); AQ_TRY(f->alloc(&f->pcg_r, C));
+    AQ_TRY(f->alloc(&f->pcg_z, C)); AQ_TRY(f->alloc(&f->pcg_p, C)); AQ_TRY(f->alloc(&f->pcg_q, C));
+    AQ_TRY(f->alloc(&f->pcg_part, (size_t)nparts));
+  }
+  cudaStream_t s = f->stream;
+  std::vector<double> hp(nparts);
+  auto dot = [&](const double* a, const double* b, double* out) -> aq_status {
+    AQ_CUDA(launch_pcg_dot(s, d.C, a, b, f->pcg_part, nparts));
+    AQ_CUDA(cudaMemcpyAsync(hp.data(), f->pcg_part, sizeof(double) * nparts, cudaMemcpyDeviceToHost, s));
+    AQ_CUDA(cudaStreamSynchronize(s));
+    double t = 0.0;
+    for (int i = 0; i < nparts; ++i) t += hp[i];
+    *out = t;
+    return AQ_OK;
+  };
+  AQ_CUDA(launch_pcg_init(s, d, f->type, f->rhs, f->pcg_b, f->pcg_x));
+  AQ_CUDA(cudaMemcpyAsync(f->pcg_r, f->pcg_b, sizeof(double) * C, cudaMemcpyDeviceToDevice, s));
+  double bb = 0.0;
+  AQ_TRY(dot(f->pcg_b, f->pcg_b, &bb));
+  const double bn = sqrt(bb);
+  AQ_CUDA(launch_pcg_precond(s, d, f->type, f->pcg_r, f->pcg_z));
+  AQ_CUDA(cudaMemcpyAsync(f->pcg_p, f->pcg_z, sizeof(double) * C, cudaMemcpyDeviceToDevice, s));
+  double rz = 0.0;
+  AQ_TRY(dot(f->pcg_r, f->pcg_z, &rz));
+  int it = 0;
+  double rn = bn;
+  if (bn > 0) {
+    for (it = 0; it < max_iter; ++it) {
+      AQ_CUDA(launch_pcg_apply(s, d, f->type, f->pcg_p, f->pcg_q));
+      double pq = 0.0;
+      AQ_TRY(dot(f->pcg_p, f->pcg_q, &pq));
+      if (!(pq > 0)) break;
+      const double alpha = rz / pq;
+      AQ_CUDA(launch_pcg_axpy(s, d.C, alpha, f->pcg_p, f->pcg_x));
+      AQ_CUDA(launch_pcg_axpy(s, d.C, -alpha, f->pcg_q, f->pcg_r));
+      double rr = 0.0;
+      AQ_TRY(dot(f->pcg_r, f->pcg_r, &rr));
+      rn = sqrt(rr);
+      if (rn <= rel_tol * bn) { ++it; break; }
+      AQ_CUDA(launch_pcg_precond(s, d, f->type, f->pcg_r, f->pcg_z));
+      double rz2 = 0.0;
+      AQ_TRY(dot(f->pcg_r, f->pcg_z, &rz2));
+      const double beta = rz2 / rz;
+      rz = rz2;
+      AQ_CUDA(launch_pcg_xpby(s, d.C, f->pcg_z, beta, f->pcg_p));
+    }
+  }
+  if (iterations) *iterations = it;
+  if (achieved) *achieved = bn > 0 ? rn / bn : 0.0;
+  std::vector<double> x(C);
+  std::vector<float> p(C);
+  std::vector<int8_t> ty(C);
+  AQ_CUDA(cudaMemcpyAsync(x.data(), f->pcg_x, sizeof(double) * C, cudaMemcpyDeviceToHost, s));
+  AQ_CUDA(cudaMemcpyAsync(p.data(), f->pa, sizeof(float) * C, cudaMemcpyDeviceToHost, s));
+  AQ_CUDA(cudaMemcpyAsync(ty.data(), f->type, C, cudaMemcpyDeviceToHost, s));
+  AQ_CUDA(cudaStreamSynchronize(s));
+  double num = 0.0, den = 0.0;
+  for (size_t c = 0; c < C; ++c) {
+    if (ty[c] != kFluid) continue;
+    const double e = (double)p[c] - x[c];
+    num += e * e;
+    den += x[c] * x[c];
+  }
+  if (rel_error) *rel_error = den > 0 ? sqrt(num / den) : 0.0;
+  if (pressure_out)
+    for (size_t c = 0; c < C; ++c) pressure_out[c] = (float)x[c];
+  return AQ_OK;
+}
+
+aq_status aq_fluid_profile_step(aq_fluid* f, float stage_ms[8]) {
+  if (!f || !stage_ms) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(f->device);
+  cudaEvent_t ev[9];
+  for (int i = 0; i < 9; ++i) AQ_CUDA(cudaEventCreate(&ev[i]));
+  AQ_CUDA(cudaEventRecord(ev[0], f->stream));
+  f->nv_cur = 2;
+  // stages 1+2 are one fused pass here: stage_ms[0] gets it, stage_ms[1] = 0
+  AQ_TRY(f->enq_particles(true));
+  AQ_CUDA(cudaEventRecord(ev[1], f->stream));
+  AQ_CUDA(cudaEventRecord(ev[2], f->stream));
+  AQ_TRY(f->enq_p2g(true));
+  AQ_CUDA(cudaEventRecord(ev[3], f->stream));
+  AQ_TRY(f->enq_divergence());
+  AQ_CUDA(cudaEventRecord(ev[4], f->stream));
+  if (f->cfg.solve_mode == AQ_SOLVE_RESIDUAL) AQ_TRY(f->enq_solve_residual_eager());
+  else AQ_TRY(f->enq_solve_fixed(f->cfg.pressure_iterations));
+  AQ_CUDA(cudaEventRecord(ev[5], f->stream));
+  AQ_TRY(f->enq_project());
+  AQ_CUDA(cudaEventRecord(ev[6], f->stream));
+  AQ_TRY(f->enq_extrapolate());
+  AQ_CUDA(cudaEventRecord(ev[7], f->stream));
+  AQ_TRY(f->enq_diffuse());
+  AQ_CUDA(cudaEventRecord(ev[8], f->stream));
+  AQ_CUDA(cudaEventSynchronize(ev[8]));
+  f->time += (double)f->cfg.timestep;
+  for (int i = 0; i < 8; ++i) AQ_CUDA(cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]));
+  for (int i = 0; i < 9; ++i) cudaEventDestroy(ev[i]);
+  return AQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,458 @@
+// Grid kernels: particle-to-grid transfer with forces and wall clamps,
+// divergence, pressure-gradient subtract, velocity extrapolation and phase
+// diffusion (stages (b), (c) and (e) except the Jacobi sweeps).
+//
+// Reference: Fluid/Fluid_3D_FLIP.cu:8-186 (P2G, divide, fractions, counts),
+// Fluid/Fluid_3D_kernels.cu:4-98 (gravity, fixBoundary), :118-207 (pressure
+// update), :210-422 (extrapolation), :426-458 (divergence), :520-556 (diffusion).
+#include "aq_kernels.cuh"
+
+namespace aqb {
+namespace {
+
+__device__ __forceinline__ float hat1(float r) { return fmaxf(0.f, 1.f - fabsf(r)); }
+
+// P2G gather for node (x,y,z) in [0,s)^3.  The reference loops over the 27
+// neighbour cells by a flat index with only a [0,C) range check, so rows at
+// the y/z edges wrap to far cells; those particles are more than h away and
+// add exactly +0 (sizes >= 4 are enforced), so only in-domain cells are
+// visited, in the same (dx,dy,dz,j) order.  A cell at dx=+1 cannot touch the
+// u-face at x (weight exactly 0 there), likewise dy=+1 for v and dz=+1 for w.
+// Weights use positions in cell units, q = p/h; the reference evaluates
+// (p - face*h)/h with approximate division (-use_fast_math).
+template <bool FORCES, bool MULTI>
+__global__ void __launch_bounds__(256) k_p2g(Dims d, StepParams sp, Particles cur, const int* __restrict__ off,
+                                            float* __restrict__ u0, float* __restrict__ v0,
+                                            float* __restrict__ w0, float* __restrict__ un,
+                                            float* __restrict__ vn, float* __restrict__ wn,
+                                            int8_t* __restrict__ type, float* __restrict__ density,
+                                            float4* __restrict__ vf, float4* __restrict__ nvf) {
+  const int z = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= d.sz || y >= d.sy) return;
+  const float fx = (float)x, fy = (float)y, fz = (float)z;
+  const float fxh = fx + 0.5f, fyh = fy + 0.5f, fzh = fz + 0.5f;
+  const float inv_h = d.inv_h;
+  float su = 0.f, sv = 0.f, sw = 0.f, wu = 0.f, wv = 0.f, ww = 0.f;
+  float4 fs = make_float4(0.f, 0.f, 0.f, 0.f);
+  float fw = 0.f;
+  int own = 0, left = 0, down = 0, back = 0;
+#pragma unroll
+  for (int dx = -1; dx <= 1; ++dx) {
+    const int X = x + dx;
+    if (X < 0 || X >= d.sx) continue;
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int Y = y + dy;
+      if (Y < 0 || Y >= d.sy) continue;
+#pragma unroll
+      for (int dz = -1; dz <= 1; ++dz) {
+        const int Z = z + dz;
+        if (Z < 0 || Z >= d.sz) continue;
+        const int c = (X * d.sy + Y) * d.sz + Z;
+        const int b = __ldg(off + c), e = __ldg(off + c + 1);
+        if (dx == 0 && dy == 0 && dz == 0) own = e - b;
+        if (dx == -1 && dy == 0 && dz == 0) left = e - b;
+        if (dx == 0 && dy == -1 && dz == 0) down = e - b;
+        if (dx == 0 && dy == 0 && dz == -1) back = e - b;
+        for (int j = b; j < e; ++j) {
+          const float qx = __ldg(cur.px + j) * inv_h;
+          const float qy = __ldg(cur.py + j) * inv_h;
+          const float qz = __ldg(cur.pz + j) * inv_h;
+          const float bx = hat1(qx - fxh), by = hat1(qy - fyh), bz = hat1(qz - fzh);
+          if (dx < 1) {
+            const float w = hat1(qx - fx) * by * bz;
+            su += w * __ldg(cur.vx + j);
+            wu += w;
+          }
+          if (dy < 1) {
+            const float w = bx * hat1(qy - fy) * bz;
+            sv += w * __ldg(cur.vy + j);
+            wv += w;
+          }
+          if (dz < 1) {
+            const float w = bx * by * hat1(qz - fz);
+            sw += w * __ldg(cur.vz + j);
+            ww += w;
+          }
+          if (MULTI && dx == 0 && dy == 0 && dz == 0) {
+            const float w = bx * by * bz;
+            const float4 f = cur.frac[j];
+            fs.x += w * f.x; fs.y += w * f.y; fs.z += w * f.z; fs.w += w * f.w;
+            fw += w;
+          }
+        }
+      }
+    }
+  }
+  // transferToCellDividePhase
+  const float u = wu > 0.f ? __fdiv_rn(su, wu) : 0.f;
+  const float v = wv > 0.f ? __fdiv_rn(sv, wv) : 0.f;
+  const float w = ww > 0.f ? __fdiv_rn(sw, ww) : 0.f;
+  const int ni = node_index(d, x, y, z);
+  const int ci = cell_index(d, x, y, z);
+  const bool fluid = own > 0;
+  u0[ni] = u; v0[ni] = v; w0[ni] = w;
+  type[ci] = fluid ? (int8_t)kFluid : (int8_t)kAir;
+  // transferVolumeFractionsToCell
+  if (MULTI) {
+    float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (fw > 0.f) {
+      f.x = __fdiv_rn(fs.x, fw); f.y = __fdiv_rn(fs.y, fw); f.z = __fdiv_rn(fs.z, fw); f.w = __fdiv_rn(fs.w, fw);
+      const float s = f.x + f.y + f.z + f.w;
+      f.x = __fdiv_rn(f.x, s); f.y = __fdiv_rn(f.y, s); f.z = __fdiv_rn(f.z, s); f.w = __fdiv_rn(f.w, s);
+    }
+    density[ci] = sp.rho[0] * f.x + sp.rho[1] * f.y + sp.rho[2] * f.z + sp.rho[3] * f.w;
+    vf[ci] = f;
+    nvf[ci] = f;
+  } else {
+    density[ci] = fluid ? sp.rho[sp.phase] : 0.f;
+  }
+  float nu = u, nv = v, nw = w;
+  if (FORCES) {
+    // applyGravityImpl: a fluid cell adds g*dt to its own three faces; an air
+    // cell receives g*dt from each fluid neighbour below it along an axis
+    // whose gravity component is nonzero.
+    if (fluid) {
+      nu += sp.gdx; nv += sp.gdy; nw += sp.gdz;
+    } else {
+      const int adds = (sp.gx_nz && left > 0) + (sp.gy_nz && down > 0) + (sp.gz_nz && back > 0);
+      for (int a = 0; a < adds; ++a) { nu += sp.gdx; nv += sp.gdy; nw += sp.gdz; }
+    }
+    // fixBoundaryX/Y/Z, low walls (the s-th layer is k_slayer's)
+    if (x == 0 && covered_x(d, y, z)) nu = fmaxf(0.f, nu);
+    if (y == 0 && covered_y(d, x, z)) nv = fmaxf(0.f, nv);
+    if (z == 0 && covered_z(d, x, y)) nw = fmaxf(0.f, nw);
+  }
+  un[ni] = nu; vn[ni] = nv; wn[ni] = nw;
+}
+
+// Nodes with a coordinate equal to s: never reset by resetCellImpl, so they
+// persist across steps; gravity reaches them only from the fluid cell below
+// along that axis and only where fixBoundary left them AIR.
+__global__ void __launch_bounds__(256) k_slayer(Dims d, StepParams sp, const int8_t* __restrict__ type,
+                                               const float* __restrict__ su, const float* __restrict__ sv,
+                                               const float* __restrict__ sw, float* __restrict__ u1,
+                                               float* __restrict__ v1, float* __restrict__ w1,
+                                               float* __restrict__ u2, float* __restrict__ v2,
+                                               float* __restrict__ w2) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int na = (d.sy + 1) * (d.sz + 1), nb = d.sx * (d.sz + 1), nc = d.sx * d.sy;
+  int x, y, z;
+  if (t < na) {
+    x = d.sx; y = t / (d.sz + 1); z = t % (d.sz + 1);
+  } else if ((t -= na) < nb) {
+    y = d.sy; x = t / (d.sz + 1); z = t % (d.sz + 1);
+  } else if ((t -= nb) < nc) {
+    z = d.sz; x = t / d.sy; y = t % d.sy;
+  } else {
+    return;
+  }
+  const bool solid = (x == d.sx && covered_x(d, y, z)) || (y == d.sy && covered_y(d, x, z)) ||
+                     (z == d.sz && covered_z(d, x, y));
+  const int ni = node_index(d, x, y, z);
+  float u = su[ni], v = sv[ni], w = sw[ni];
+  if (!solid) {
+    bool add = false;
+    if (x == d.sx && y < d.sy && z < d.sz) add = sp.gx_nz && type[cell_index(d, x - 1, y, z)] == kFluid;
+    else if (y == d.sy && x < d.sx && z < d.sz) add = sp.gy_nz && type[cell_index(d, x, y - 1, z)] == kFluid;
+    else if (z == d.sz && x < d.sx && y < d.sy) add = sp.gz_nz && type[cell_index(d, x, y, z - 1)] == kFluid;
+    if (add) { u += sp.gdx; v += sp.gdy; w += sp.gdz; }
+  }
+  if (covered_x(d, y, z)) {
+    if (x == 0) u = fmaxf(0.f, u);
+    if (x == d.sx) u = fminf(0.f, u);
+  }
+  if (covered_y(d, x, z)) {
+    if (y == 0) v = fmaxf(0.f, v);
+    if (y == d.sy) v = fminf(0.f, v);
+  }
+  if (covered_z(d, x, y)) {
+    if (z == 0) w = fmaxf(0.f, w);
+    if (z == d.sz) w = fminf(0.f, w);
+  }
+  u1[ni] = u; v1[ni] = v; w1[ni] = w;
+  u2[ni] = u; v2[ni] = v; w2[ni] = w;
+}
+
+// One 8x8x8 brick per CTA (threads z,y,x).
+__global__ void __launch_bounds__(512) k_divergence(Dims d, const int* __restrict__ off,
+                                                   const int8_t* __restrict__ type,
+                                                   const float* __restrict__ density,
+                                                   const float* __restrict__ un, const float* __restrict__ vn,
+                                                   const float* __restrict__ wn, int* __restrict__ pcount,
+                                                   float* __restrict__ div_out, float* __restrict__ rhs,
+                                                   float* __restrict__ pa, float* __restrict__ pb, int zero_init,
+                                                   uint8_t* __restrict__ brick_active,
+                                                   double* __restrict__ part_b2, int* __restrict__ part_nf) {
+  const int z = blockIdx.x * kBrick + threadIdx.x;
+  const int y = blockIdx.y * kBrick + threadIdx.y;
+  const int x = blockIdx.z * kBrick + threadIdx.z;
+  double b2 = 0.0;
+  int nf = 0;
+  if (x < d.sx && y < d.sy && z < d.sz) {
+    const int c = cell_index(d, x, y, z);
+    const int ni = node_index(d, x, y, z);
+    const int cnt = off[c + 1] - off[c];
+    const int pc = cnt > 0 ? cnt - 1 : 0;  // cellEnd - cellStart (inclusive end; -1 - -1 when empty)
+    pcount[c] = pc;
+    float dv = vn[ni + d.nz] - vn[ni] + un[ni + d.nyz] - un[ni] + wn[ni + 1] - wn[ni];
+    dv = (float)__dsub_rn((double)dv, __dmul_rn((double)((float)pc - 8.0f), 0.001));
+    div_out[c] = dv;
+    const bool fluid = type[c] == kFluid;
+    const float b = fluid ? (-dv) * density[c] : 0.f;
+    rhs[c] = b;
+    if (!fluid || zero_init) { pa[c] = 0.f; pb[c] = 0.f; }
+    if (fluid) { b2 = (double)b * (double)b; nf = 1; }
+  }
+  const int any = __syncthreads_or(nf);
+  // deterministic block reduction
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    b2 += __shfl_xor_sync(0xffffffffu, b2, o);
+    nf += __shfl_xor_sync(0xffffffffu, nf, o);
+  }
+  __shared__ double sb[16];
+  __shared__ int sn[16];
+  const int tid = threadIdx.x + kBrick * (threadIdx.y + kBrick * threadIdx.z);
+  if ((tid & 31) == 0) { sb[tid >> 5] = b2; sn[tid >> 5] = nf; }
+  __syncthreads();
+  if (tid == 0) {
+    double tb = 0.0;
+    int tn = 0;
+    for (int k = 0; k < 16; ++k) { tb += sb[k]; tn += sn[k]; }
+    const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    part_b2[bid] = tb;
+    part_nf[bid] = tn;
+    brick_active[(blockIdx.z * d.by + blockIdx.y) * d.bz + blockIdx.x] = any ? 1 : 0;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_b2_finalize(const double* __restrict__ part_b2,
+                                                     const int* __restrict__ part_nf, int nb,
+                                                     SolveState* __restrict__ ss) {
+  __shared__ double sb[1024];
+  __shared__ int sn[1024];
+  double b = 0.0;
+  int n = 0;
+  for (int i = threadIdx.x; i < nb; i += 1024) { b += part_b2[i]; n += part_nf[i]; }
+  sb[threadIdx.x] = b;
+  sn[threadIdx.x] = n;
+  __syncthreads();
+  for (int o = 512; o > 0; o >>= 1) {
+    if (threadIdx.x < o) { sb[threadIdx.x] += sb[threadIdx.x + o]; sn[threadIdx.x] += sn[threadIdx.x + o]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    ss->b2 = sb[0];
+    ss->fluid_cells = sn[0];
+    ss->iterations = 0;
+    ss->bodies = 0;
+    ss->converged = 0;
+    ss->nonfinite = 0;
+    ss->rel_residual = -1.0;
+    ss->r2 = -1.0;
+  }
+}
+
+// updateVelocityWithPressureImpl (Fluid/Fluid_3D_kernels.cu:118-207).
+__global__ void __launch_bounds__(256) k_project(Dims d, const int8_t* __restrict__ type,
+                                                const float* __restrict__ p, const float* __restrict__ dens,
+                                                float* __restrict__ u, float* __restrict__ v,
+                                                float* __restrict__ w, uint8_t* __restrict__ has) {
+  const int z = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= d.sz || y >= d.sy) return;
+  const int c = cell_index(d, x, y, z), ni = node_index(d, x, y, z);
+  const bool t = type[c] == kFluid;
+  const float pc = p[c], dc = dens[c];
+  float uu = u[ni], vv = v[ni], ww = w[ni];
+  uint8_t hb = 0;
+  if (x > 0) {
+    const int o = c - d.sy * d.sz;
+    const bool lc = type[o] == kFluid;
+    if (t || lc) {
+      const float ld = dens[o];
+      const float du = (t && lc) ? (ld + dc) / 2 : (lc ? ld : dc);
+      uu = uu - __fdiv_rn(pc - p[o], du);
+      hb |= 1;
+    }
+  }
+  if (y > 0) {
+    const int o = c - d.sz;
+    const bool lc = type[o] == kFluid;
+    if (t || lc) {
+      const float ld = dens[o];
+      const float du = (t && lc) ? (ld + dc) / 2 : (lc ? ld : dc);
+      vv = vv - __fdiv_rn(pc - p[o], du);
+      hb |= 2;
+    }
+  }
+  if (z > 0) {
+    const int o = c - 1;
+    const bool lc = type[o] == kFluid;
+    if (t || lc) {
+      const float ld = dens[o];
+      const float du = (t && lc) ? (ld + dc) / 2 : (lc ? ld : dc);
+      ww = ww - __fdiv_rn(pc - p[o], du);
+      hb |= 4;
+    }
+  }
+  u[ni] = uu; v[ni] = vv; w[ni] = ww;
+  has[ni] = hb;
+}
+
+// extrapolateVelocityByOne (Fluid/Fluid_3D_kernels.cu:210-422), reading the
+// previous pass only.  Neighbour order: left, down, back, right, up, front;
+// each neighbour counts if it has the component and its velocity along the
+// neighbour direction passes the epsilon test.
+__global__ void __launch_bounds__(256) k_extrapolate(Dims d, const float* __restrict__ ui,
+                                                    const float* __restrict__ vi, const float* __restrict__ wi,
+                                                    const uint8_t* __restrict__ hi, float* __restrict__ uo,
+                                                    float* __restrict__ vo, float* __restrict__ wo,
+                                                    uint8_t* __restrict__ ho) {
+  const int z = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= d.sz || y >= d.sy) return;
+  const float eps = (float)(-1 + 1e-6);
+  const int ni = node_index(d, x, y, z);
+  uint8_t h = hi[ni];
+  float val[3] = {ui[ni], vi[ni], wi[ni]};
+  if (h != 7) {
+    // neighbours: offset, exists, direction component, sign of the test
+    const int offs[6] = {-d.nyz, -d.nz, -1, d.nyz, d.nz, 1};
+    const bool ok[6] = {x > 0, y > 0, z > 0, x < d.sx - 1, y < d.sy - 1, z < d.sz - 1};
+    uint8_t nh[6];
+    float nvv[6][3];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      if (ok[k]) {
+        const int o = ni + offs[k];
+        nh[k] = hi[o];
+        nvv[k][0] = ui[o]; nvv[k][1] = vi[o]; nvv[k][2] = wi[o];
+      } else {
+        nh[k] = 0;
+        nvv[k][0] = nvv[k][1] = nvv[k][2] = 0.f;
+      }
+    }
+    uint8_t hn = h;
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      if (h & (1 << comp)) continue;
+      float sum = 0.f;
+      int cnt = 0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const int dir = k % 3;
+        const bool pass = k < 3 ? nvv[k][dir] > eps : nvv[k][dir] < -eps;
+        if (ok[k] && (nh[k] & (1 << comp)) && pass) { sum += nvv[k][comp]; cnt++; }
+      }
+      if (cnt > 0) {
+        val[comp] = __fdiv_rn(sum, (float)cnt);
+        hn |= (uint8_t)(1 << comp);
+      }
+    }
+    h = hn;
+  }
+  uo[ni] = val[0]; vo[ni] = val[1]; wo[ni] = val[2];
+  ho[ni] = h;
+}
+
+// diffusionJacobiImpl (Fluid/Fluid_3D_kernels.cu:520-556), ping-pong.  Air
+// cells keep their fractions (their pressure is already 0 after the solve).
+__global__ void __launch_bounds__(256) k_diffuse(Dims d, const int8_t* __restrict__ type, float lambda,
+                                                const float4* __restrict__ fin, float4* __restrict__ fout) {
+  const int z = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= d.sz || y >= d.sy) return;
+  const int c = cell_index(d, x, y, z);
+  if (type[c] != kFluid) { fout[c] = fin[c]; return; }
+  const int nb[6] = {x + 1 < d.sx ? c + d.sy * d.sz : c, x - 1 >= 0 ? c - d.sy * d.sz : c,
+                     y + 1 < d.sy ? c + d.sz : c, y - 1 >= 0 ? c - d.sz : c,
+                     z + 1 < d.sz ? c + 1 : c, z - 1 >= 0 ? c - 1 : c};
+  float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const float4 f = fin[nb[k]];
+    r.x += f.x * lambda; r.y += f.y * lambda; r.z += f.z * lambda; r.w += f.w * lambda;
+  }
+  const float4 s0 = fin[c];
+  r.x += s0.x; r.y += s0.y; r.z += s0.z; r.w += s0.w;
+  const float center = 1.f + 2 * lambda;
+  r.x = __fdiv_rn(r.x, center); r.y = __fdiv_rn(r.y, center);
+  r.z = __fdiv_rn(r.z, center); r.w = __fdiv_rn(r.w, center);
+  const float s = r.x + r.y + r.z + r.w;
+  r.x = __fdiv_rn(r.x, s); r.y = __fdiv_rn(r.y, s); r.z = __fdiv_rn(r.z, s); r.w = __fdiv_rn(r.w, s);
+  fout[c] = r;
+}
+
+inline dim3 node_grid(const Dims& d) { return dim3((d.sz + 31) / 32, (d.sy + 7) / 8, d.sx); }
+
+}  // namespace
+
+cudaError_t launch_p2g(cudaStream_t st, const Dims& d, const StepParams& sp, bool forces, Particles cur,
+                       const int* off, int n, float* u0, float* v0, float* w0, float* un, float* vn,
+                       float* wn, int8_t* type, float* density, float4* vf, float4* nvf) {
+  (void)n;
+  const dim3 g = node_grid(d), b(32, 8);
+  const bool multi = sp.multiphase != 0;
+  if (forces && multi)
+    k_p2g<true, true><<<g, b, 0, st>>>(d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+  else if (forces)
+    k_p2g<true, false><<<g, b, 0, st>>>(d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+  else if (multi)
+    k_p2g<false, true><<<g, b, 0, st>>>(d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+  else
+    k_p2g<false, false><<<g, b, 0, st>>>(d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_slayer(cudaStream_t st, const Dims& d, const StepParams& sp, const int8_t* type,
+                          const float* su, const float* sv, const float* sw, float* u1, float* v1, float* w1,
+                          float* u2, float* v2, float* w2) {
+  const int m = d.F - d.C;
+  k_slayer<<<(m + 255) / 256, 256, 0, st>>>(d, sp, type, su, sv, sw, u1, v1, w1, u2, v2, w2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_divergence(cudaStream_t st, const Dims& d, const int* off, const int8_t* type,
+                              const float* density, const float* un, const float* vn, const float* wn,
+                              int* pcount, float* div, float* rhs, float* pa, float* pb, bool zero_init,
+                              uint8_t* brick_active, double* part_b2, int* part_nf, int* nblocks_out) {
+  const dim3 g(d.bz, d.by, d.bx), b(kBrick, kBrick, kBrick);
+  if (nblocks_out) *nblocks_out = d.bx * d.by * d.bz;
+  k_divergence<<<g, b, 0, st>>>(d, off, type, density, un, vn, wn, pcount, div, rhs, pa, pb, zero_init ? 1 : 0,
+                                brick_active, part_b2, part_nf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_b2_finalize(cudaStream_t st, const double* part_b2, const int* part_nf, int nblocks,
+                               SolveState* ss) {
+  k_b2_finalize<<<1, 1024, 0, st>>>(part_b2, part_nf, nblocks, ss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_project(cudaStream_t st, const Dims& d, const int8_t* type, const float* p,
+                           const float* density, float* u, float* v, float* w, uint8_t* has) {
+  k_project<<<node_grid(d), dim3(32, 8), 0, st>>>(d, type, p, density, u, v, w, has);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_extrapolate(cudaStream_t st, const Dims& d, const float* ui, const float* vi,
+                               const float* wi, const uint8_t* hi, float* uo, float* vo, float* wo,
+                               uint8_t* ho) {
+  k_extrapolate<<<node_grid(d), dim3(32, 8), 0, st>>>(d, ui, vi, wi, hi, uo, vo, wo, ho);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_diffuse(cudaStream_t st, const Dims& d, const int8_t* type, float lambda,
+                           const float4* fin, float4* fout) {
+  k_diffuse<<<node_grid(d), dim3(32, 8), 0, st>>>(d, type, lambda, fin, fout);
+  return cudaGetLastError();
+}
+
+}  // namespace aqb

@@ -1,0 +1,412 @@
+// Pressure Jacobi sweeps, temporally blocked (stage (c), hot loop #1).
+//
+// Reference: jacobiImpl (Fluid/Fluid_3D_kernels.cu:460-505), launched
+// pressureIterations times (Fluid/Fluid_3D_common.cu:48-55).  Per fluid cell
+//   p' = (p[x+1] + p[x-1] + p[y+1] + p[y-1] + p[z+1] + p[z-1] + rhs) / 6,
+// rhs = -div*rho, air cells 0, out-of-domain neighbours clamped to the cell
+// itself (Neumann walls), summed in that order.  The reference updates in
+// place; this is the race-free Jacobi reading of it (ping-pong buffers).
+//
+// Blocking: a CTA of 32 x BY threads owns one (y,z) column each of a tile
+// with an H-cell halo and streams along x over `xc` output planes.  Level 0
+// loads a plane; level l = 1..L computes plane xi-l from level l-1.  Each
+// thread keeps the three x-neighbours of every level in registers; the four
+// in-plane neighbours come from a double-buffered shared-memory plane per
+// level.  Only level L is written back, so HBM/L2 traffic per sweep is about
+// 1/L of a plain sweep.  With RESID an extra level evaluates the FP64
+// residual b - A p of the written iterate on the CTA's output cells.
+#include <algorithm>
+
+#include "aq_kernels.cuh"
+
+namespace aqb {
+namespace {
+
+template <int L, bool RESID, int BY>
+__global__ void __launch_bounds__(32 * BY) k_jacobi(Dims d, int xc, const float* __restrict__ pin,
+                                                   float* __restrict__ pout, const float* __restrict__ rhs,
+                                                   const int8_t* __restrict__ type,
+                                                   const uint8_t* __restrict__ bact, double* __restrict__ part) {
+  constexpr int H = L + (RESID ? 1 : 0);
+  constexpr int TZ = 32 - 2 * H;
+  constexpr int TY = BY - 2 * H;
+  static_assert(TZ > 0 && TY > 0, "tile too small for the halo");
+  extern __shared__ float smem[];  // [2][H][BY][32]
+  __shared__ int s_active;
+  __shared__ double s_red[BY];
+
+  const int tz = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * 32 + tz;
+  const int z0 = blockIdx.x * TZ, y0 = blockIdx.y * TY, x0 = blockIdx.z * xc;
+  const int z = z0 - H + tz, y = y0 - H + ty;
+  const int x_end = min(x0 + xc, d.sx);
+  const bool col_in = z >= 0 && z < d.sz && y >= 0 && y < d.sy;
+  const bool col_out = col_in && tz >= H && tz < H + TZ && ty >= H && ty < H + TY;
+  const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+
+  // Skip tiles whose output region holds no fluid: it is all air, 0 in both
+  // buffers, and stays so for the whole solve.
+  if (tid == 0) s_active = 0;
+  __syncthreads();
+  {
+    const int bx0 = x0 / kBrick, bx1 = (x_end - 1) / kBrick;
+    const int by0 = y0 / kBrick, by1 = (min(y0 + TY, d.sy) - 1) / kBrick;
+    const int bz0 = z0 / kBrick, bz1 = (min(z0 + TZ, d.sz) - 1) / kBrick;
+    const int nbz = bz1 - bz0 + 1, nby = by1 - by0 + 1, nbx = bx1 - bx0 + 1;
+    const int total = nbx * nby * nbz;
+    for (int k = tid; k < total; k += 32 * BY) {
+      const int kz = k % nbz, ky = (k / nbz) % nby, kx = k / (nbz * nby);
+      if (bact[((bx0 + kx) * d.by + (by0 + ky)) * d.bz + (bz0 + kz)]) s_active = 1;
+    }
+  }
+  __syncthreads();
+  if (!s_active) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;");
+    if (RESID && tid == 0) part[bid] = 0.0;
+    return;
+  }
+
+  // programmatic dependent launch: the previous sweep must be complete (and
+  // done reading the buffer this launch writes) before any buffer access
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+
+  float R[H][3];
+  float rq[H + 1];
+  unsigned tq = 0;
+#pragma unroll
+  for (int l = 0; l < H; ++l) R[l][0] = R[l][1] = R[l][2] = 0.f;
+#pragma unroll
+  for (int k = 0; k <= H; ++k) rq[k] = 0.f;
+  double racc = 0.0;
+
+  const int tym = max(ty - 1, 0), typ = min(ty + 1, BY - 1);
+  const int tzm = max(tz - 1, 0), tzp = min(tz + 1, 31);
+  const bool has_ym = y - 1 >= 0, has_yp = y + 1 < d.sy;
+  const bool has_zm = z - 1 >= 0, has_zp = z + 1 < d.sz;
+  const int plane = d.sy * d.sz;
+  const int colofs = y * d.sz + z;
+
+  const int xs = max(x0 - H, 0);
+  const int xlast = x_end - 1 + H;
+  int par = 0;
+  for (int xi = xs; xi <= xlast; ++xi, par ^= 1) {
+    float pv = 0.f, rv = 0.f;
+    unsigned tv = 0;
+    if (col_in && xi < d.sx) {
+      const int c = xi * plane + colofs;
+      pv = pin[c];
+      rv = rhs[c];
+      tv = type[c] == kFluid ? 1u : 0u;
+    }
+    R[0][0] = R[0][1];
+    R[0][1] = R[0][2];
+    R[0][2] = pv;
+#pragma unroll
+    for (int k = H; k > 0; --k) rq[k] = rq[k - 1];
+    rq[0] = rv;
+    tq = (tq << 1) | tv;
+
+#pragma unroll
+    for (int l = 1; l <= H; ++l) {
+      float* E = smem + ((par * H + (l - 1)) * BY) * 32;
+      E[ty * 32 + tz] = R[l - 1][1];
+      __syncthreads();
+      const int c = xi - l;
+      const float self = R[l - 1][1];
+      const float xm = c - 1 >= 0 ? R[l - 1][0] : self;
+      const float xp = c + 1 < d.sx ? R[l - 1][2] : self;
+      const float ym = has_ym ? E[tym * 32 + tz] : self;
+      const float yp = has_yp ? E[typ * 32 + tz] : self;
+      const float zm = has_zm ? E[ty * 32 + tzm] : self;
+      const float zp = has_zp ? E[ty * 32 + tzp] : self;
+      const bool fl = (tq >> l) & 1u;
+      if (l <= L) {
+        float s = xp + xm;
+        s += yp;
+        s += ym;
+        s += zp;
+        s += zm;
+        s += rq[l];
+        const float nv = fl ? __fdiv_rn(s, 6.f) : 0.f;
+        if (l < H) {
+          R[l][0] = R[l][1];
+          R[l][1] = R[l][2];
+          R[l][2] = nv;
+        }
+        if (l == L && col_out && c >= x0 && c < x_end) pout[c * plane + colofs] = nv;
+      } else if (RESID) {
+        if (fl && col_out && c >= x0 && c < x_end) {
+          double s = (double)xp;
+          s += (double)xm;
+          s += (double)yp;
+          s += (double)ym;
+          s += (double)zp;
+          s += (double)zm;
+          const double r = (double)rq[l] + s - 6.0 * (double)self;
+          racc += r * r;
+        }
+      }
+    }
+  }
+
+  if (RESID) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) racc += __shfl_xor_sync(0xffffffffu, racc, o);
+    if (tz == 0) s_red[ty] = racc;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+      for (int k = 0; k < BY; ++k) t += s_red[k];
+      part[bid] = t;
+    }
+  }
+}
+
+
+// One sweep per launch, 4 consecutive z cells per thread (float4), no shared
+// memory: x and y neighbours come from L1/L2, z neighbours across threads by
+// warp shuffle.  Needs sz % 4 == 0.  Blocks of 32 z-quads x 8 rows on one
+// x plane; blocks whose 8 rows x 128 z cells hold no active brick return.
+__global__ void __launch_bounds__(256) k_jacobi_flat(Dims d, const float* __restrict__ pin,
+                                                    float* __restrict__ pout, const float* __restrict__ rhs,
+                                                    const int8_t* __restrict__ type,
+                                                    const uint8_t* __restrict__ bact) {
+  const int lane = threadIdx.x;
+  const int zq = blockIdx.x * 32 + lane;
+  const int z = zq * 4;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  const int x = blockIdx.z;
+  // brick check: the block spans one x brick, one y brick, 16 z bricks
+  const int bz0 = blockIdx.x * 16;
+  const int tid = threadIdx.y * 32 + lane;
+  int act = 0;
+  if (tid < 16 && bz0 + tid < d.bz) act = bact[((x / kBrick) * d.by + blockIdx.y) * d.bz + bz0 + tid];
+  act = __syncthreads_or(act);
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  if (!act) return;
+  const bool in = y < d.sy && z < d.sz;
+  const int plane = d.sy * d.sz;
+  const int c = x * plane + y * d.sz + z;
+  float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (in) p = *reinterpret_cast<const float4*>(pin + c);
+  // z neighbours across lanes (lanes of one row are consecutive quads)
+  float zlo = __shfl_up_sync(0xffffffffu, p.w, 1);
+  float zhi = __shfl_down_sync(0xffffffffu, p.x, 1);
+  if (!in) return;
+  if (lane == 0) zlo = z > 0 ? pin[c - 1] : p.x;
+  else if (z == 0) zlo = p.x;
+  if (lane == 31 || z + 4 >= d.sz) zhi = z + 4 < d.sz ? pin[c + 4] : p.w;
+  const float4 xp = x + 1 < d.sx ? *reinterpret_cast<const float4*>(pin + c + plane) : p;
+  const float4 xm = x > 0 ? *reinterpret_cast<const float4*>(pin + c - plane) : p;
+  const float4 yp = y + 1 < d.sy ? *reinterpret_cast<const float4*>(pin + c + d.sz) : p;
+  const float4 ym = y > 0 ? *reinterpret_cast<const float4*>(pin + c - d.sz) : p;
+  const float4 b = *reinterpret_cast<const float4*>(rhs + c);
+  const char4 t = *reinterpret_cast<const char4*>(type + c);
+  float4 o;
+  // p' = (x+1, x-1, y+1, y-1, z+1, z-1 summed in that order, + rhs) / 6
+  {
+    float s = xp.x + xm.x; s += yp.x; s += ym.x; s += p.y; s += zlo; s += b.x;
+    o.x = t.x == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+  }
+  {
+    float s = xp.y + xm.y; s += yp.y; s += ym.y; s += p.z; s += p.x; s += b.y;
+    o.y = t.y == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+  }
+  {
+    float s = xp.z + xm.z; s += yp.z; s += ym.z; s += p.w; s += p.y; s += b.z;
+    o.z = t.z == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+  }
+  {
+    float s = xp.w + xm.w; s += yp.w; s += ym.w; s += zhi; s += p.z; s += b.w;
+    o.w = t.w == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+  }
+  *reinterpret_cast<float4*>(pout + c) = o;
+}
+
+__global__ void __launch_bounds__(1024) k_resid_finalize(const double* __restrict__ part, int nparts,
+                                                        SolveState* __restrict__ ss, int sweeps, double tol,
+                                                        int max_iters, int set_cond,
+                                                        cudaGraphConditionalHandle handle) {
+  __shared__ double sb[1024];
+  double a = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += 1024) a += part[i];
+  sb[threadIdx.x] = a;
+  __syncthreads();
+  for (int o = 512; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sb[threadIdx.x] += sb[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double r2 = sb[0];
+    ss->iterations += sweeps;
+    ss->bodies += 1;
+    ss->total_sweeps += sweeps;
+    ss->total_bodies += 1;
+    ss->r2 = r2;
+    const double rel = ss->b2 > 0.0 ? sqrt(r2) / sqrt(ss->b2) : 0.0;
+    ss->rel_residual = rel;
+    const bool finite = isfinite(rel);
+    if (!finite) ss->nonfinite = 1;
+    const bool conv = finite && rel <= tol;
+    ss->converged = conv ? 1 : 0;
+    if (set_cond) {
+      const bool more = finite && !conv && ss->iterations < max_iters;
+      cudaGraphSetConditional(handle, more ? 1u : 0u);
+    }
+  }
+}
+
+template <int L, bool RESID, int BY>
+cudaError_t launch_one(cudaStream_t st, const Dims& d, int xc, const float* pin, float* pout, const float* rhs,
+                       const int8_t* type, const uint8_t* bact, double* part, int* nparts) {
+  constexpr int H = L + (RESID ? 1 : 0);
+  constexpr int TZ = 32 - 2 * H, TY = BY - 2 * H;
+  const dim3 grid((d.sz + TZ - 1) / TZ, (d.sy + TY - 1) / TY, (d.sx + xc - 1) / xc);
+  const size_t sm = sizeof(float) * 2 * H * BY * 32;
+  if (nparts) *nparts = (int)(grid.x * grid.y * grid.z);
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = grid;
+  lc.blockDim = dim3(32, BY);
+  lc.dynamicSmemBytes = sm;
+  lc.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  return cudaLaunchKernelEx(&lc, k_jacobi<L, RESID, BY>, d, xc, pin, pout, rhs, type, bact, part);
+}
+
+template <int L, bool RESID, int BY>
+cudaError_t set_smem_attr() {
+  constexpr int H = L + (RESID ? 1 : 0);
+  if constexpr (BY - 2 * H > 0 && 32 - 2 * H > 0) {
+    return cudaFuncSetAttribute(k_jacobi<L, RESID, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(float) * 2 * H * BY * 32));
+  }
+  return cudaSuccess;
+}
+
+template <int BY>
+cudaError_t prepare_by() {
+  cudaError_t e = cudaSuccess;
+  if ((e = set_smem_attr<1, false, BY>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<1, true, BY>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<2, false, BY>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<2, true, BY>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<4, false, BY>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<4, true, BY>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<8, false, BY>()) != cudaSuccess) return e;
+  return set_smem_attr<8, true, BY>();
+}
+
+template <int L, bool RESID>
+cudaError_t dispatch_by(cudaStream_t st, const Dims& d, int by, int xc, const float* pin, float* pout,
+                        const float* rhs, const int8_t* type, const uint8_t* bact, double* part, int* np) {
+  constexpr int H = L + (RESID ? 1 : 0);
+  if (by == 8) {
+    if constexpr (8 - 2 * H > 0) return launch_one<L, RESID, 8>(st, d, xc, pin, pout, rhs, type, bact, part, np);
+  } else if (by == 16) {
+    if constexpr (16 - 2 * H > 0) return launch_one<L, RESID, 16>(st, d, xc, pin, pout, rhs, type, bact, part, np);
+  } else if (by == 32) {
+    if constexpr (32 - 2 * H > 0) return launch_one<L, RESID, 32>(st, d, xc, pin, pout, rhs, type, bact, part, np);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <bool RESID>
+cudaError_t dispatch_levels(cudaStream_t st, const Dims& d, const JacobiPlan& p, const float* pin, float* pout,
+                            const float* rhs, const int8_t* type, const uint8_t* bact, double* part, int* np) {
+  switch (p.levels) {
+    case 1: return dispatch_by<1, RESID>(st, d, p.by, p.xc, pin, pout, rhs, type, bact, part, np);
+    case 2: return dispatch_by<2, RESID>(st, d, p.by, p.xc, pin, pout, rhs, type, bact, part, np);
+    case 4: return dispatch_by<4, RESID>(st, d, p.by, p.xc, pin, pout, rhs, type, bact, part, np);
+    case 8: return dispatch_by<8, RESID>(st, d, p.by, p.xc, pin, pout, rhs, type, bact, part, np);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+cudaError_t jacobi_prepare() {
+  cudaError_t e = prepare_by<8>();
+  if (e == cudaSuccess) e = prepare_by<16>();
+  if (e == cudaSuccess) e = prepare_by<32>();
+  return e;
+}
+
+long long jacobi_cells_updated(const Dims& d, const JacobiPlan& p, const uint8_t* bact_host) {
+  if (p.by == 0) {
+    long long cells = 0;  // flat: 1 x plane x 8 rows x 128 z per block
+    for (int x = 0; x < d.sx; ++x)
+      for (int y0 = 0; y0 < d.sy; y0 += 8)
+        for (int z0 = 0; z0 < d.sz; z0 += 128) {
+          bool act = false;
+          for (int bz = z0 / kBrick; bz < (z0 + 128) / kBrick && bz < d.bz && !act; ++bz)
+            act = bact_host[((x / kBrick) * d.by + y0 / kBrick) * d.bz + bz] != 0;
+          if (act) cells += (long long)std::min(8, d.sy - y0) * std::min(128, d.sz - z0);
+        }
+    return cells;
+  }
+  const int H = p.levels;
+  const int TZ = 32 - 2 * H, TY = p.by - 2 * H;
+  if (TZ <= 0 || TY <= 0 || p.xc <= 0) return -1;
+  long long cells = 0;
+  for (int x0 = 0; x0 < d.sx; x0 += p.xc)
+    for (int y0 = 0; y0 < d.sy; y0 += TY)
+      for (int z0 = 0; z0 < d.sz; z0 += TZ) {
+        const int x1 = x0 + p.xc < d.sx ? x0 + p.xc : d.sx;
+        const int y1 = y0 + TY < d.sy ? y0 + TY : d.sy;
+        const int z1 = z0 + TZ < d.sz ? z0 + TZ : d.sz;
+        bool act = false;
+        for (int bx = x0 / kBrick; bx <= (x1 - 1) / kBrick && !act; ++bx)
+          for (int by = y0 / kBrick; by <= (y1 - 1) / kBrick && !act; ++by)
+            for (int bz = z0 / kBrick; bz <= (z1 - 1) / kBrick && !act; ++bz)
+              act = bact_host[(bx * d.by + by) * d.bz + bz] != 0;
+        if (act) cells += (long long)(x1 - x0) * (y1 - y0) * (z1 - z0);
+      }
+  return cells;
+}
+
+int jacobi_parts(const Dims& d, const JacobiPlan& p, bool resid) {
+  if (p.by == 0) return resid ? -1 : 1;
+  const int H = p.levels + (resid ? 1 : 0);
+  const int TZ = 32 - 2 * H, TY = p.by - 2 * H;
+  if (TZ <= 0 || TY <= 0 || p.xc <= 0) return -1;
+  return ((d.sz + TZ - 1) / TZ) * ((d.sy + TY - 1) / TY) * ((d.sx + p.xc - 1) / p.xc);
+}
+
+cudaError_t launch_jacobi(cudaStream_t st, const Dims& d, const JacobiPlan& plan, bool resid, const float* pin,
+                          float* pout, const float* rhs, const int8_t* type, const uint8_t* brick_active,
+                          double* part, int* nparts_out) {
+  if (plan.by == 0) {
+    // flat plan: one sweep, no residual variant (the caller uses a tiled one)
+    if (resid || d.sz % 4 != 0) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((d.sz / 4 + 31) / 32, (d.sy + 7) / 8, d.sx);
+    lc.blockDim = dim3(32, 8);
+    lc.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    if (nparts_out) *nparts_out = 0;
+    return cudaLaunchKernelEx(&lc, k_jacobi_flat, d, pin, pout, rhs, type, brick_active);
+  }
+  if (resid) return dispatch_levels<true>(st, d, plan, pin, pout, rhs, type, brick_active, part, nparts_out);
+  return dispatch_levels<false>(st, d, plan, pin, pout, rhs, type, brick_active, part, nparts_out);
+}
+
+cudaError_t launch_resid_finalize(cudaStream_t st, const double* part, int nparts, SolveState* ss,
+                                  int sweeps_done_per_call, double tol, int max_iters, bool set_cond,
+                                  unsigned long long cond_handle) {
+  k_resid_finalize<<<1, 1024, 0, st>>>(part, nparts, ss, sweeps_done_per_call, tol, max_iters, set_cond ? 1 : 0,
+                                       (cudaGraphConditionalHandle)cond_handle);
+  return cudaGetLastError();
+}
+
+}  // namespace aqb

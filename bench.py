@@ -1,0 +1,318 @@
+"""Benchmark of the B200 FLIP step on the 128^3 ball-drop workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the configuration the headline metric is quoted on): 128^3 MAC grid,
+domain 10, pool y < 0.3 plus a sphere r = 0.12 at (0.5, 0.7, 0.5), 8 jittered
+particles per fluid cell (5.23M particles, seeded rand() sequence), dt 0.005,
+FLIP 0.95, gravity (0,-9.8,0), zero initial pressure each step, Jacobi run to
+relative residual 1e-4 (FP64, checked every 40 sweeps), capped at 2000 sweeps.
+A step is one simulationStep of that scene; its per-step working set
+(particle state ~250 MB plus grids) exceeds the 126 MB L2, so no flush is
+needed between steps.
+
+One JSON line on rank 0.  With N > 1 (torchrun) each rank steps its own
+replica of the scene (the path has no data exchange): weak scaling, time =
+max over ranks.  `--impl reference` times the CPU restatement of the
+reference step (oracle/, the reference has no CPU implementation of its own)
+on the host cores, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "FLIP steps/s at 128^3 x 8ppc, Jacobi to relative residual 1e-4 (plain, zero-init)"
+UNIT = "steps/s"
+MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+JACOBI_BYTES_PER_CELL = 13  # p read 4 + p write 4 + rhs 4 + cell type 1
+
+
+def workload_config(size=128, pressure_init="zero"):
+    from aquarius_b200 import _abi
+    vols = [dict(shape="box", min=(0, 0, 0), max=(1, 0.3, 1), phase=0),
+            dict(shape="sphere", center=(0.5, 0.7, 0.5), radius=0.12, phase=0)]
+    return _abi.make_config(
+        (size, size, size), vols, timestep=0.005, flip_coeff=0.95, particle_jitter=0.05,
+        pressure_init=_abi.PRESSURE_ZERO if pressure_init == "zero" else _abi.PRESSURE_CARRY,
+        solve_mode=_abi.SOLVE_RESIDUAL, rel_residual=1e-4, max_iterations=2000, check_interval=40)
+
+
+def config_desc(size, pressure_init):
+    return {"workload": f"ball drop {size}^3 x 8ppc (pool y<0.3 + sphere r=0.12), dt=0.005, "
+                        f"Jacobi to rel-res 1e-4 cap 2000, {pressure_init}-init pressure",
+            "grid": [size, size, size], "particles_per_cell": 8, "pressure_init": pressure_init,
+            "l2": "per-step working set > 126 MB L2 (no flush needed)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    try:
+        d = json.loads(MEASURED_PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def cpu_baseline_sample(size: int, pressure_init: str, steps: int = 1) -> dict:
+    """Times the CPU oracle on `steps` full steps of the same workload."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
+    import oracle_binding  # test infrastructure: the CPU restatement of the reference step
+    cfg = workload_config(size, pressure_init)
+    t0 = time.perf_counter()
+    o = oracle_binding.Oracle(cfg)
+    t_init = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    st = o.solve_stats()
+    o.close()
+    return {"value": steps / dt, "unit": UNIT, "cores": oracle_binding.oracle_threads(), "kind": "port",
+            "sample": f"{steps} full step(s) of the {size}^3 workload on the OpenMP oracle "
+                      f"(init {t_init:.1f}s excluded; last solve {st['iterations']} sweeps)",
+            "seconds": dt}
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    # each timed step is one full CPU step of the workload; warm-up steps are
+    # bounded to one, and timed steps to what fits in a few minutes
+    sys.path.insert(0, str(ROOT / "tests"))
+    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
+    import oracle_binding
+    cfg = workload_config(args.size, args.pressure_init)
+    o = oracle_binding.Oracle(cfg)
+    o.step(min(args.warmup, 1))
+    budget_s = 150.0
+    done, t0 = 0, time.perf_counter()
+    while done < args.steps:
+        o.step(1)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    v = done / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": done,
+            "warmup": min(args.warmup, 1), "ms_per_step": 1000 * dt / done, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_desc(args.size, args.pressure_init),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": oracle_binding.oracle_threads(), "kind": "port",
+                             "sample": f"{done} full CPU step(s) of the workload, OpenMP restatement of the "
+                                       f"reference step (the reference has no CPU path)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, dist):
+    import numpy as np
+    import torch
+
+    import aquarius_b200 as aq
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    cfg = workload_config(args.size, args.pressure_init)
+    cfg.device = dev
+    f = aq.Fluid(cfg)
+    stream = torch.cuda.ExternalStream(f.stream(), device=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (builds and instantiates the step graph)
+    f.step(args.warmup)
+    f.synchronize()
+    st0 = f.solve_stats()
+    per_step, per_block = f.launch_counts()
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.4)
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        f.step(args.steps)
+        ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms)
+    st1 = f.solve_stats()
+    sweeps = st1["total_sweeps"] - st0["total_sweeps"]
+    blocks = st1["total_blocks"] - st0["total_blocks"]
+    launches = args.steps * per_step + blocks * per_block
+    value = world * args.steps / (ms_max / 1000.0)
+
+    # e2e: the same steps through the C-ABI host-buffer entry point; every step
+    # uploads the particle state from pinned host memory and reads it back
+    n = f.particleCount
+    pin_pos = torch.empty((3, n), dtype=torch.float32).pin_memory()
+    pin_vel = torch.empty((3, n), dtype=torch.float32).pin_memory()
+    pos_np, vel_np = pin_pos.numpy(), pin_vel.numpy()
+    f.step_host(0, None, None, pos_np, vel_np)
+    e2e_steps = max(1, min(args.steps, 10))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            f.step_host(1, pos_np, vel_np, pos_np, vel_np)
+        e1.record(stream)
+    e1.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_wall = time.perf_counter() - t0
+    e2e_value = world * e2e_steps / (e2e_ms / 1000.0)
+
+    # roofline of the dominant kernel: Jacobi sweeps on the last step's system
+    hbm_peak, peak_kind = measured_hbm_peak()
+    jb = f.benchmark_pressure(400)
+    sweep_ms = jb["ms"] / 400
+    cells = jb["cells_per_sweep"]
+    achieved_gbs = JACOBI_BYTES_PER_CELL * cells / (sweep_ms / 1000.0) / 1e9
+    C = args.size ** 3
+    full_gbs = JACOBI_BYTES_PER_CELL * C / (sweep_ms / 1000.0) / 1e9
+
+    # pressure error of the plain solve against FP64 PCG on the same system
+    f.step(1)
+    pstats = f.solve_stats()
+    pcg = f.pcg_reference(rel_tol=1e-12, max_iter=200000)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_desc(args.size, args.pressure_init),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 12 * n,
+                "d2h_bytes_per_step": 2 * 12 * n, "steps": e2e_steps, "wall_s": e2e_wall,
+                "path": "aq_fluid_step_host (C ABI), pinned host particle state in and out every step"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "k_jacobi (temporally blocked)", "achieved": achieved_gbs,
+                     "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
+                     "traffic": None,
+                     "algorithmic_bytes": f"{JACOBI_BYTES_PER_CELL} B per updated cell per sweep x {cells} cells",
+                     "sweep_us": sweep_ms * 1000.0, "full_domain_equiv_gbs": full_gbs},
+        "clocks": clk,
+        "solver": {"sweeps_per_step": sweeps / args.steps, "blocks_per_step": blocks / args.steps,
+                   "last_rel_residual": pstats["rel_residual"], "last_iterations": pstats["iterations"],
+                   "converged": pstats["converged"], "fluid_cells": pstats["fluid_cells"],
+                   "pressure_rel_error_vs_fp64_pcg": pcg["rel_error"], "pcg_iterations": pcg["iterations"]},
+        "particles": n,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(args.size, args.pressure_init, steps=1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    f.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--pressure-init", default="zero", choices=["zero", "carry"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,262 @@
+/*
+ * aquarius_b200 — C ABI of the B200-native 3D FLIP step.
+ *
+ * This is the drop-in boundary for the reference solver plugin
+ * (AmesingFlank/Aquarius).  Each entry point below replaces one piece of the
+ * reference's `Fluid` / `Fluid_3D_FLIP::Fluid` surface:
+ *
+ *   reference                                           replacement
+ *   -------------------------------------------------   ------------------------------
+ *   FluidConfig / ConfigFLIP / InitializationVolume      aq_config / aq_volume
+ *     (Fluid/FluidConfig.cuh:16-97)
+ *   make_shared<Fluid_3D_FLIP::Fluid>() + init(config)   aq_fluid_create
+ *     (main.cu:158-170, Fluid/Fluid_3D_FLIP.cu:435-505)
+ *   Fluid::simulationStep() (Fluid/Fluid_3D_FLIP.cu:316)  aq_fluid_step
+ *   Fluid::physicalTime (Fluid/Fluid.h:10)               aq_fluid_time
+ *   Fluid_3D::getCenter / getContainerSize               aq_fluid_container
+ *     (Fluid/Fluid_3D.cuh:7-12, Fluid/Fluid_3D_FLIP.cu:728-733)
+ *   public members particles / grid->volumes / cellStart aq_fluid_download_state /
+ *     / cellEnd (Fluid/Fluid_3D_FLIP.cuh:54-111)           aq_fluid_upload_state
+ *   ~Fluid() (Fluid/Fluid_3D_FLIP.cu:735-748)            aq_fluid_destroy
+ *   print + exit(EXIT_FAILURE) (Common/GpuCommons.h:118)  aq_status + aq_last_error
+ *
+ * No entry point takes or returns a framework type: plain pointers, sizes and
+ * POD structs only.  Every call returns an aq_status; nothing exits or throws
+ * across the boundary.
+ */
+#ifndef AQUARIUS_B200_H
+#define AQUARIUS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AQ_ABI_VERSION 1
+#define AQ_MAX_VOLUMES 16
+#define AQ_MAX_PHASES 4
+
+/* Status codes.  The reference prints and calls exit() on any CUDA error
+ * (Common/GpuCommons.h:118-142) and throws a const char* for phaseCount > 4
+ * (Fluid/Fluid_3D_FLIP.cu:449-451); here both become return codes. */
+typedef enum aq_status {
+  AQ_OK = 0,
+  AQ_ERR_INVALID_CONFIG = 1,
+  AQ_ERR_INVALID_ARGUMENT = 2,
+  AQ_ERR_OUT_OF_MEMORY = 3,
+  AQ_ERR_CUDA = 4,
+  AQ_ERR_NOT_CONVERGED = 5,
+  AQ_ERR_NONFINITE = 6,
+  AQ_ERR_NO_DEVICE = 7
+} aq_status;
+
+/* ShapeType {Sphere, Square} (Fluid/FluidConfig.cuh:16-18). */
+typedef enum aq_shape { AQ_SHAPE_SPHERE = 0, AQ_SHAPE_SQUARE = 1 } aq_shape;
+
+/* Pressure initial guess for each step's solve.
+ * CARRY: the reference behaviour — pressure persists across steps (it is only
+ *        cleared when the grid is created, Fluid/MAC_Grid_3D.cu:54).
+ * ZERO:  pressure is zeroed before every solve. */
+typedef enum aq_pressure_init { AQ_PRESSURE_CARRY = 0, AQ_PRESSURE_ZERO = 1 } aq_pressure_init;
+
+/* FIXED: exactly pressure_iterations Jacobi sweeps (Fluid/Fluid_3D_common.cu:48-55).
+ * RESIDUAL: sweep in blocks of check_interval until the relative residual
+ *           ||b - A p||_2 / ||b||_2 over fluid cells (FP64) is <= rel_residual,
+ *           or max_iterations sweeps were done.  No counterpart in the reference. */
+typedef enum aq_solve_mode { AQ_SOLVE_FIXED = 0, AQ_SOLVE_RESIDUAL = 1 } aq_solve_mode;
+
+/* InitializationVolume (Fluid/FluidConfig.cuh:20-38).  Coordinates are the
+ * reference's normalised [0,1] container coordinates; ball_radius is in units
+ * of the container's y extent. */
+typedef struct aq_volume {
+  int32_t shape;
+  float box_min[3];
+  float box_max[3];
+  float ball_center[3];
+  float ball_radius;
+  int32_t phase;
+} aq_volume;
+
+/* POD mirror of FluidConfig + ConfigFLIP (Fluid/FluidConfig.cuh:41-97),
+ * fixed-size so it crosses a C boundary.  aq_config_default() fills the
+ * reference defaults. */
+typedef struct aq_config {
+  /* FluidConfig */
+  int32_t volume_count;
+  aq_volume volumes[AQ_MAX_VOLUMES];
+  float gravity[3];
+  int32_t phase_count;
+  float phase_densities[4];
+  float diffusion_coeff;
+  /* ConfigFLIP */
+  int32_t size_x, size_y, size_z;
+  int32_t pressure_iterations;
+  int32_t diffusion_iterations;
+  float timestep;
+  float flip_coeff;
+  float particle_jitter;
+  /* Fluid_3D_FLIP::Fluid::gridPhysicalSize (Fluid/Fluid_3D_FLIP.cuh:62) */
+  float domain_size;
+  /* Seed of the glibc rand() sequence used for particle jitter.  The
+   * reference never calls srand(), which is the same sequence as seed 1. */
+  uint32_t seed;
+  /* Extensions with no counterpart in the reference. */
+  int32_t pressure_init;   /* aq_pressure_init */
+  int32_t solve_mode;      /* aq_solve_mode */
+  float rel_residual;      /* RESIDUAL mode target, e.g. 1e-4 */
+  int32_t max_iterations;  /* RESIDUAL mode cap, e.g. 2000 */
+  int32_t check_interval;  /* RESIDUAL mode: sweeps between residual checks */
+  int32_t device;          /* CUDA device ordinal */
+  void* stream;            /* cudaStream_t to run on; NULL = library-owned stream */
+} aq_config;
+
+/* Host-side copy of the simulation state in one canonical layout.
+ *   cells  (C = sx*sy*sz):          index (x*sy + y)*sz + z
+ *   nodes  (F = (sx+1)(sy+1)(sz+1)): index (x*(sy+1) + y)*(sz+1) + z
+ * Velocity node (x,y,z) holds u on the x-face at (x, y+1/2, z+1/2)h, v on the
+ * y-face at (x+1/2, y, z+1/2)h and w on the z-face at (x+1/2, y+1/2, z)h
+ * (Fluid/MAC_Grid_3D.cuh:100-130).  Multi-component fields are planar:
+ * component k of element i is at [k*count + i].
+ * Any pointer may be NULL, in which case that field is skipped. */
+typedef struct aq_host_state {
+  int32_t size_x, size_y, size_z;  /* must match the fluid */
+  int32_t particle_count;          /* must match the fluid */
+  double physical_time;
+  float* position;          /* [3][N] */
+  float* velocity_p;        /* [3][N] particle velocity */
+  float* fractions;         /* [4][N] particle volume fractions */
+  int32_t* content;         /* [F]   0 air, 1 fluid, 2 solid */
+  float* velocity;          /* [3][F] grid velocity after the particle->grid transfer */
+  float* new_velocity;      /* [3][F] grid velocity after forces, pressure, extrapolation */
+  float* pressure;          /* [C] */
+  float* divergence;        /* [C] */
+  int32_t* particle_count_cell; /* [C] cellEnd - cellStart, as the reference stores it */
+  int32_t* has_velocity;    /* [3][C] 0/1 */
+  float* volume_fractions;  /* [4][C] */
+  float* new_volume_fractions; /* [4][C] */
+  float* density;           /* [C] */
+  int32_t* cell_start;      /* [C] first sorted particle of the cell, -1 if empty */
+  int32_t* cell_end;        /* [C] last sorted particle of the cell (inclusive), -1 if empty */
+  int32_t* particle_hash;   /* [N] cell index of each (sorted) particle */
+  int32_t* sort_index;      /* [N] pre-sort index of each sorted particle (particleIndices) */
+} aq_host_state;
+
+/* Sub-stages of one simulationStep, in order (Fluid/Fluid_3D_FLIP.cu:316-352).
+ * A full step runs 1..8 and advances physical time. */
+typedef enum aq_stage {
+  AQ_STAGE_G2P_ADVECT = 1,  /* transferToParticles + moveParticles */
+  AQ_STAGE_SORT = 2,        /* performSpatialHashing2 (hash, stable sort, cell tables) */
+  AQ_STAGE_P2G = 3,         /* resetCell + P2G + divide + fractions + applyGravity + fixBoundary */
+  AQ_STAGE_DIVERGENCE = 4,  /* countParticlesInCells + computeDivergence */
+  AQ_STAGE_PRESSURE = 5,    /* solvePressureJacobi */
+  AQ_STAGE_PROJECT = 6,     /* updateVelocityWithPressure */
+  AQ_STAGE_EXTRAPOLATE = 7, /* extrapolateVelocity (3 passes) */
+  AQ_STAGE_DIFFUSE = 8      /* solveDiffusionJacobi */
+} aq_stage;
+
+typedef struct aq_fluid aq_fluid;
+
+/* Statistics of the most recent pressure solve. */
+typedef struct aq_solve_stats {
+  int32_t iterations;       /* Jacobi sweeps done */
+  double rel_residual;      /* ||b - A p|| / ||b|| over fluid cells, FP64; -1 if not computed */
+  double b_norm;            /* ||b||_2 */
+  int32_t fluid_cells;
+  int32_t converged;        /* RESIDUAL mode: 1 if rel_residual <= target */
+  int32_t blocks;           /* residual-check blocks of the last solve */
+  int64_t total_sweeps;     /* sweeps since creation */
+  int64_t total_blocks;     /* residual-check blocks since creation */
+} aq_solve_stats;
+
+/* Fills *cfg with the reference defaults (Fluid/FluidConfig.cuh:20-97):
+ * 50^3, 100 Jacobi and 100 diffusion iterations, dt 0.033, FLIP 0.95,
+ * jitter 0.05, gravity (0,-9.8,0), 2 phases, densities 1, D 0.001, a box
+ * (0,0,0)-(1,0.1875,1) and a ball at (0.5,0.75,0.5) r 0.125, domain 10. */
+aq_status aq_config_default(aq_config* cfg);
+
+/* Validates cfg without touching the GPU. */
+aq_status aq_config_validate(const aq_config* cfg);
+
+/* Creates the solver and runs Fluid::init: grid allocation, particle seeding,
+ * boundary marking and the first particle->grid transfer. */
+aq_status aq_fluid_create(const aq_config* cfg, aq_fluid** out);
+
+/* Runs n_steps simulationStep()s.  Asynchronous on the fluid's stream. */
+aq_status aq_fluid_step(aq_fluid* f, int32_t n_steps);
+
+/* Host-buffer step, for callers that keep the particle state in host memory:
+ * uploads position_in/velocity_in ([3][N] each, may be NULL to keep the device
+ * copy), runs n_steps, downloads position_out/velocity_out ([3][N], may be
+ * NULL) and synchronizes.  Pinned buffers make the copies asynchronous. */
+aq_status aq_fluid_step_host(aq_fluid* f, int32_t n_steps,
+                             const float* position_in, const float* velocity_in,
+                             float* position_out, float* velocity_out);
+
+/* Runs one sub-stage (aq_stage) of a step; used to compare stages in
+ * isolation.  AQ_STAGE_DIFFUSE also advances physical time, as the last
+ * statement of simulationStep does. */
+aq_status aq_fluid_run_stage(aq_fluid* f, int32_t stage);
+
+/* Waits for all work of the fluid. */
+aq_status aq_fluid_synchronize(aq_fluid* f);
+
+aq_status aq_fluid_time(const aq_fluid* f, double* physical_time);
+aq_status aq_fluid_particle_count(const aq_fluid* f, int32_t* n);
+/* center[3] and the container size, as Fluid_3D::getCenter/getContainerSize. */
+aq_status aq_fluid_container(const aq_fluid* f, float center[3], float* size);
+/* The cudaStream_t the fluid runs on. */
+aq_status aq_fluid_stream(const aq_fluid* f, void** stream);
+
+aq_status aq_fluid_download_state(aq_fluid* f, aq_host_state* s);
+aq_status aq_fluid_upload_state(aq_fluid* f, const aq_host_state* s);
+
+aq_status aq_fluid_solve_stats(const aq_fluid* f, aq_solve_stats* st);
+
+/* Tile plan of the Jacobi kernel: sweeps per launch (1, 2, 4 or 8), tile
+ * rows (8, 16 or 32) and x planes per CTA (>= 1).  Chosen per grid by the
+ * tuner; invalid plans are rejected. */
+aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, int32_t x_planes);
+aq_status aq_fluid_get_jacobi_plan(const aq_fluid* f, int32_t* levels, int32_t* rows, int32_t* x_planes);
+
+/* FP64 preconditioned conjugate gradient on the current pressure system
+ * (the one the last AQ_STAGE_DIVERGENCE built), to rel_tol.  Writes the FP64
+ * solution as float into pressure_out ([C], host, may be NULL) and reports
+ * the relative L2 error of the fluid's current pressure against it over
+ * fluid cells.  Not part of a step; used to state pressure error. */
+aq_status aq_fluid_pcg_reference(aq_fluid* f, double rel_tol, int32_t max_iter,
+                                 float* pressure_out, double* rel_error,
+                                 int32_t* iterations, double* achieved_residual);
+
+/* Per-stage device times (ms) of one eagerly launched step; stage_ms[k-1]
+ * receives stage k (aq_stage).  Advances the simulation by one step. */
+aq_status aq_fluid_profile_step(aq_fluid* f, float stage_ms[8]);
+
+/* Kernel launches of the last step (graph nodes included; in RESIDUAL mode
+ * this depends on the residual-check blocks the last solve ran). */
+aq_status aq_fluid_launches_per_step(const aq_fluid* f, int32_t* launches);
+/* Kernel launches of a step outside the residual loop, and per loop block. */
+aq_status aq_fluid_launch_counts(const aq_fluid* f, int32_t* per_step, int32_t* per_block);
+
+/* Times `sweeps` Jacobi sweeps of the current pressure system on the fluid's
+ * stream: the launches are captured into a CUDA graph, replayed once to warm
+ * up and once between CUDA events (advances the pressure iterate twice).
+ * Reports the elapsed ms, the number of launches and the cells each sweep
+ * updates (cells of the tiles that hold fluid; the rest stay 0 untouched). */
+aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, int32_t* launches,
+                                      int64_t* cells_per_sweep);
+
+void aq_fluid_destroy(aq_fluid* f);
+
+/* Thread-local message of the last failed call ("" if none). */
+const char* aq_last_error(void);
+
+/* Library ABI version (AQ_ABI_VERSION). */
+int32_t aq_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AQUARIUS_B200_H */

@@ -1,0 +1,60 @@
+/*
+ * CPU oracle of the Aquarius 3D FLIP step — TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C (OpenMP) restatement of Fluid_3D_FLIP::Fluid::init and
+ * ::simulationStep (AmesingFlank/Aquarius, Fluid/Fluid_3D_FLIP.cu:316-594,
+ * Fluid/Fluid_3D_kernels.cu, Fluid/Fluid_3D_common.{cu,cuh},
+ * Fluid/MAC_Grid_3D.cuh, Fluid/WeightKernels.cuh:131-146).  It is the checker
+ * for the CUDA library and the timed CPU baseline; the library never links,
+ * loads or calls it.
+ *
+ * Where the reference kernels race (in-place Jacobi, in-place diffusion,
+ * in-place extrapolation, read-modify-write gravity on neighbour faces) this
+ * oracle uses the race-free reading: every sweep/pass reads the previous
+ * sweep's values.  Air-cell pressure is cleared before the first sweep.
+ *
+ * Parity is pinned against the reference's own kernels built headless
+ * (oracle/_ref, see oracle/Makefile) through fixtures under tests/golden/.
+ */
+#ifndef AQ_FLIP_ORACLE_H
+#define AQ_FLIP_ORACLE_H
+
+#include "../include/aquarius_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_fluid orc_fluid;
+
+/* Fluid::init (Fluid/Fluid_3D_FLIP.cu:435-505). NULL on invalid config. */
+orc_fluid* orc_create(const aq_config* cfg);
+void orc_destroy(orc_fluid* o);
+
+int orc_particle_count(const orc_fluid* o);
+/* One sub-stage (aq_stage numbering); returns 0 on success. */
+int orc_run_stage(orc_fluid* o, int stage);
+/* n full simulationStep()s. */
+int orc_step(orc_fluid* o, int n);
+
+/* Copies the state out / in using the canonical aq_host_state layout.
+ * Returns 0 on success, nonzero on a size mismatch. */
+int orc_get_state(const orc_fluid* o, aq_host_state* s);
+int orc_set_state(orc_fluid* o, const aq_host_state* s);
+
+/* Last pressure solve: sweeps, relative residual (FP64), ||b||, fluid cells. */
+void orc_solve_stats(const orc_fluid* o, int* iters, double* rel_res, double* b_norm, int* fluid_cells);
+
+/* Relative residual of the current pressure for the current system. */
+double orc_pressure_residual(const orc_fluid* o);
+
+/* Fills a default config (same values as aq_config_default). */
+void orc_config_default(aq_config* cfg);
+
+/* Number of OpenMP threads the oracle uses (omp_get_max_threads). */
+int orc_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

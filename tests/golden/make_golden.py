@@ -1,0 +1,202 @@
+"""Generates the golden fixtures in tests/golden/ from the reference's own
+FLIP kernels (oracle/_ref/libaqref.so, built headless by `make -C oracle ref`
+where the reference sources are present).  Needs a GPU.
+
+    python tests/golden/make_golden.py --out tests/golden
+
+For each scene it records the reference's init state and, for every stage of
+the first steps, the fields that stage writes, starting each stage from the
+reference's own state (teacher forcing).  It also records:
+  * the texture address probe: what the reference's tex3D returns for
+    out-of-range y/z coordinates (createField3D sets only addressMode[0],
+    Fluid/VolumeData.cuh:58-67);
+  * the reference's run-to-run spread per stage (its Jacobi, diffusion and
+    extrapolation kernels update in place and race).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as ct
+import json
+import pathlib
+import sys
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+from aquarius_b200 import _abi  # noqa: E402
+from oracle_binding import RefFluid, probe_texture  # noqa: E402
+from scenes import SCENES, rel_l2  # noqa: E402
+
+STAGE_FIELDS = {
+    1: ["position", "velocity_p", "fractions"],
+    2: ["position", "velocity_p", "fractions", "cell_start", "cell_end", "particle_hash", "sort_index"],
+    3: ["content", "velocity", "new_velocity", "density", "volume_fractions", "new_volume_fractions"],
+    4: ["particle_count_cell", "divergence"],
+    5: ["pressure"],
+    6: ["new_velocity", "has_velocity"],
+    7: ["new_velocity", "has_velocity"],
+    8: ["new_volume_fractions"],
+}
+
+GOLDEN_SCENES = {"cfg1_16": 2, "aniso": 1, "multi_16": 1}
+
+
+def record_scene(name: str, steps: int) -> dict:
+    cfg = SCENES[name]()
+    ref = RefFluid(cfg)
+    out = {"config": np.frombuffer(bytes(cfg), dtype=np.uint8).copy()}
+    st = ref.get_state()
+    for k, v in st.items():
+        if k != "physical_time":
+            out[f"init/{k}"] = v
+    spread = {}
+    for s in range(steps):
+        for k in range(1, 9):
+            before = ref.get_state()
+            ref.stage(k)
+            after = ref.get_state()
+            for f in STAGE_FIELDS[k]:
+                out[f"s{s}/k{k}/{f}"] = after[f]
+            # run-to-run spread: replay the stage from the same state, then
+            # continue from the first run (the one recorded above)
+            ref.set_state(before)
+            ref.stage(k)
+            again = ref.get_state(STAGE_FIELDS[k])
+            for f in STAGE_FIELDS[k]:
+                if after[f].dtype.kind == "f":
+                    spread[f"s{s}/k{k}/{f}"] = rel_l2(again[f], after[f])
+                else:
+                    spread[f"s{s}/k{k}/{f}"] = int((again[f] != after[f]).sum())
+            ref.set_state(after)
+    ref.close()
+    return out, spread
+
+
+def record_special() -> dict:
+    """Race-free settings of the reference's in-place kernels.
+
+    jacobi_converged: 3000 in-place sweeps from the state after stage 4; the
+        racy sweep order no longer matters at the fixed point, which pins the
+        operator (coefficients, rhs, walls, air).
+    jacobi_isolated: one sweep where every fluid cell is surrounded by air
+        with p = 0, so no cell reads a value written in the same sweep.
+    extrap_isolated: extrapolation where every cell lacking a component is
+        surrounded by cells that have it; those never change, so the pass
+        reads no value written in the same pass.
+    """
+    out = {}
+    rng = np.random.default_rng(7)
+    cfg = SCENES["cfg1_16"](pressure_iterations=3000)
+    ref = RefFluid(cfg)
+    for k in range(1, 5):
+        ref.stage(k)
+    st = ref.get_state()
+    out["jacobi_converged/config"] = np.frombuffer(bytes(cfg), dtype=np.uint8).copy()
+    for f, v in st.items():
+        if f != "physical_time":
+            out[f"jacobi_converged/in/{f}"] = v
+    ref.stage(5)
+    out["jacobi_converged/out/pressure"] = ref.get_state(["pressure"])["pressure"]
+    ref.close()
+
+    cfg = SCENES["cfg1_16"](pressure_iterations=1)
+    ref = RefFluid(cfg)
+    st = ref.get_state()
+    sx, sy, sz = cfg.size_x, cfg.size_y, cfg.size_z
+    x, y, z = np.meshgrid(np.arange(sx + 1), np.arange(sy + 1), np.arange(sz + 1), indexing="ij")
+    inner = (x < sx) & (y < sy) & (z < sz)
+    iso = ((x + 2 * y + 4 * z) % 8 == 3) & inner
+    content = st["content"].reshape(sx + 1, sy + 1, sz + 1).copy()
+    content[inner] = 0
+    content[iso] = 1
+    st["content"] = content.ravel().astype(np.int32)
+    st["pressure"] = np.zeros_like(st["pressure"])
+    st["divergence"] = rng.uniform(-1, 1, st["divergence"].shape).astype(np.float32)
+    st["density"] = rng.uniform(0.5, 2, st["density"].shape).astype(np.float32)
+    ref.set_state(st)
+    ref.stage(5)
+    out["jacobi_isolated/config"] = np.frombuffer(bytes(cfg), dtype=np.uint8).copy()
+    for f in ["content", "pressure", "divergence", "density"]:
+        out[f"jacobi_isolated/in/{f}"] = st[f]
+    out["jacobi_isolated/out/pressure"] = ref.get_state(["pressure"])["pressure"]
+
+    st = ref.get_state()
+    nv = rng.uniform(-2, 2, st["new_velocity"].shape).astype(np.float32)
+    has = np.ones_like(st["has_velocity"])
+    xc, yc, zc = np.meshgrid(np.arange(sx), np.arange(sy), np.arange(sz), indexing="ij")
+    # With S = x + 2y + 4z, component a lacks velocity where S = r[a] (mod 8).
+    # A neighbour along axis d sits at S +- (1, 2, 4)[d]; the residues below
+    # keep every neighbour a hole reads (its averaged component and its
+    # velocity along the neighbour direction) out of the holes, so no value
+    # read in a pass is written in that pass.
+    residue = (0, 3, 2)
+    for comp in range(3):
+        holes = ((xc + 2 * yc + 4 * zc) % 8 == residue[comp]).ravel()
+        has[comp][holes] = 0
+    st["new_velocity"] = nv
+    st["has_velocity"] = has.astype(np.int32)
+    ref.set_state(st)
+    ref.stage(7)
+    got = ref.get_state(["new_velocity", "has_velocity"])
+    out["extrap_isolated/config"] = np.frombuffer(bytes(cfg), dtype=np.uint8).copy()
+    for f in ["new_velocity", "has_velocity", "content"]:
+        out[f"extrap_isolated/in/{f}"] = st[f]
+    out["extrap_isolated/out/new_velocity"] = got["new_velocity"]
+    out["extrap_isolated/out/has_velocity"] = got["has_velocity"]
+    ref.close()
+    return out
+
+
+def texture_probe() -> dict:
+    w, h, d = 6, 5, 4
+    coords = [(2, -1, 2), (2, h, 2), (2, 2, -1), (2, 2, d), (-1, 2, 2), (w, 2, 2), (2, h - 1, 2), (2, 0, 2),
+              (2, 2, d - 1), (2, 2, 0), (0, 2, 2), (w - 1, 2, 2)]
+    vals = probe_texture(w, h, d, coords)
+    field = lambda x, y, z: float(x + 100 * y + 10000 * z)
+    res = {"extent": [w, h, d], "reads": [[list(c), float(v)] for c, v in zip(coords, vals)]}
+
+    def mode(v, clamp, wrap):
+        if v == clamp:
+            return "clamp"
+        if v == wrap:
+            return "wrap"
+        if v == 0.0:
+            return "border"
+        return f"other({v})"
+    res["y_low"] = mode(vals[0], field(2, 0, 2), field(2, h - 1, 2))
+    res["y_high"] = mode(vals[1], field(2, h - 1, 2), field(2, 0, 2))
+    res["z_low"] = mode(vals[2], field(2, 2, 0), field(2, 2, d - 1))
+    res["z_high"] = mode(vals[3], field(2, 2, d - 1), field(2, 2, 0))
+    res["x_low"] = mode(vals[4], field(0, 2, 2), field(w - 1, 2, 2))
+    res["x_high"] = mode(vals[5], field(w - 1, 2, 2), field(0, 2, 2))
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=str(HERE))
+    a = ap.parse_args()
+    out = pathlib.Path(a.out)
+    out.mkdir(parents=True, exist_ok=True)
+    probe = texture_probe()
+    (out / "texture_probe.json").write_text(json.dumps(probe, indent=1))
+    print("texture probe:", {k: v for k, v in probe.items() if k != "reads"})
+    spreads = {}
+    for name, steps in GOLDEN_SCENES.items():
+        data, spread = record_scene(name, steps)
+        np.savez_compressed(out / f"ref_{name}.npz", **data)
+        spreads[name] = spread
+        print(name, "recorded", len(data), "arrays; max float spread",
+              max([v for k, v in spread.items() if isinstance(v, float)] + [0.0]))
+    (out / "reference_spread.json").write_text(json.dumps(spreads, indent=1, sort_keys=True))
+    np.savez_compressed(out / "ref_special.npz", **record_special())
+    print("special fixtures recorded")
+
+
+if __name__ == "__main__":
+    main()

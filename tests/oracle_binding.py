@@ -1,0 +1,207 @@
+"""ctypes bindings of the two checkers, for tests only.
+
+* ``Oracle``: the CPU restatement, oracle/liborc.so (flip_oracle.c).
+* ``RefFluid``: the reference's own kernels built headless, oracle/_ref/libaqref.so
+  (needs a GPU; present only where oracle/Makefile's ``ref`` target was built).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+from aquarius_b200 import _abi
+
+ROOT = pathlib.Path(__file__).resolve().parent.parent
+ORACLE_SO = ROOT / "oracle" / "liborc.so"
+REF_SO = ROOT / "oracle" / "_ref" / "libaqref.so"
+
+_orc = None
+_ref = None
+
+
+def _load_oracle():
+    global _orc
+    if _orc is None:
+        if not ORACLE_SO.exists():
+            subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
+        lib = ct.CDLL(str(ORACLE_SO))
+        lib.orc_create.restype = ct.c_void_p
+        lib.orc_create.argtypes = [ct.POINTER(_abi.Config)]
+        lib.orc_destroy.argtypes = [ct.c_void_p]
+        lib.orc_particle_count.restype = ct.c_int
+        lib.orc_particle_count.argtypes = [ct.c_void_p]
+        lib.orc_run_stage.restype = ct.c_int
+        lib.orc_run_stage.argtypes = [ct.c_void_p, ct.c_int]
+        lib.orc_step.restype = ct.c_int
+        lib.orc_step.argtypes = [ct.c_void_p, ct.c_int]
+        lib.orc_get_state.restype = ct.c_int
+        lib.orc_get_state.argtypes = [ct.c_void_p, ct.POINTER(_abi.HostState)]
+        lib.orc_set_state.restype = ct.c_int
+        lib.orc_set_state.argtypes = [ct.c_void_p, ct.POINTER(_abi.HostState)]
+        lib.orc_solve_stats.argtypes = [ct.c_void_p, ct.POINTER(ct.c_int), ct.POINTER(ct.c_double),
+                                        ct.POINTER(ct.c_double), ct.POINTER(ct.c_int)]
+        lib.orc_pressure_residual.restype = ct.c_double
+        lib.orc_pressure_residual.argtypes = [ct.c_void_p]
+        lib.orc_threads.restype = ct.c_int
+        _orc = lib
+    return _orc
+
+
+def _load_ref():
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(str(REF_SO))
+        lib = ct.CDLL(str(REF_SO))
+        lib.aqref_create.restype = ct.c_void_p
+        lib.aqref_create.argtypes = [ct.POINTER(_abi.Config)]
+        lib.aqref_destroy.argtypes = [ct.c_void_p]
+        lib.aqref_particle_count.restype = ct.c_int
+        lib.aqref_particle_count.argtypes = [ct.c_void_p]
+        lib.aqref_step.restype = ct.c_int
+        lib.aqref_step.argtypes = [ct.c_void_p, ct.c_int]
+        lib.aqref_stage.restype = ct.c_int
+        lib.aqref_stage.argtypes = [ct.c_void_p, ct.c_int]
+        lib.aqref_get_state.restype = ct.c_int
+        lib.aqref_get_state.argtypes = [ct.c_void_p, ct.POINTER(_abi.HostState)]
+        lib.aqref_set_state.restype = ct.c_int
+        lib.aqref_set_state.argtypes = [ct.c_void_p, ct.POINTER(_abi.HostState)]
+        lib.aqref_probe_texture.restype = ct.c_int
+        lib.aqref_probe_texture.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int]
+        lib.aqref_error.restype = ct.c_int
+        _ref = lib
+    return _ref
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+class _StateIO:
+    """get_state/set_state over numpy dicts, shared by both checkers."""
+
+    size: tuple
+    n: int
+
+    def get_state(self, fields=None) -> dict:
+        sx, sy, sz = self.size
+        arrs = _abi.alloc_state(sx, sy, sz, self.n, fields)
+        st = _abi.make_host_state(sx, sy, sz, self.n, arrs)
+        rc = self._get(ct.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"get_state failed: {rc}")
+        arrs["physical_time"] = st.physical_time
+        return arrs
+
+    def set_state(self, state: dict):
+        sx, sy, sz = self.size
+        arrs = {k: np.ascontiguousarray(v) for k, v in state.items() if k in _abi.STATE_FIELDS}
+        st = _abi.make_host_state(sx, sy, sz, self.n, arrs, float(state.get("physical_time", 0.0)))
+        rc = self._set(ct.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"set_state failed: {rc}")
+
+
+class Oracle(_StateIO):
+    """CPU restatement of the reference step (test infrastructure)."""
+
+    def __init__(self, cfg: _abi.Config):
+        self.lib = _load_oracle()
+        self.cfg = cfg
+        self.h = self.lib.orc_create(ct.byref(cfg))
+        if not self.h:
+            raise ValueError("oracle rejected the config")
+        self.size = (cfg.size_x, cfg.size_y, cfg.size_z)
+        self.n = self.lib.orc_particle_count(self.h)
+
+    def _get(self, p):
+        return self.lib.orc_get_state(self.h, p)
+
+    def _set(self, p):
+        return self.lib.orc_set_state(self.h, p)
+
+    def stage(self, k: int):
+        if self.lib.orc_run_stage(self.h, k) != 0:
+            raise RuntimeError("bad stage")
+
+    def step(self, n: int = 1):
+        if self.lib.orc_step(self.h, n) != 0:
+            raise RuntimeError("step failed")
+
+    def solve_stats(self):
+        it, nf = ct.c_int(), ct.c_int()
+        rr, bn = ct.c_double(), ct.c_double()
+        self.lib.orc_solve_stats(self.h, ct.byref(it), ct.byref(rr), ct.byref(bn), ct.byref(nf))
+        return {"iterations": it.value, "rel_residual": rr.value, "b_norm": bn.value, "fluid_cells": nf.value}
+
+    def pressure_residual(self) -> float:
+        return self.lib.orc_pressure_residual(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RefFluid(_StateIO):
+    """The reference's Fluid_3D_FLIP::Fluid on the GPU (test infrastructure)."""
+
+    def __init__(self, cfg: _abi.Config):
+        self.lib = _load_ref()
+        self.h = self.lib.aqref_create(ct.byref(cfg))
+        if not self.h:
+            raise RuntimeError(f"reference init failed: cuda error {self.lib.aqref_error()}")
+        self.size = (cfg.size_x, cfg.size_y, cfg.size_z)
+        self.n = self.lib.aqref_particle_count(self.h)
+
+    def _get(self, p):
+        return self.lib.aqref_get_state(self.h, p)
+
+    def _set(self, p):
+        return self.lib.aqref_set_state(self.h, p)
+
+    def stage(self, k: int):
+        rc = self.lib.aqref_stage(self.h, k)
+        if rc != 0:
+            raise RuntimeError(f"reference stage {k} failed: {rc}")
+
+    def step(self, n: int = 1):
+        rc = self.lib.aqref_step(self.h, n)
+        if rc != 0:
+            raise RuntimeError(f"reference step failed: {rc}")
+
+    def close(self):
+        if self.h:
+            self.lib.aqref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def probe_texture(w, h, d, coords) -> np.ndarray:
+    """Reads the reference's createField3D<float> texture at coords ([k,3])."""
+    lib = _load_ref()
+    c = np.ascontiguousarray(np.asarray(coords, dtype=np.float32))
+    out = np.zeros(len(c), dtype=np.float32)
+    rc = lib.aqref_probe_texture(w, h, d, c.ctypes.data, out.ctypes.data, len(c))
+    if rc != 0:
+        raise RuntimeError(f"probe failed {rc}")
+    return out
+
+
+def oracle_threads() -> int:
+    return _load_oracle().orc_threads()
