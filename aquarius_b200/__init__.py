@@ -68,6 +68,7 @@ def load_library() -> ct.CDLL:
         "aq_fluid_step": (ct.c_int, [P, ct.c_int32]),
         "aq_fluid_step_host": (ct.c_int, [P, ct.c_int32, P, P, P, P]),
         "aq_fluid_run_stage": (ct.c_int, [P, ct.c_int32]),
+        "aq_fluid_set_graph_mode": (ct.c_int, [P, ct.c_int32]),
         "aq_fluid_synchronize": (ct.c_int, [P]),
         "aq_fluid_time": (ct.c_int, [P, ct.POINTER(ct.c_double)]),
         "aq_fluid_particle_count": (ct.c_int, [P, ct.POINTER(ct.c_int32)]),
@@ -241,6 +242,10 @@ class Fluid:
             return None if a is None else a.ctypes.data
         _check(self._lib.aq_fluid_step_host(self._h, n, ptr(position_in), ptr(velocity_in), ptr(position_out),
                                             ptr(velocity_out)))
+
+    def set_graph_mode(self, use_graph: bool):
+        """True (default): one CUDA-graph launch per step; False: kernel by kernel."""
+        _check(self._lib.aq_fluid_set_graph_mode(self._h, 1 if use_graph else 0))
 
     def run_stage(self, stage):
         k = STAGES[stage] if isinstance(stage, str) else int(stage)

@@ -184,6 +184,7 @@ struct aq_fluid {
 
   JacobiPlan plan{4, 16, 32};
   cudaGraphExec_t exec = nullptr;
+  bool use_graph = true;
   int graph_launches = 0;  // launches outside the residual loop
   int body_launches = 0;   // launches per residual-loop iteration
 
@@ -575,6 +576,17 @@ aq_status aq_fluid::build_graph() {
 }
 
 aq_status aq_fluid::step(int nsteps) {
+  if (!use_graph) {
+    for (int i = 0; i < nsteps; ++i) {
+      AQ_TRY(enq_pre_solve());
+      if (cfg.solve_mode == AQ_SOLVE_RESIDUAL) AQ_TRY(enq_solve_residual_eager());
+      else AQ_TRY(enq_solve_fixed(cfg.pressure_iterations));
+      AQ_TRY(enq_post_solve());
+      time += (double)cfg.timestep;
+    }
+    nv_cur = has_cur = 2;
+    return AQ_OK;
+  }
   if (!exec) AQ_TRY(build_graph());
   for (int i = 0; i < nsteps; ++i) {
     AQ_CUDA(cudaGraphLaunch(exec, stream));
@@ -1103,6 +1115,12 @@ aq_status aq_fluid_step_host(aq_fluid* f, int32_t n_steps, const float* pin, con
     }
   }
   AQ_CUDA(cudaStreamSynchronize(s));
+  return AQ_OK;
+}
+
+aq_status aq_fluid_set_graph_mode(aq_fluid* f, int32_t use_graph) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  f->use_graph = use_graph != 0;
   return AQ_OK;
 }
 

@@ -194,6 +194,12 @@ aq_status aq_fluid_step_host(aq_fluid* f, int32_t n_steps,
                              const float* position_in, const float* velocity_in,
                              float* position_out, float* velocity_out);
 
+/* use_graph = 1 (default): a step is one CUDA-graph launch.  0: the step's
+ * kernels are launched one by one (RESIDUAL mode then reads the residual on
+ * the host after each check block); same kernels, same results, used to
+ * profile individual launches. */
+aq_status aq_fluid_set_graph_mode(aq_fluid* f, int32_t use_graph);
+
 /* Runs one sub-stage (aq_stage) of a step; used to compare stages in
  * isolation.  AQ_STAGE_DIFFUSE also advances physical time, as the last
  * statement of simulationStep does. */
@@ -248,6 +254,7 @@ aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, in
                                       int64_t* cells_per_sweep);
 
 void aq_fluid_destroy(aq_fluid* f);
+
 
 /* Thread-local message of the last failed call ("" if none). */
 const char* aq_last_error(void);
