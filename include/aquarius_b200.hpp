@@ -1,0 +1,186 @@
+// Header-only C++ wrapper over the C ABI (aquarius_b200.h) that mirrors the
+// reference's plugin surface, so code written against
+// Fluid_3D_FLIP::Fluid / FluidConfig (AmesingFlank/Aquarius) changes only its
+// include and namespace:
+//
+//   reference                                      here
+//   ShapeType, InitializationVolume, ConfigFLIP,    aquarius_b200::ShapeType, ...
+//   FluidConfig  (Fluid/FluidConfig.cuh:16-97)       (same members, same defaults)
+//   Fluid_3D_FLIP::Fluid::init(FluidConfig)          aquarius_b200::Fluid_3D_FLIP::Fluid::init
+//   ::simulationStep(), ::physicalTime,              same names
+//   ::getCenter(), ::getContainerSize()
+//     (Fluid/Fluid.h:4-12, Fluid/Fluid_3D.cuh:7-12)
+//
+// Differences: errors throw aquarius_b200::Error (the reference prints and
+// exits); draw() is a no-op (rendering is not part of this library); the
+// centre is returned as std::array<float,3> instead of glm::vec3.
+#pragma once
+
+#include <array>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "aquarius_b200.h"
+
+namespace aquarius_b200 {
+
+struct Error : std::runtime_error {
+  aq_status status;
+  Error(aq_status st, const std::string& what) : std::runtime_error(what), status(st) {}
+};
+
+inline void check(aq_status st, const char* call) {
+  if (st != AQ_OK) throw Error(st, std::string(call) + ": " + aq_last_error());
+}
+
+struct float3_ {
+  float x, y, z;
+};
+
+enum class ShapeType { Sphere, Square };  // Fluid/FluidConfig.cuh:16-18
+
+struct InitializationVolume {  // Fluid/FluidConfig.cuh:20-38
+  ShapeType shapeType = ShapeType::Square;
+  float3_ boxMin{0, 0, 0};
+  float3_ boxMax{1, 0.1875f, 1};
+  float3_ ballCenter{0.5f, 0.75f, 0.5f};
+  float ballRadius = 0.125f;
+  int phase = 0;
+  InitializationVolume() = default;
+  explicit InitializationVolume(ShapeType type) : shapeType(type) {}
+};
+
+struct ConfigFLIP {  // Fluid/FluidConfig.cuh:41-50
+  int sizeX = 50;
+  int sizeY = 50;
+  int sizeZ = 50;
+  int pressureIterations = 100;
+  int diffusionIterations = 100;
+  float timestep = 0.033f;
+  float FLIPcoeff = 0.95f;
+  float particleJitter = 0.05f;
+};
+
+struct FluidConfig {  // Fluid/FluidConfig.cuh:68-97
+  std::string method = "FLIP";
+  std::vector<InitializationVolume> initialVolumes;
+  float3_ gravity{0, -9.8f, 0};
+  int phaseCount = 2;
+  std::array<float, 4> phaseDensities{1, 1, 1, 1};
+  float diffusionCoeff = 0.001f;
+  ConfigFLIP FLIP;
+  // Extensions (no reference counterpart); defaults reproduce the reference.
+  float gridPhysicalSize = 10.f;
+  unsigned seed = 1;
+  aq_pressure_init pressureInit = AQ_PRESSURE_CARRY;
+  aq_solve_mode solveMode = AQ_SOLVE_FIXED;
+  float relResidual = 1e-4f;
+  int maxIterations = 2000;
+  int checkInterval = 40;
+  int device = 0;
+  void* stream = nullptr;
+
+  FluidConfig() {
+    initialVolumes.emplace_back(ShapeType::Square);
+    initialVolumes.emplace_back(ShapeType::Sphere);
+  }
+
+  aq_config to_c() const {
+    if (method != "FLIP") throw Error(AQ_ERR_INVALID_CONFIG, "only the FLIP method is implemented");
+    if (initialVolumes.size() > AQ_MAX_VOLUMES) throw Error(AQ_ERR_INVALID_CONFIG, "too many volumes");
+    aq_config c;
+    check(aq_config_default(&c), "aq_config_default");
+    c.volume_count = (int32_t)initialVolumes.size();
+    for (size_t i = 0; i < initialVolumes.size(); ++i) {
+      const InitializationVolume& v = initialVolumes[i];
+      aq_volume& o = c.volumes[i];
+      o.shape = v.shapeType == ShapeType::Sphere ? AQ_SHAPE_SPHERE : AQ_SHAPE_SQUARE;
+      o.box_min[0] = v.boxMin.x; o.box_min[1] = v.boxMin.y; o.box_min[2] = v.boxMin.z;
+      o.box_max[0] = v.boxMax.x; o.box_max[1] = v.boxMax.y; o.box_max[2] = v.boxMax.z;
+      o.ball_center[0] = v.ballCenter.x; o.ball_center[1] = v.ballCenter.y; o.ball_center[2] = v.ballCenter.z;
+      o.ball_radius = v.ballRadius;
+      o.phase = v.phase;
+    }
+    c.gravity[0] = gravity.x; c.gravity[1] = gravity.y; c.gravity[2] = gravity.z;
+    c.phase_count = phaseCount;
+    for (int k = 0; k < 4; ++k) c.phase_densities[k] = phaseDensities[k];
+    c.diffusion_coeff = diffusionCoeff;
+    c.size_x = FLIP.sizeX; c.size_y = FLIP.sizeY; c.size_z = FLIP.sizeZ;
+    c.pressure_iterations = FLIP.pressureIterations;
+    c.diffusion_iterations = FLIP.diffusionIterations;
+    c.timestep = FLIP.timestep;
+    c.flip_coeff = FLIP.FLIPcoeff;
+    c.particle_jitter = FLIP.particleJitter;
+    c.domain_size = gridPhysicalSize;
+    c.seed = seed;
+    c.pressure_init = pressureInit;
+    c.solve_mode = solveMode;
+    c.rel_residual = relResidual;
+    c.max_iterations = maxIterations;
+    c.check_interval = checkInterval;
+    c.device = device;
+    c.stream = stream;
+    return c;
+  }
+};
+
+namespace Fluid_3D_FLIP {
+
+class Fluid {
+ public:
+  Fluid() = default;
+  explicit Fluid(const FluidConfig& config) { init(config); }
+  Fluid(const Fluid&) = delete;
+  Fluid& operator=(const Fluid&) = delete;
+  ~Fluid() { release(); }
+
+  // Fluid::init (Fluid/Fluid_3D_FLIP.cu:435-505)
+  void init(const FluidConfig& config) {
+    release();
+    const aq_config c = config.to_c();
+    check(aq_fluid_create(&c, &f_), "aq_fluid_create");
+    config_ = config;
+    physicalTime = 0;
+  }
+  // Fluid::simulationStep (Fluid/Fluid_3D_FLIP.cu:316-352); asynchronous
+  void simulationStep() {
+    check(aq_fluid_step(f_, 1), "aq_fluid_step");
+    double t = 0;
+    check(aq_fluid_time(f_, &t), "aq_fluid_time");
+    physicalTime = (float)t;
+  }
+  template <typename DrawCommand>
+  void draw(const DrawCommand&) {}  // headless
+  std::array<float, 3> getCenter() const {
+    std::array<float, 3> c{};
+    check(aq_fluid_container(f_, c.data(), nullptr), "aq_fluid_container");
+    return c;
+  }
+  float getContainerSize() const {
+    float s = 0;
+    check(aq_fluid_container(f_, nullptr, &s), "aq_fluid_container");
+    return s;
+  }
+  int particleCount() const {
+    int32_t n = 0;
+    check(aq_fluid_particle_count(f_, &n), "aq_fluid_particle_count");
+    return n;
+  }
+  void synchronize() { check(aq_fluid_synchronize(f_), "aq_fluid_synchronize"); }
+  aq_fluid* handle() const { return f_; }
+  const FluidConfig& config() const { return config_; }
+
+  float physicalTime = 0;  // Fluid/Fluid.h:10
+
+ private:
+  void release() {
+    if (f_) aq_fluid_destroy(f_);
+    f_ = nullptr;
+  }
+  aq_fluid* f_ = nullptr;
+  FluidConfig config_;
+};
+
+}  // namespace Fluid_3D_FLIP
+}  // namespace aquarius_b200
