@@ -2,9 +2,15 @@
 // of its launch; all work is enqueued on `st`.
 #pragma once
 
+#include <string>
+
+#include "../../include/aquarius_b200.h"
 #include "aq_common.cuh"
 
 namespace aqb {
+
+// Records the message aq_last_error() returns on this thread; returns st.
+aq_status set_last_error(aq_status st, const std::string& msg);
 
 // ---- particles (k_particles.cu) -------------------------------------------
 // Stage (d)+(a) front half: grid-to-particle FLIP/PIC blend and RK3 advection

@@ -145,6 +145,11 @@ struct Seeder {
 
 }  // namespace
 
+aq_status aqb::set_last_error(aq_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+
 // =================================================================== fluid
 struct aq_fluid {
   aq_config cfg{};

@@ -255,6 +255,30 @@ aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, in
 
 void aq_fluid_destroy(aq_fluid* f);
 
+/* Largest grid (sx*sy*sz cells) aq_jacobi_sweeps_noalloc accepts. */
+#define AQ_NOALLOC_MAX_CELLS (64 * 64 * 64)
+
+/* Pressure Jacobi sweeps on caller-owned device buffers that allocate
+ * nothing.  No counterpart in the reference: it is for callers that cannot
+ * allocate device memory while they run the solver (a fixed memory pool
+ * handed over by a host application, a memory-budgeted frame loop, a plugin
+ * that must not touch its host process's allocator).
+ *
+ * cell_type [C] (0 air, 1 fluid), rhs [C] (-divergence*density on fluid
+ * cells) and pressure [C] (initial guess in, result out) are device buffers
+ * in the cell layout of aq_host_state; `sweeps` Jacobi sweeps are run on
+ * `stream` (NULL = the legacy default stream) exactly as the pressure stage
+ * of aq_fluid_step does in AQ_SOLVE_FIXED mode, including clearing air
+ * pressure first.  The second Jacobi buffer and the activity flags are a
+ * fixed device array of AQ_NOALLOC_MAX_CELLS floats that every GPU loading
+ * this library holds until exit; larger grids return AQ_ERR_INVALID_ARGUMENT.
+ * The first call on a device looks the array up (cudaGetSymbolAddress) and
+ * must come before any stream capture.  All calls on a device share the
+ * array, so calls that overlap on the GPU race: serialise them. */
+aq_status aq_jacobi_sweeps_noalloc(int32_t sx, int32_t sy, int32_t sz, const int8_t* cell_type,
+                                   const float* rhs, float* pressure, int32_t sweeps, void* stream);
+/* AQ_NOALLOC_MAX_CELLS, as compiled into the library. */
+int32_t aq_jacobi_noalloc_max_cells(void);
 
 /* Thread-local message of the last failed call ("" if none). */
 const char* aq_last_error(void);
