@@ -18,6 +18,7 @@ STATUS_NAMES = {
     5: "AQ_ERR_NOT_CONVERGED",
     6: "AQ_ERR_NONFINITE",
     7: "AQ_ERR_NO_DEVICE",
+    8: "AQ_ERR_TIMEOUT",
 }
 
 SHAPE_SPHERE = 0

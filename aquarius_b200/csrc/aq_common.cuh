@@ -80,7 +80,7 @@ struct SolveState {
   double b2;            // ||b||^2 over fluid cells
   double r2;            // ||b - A p||^2 of the returned iterate
   int fluid_cells;
-  int pad;
+  int sync_timeout;  // the persistent solve gave up waiting at a grid barrier
   long long total_sweeps;  // cumulative over the fluid's life
   long long total_bodies;
 };

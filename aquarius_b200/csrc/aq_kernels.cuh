@@ -65,9 +65,24 @@ cudaError_t launch_diffuse(cudaStream_t st, const Dims& d, const int8_t* type, f
 // ---- pressure (k_jacobi.cu) -------------------------------------------------
 struct JacobiPlan {
   int levels;      // sweeps per launch (1,2,4,8)
-  int by;          // tile rows (y threads)
+  int by;          // tile rows (y threads); 0 = flat kernel; 1 = persistent solve
   int xc;          // x planes per CTA
 };
+
+// ---- persistent solve (k_jacobi.cu) ------------------------------------------
+// The whole pressure solve in one cooperative launch: every CTA sweeps its
+// share of a compact list of active flat work items (1 x plane x 8 rows x 128
+// z cells), a bounded grid barrier separates sweeps, and the residual check
+// and stop decision are made identically by every CTA.
+int persist_items(const Dims& d);
+int persist_ctas(int device);  // co-resident CTAs of the cooperative launch
+// Builds the ordered list of active items and clears the barrier counter.
+cudaError_t launch_items_compact(cudaStream_t st, const Dims& d, const uint8_t* brick_active, int* items,
+                                 int* n_items, unsigned int* bar);
+// fixed_sweeps > 0: that many sweeps then one residual; else residual mode.
+cudaError_t launch_persist_solve(cudaStream_t st, const Dims& d, int ctas, float* pa, float* pb, const float* rhs,
+                                 const int8_t* type, const int* items, const int* n_items, unsigned int* bar,
+                                 double* part, SolveState* ss, int fixed_sweeps, int check, int max_iters, double tol);
 // Temporally blocked Jacobi: `levels` sweeps from pin to pout; with resid it
 // also writes per-CTA FP64 partial sums of ||b - A p_out||^2 to part.
 cudaError_t launch_jacobi(cudaStream_t st, const Dims& d, const JacobiPlan& plan, bool resid,
@@ -78,6 +93,10 @@ int jacobi_parts(const Dims& d, const JacobiPlan& plan, bool resid);
 long long jacobi_cells_updated(const Dims& d, const JacobiPlan& plan, const uint8_t* bact_host);
 // Sets the dynamic shared-memory limits of every Jacobi variant (call before capture).
 cudaError_t jacobi_prepare();
+// FP64 ||b - A p||^2 partial sums of one iterate (flat layout; sz % 4 == 0).
+cudaError_t launch_resid_flat(cudaStream_t st, const Dims& d, const float* p, const float* rhs, const int8_t* type,
+                              const uint8_t* brick_active, double* part);
+int resid_flat_parts(const Dims& d);
 // Sums residual partials; updates ss; in a conditional loop body it also
 // sets the loop's condition (continue while not converged and under cap).
 cudaError_t launch_resid_finalize(cudaStream_t st, const double* part, int nparts, SolveState* ss,

@@ -186,6 +186,12 @@ struct aq_fluid {
   int jpart_cap = 0;
   SolveState* ss = nullptr;
   SolveState* ss_host = nullptr;
+  // persistent solve
+  int* items = nullptr;
+  int* n_items = nullptr;
+  unsigned int* bar = nullptr;
+  double* ppart = nullptr;
+  int ctas = 0;
 
   JacobiPlan plan{4, 16, 32};
   cudaGraphExec_t exec = nullptr;
@@ -291,11 +297,18 @@ aq_status aq_fluid::allocate() {
   AQ_TRY(alloc(&jpart, (size_t)jpart_cap));
   AQ_TRY(alloc(&ss, 1));
   AQ_CUDA(cudaMallocHost(&ss_host, sizeof(SolveState)));
+  if (d.sz % 4 == 0) {
+    ctas = persist_ctas(device);
+    AQ_TRY(alloc(&items, (size_t)persist_items(d)));
+    AQ_TRY(alloc(&n_items, 1));
+    AQ_TRY(alloc(&bar, 1));
+    AQ_TRY(alloc(&ppart, (size_t)std::max(ctas, 1)));
+  }
   // default Jacobi plan: one vectorised sweep per launch where z allows it,
   // otherwise the tiled kernel with two sweeps per launch
   plan = d.sz % 4 == 0 ? JacobiPlan{1, 0, 1} : JacobiPlan{2, 16, 16};
-  if (jacobi_parts(d, JacobiPlan{1, 16, 16}, true) > jpart_cap) {
-    jpart_cap = jacobi_parts(d, JacobiPlan{1, 16, 16}, true);
+  if (d.sz % 4 == 0 && resid_flat_parts(d) > jpart_cap) {
+    jpart_cap = resid_flat_parts(d);
     AQ_TRY(alloc(&jpart, (size_t)jpart_cap));
   }
   memset(ss_host, 0, sizeof(SolveState));
@@ -344,29 +357,29 @@ static std::vector<int> split_sweeps(int sweeps, int levels) {
 
 int aq_fluid::count_jacobi_launches(int sweeps) const {
   const int k = (int)split_sweeps(sweeps, plan.levels).size();
-  return k + (k % 2) + 1;  // launches, parity copy, finalize
+  return k + (k % 2) + 1 + (plan.by == 0 ? 1 : 0);  // sweeps, parity copy, finalize, flat residual pass
 }
 
 // `sweeps` Jacobi sweeps from pa; the last launch also writes the residual
 // partials of its output; the result ends in pa.
-static JacobiPlan resid_plan(const JacobiPlan& p, int levels) {
-  JacobiPlan q = p;
-  q.levels = levels;
-  if (q.by == 0) q = JacobiPlan{1, 16, 16};  // flat sweeps end with a tiled residual sweep
-  return q;
-}
-
-static aq_status enqueue_sweeps(aq_fluid* f, int sweeps) {
+// `sweeps` Jacobi sweeps from pa; the FP64 residual partials of the final
+// iterate are written to jpart; the result ends in pa.  Tiled plans fuse the
+// residual into their last launch (one extra level); the flat plan computes
+// it with one residual pass over the final iterate.
+static aq_status enqueue_sweeps(aq_fluid* f, int sweeps, bool with_residual = true) {
   const std::vector<int> parts = split_sweeps(sweeps, f->plan.levels);
+  const bool flat = f->plan.by == 0;
   float* bufs[2] = {f->pa, f->pb};
   for (size_t k = 0; k < parts.size(); ++k) {
     const bool last = k + 1 == parts.size();
-    JacobiPlan p = last ? resid_plan(f->plan, parts[k]) : f->plan;
+    JacobiPlan p = f->plan;
     p.levels = parts[k];
     int np = 0;
-    AQ_CUDA(launch_jacobi(f->stream, f->d, p, last, bufs[k % 2], bufs[(k + 1) % 2], f->rhs, f->type, f->bact,
-                          f->jpart, &np));
+    AQ_CUDA(launch_jacobi(f->stream, f->d, p, last && with_residual && !flat, bufs[k % 2], bufs[(k + 1) % 2],
+                          f->rhs, f->type, f->bact, f->jpart, &np));
   }
+  if (flat && with_residual && !parts.empty())
+    AQ_CUDA(launch_resid_flat(f->stream, f->d, bufs[parts.size() % 2], f->rhs, f->type, f->bact, f->jpart));
   if (parts.size() % 2 == 1) {
     k_copy_f<<<(f->d.C + 255) / 256, 256, 0, f->stream>>>(f->pb, f->pa, f->d.C);
     AQ_CUDA(cudaGetLastError());
@@ -377,11 +390,24 @@ static aq_status enqueue_sweeps(aq_fluid* f, int sweeps) {
 static int last_parts(const aq_fluid* f, int sweeps) {
   const std::vector<int> parts = split_sweeps(sweeps, f->plan.levels);
   if (parts.empty()) return 0;
-  return jacobi_parts(f->d, resid_plan(f->plan, parts.back()), true);
+  if (f->plan.by == 0) return resid_flat_parts(f->d);
+  JacobiPlan p = f->plan;
+  p.levels = parts.back();
+  return jacobi_parts(f->d, p, true);
+}
+
+// The whole solve as one cooperative launch (plan.by == 1).
+static aq_status enqueue_persistent(aq_fluid* f, int fixed_sweeps) {
+  AQ_CUDA(launch_items_compact(f->stream, f->d, f->bact, f->items, f->n_items, f->bar));
+  AQ_CUDA(launch_persist_solve(f->stream, f->d, f->ctas, f->pa, f->pb, f->rhs, f->type, f->items, f->n_items, f->bar,
+                               f->ppart, f->ss, fixed_sweeps, f->cfg.check_interval, f->cfg.max_iterations,
+                               (double)f->cfg.rel_residual));
+  return AQ_OK;
 }
 
 aq_status aq_fluid::enq_solve_fixed(int sweeps) {
   if (sweeps <= 0) return AQ_OK;
+  if (plan.by == 1) return enqueue_persistent(this, sweeps);
   AQ_TRY(enqueue_sweeps(this, sweeps));
   AQ_CUDA(launch_resid_finalize(stream, jpart, last_parts(this, sweeps), ss, sweeps, 0.0, 0, false, 0));
   return AQ_OK;
@@ -398,6 +424,7 @@ aq_status aq_fluid::enq_solve_body(bool set_cond, unsigned long long handle, int
 
 // Residual mode without a graph: the host reads the solve state after each block.
 aq_status aq_fluid::enq_solve_residual_eager() {
+  if (plan.by == 1) return enqueue_persistent(this, 0);
   for (int guard = 0; guard < 1000000; ++guard) {
     AQ_TRY(enq_solve_body(false, 0, nullptr));
     AQ_CUDA(cudaMemcpyAsync(ss_host, ss, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
@@ -535,7 +562,17 @@ aq_status aq_fluid::build_graph() {
   };
   aq_status st = AQ_OK;
   launches += (n > 0 ? 6 : 3) + 2 + 2;  // particles (+3 scan kernels), p2g, slayer, divergence, b2
-  if (cfg.solve_mode == AQ_SOLVE_RESIDUAL) {
+  if (cfg.solve_mode == AQ_SOLVE_RESIDUAL && plan.by == 1) {
+    st = capture(g, nullptr, 0, [&]() {
+      aq_status s2 = enq_pre_solve();
+      if (s2 != AQ_OK) return s2;
+      s2 = enqueue_persistent(this, 0);
+      if (s2 != AQ_OK) return s2;
+      return enq_post_solve();
+    });
+    launches += 2;
+    body_launches = 0;
+  } else if (cfg.solve_mode == AQ_SOLVE_RESIDUAL) {
     st = capture(g, nullptr, 0, [&]() { return enq_pre_solve(); });
     if (st != AQ_OK) { cudaGraphDestroy(g); return st; }
     std::vector<cudaGraphNode_t> leaves;
@@ -1192,6 +1229,7 @@ aq_status aq_fluid_solve_stats(const aq_fluid* f, aq_solve_stats* st) {
   st->b_norm = s.b2 >= 0 ? sqrt(s.b2) : -1.0;
   st->fluid_cells = s.fluid_cells;
   st->converged = s.converged;
+  if (s.sync_timeout) return fail(AQ_ERR_TIMEOUT, "persistent pressure solve timed out at a grid barrier");
   st->blocks = s.bodies;
   st->total_sweeps = s.total_sweeps;
   st->total_blocks = s.total_bodies;
@@ -1213,26 +1251,43 @@ aq_status aq_fluid_launches_per_step(const aq_fluid* f, int32_t* launches) {
 
 aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, int32_t x_planes) {
   if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  if (rows == 1) {  // persistent cooperative solve
+    if (levels != 1 || f->d.sz % 4 != 0 || f->ctas <= 0)
+      return fail(AQ_ERR_INVALID_ARGUMENT, "persistent solve needs sz % 4 == 0");
+    cudaSetDevice(f->device);
+    AQ_CUDA(cudaStreamSynchronize(f->stream));
+    f->plan = JacobiPlan{1, 1, 1};
+    f->invalidate_graph();
+    return AQ_OK;
+  }
   const bool flat = rows == 0;
-  if (flat ? (levels != 1 || f->d.sz % 4 != 0)
+  if (flat ? (levels != 1 || f->d.sz % 4 != 0 || !(x_planes == 1 || x_planes == 2 || x_planes == 4 || x_planes == 8))
            : (!(levels == 1 || levels == 2 || levels == 4 || levels == 8) || !(rows == 8 || rows == 16 || rows == 32) ||
               x_planes < 1))
     return fail(AQ_ERR_INVALID_ARGUMENT, "unsupported Jacobi plan");
-  JacobiPlan p{levels, rows, flat ? 1 : x_planes};
-  // every level count the sweeps split into must fit the tile with its halo,
-  // including the residual variant (one more level)
-  for (int l = levels; l >= 1; l >>= 1) {
-    const JacobiPlan q = resid_plan(p, l);
-    JacobiPlan q2 = p;
-    q2.levels = l;
-    if (jacobi_parts(f->d, q, true) <= 0 || jacobi_parts(f->d, q2, false) <= 0)
-      return fail(AQ_ERR_INVALID_ARGUMENT, "tile too small for the plan's halo");
+  JacobiPlan p{levels, rows, x_planes};
+  if (!flat) {
+    // every level count the sweeps split into must fit the tile with its
+    // halo, including the residual variant (one more level)
+    for (int l = levels; l >= 1; l >>= 1) {
+      JacobiPlan q = p;
+      q.levels = l;
+      if (jacobi_parts(f->d, q, true) <= 0 || jacobi_parts(f->d, q, false) <= 0)
+        return fail(AQ_ERR_INVALID_ARGUMENT, "tile too small for the plan's halo");
+    }
   }
   cudaSetDevice(f->device);
   AQ_CUDA(cudaStreamSynchronize(f->stream));
   int need = 0;
-  for (int l = levels; l >= 1; l >>= 1)
-    need = std::max(need, jacobi_parts(f->d, resid_plan(p, l), true));
+  if (flat) {
+    need = resid_flat_parts(f->d);
+  } else {
+    for (int l = levels; l >= 1; l >>= 1) {
+      JacobiPlan q = p;
+      q.levels = l;
+      need = std::max(need, jacobi_parts(f->d, q, true));
+    }
+  }
   if (need > f->jpart_cap) {
     double* np_ = nullptr;
     AQ_TRY(f->alloc(&np_, (size_t)need));
@@ -1266,7 +1321,7 @@ aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, in
   // The sweeps are captured into a graph and replayed, as inside a step.
   cudaGraph_t g = nullptr;
   AQ_CUDA(cudaStreamBeginCapture(f->stream, cudaStreamCaptureModeThreadLocal));
-  aq_status st = enqueue_sweeps(f, sweeps);
+  aq_status st = f->plan.by == 1 ? enqueue_persistent(f, sweeps) : enqueue_sweeps(f, sweeps, false);
   cudaGraph_t got = nullptr;
   cudaError_t ce = cudaStreamEndCapture(f->stream, &got);
   if (st != AQ_OK) { if (got) cudaGraphDestroy(got); return st; }
@@ -1291,11 +1346,11 @@ aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, in
   cudaEventDestroy(b);
   const std::vector<int> parts = split_sweeps(sweeps, f->plan.levels);
   if (ms) *ms = t;
-  if (launches) *launches = (int32_t)(parts.size() + parts.size() % 2);
+  if (launches) *launches = f->plan.by == 1 ? 2 : (int32_t)(parts.size() + parts.size() % 2);
   if (cells_per_sweep) {
     std::vector<uint8_t> act((size_t)f->nbricks);
     AQ_CUDA(cudaMemcpy(act.data(), f->bact, act.size(), cudaMemcpyDeviceToHost));
-    *cells_per_sweep = jacobi_cells_updated(f->d, f->plan, act.data());
+    *cells_per_sweep = jacobi_cells_updated(f->d, f->plan.by == 1 ? JacobiPlan{1, 0, 1} : f->plan, act.data());
   }
   return AQ_OK;
 }

@@ -165,48 +165,196 @@ __global__ void __launch_bounds__(32 * BY) k_jacobi(Dims d, int xc, const float*
 }
 
 
-// One sweep per launch, 4 consecutive z cells per thread (float4), no shared
-// memory: x and y neighbours come from L1/L2, z neighbours across threads by
-// warp shuffle.  Needs sz % 4 == 0.  Blocks of 32 z-quads x 8 rows on one
-// x plane; blocks whose 8 rows x 128 z cells hold no active brick return.
+// One sweep per launch, 4 consecutive z cells per thread (float4).  A block
+// is 8 warps (rows y) x 32 lanes (z-quads, 128 cells) and streams XS
+// consecutive x planes, keeping the x-1, x, x+1 planes of its quads in
+// registers and prefetching the next one; y neighbours come from L1/L2, z
+// neighbours across lanes by warp shuffle.  Each warp checks the activity
+// bricks of its own rows itself (no block barrier) and leaves if none holds
+// fluid.  Needs sz % 4 == 0.
+__device__ __forceinline__ bool warp_active(const Dims& d, const uint8_t* __restrict__ bact, int x0, int x1, int y,
+                                            int zb0) {
+  // bricks: x in [x0/8, (x1-1)/8], one y brick, z bricks zb0 .. zb0+15
+  const int lane = threadIdx.x;
+  int a = 0;
+  if (lane < 16 && zb0 + lane < d.bz)
+    for (int bx = x0 / kBrick; bx <= (x1 - 1) / kBrick; ++bx)
+      a |= bact[(bx * d.by + y / kBrick) * d.bz + zb0 + lane];
+  return __any_sync(0xffffffffu, a) != 0;
+}
+
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+template <int XS>
 __global__ void __launch_bounds__(256) k_jacobi_flat(Dims d, const float* __restrict__ pin,
                                                     float* __restrict__ pout, const float* __restrict__ rhs,
                                                     const int8_t* __restrict__ type,
                                                     const uint8_t* __restrict__ bact) {
   const int lane = threadIdx.x;
-  const int zq = blockIdx.x * 32 + lane;
-  const int z = zq * 4;
+  const int z = (blockIdx.x * 32 + lane) * 4;
   const int y = blockIdx.y * 8 + threadIdx.y;
-  const int x = blockIdx.z;
-  // brick check: the block spans one x brick, one y brick, 16 z bricks
-  const int bz0 = blockIdx.x * 16;
-  const int tid = threadIdx.y * 32 + lane;
-  int act = 0;
-  if (tid < 16 && bz0 + tid < d.bz) act = bact[((x / kBrick) * d.by + blockIdx.y) * d.bz + bz0 + tid];
-  act = __syncthreads_or(act);
+  const int x0 = blockIdx.z * XS;
+  const int x1 = min(x0 + XS, d.sx);
+  const bool act = y < d.sy && warp_active(d, bact, x0, x1, y, blockIdx.x * 16);
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;");
   if (!act) return;
-  const bool in = y < d.sy && z < d.sz;
+  const bool in = z < d.sz;
+  const int plane = d.sy * d.sz;
+  const int col = y * d.sz + z;
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 pm = zero, pc = zero, pp = zero;
+  if (in) {
+    pc = ld4(pin + x0 * plane + col);
+    pm = x0 > 0 ? ld4(pin + (x0 - 1) * plane + col) : pc;
+    pp = x0 + 1 < d.sx ? ld4(pin + (x0 + 1) * plane + col) : pc;
+  }
+  for (int x = x0; x < x1; ++x) {
+    const int c = x * plane + col;
+    // prefetch the plane after next before this plane's arithmetic
+    float4 pn = pp;
+    if (in && x + 2 < d.sx && x + 1 < x1) pn = ld4(pin + c + 2 * plane);
+    float4 ym = pc, yp = pc, b = zero;
+    char4 t = make_char4(0, 0, 0, 0);
+    if (in) {
+      if (y > 0) ym = ld4(pin + c - d.sz);
+      if (y + 1 < d.sy) yp = ld4(pin + c + d.sz);
+      b = ld4(rhs + c);
+      t = *reinterpret_cast<const char4*>(type + c);
+    }
+    float zlo = __shfl_up_sync(0xffffffffu, pc.w, 1);
+    float zhi = __shfl_down_sync(0xffffffffu, pc.x, 1);
+    if (in) {
+      if (lane == 0) zlo = z > 0 ? pin[c - 1] : pc.x;
+      if (lane == 31 || z + 4 >= d.sz) zhi = z + 4 < d.sz ? pin[c + 4] : pc.w;
+      const float4 xm = pm, xp = pp;
+      float4 o;
+      // p' = (x+1, x-1, y+1, y-1, z+1, z-1 summed in that order, + rhs) / 6
+      {
+        float s = xp.x + xm.x; s += yp.x; s += ym.x; s += pc.y; s += zlo; s += b.x;
+        o.x = t.x == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+      }
+      {
+        float s = xp.y + xm.y; s += yp.y; s += ym.y; s += pc.z; s += pc.x; s += b.y;
+        o.y = t.y == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+      }
+      {
+        float s = xp.z + xm.z; s += yp.z; s += ym.z; s += pc.w; s += pc.y; s += b.z;
+        o.z = t.z == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+      }
+      {
+        float s = xp.w + xm.w; s += yp.w; s += ym.w; s += zhi; s += pc.z; s += b.w;
+        o.w = t.w == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+      }
+      *reinterpret_cast<float4*>(pout + c) = o;
+    }
+    pm = pc;
+    pc = pp;
+    pp = (x + 2 < d.sx) ? pn : pc;
+  }
+}
+
+// FP64 residual ||b - A p||^2 of one iterate over fluid cells, in the flat
+// layout (one x plane x 8 rows x 128 z per block); per-block partial sums in
+// a fixed order.
+__global__ void __launch_bounds__(256) k_resid_flat(Dims d, const float* __restrict__ p,
+                                                   const float* __restrict__ rhs, const int8_t* __restrict__ type,
+                                                   const uint8_t* __restrict__ bact, double* __restrict__ part) {
+  const int lane = threadIdx.x;
+  const int z = (blockIdx.x * 32 + lane) * 4;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  const int x = blockIdx.z;
+  const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  const bool act = y < d.sy && warp_active(d, bact, x, x + 1, y, blockIdx.x * 16);
+  double acc = 0.0;
+  const bool in = act && z < d.sz;
+  const int plane = d.sy * d.sz;
+  const int c = x * plane + y * d.sz + z;
+  float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (in) pc = ld4(p + c);
+  float zlo = __shfl_up_sync(0xffffffffu, pc.w, 1);
+  float zhi = __shfl_down_sync(0xffffffffu, pc.x, 1);
+  if (in) {
+    if (lane == 0) zlo = z > 0 ? p[c - 1] : pc.x;
+    if (lane == 31 || z + 4 >= d.sz) zhi = z + 4 < d.sz ? p[c + 4] : pc.w;
+    const float4 xm = x > 0 ? ld4(p + c - plane) : pc;
+    const float4 xp = x + 1 < d.sx ? ld4(p + c + plane) : pc;
+    const float4 ym = y > 0 ? ld4(p + c - d.sz) : pc;
+    const float4 yp = y + 1 < d.sy ? ld4(p + c + d.sz) : pc;
+    const float4 b = ld4(rhs + c);
+    const char4 t = *reinterpret_cast<const char4*>(type + c);
+    const float self[4] = {pc.x, pc.y, pc.z, pc.w};
+    const float zp[4] = {pc.y, pc.z, pc.w, zhi};
+    const float zm[4] = {zlo, pc.x, pc.y, pc.z};
+    const float vxp[4] = {xp.x, xp.y, xp.z, xp.w}, vxm[4] = {xm.x, xm.y, xm.z, xm.w};
+    const float vyp[4] = {yp.x, yp.y, yp.z, yp.w}, vym[4] = {ym.x, ym.y, ym.z, ym.w};
+    const float vb[4] = {b.x, b.y, b.z, b.w};
+    const signed char vt[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (vt[k] != kFluid) continue;
+      double s = (double)vxp[k];
+      s += (double)vxm[k];
+      s += (double)vyp[k];
+      s += (double)vym[k];
+      s += (double)zp[k];
+      s += (double)zm[k];
+      const double r = (double)vb[k] + s - 6.0 * (double)self[k];
+      acc += r * r;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double s_red[8];
+  if (lane == 0) s_red[threadIdx.y] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    double t = 0.0;
+    for (int k = 0; k < 8; ++k) t += s_red[k];
+    part[bid] = t;
+  }
+}
+
+
+// ---------------------------------------------------------------- persistent
+// Flat work item id = (x * gy + yb) * gz + zb, gy = ceil(sy/8), gz = ceil(sz/128).
+__device__ __forceinline__ void item_coords(const Dims& d, int id, int& x, int& yb, int& zb) {
+  const int gz = (d.sz / 4 + 31) / 32, gy = (d.sy + 7) / 8;
+  zb = id % gz;
+  const int t = id / gz;
+  yb = t % gy;
+  x = t / gy;
+}
+
+// One Jacobi sweep of one item by a 256-thread CTA (8 warps = 8 rows).  The
+// ping-pong buffers are rewritten by other SMs between sweeps of the same
+// launch, so their loads bypass L1 (ld.global.cg); rhs and type are constant.
+__device__ __forceinline__ void sweep_item(const Dims& d, int id, const float* __restrict__ pin,
+                                           float* __restrict__ pout, const float* __restrict__ rhs,
+                                           const int8_t* __restrict__ type) {
+  int x, yb, zb;
+  item_coords(d, id, x, yb, zb);
+  const int lane = threadIdx.x & 31, row = (threadIdx.x & 255) >> 5;
+  const int y = yb * 8 + row;
+  if (y >= d.sy) return;  // warp-uniform
+  const int z = (zb * 32 + lane) * 4;
+  const bool in = z < d.sz;
   const int plane = d.sy * d.sz;
   const int c = x * plane + y * d.sz + z;
   float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (in) p = *reinterpret_cast<const float4*>(pin + c);
-  // z neighbours across lanes (lanes of one row are consecutive quads)
+  if (in) p = __ldcg(reinterpret_cast<const float4*>(pin + c));
   float zlo = __shfl_up_sync(0xffffffffu, p.w, 1);
   float zhi = __shfl_down_sync(0xffffffffu, p.x, 1);
   if (!in) return;
-  if (lane == 0) zlo = z > 0 ? pin[c - 1] : p.x;
-  else if (z == 0) zlo = p.x;
-  if (lane == 31 || z + 4 >= d.sz) zhi = z + 4 < d.sz ? pin[c + 4] : p.w;
-  const float4 xp = x + 1 < d.sx ? *reinterpret_cast<const float4*>(pin + c + plane) : p;
-  const float4 xm = x > 0 ? *reinterpret_cast<const float4*>(pin + c - plane) : p;
-  const float4 yp = y + 1 < d.sy ? *reinterpret_cast<const float4*>(pin + c + d.sz) : p;
-  const float4 ym = y > 0 ? *reinterpret_cast<const float4*>(pin + c - d.sz) : p;
-  const float4 b = *reinterpret_cast<const float4*>(rhs + c);
+  if (lane == 0) zlo = z > 0 ? __ldcg(pin + c - 1) : p.x;
+  if (lane == 31 || z + 4 >= d.sz) zhi = z + 4 < d.sz ? __ldcg(pin + c + 4) : p.w;
+  const float4 xp = x + 1 < d.sx ? __ldcg(reinterpret_cast<const float4*>(pin + c + plane)) : p;
+  const float4 xm = x > 0 ? __ldcg(reinterpret_cast<const float4*>(pin + c - plane)) : p;
+  const float4 yp = y + 1 < d.sy ? __ldcg(reinterpret_cast<const float4*>(pin + c + d.sz)) : p;
+  const float4 ym = y > 0 ? __ldcg(reinterpret_cast<const float4*>(pin + c - d.sz)) : p;
+  const float4 b = __ldg(reinterpret_cast<const float4*>(rhs + c));
   const char4 t = *reinterpret_cast<const char4*>(type + c);
   float4 o;
-  // p' = (x+1, x-1, y+1, y-1, z+1, z-1 summed in that order, + rhs) / 6
   {
     float s = xp.x + xm.x; s += yp.x; s += ym.x; s += p.y; s += zlo; s += b.x;
     o.x = t.x == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
@@ -224,6 +372,232 @@ __global__ void __launch_bounds__(256) k_jacobi_flat(Dims d, const float* __rest
     o.w = t.w == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
   }
   *reinterpret_cast<float4*>(pout + c) = o;
+}
+
+// ||b - A p||^2 of one item's fluid cells (per thread).
+__device__ __forceinline__ double resid_item(const Dims& d, int id, const float* __restrict__ pv,
+                                             const float* __restrict__ rhs, const int8_t* __restrict__ type) {
+  int x, yb, zb;
+  item_coords(d, id, x, yb, zb);
+  const int lane = threadIdx.x & 31, row = (threadIdx.x & 255) >> 5;
+  const int y = yb * 8 + row;
+  if (y >= d.sy) return 0.0;
+  const int z = (zb * 32 + lane) * 4;
+  const bool in = z < d.sz;
+  const int plane = d.sy * d.sz;
+  const int c = x * plane + y * d.sz + z;
+  float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (in) pc = __ldcg(reinterpret_cast<const float4*>(pv + c));
+  float zlo = __shfl_up_sync(0xffffffffu, pc.w, 1);
+  float zhi = __shfl_down_sync(0xffffffffu, pc.x, 1);
+  if (!in) return 0.0;
+  if (lane == 0) zlo = z > 0 ? __ldcg(pv + c - 1) : pc.x;
+  if (lane == 31 || z + 4 >= d.sz) zhi = z + 4 < d.sz ? __ldcg(pv + c + 4) : pc.w;
+  const float4 xm = x > 0 ? __ldcg(reinterpret_cast<const float4*>(pv + c - plane)) : pc;
+  const float4 xp = x + 1 < d.sx ? __ldcg(reinterpret_cast<const float4*>(pv + c + plane)) : pc;
+  const float4 ym = y > 0 ? __ldcg(reinterpret_cast<const float4*>(pv + c - d.sz)) : pc;
+  const float4 yp = y + 1 < d.sy ? __ldcg(reinterpret_cast<const float4*>(pv + c + d.sz)) : pc;
+  const float4 b = __ldg(reinterpret_cast<const float4*>(rhs + c));
+  const char4 t = *reinterpret_cast<const char4*>(type + c);
+  const float self[4] = {pc.x, pc.y, pc.z, pc.w};
+  const float zp[4] = {pc.y, pc.z, pc.w, zhi};
+  const float zm[4] = {zlo, pc.x, pc.y, pc.z};
+  const float vxp[4] = {xp.x, xp.y, xp.z, xp.w}, vxm[4] = {xm.x, xm.y, xm.z, xm.w};
+  const float vyp[4] = {yp.x, yp.y, yp.z, yp.w}, vym[4] = {ym.x, ym.y, ym.z, ym.w};
+  const float vb[4] = {b.x, b.y, b.z, b.w};
+  const signed char vt[4] = {t.x, t.y, t.z, t.w};
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (vt[k] != kFluid) continue;
+    double s = (double)vxp[k];
+    s += (double)vxm[k];
+    s += (double)vyp[k];
+    s += (double)vym[k];
+    s += (double)zp[k];
+    s += (double)zm[k];
+    const double r = (double)vb[k] + s - 6.0 * (double)self[k];
+    acc += r * r;
+  }
+  return acc;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned int* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+constexpr unsigned kSpinLimit = 1u << 25;  // with 32 ns sleeps: ~1 s before giving up
+
+// Grid barrier on a counter that only grows: arrival e of every CTA waits for
+// e * gridDim.x arrivals.  Bounded: on timeout it sets *fail and returns
+// false; after any failure every barrier returns false at once.
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned target, int* fail) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    if (*reinterpret_cast<volatile int*>(fail)) {
+      ok = 0;
+    } else {
+      __threadfence();
+      atomicAdd(bar, 1u);
+      unsigned spins = 0;
+      while (ld_acquire(bar) < target) {
+        if (++spins > kSpinLimit || *reinterpret_cast<volatile int*>(fail)) {
+          atomicExch(fail, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+      __threadfence();
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__global__ void __launch_bounds__(1024) k_items_compact(Dims d, const uint8_t* __restrict__ bact, int* __restrict__ items,
+                                                        int* __restrict__ n_items, unsigned int* __restrict__ bar) {
+  __shared__ int s_cnt[32], s_pre[32];
+  __shared__ int s_tot, s_base;
+  const int gz = (d.sz / 4 + 31) / 32, gy = (d.sy + 7) / 8;
+  const int total = gz * gy * d.sx;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    s_base = 0;
+    *bar = 0u;
+  }
+  __syncthreads();
+  for (int base = 0; base < total; base += 1024) {
+    const int id = base + threadIdx.x;
+    int a = 0;
+    if (id < total) {
+      int x, yb, zb;
+      item_coords(d, id, x, yb, zb);
+      for (int k = 0; k < 16 && zb * 16 + k < d.bz && !a; ++k)
+        a = bact[((x / kBrick) * d.by + yb) * d.bz + zb * 16 + k] ? 1 : 0;
+    }
+    // ordered compaction: block-wide exclusive scan of the flags
+    const unsigned m = __ballot_sync(0xffffffffu, a);
+    const int pre = __popc(m & ((1u << lane) - 1u));
+    if (lane == 0) s_cnt[w] = __popc(m);
+    __syncthreads();
+    if (w == 0) {
+      const int v = s_cnt[lane];
+      int incl = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      s_pre[lane] = incl - v;
+      if (lane == 31) s_tot = incl;
+    }
+    __syncthreads();
+    if (a) items[s_base + s_pre[w] + pre] = id;
+    __syncthreads();
+    if (threadIdx.x == 0) s_base += s_tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *n_items = s_base;
+}
+
+__global__ void __launch_bounds__(1024) k_persist_solve(Dims d, float* __restrict__ pa, float* __restrict__ pb,
+                                                      const float* __restrict__ rhs, const int8_t* __restrict__ type,
+                                                      const int* __restrict__ items, const int* __restrict__ n_items,
+                                                      unsigned int* __restrict__ bar, double* __restrict__ part,
+                                                      SolveState* __restrict__ ss, int fixed_sweeps, int check,
+                                                      int max_iters, double tol) {
+  __shared__ double s_red[32];
+  __shared__ double s_r2;
+  // one CTA per SM; four groups of 256 threads each sweep one item at a time
+  const int P = gridDim.x, cta = blockIdx.x;
+  const int G = 4, grp = threadIdx.x >> 8;
+  const int first = cta * G + grp, stride = P * G;
+  const int n = *n_items;
+  int* fail = &ss->sync_timeout;
+  unsigned epoch = 0;
+  float* bufs[2] = {pa, pb};
+  int cur = 0;
+  int it = 0, checks = 0;
+  bool ok = true;
+  double r2 = -1.0, rel = -1.0;
+
+  auto sweep = [&]() {
+    for (int i = first; i < n; i += stride) sweep_item(d, items[i], bufs[cur], bufs[cur ^ 1], rhs, type);
+    cur ^= 1;
+    ++epoch;
+    ok = ok && grid_barrier(bar, epoch * (unsigned)P, fail);
+  };
+  // residual of the current iterate; every CTA ends with the same r2
+  auto residual = [&]() {
+    double acc = 0.0;
+    for (int i = first; i < n; i += stride) acc += resid_item(d, items[i], bufs[cur], rhs, type);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < 32; ++k) t += s_red[k];
+      part[cta] = t;
+    }
+    ++epoch;
+    ok = ok && grid_barrier(bar, epoch * (unsigned)P, fail);
+    if (threadIdx.x < 32) {
+      double t = 0.0;
+      for (int k = threadIdx.x; k < P; k += 32) t += *reinterpret_cast<volatile double*>(part + k);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (threadIdx.x == 0) s_r2 = t;
+    }
+    __syncthreads();
+    r2 = s_r2;
+    rel = ss->b2 > 0.0 ? sqrt(r2) / sqrt(ss->b2) : 0.0;
+    ++checks;
+  };
+
+  if (fixed_sweeps > 0) {
+    for (int k = 0; k < fixed_sweeps && ok; ++k) sweep();
+    it = fixed_sweeps;
+    if (ok) residual();
+  } else {
+    while (ok) {
+      for (int k = 0; k < check && ok; ++k) sweep();
+      it += check;
+      if (!ok) break;
+      residual();
+      if (!(rel > tol) || !isfinite(rel) || it >= max_iters) break;
+    }
+  }
+  // the result belongs in pa: copy this CTA's items when it ended in pb
+  if (cur == 1) {
+    for (int i = first; i < n; i += stride) {
+      int x, yb, zb;
+      item_coords(d, items[i], x, yb, zb);
+      const int y = yb * 8 + ((threadIdx.x & 255) >> 5);
+      const int z = (zb * 32 + (threadIdx.x & 31)) * 4;
+      if (y < d.sy && z < d.sz) {
+        const int c = x * d.sy * d.sz + y * d.sz + z;
+        *reinterpret_cast<float4*>(pa + c) = __ldcg(reinterpret_cast<const float4*>(pb + c));
+      }
+    }
+  }
+  if (cta == 0 && threadIdx.x == 0) {
+    ss->iterations = it;
+    ss->bodies = checks;
+    ss->total_sweeps += it;
+    ss->total_bodies += checks;
+    ss->r2 = r2;
+    ss->rel_residual = rel;
+    const bool finite = isfinite(rel);
+    if (!finite) ss->nonfinite = 1;
+    ss->converged = (ok && finite && rel >= 0.0 && rel <= tol) ? 1 : 0;
+  }
 }
 
 __global__ void __launch_bounds__(1024) k_resid_finalize(const double* __restrict__ part, int nparts,
@@ -340,14 +714,16 @@ cudaError_t jacobi_prepare() {
 
 long long jacobi_cells_updated(const Dims& d, const JacobiPlan& p, const uint8_t* bact_host) {
   if (p.by == 0) {
-    long long cells = 0;  // flat: 1 x plane x 8 rows x 128 z per block
-    for (int x = 0; x < d.sx; ++x)
-      for (int y0 = 0; y0 < d.sy; y0 += 8)
+    long long cells = 0;  // flat: xc x planes x 8 rows (one warp per row) x 128 z per block
+    for (int x0 = 0; x0 < d.sx; x0 += p.xc)
+      for (int y = 0; y < d.sy; ++y)
         for (int z0 = 0; z0 < d.sz; z0 += 128) {
+          const int x1 = std::min(x0 + p.xc, d.sx);
           bool act = false;
-          for (int bz = z0 / kBrick; bz < (z0 + 128) / kBrick && bz < d.bz && !act; ++bz)
-            act = bact_host[((x / kBrick) * d.by + y0 / kBrick) * d.bz + bz] != 0;
-          if (act) cells += (long long)std::min(8, d.sy - y0) * std::min(128, d.sz - z0);
+          for (int bx = x0 / kBrick; bx <= (x1 - 1) / kBrick && !act; ++bx)
+            for (int bz = z0 / kBrick; bz < (z0 + 128) / kBrick && bz < d.bz && !act; ++bz)
+              act = bact_host[(bx * d.by + y / kBrick) * d.bz + bz] != 0;
+          if (act) cells += (long long)(x1 - x0) * std::min(128, d.sz - z0);
         }
     return cells;
   }
@@ -383,10 +759,9 @@ cudaError_t launch_jacobi(cudaStream_t st, const Dims& d, const JacobiPlan& plan
                           float* pout, const float* rhs, const int8_t* type, const uint8_t* brick_active,
                           double* part, int* nparts_out) {
   if (plan.by == 0) {
-    // flat plan: one sweep, no residual variant (the caller uses a tiled one)
+    // flat plan: one sweep per launch, XS = plan.xc x planes per block
     if (resid || d.sz % 4 != 0) return cudaErrorInvalidValue;
     cudaLaunchConfig_t lc = {};
-    lc.gridDim = dim3((d.sz / 4 + 31) / 32, (d.sy + 7) / 8, d.sx);
     lc.blockDim = dim3(32, 8);
     lc.stream = st;
     cudaLaunchAttribute at[1];
@@ -395,10 +770,59 @@ cudaError_t launch_jacobi(cudaStream_t st, const Dims& d, const JacobiPlan& plan
     lc.attrs = at;
     lc.numAttrs = 1;
     if (nparts_out) *nparts_out = 0;
-    return cudaLaunchKernelEx(&lc, k_jacobi_flat, d, pin, pout, rhs, type, brick_active);
+    const dim3 g((d.sz / 4 + 31) / 32, (d.sy + 7) / 8, 1);
+    switch (plan.xc) {
+      case 1: lc.gridDim = dim3(g.x, g.y, d.sx); return cudaLaunchKernelEx(&lc, k_jacobi_flat<1>, d, pin, pout, rhs, type, brick_active);
+      case 2: lc.gridDim = dim3(g.x, g.y, (d.sx + 1) / 2); return cudaLaunchKernelEx(&lc, k_jacobi_flat<2>, d, pin, pout, rhs, type, brick_active);
+      case 4: lc.gridDim = dim3(g.x, g.y, (d.sx + 3) / 4); return cudaLaunchKernelEx(&lc, k_jacobi_flat<4>, d, pin, pout, rhs, type, brick_active);
+      case 8: lc.gridDim = dim3(g.x, g.y, (d.sx + 7) / 8); return cudaLaunchKernelEx(&lc, k_jacobi_flat<8>, d, pin, pout, rhs, type, brick_active);
+      default: return cudaErrorInvalidValue;
+    }
   }
   if (resid) return dispatch_levels<true>(st, d, plan, pin, pout, rhs, type, brick_active, part, nparts_out);
   return dispatch_levels<false>(st, d, plan, pin, pout, rhs, type, brick_active, part, nparts_out);
+}
+
+int persist_items(const Dims& d) { return ((d.sz / 4 + 31) / 32) * ((d.sy + 7) / 8) * d.sx; }
+
+int persist_ctas(int device) {
+  int sms = 0, occ = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persist_solve, 1024, 0) != cudaSuccess) return 0;
+  return sms * (occ < 1 ? 0 : 1);
+}
+
+cudaError_t launch_items_compact(cudaStream_t st, const Dims& d, const uint8_t* brick_active, int* items,
+                                 int* n_items, unsigned int* bar) {
+  k_items_compact<<<1, 1024, 0, st>>>(d, brick_active, items, n_items, bar);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_persist_solve(cudaStream_t st, const Dims& d, int ctas, float* pa, float* pb, const float* rhs,
+                                 const int8_t* type, const int* items, const int* n_items, unsigned int* bar,
+                                 double* part, SolveState* ss, int fixed_sweeps, int check, int max_iters, double tol) {
+  if (d.sz % 4 != 0 || ctas <= 0) return cudaErrorInvalidValue;
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(ctas);
+  lc.blockDim = dim3(1024);
+  lc.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;  // all CTAs co-resident, or the launch fails
+  at[0].val.cooperative = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  return cudaLaunchKernelEx(&lc, k_persist_solve, d, pa, pb, rhs, type, items, n_items, bar, part, ss, fixed_sweeps,
+                            check, max_iters, tol);
+}
+
+int resid_flat_parts(const Dims& d) { return ((d.sz / 4 + 31) / 32) * ((d.sy + 7) / 8) * d.sx; }
+
+cudaError_t launch_resid_flat(cudaStream_t st, const Dims& d, const float* p, const float* rhs, const int8_t* type,
+                              const uint8_t* brick_active, double* part) {
+  if (d.sz % 4 != 0) return cudaErrorInvalidValue;
+  k_resid_flat<<<dim3((d.sz / 4 + 31) / 32, (d.sy + 7) / 8, d.sx), dim3(32, 8), 0, st>>>(d, p, rhs, type,
+                                                                                        brick_active, part);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_resid_finalize(cudaStream_t st, const double* part, int nparts, SolveState* ss,

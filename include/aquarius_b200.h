@@ -49,7 +49,8 @@ typedef enum aq_status {
   AQ_ERR_CUDA = 4,
   AQ_ERR_NOT_CONVERGED = 5,
   AQ_ERR_NONFINITE = 6,
-  AQ_ERR_NO_DEVICE = 7
+  AQ_ERR_NO_DEVICE = 7,
+  AQ_ERR_TIMEOUT = 8
 } aq_status;
 
 /* ShapeType {Sphere, Square} (Fluid/FluidConfig.cuh:16-18). */
@@ -220,8 +221,12 @@ aq_status aq_fluid_upload_state(aq_fluid* f, const aq_host_state* s);
 
 aq_status aq_fluid_solve_stats(const aq_fluid* f, aq_solve_stats* st);
 
-/* Tile plan of the Jacobi kernel: sweeps per launch (1, 2, 4 or 8), tile
- * rows (8, 16 or 32) and x planes per CTA (>= 1).  Chosen per grid by the
+/* Plan of the Jacobi kernels.  rows = 0: one vectorised sweep per launch
+ * (levels 1, x_planes in {1,2,4,8} planes per block; sz % 4 == 0).
+ * rows = 1: the whole solve in one persistent cooperative launch with a
+ * grid barrier between sweeps (levels 1; sz % 4 == 0).  rows = 8, 16, 32:
+ * the temporally blocked kernel with `levels` sweeps (1, 2, 4, 8) per launch
+ * over tiles of that many rows and x_planes planes.  Chosen per grid by the
  * tuner; invalid plans are rejected. */
 aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, int32_t x_planes);
 aq_status aq_fluid_get_jacobi_plan(const aq_fluid* f, int32_t* levels, int32_t* rows, int32_t* x_planes);

@@ -333,3 +333,48 @@ def test_full_size_invariants():
     np.testing.assert_array_equal((q[0] * 128 + q[1]) * 128 + q[2], h)
     st = f.solve_stats()
     assert st["iterations"] > 0 and (st["converged"] or st["iterations"] >= 2000)
+
+
+@pytest.mark.parametrize("mode", ["fixed", "residual"])
+def test_jacobi_plans_agree(mode):
+    """Every Jacobi plan (flat, persistent cooperative, temporally blocked)
+    computes the same iterates: same arithmetic per cell, same order."""
+    kw = dict(pressure_init=_abi.PRESSURE_ZERO)
+    if mode == "residual":
+        kw.update(solve_mode=_abi.SOLVE_RESIDUAL, rel_residual=1e-4, max_iterations=800, check_interval=40)
+    else:
+        kw.update(pressure_iterations=61)
+    cfg = SCENES["cfg2_32"](**kw)
+    o = Oracle(cfg)
+    warm(o, 3)
+    for k in range(1, 5):
+        o.stage(k)
+    st = o.get_state()
+    results = {}
+    for plan in [(1, 0, 1), (1, 1, 1), (1, 0, 2), (2, 16, 16), (4, 32, 16)]:
+        f = aq.Fluid(cfg)
+        f.set_jacobi_plan(*plan)
+        f.upload_state(st)
+        f.run_stage(_abi.STAGE_PRESSURE)
+        results[plan] = (f.download_state(["pressure"])["pressure"], f.solve_stats())
+        f.close()
+    p0, s0 = results[(1, 0, 1)]
+    for plan, (p, s) in results.items():
+        np.testing.assert_array_equal(p, p0, err_msg=str(plan))
+        assert s["iterations"] == s0["iterations"], plan
+        assert s["rel_residual"] == pytest.approx(s0["rel_residual"], rel=1e-9), plan
+    o.stage(_abi.STAGE_PRESSURE)
+    assert rel_l2(p0, o.get_state(["pressure"])["pressure"]) <= TOL
+    assert s0["iterations"] == o.solve_stats()["iterations"]
+
+
+def test_persistent_step_graph_matches_flat():
+    cfg = SCENES["cfg2_32"](solve_mode=_abi.SOLVE_RESIDUAL, rel_residual=1e-4, max_iterations=400, check_interval=40)
+    f1, f2 = aq.Fluid(cfg), aq.Fluid(cfg)
+    f2.set_jacobi_plan(1, 1, 1)
+    f1.step(4)
+    f2.step(4)
+    a, b = f1.download_state(), f2.download_state()
+    for k in a:
+        if k != "physical_time":
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
