@@ -87,6 +87,7 @@ def load_library() -> ct.CDLL:
         "aq_fluid_set_jacobi_plan": (ct.c_int, [P, ct.c_int32, ct.c_int32, ct.c_int32]),
         "aq_fluid_get_jacobi_plan": (ct.c_int, [P, ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int32),
                                                 ct.POINTER(ct.c_int32)]),
+        "aq_fluid_autotune": (ct.c_int, [P, ct.c_int32, ct.c_char_p, ct.POINTER(_abi.TuneResult)]),
         "aq_fluid_destroy": (None, [P]),
     }
     for name, (res, args) in sigs.items():
@@ -310,6 +311,15 @@ class Fluid:
         a, b, c = ct.c_int32(), ct.c_int32(), ct.c_int32()
         _check(self._lib.aq_fluid_get_jacobi_plan(self._h, ct.byref(a), ct.byref(b), ct.byref(c)))
         return a.value, b.value, c.value
+
+    def autotune(self, sweeps_per_trial: int = 200, cache_path=None) -> dict:
+        """Times the candidate Jacobi plans on the current system and keeps the
+        fastest (optionally cached per GPU and grid in a JSON file)."""
+        r = _abi.TuneResult()
+        path = None if cache_path is None else str(cache_path).encode()
+        _check(self._lib.aq_fluid_autotune(self._h, sweeps_per_trial, path, ct.byref(r)))
+        return {"plan": (r.levels, r.rows, r.x_planes), "sweep_us": r.sweep_us, "candidates": r.candidates,
+                "from_cache": bool(r.from_cache)}
 
     def launch_counts(self) -> tuple:
         a, b = ct.c_int32(), ct.c_int32()

@@ -127,6 +127,17 @@ class SolveStats(ct.Structure):
     ]
 
 
+class TuneResult(ct.Structure):
+    _fields_ = [
+        ("levels", ct.c_int32),
+        ("rows", ct.c_int32),
+        ("x_planes", ct.c_int32),
+        ("sweep_us", ct.c_float),
+        ("candidates", ct.c_int32),
+        ("from_cache", ct.c_int32),
+    ]
+
+
 # name -> (dtype, shape builder(N, C, F))
 STATE_FIELDS = {
     "position": (np.float32, lambda n, c, f: (3, n)),

@@ -7,7 +7,10 @@
 #include <cmath>
 #include <cstdlib>
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <sstream>
 #include <stdlib.h>
 #include <string>
 #include <vector>
@@ -1352,6 +1355,97 @@ aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, in
     AQ_CUDA(cudaMemcpy(act.data(), f->bact, act.size(), cudaMemcpyDeviceToHost));
     *cells_per_sweep = jacobi_cells_updated(f->d, f->plan.by == 1 ? JacobiPlan{1, 0, 1} : f->plan, act.data());
   }
+  return AQ_OK;
+}
+
+namespace {
+
+std::string tune_key(int device, const Dims& d) {
+  cudaDeviceProp prop;
+  std::string name = "unknown";
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) name = prop.name;
+  for (char& c : name)
+    if (c == '"' || c == '\\') c = '_';
+  return name + "|" + std::to_string(d.sx) + "x" + std::to_string(d.sy) + "x" + std::to_string(d.sz);
+}
+
+// The cache is a JSON object of "key": [levels, rows, x_planes, sweep_us];
+// written and read by this function only (one entry per line).
+bool tune_cache_lookup(const char* path, const std::string& key, int plan[3], float* us) {
+  std::ifstream in(path);
+  if (!in) return false;
+  std::string line;
+  const std::string pat = "\"" + key + "\": [";
+  while (std::getline(in, line)) {
+    const size_t p = line.find(pat);
+    if (p == std::string::npos) continue;
+    std::istringstream ss(line.substr(p + pat.size()));
+    char comma;
+    if (ss >> plan[0] >> comma >> plan[1] >> comma >> plan[2] >> comma >> *us) return true;
+  }
+  return false;
+}
+
+void tune_cache_store(const char* path, const std::string& key, const int plan[3], float us) {
+  std::vector<std::string> lines;
+  {
+    std::ifstream in(path);
+    std::string line;
+    while (in && std::getline(in, line)) {
+      if (line.find("\": [") != std::string::npos && line.find("\"" + key + "\"") == std::string::npos) {
+        while (!line.empty() && (line.back() == ',' || line.back() == ' ')) line.pop_back();
+        lines.push_back(line);
+      }
+    }
+  }
+  char buf[512];
+  snprintf(buf, sizeof(buf), "  \"%s\": [%d, %d, %d, %.4f]", key.c_str(), plan[0], plan[1], plan[2], us);
+  lines.push_back(buf);
+  std::ofstream out(path, std::ios::trunc);
+  out << "{\n";
+  for (size_t i = 0; i < lines.size(); ++i) out << lines[i] << (i + 1 < lines.size() ? ",\n" : "\n");
+  out << "}\n";
+}
+
+}  // namespace
+
+aq_status aq_fluid_autotune(aq_fluid* f, int32_t sweeps_per_trial, const char* cache_path, aq_tune_result* out) {
+  if (!f || sweeps_per_trial < 8) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(f->device);
+  const std::string key = tune_key(f->device, f->d);
+  aq_tune_result r;
+  memset(&r, 0, sizeof(r));
+  int plan[3];
+  float us = 0.f;
+  if (cache_path && tune_cache_lookup(cache_path, key, plan, &us) &&
+      aq_fluid_set_jacobi_plan(f, plan[0], plan[1], plan[2]) == AQ_OK) {
+    r.levels = plan[0]; r.rows = plan[1]; r.x_planes = plan[2];
+    r.sweep_us = us;
+    r.from_cache = 1;
+    if (out) *out = r;
+    return AQ_OK;
+  }
+  const int cands[][3] = {{1, 0, 1}, {1, 0, 2}, {1, 1, 1}, {1, 16, 8}, {2, 16, 16}, {2, 32, 16}, {4, 32, 16}};
+  float best = 1e30f;
+  int bestp[3] = {f->plan.levels, f->plan.by, f->plan.xc};
+  for (const auto& c : cands) {
+    if (aq_fluid_set_jacobi_plan(f, c[0], c[1], c[2]) != AQ_OK) continue;
+    float ms = 0.f, ms2 = 0.f;
+    if (aq_fluid_benchmark_pressure(f, sweeps_per_trial, &ms, nullptr, nullptr) != AQ_OK) continue;
+    if (aq_fluid_benchmark_pressure(f, sweeps_per_trial, &ms2, nullptr, nullptr) != AQ_OK) continue;
+    const float t = std::min(ms, ms2) * 1000.f / (float)sweeps_per_trial;
+    r.candidates++;
+    if (t < best) {
+      best = t;
+      bestp[0] = c[0]; bestp[1] = c[1]; bestp[2] = c[2];
+    }
+  }
+  AQ_TRY(aq_fluid_set_jacobi_plan(f, bestp[0], bestp[1], bestp[2]));
+  r.levels = bestp[0]; r.rows = bestp[1]; r.x_planes = bestp[2];
+  r.sweep_us = best;
+  if (cache_path && r.candidates > 0) tune_cache_store(cache_path, key, bestp, best);
+  if (out) *out = r;
+  g_last_error.clear();
   return AQ_OK;
 }
 

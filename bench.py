@@ -108,11 +108,41 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def reduce_max(x: float, dist, device: str) -> float:
+    """Max of a per-rank scalar over all ranks (identity without a process group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_scaling_value(steps_per_rank: int, world: int, max_ms: float) -> float:
+    """Whole-job steps/s: every rank steps its own replica; time = slowest rank."""
+    return world * steps_per_rank / (max_ms / 1000.0)
+
+
 def jacobi_kernel_name(f) -> str:
     levels, rows, xplanes = f.jacobi_plan()
+    if rows == 1:
+        return "k_persist_solve (whole solve in one cooperative launch)"
     if rows == 0:
-        return "k_jacobi_flat (1 sweep/launch, float4 z-quads)"
+        return f"k_jacobi_flat<{xplanes}> (1 sweep/launch, float4 z-quads)"
     return f"k_jacobi<{levels} sweeps/launch, {rows} rows, {xplanes} x-planes> (temporally blocked)"
+
+
+def measured_traffic(f):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/roofline_traffic.json), when it covers this kernel."""
+    try:
+        d = json.loads((ROOT / "profiles" / "roofline_traffic.json").read_text())
+        levels, rows, xplanes = f.jacobi_plan()
+        if rows == 0 and xplanes == 1 and "k_jacobi_flat" in d:
+            return d["k_jacobi_flat"]["bytes_per_launch"]
+    except Exception:
+        pass
+    return None
 
 
 def measured_hbm_peak():
@@ -194,14 +224,14 @@ def run_ours(args, rank: int, world: int, dist):
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, f"cuda:{dev}")
 
-    # warm-up (builds and instantiates the step graph)
+    # warm-up (builds and instantiates the step graph); the Jacobi plan is
+    # tuned on the warmed-up system, then the graph is rebuilt and warmed again
     f.step(args.warmup)
+    f.synchronize()
+    tune = f.autotune(200) if not args.no_tune else {"plan": f.jacobi_plan(), "sweep_us": None}
+    f.step(1)
     f.synchronize()
     st0 = f.solve_stats()
     per_step, per_block = f.launch_counts()
@@ -226,7 +256,7 @@ def run_ours(args, rank: int, world: int, dist):
     sweeps = st1["total_sweeps"] - st0["total_sweeps"]
     blocks = st1["total_blocks"] - st0["total_blocks"]
     launches = args.steps * per_step + blocks * per_block
-    value = world * args.steps / (ms_max / 1000.0)
+    value = weak_scaling_value(args.steps, world, ms_max)
 
     # e2e: the same steps through the C-ABI host-buffer entry point; every step
     # uploads the particle state from pinned host memory and reads it back
@@ -248,7 +278,7 @@ def run_ours(args, rank: int, world: int, dist):
     e1.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     e2e_wall = time.perf_counter() - t0
-    e2e_value = world * e2e_steps / (e2e_ms / 1000.0)
+    e2e_value = weak_scaling_value(e2e_steps, world, e2e_ms)
 
     # roofline of the dominant kernel: Jacobi sweeps on the last step's system
     hbm_peak, peak_kind = measured_hbm_peak()
@@ -276,7 +306,7 @@ def run_ours(args, rank: int, world: int, dist):
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": jacobi_kernel_name(f), "achieved": achieved_gbs,
                      "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
-                     "traffic": None,
+                     "traffic": measured_traffic(f),
                      "algorithmic_bytes": f"{JACOBI_BYTES_PER_CELL} B per updated cell per sweep x {cells} cells",
                      "sweep_us": sweep_ms * 1000.0, "full_domain_equiv_gbs": full_gbs},
         "clocks": clk,
@@ -285,6 +315,8 @@ def run_ours(args, rank: int, world: int, dist):
                    "converged": pstats["converged"], "fluid_cells": pstats["fluid_cells"],
                    "pressure_rel_error_vs_fp64_pcg": pcg["rel_error"], "pcg_iterations": pcg["iterations"]},
         "particles": n,
+        "jacobi_plan": {"levels": tune["plan"][0], "rows": tune["plan"][1], "x_planes": tune["plan"][2],
+                        "tuned_sweep_us": tune["sweep_us"]},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(args.size, args.pressure_init, steps=1)
@@ -302,6 +334,7 @@ def main():
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--pressure-init", default="zero", choices=["zero", "carry"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default Jacobi plan")
     ap.add_argument("--eager", action="store_true",
                     help="launch the step kernel by kernel instead of one CUDA graph (for launch lists)")
     args = ap.parse_args()

@@ -231,6 +231,23 @@ aq_status aq_fluid_solve_stats(const aq_fluid* f, aq_solve_stats* st);
 aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, int32_t x_planes);
 aq_status aq_fluid_get_jacobi_plan(const aq_fluid* f, int32_t* levels, int32_t* rows, int32_t* x_planes);
 
+/* Result of aq_fluid_autotune: the chosen plan and its measured sweep time. */
+typedef struct aq_tune_result {
+  int32_t levels, rows, x_planes;
+  float sweep_us;           /* graph-timed wall time per sweep of the chosen plan */
+  int32_t candidates;       /* plans timed (0 when taken from the cache) */
+  int32_t from_cache;
+} aq_tune_result;
+
+/* Project-written autotuner of the Jacobi plan.  Times every candidate plan
+ * (flat with 1 or 2 planes per block, persistent cooperative, temporally
+ * blocked shapes) on the fluid's current pressure system with graph-replayed
+ * sweeps, keeps the fastest and sets it.  Needs a system with fluid, i.e.
+ * call after at least one step; it advances the pressure iterate.
+ * cache_path (may be NULL): a JSON file keyed by GPU name and grid size; a
+ * hit sets the cached plan without timing, a miss appends the new choice. */
+aq_status aq_fluid_autotune(aq_fluid* f, int32_t sweeps_per_trial, const char* cache_path, aq_tune_result* out);
+
 /* FP64 preconditioned conjugate gradient on the current pressure system
  * (the one the last AQ_STAGE_DIVERGENCE built), to rel_tol.  Writes the FP64
  * solution as float into pressure_out ([C], host, may be NULL) and reports
