@@ -28,7 +28,7 @@ from . import _abi
 
 __all__ = [
     "ShapeType", "InitializationVolume", "ConfigFLIP", "FluidConfig", "Fluid", "AquariusError",
-    "library_path", "load_library", "STAGES",
+    "library_path", "load_library", "STAGES", "Batch",
 ]
 
 STAGES = _abi.STAGES
@@ -89,6 +89,20 @@ def load_library() -> ct.CDLL:
                                                 ct.POINTER(ct.c_int32)]),
         "aq_fluid_autotune": (ct.c_int, [P, ct.c_int32, ct.c_char_p, ct.POINTER(_abi.TuneResult)]),
         "aq_fluid_destroy": (None, [P]),
+        "aq_batch_create": (ct.c_int, [ct.POINTER(_abi.Config), ct.c_int32, ct.POINTER(P)]),
+        "aq_batch_step": (ct.c_int, [P, ct.c_int32]),
+        "aq_batch_synchronize": (ct.c_int, [P]),
+        "aq_batch_step_host": (ct.c_int, [P, ct.c_int32, P, P, P, P]),
+        "aq_batch_stream": (ct.c_int, [P, ct.POINTER(P)]),
+        "aq_batch_scene_count": (ct.c_int32, [P]),
+        "aq_batch_scene_info": (ct.c_int, [P, ct.c_int32, ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int64)]),
+        "aq_batch_totals": (ct.c_int, [P, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)]),
+        "aq_batch_download_scene": (ct.c_int, [P, ct.c_int32, ct.POINTER(_abi.HostState)]),
+        "aq_batch_solve_stats": (ct.c_int, [P, ct.c_int32, ct.POINTER(_abi.SolveStats)]),
+        "aq_batch_launch_counts": (ct.c_int, [P, ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int32)]),
+        "aq_batch_set_grid_multiple": (ct.c_int, [P, ct.c_int32]),
+        "aq_batch_benchmark_pressure": (ct.c_int, [P, ct.c_int32, ct.POINTER(ct.c_float), ct.POINTER(ct.c_int64)]),
+        "aq_batch_destroy": (None, [P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -335,6 +349,102 @@ class Fluid:
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
             self._lib.aq_fluid_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def _solve_stats_dict(s) -> dict:
+    return {"iterations": s.iterations, "rel_residual": s.rel_residual, "b_norm": s.b_norm,
+            "fluid_cells": s.fluid_cells, "converged": bool(s.converged), "blocks": s.blocks,
+            "total_sweeps": s.total_sweeps, "total_blocks": s.total_blocks}
+
+
+class Batch:
+    """Many independent single-phase scenes stepped together (no reference
+    counterpart): one launch per stage over all scenes, one CUDA graph per
+    step.  Scene s evolves bit for bit as Fluid(configs[s]) with the default
+    Jacobi plan."""
+
+    def __init__(self, configs):
+        self._lib = load_library()
+        self._h = ct.c_void_p()
+        cs = [c.to_c() if isinstance(c, FluidConfig) else c for c in configs]
+        arr = (_abi.Config * len(cs))(*cs)
+        _check(self._lib.aq_batch_create(arr, len(cs), ct.byref(self._h)))
+        self.scene_count = self._lib.aq_batch_scene_count(self._h)
+        self.sizes, self.particle_counts = [], []
+        for i in range(self.scene_count):
+            sz = (ct.c_int32 * 3)()
+            n = ct.c_int64()
+            _check(self._lib.aq_batch_scene_info(self._h, i, sz, ct.byref(n)))
+            self.sizes.append(tuple(sz))
+            self.particle_counts.append(n.value)
+
+    def step(self, n: int = 1):
+        _check(self._lib.aq_batch_step(self._h, n))
+
+    def synchronize(self):
+        _check(self._lib.aq_batch_synchronize(self._h))
+
+    def step_host(self, n: int, position_in=None, velocity_in=None, position_out=None, velocity_out=None):
+        """Steps with the particle state of all scenes in host arrays ([3][N],
+        scenes concatenated in batch order); synchronous."""
+        def ptr(a):
+            return None if a is None else a.ctypes.data
+        _check(self._lib.aq_batch_step_host(self._h, n, ptr(position_in), ptr(velocity_in), ptr(position_out),
+                                            ptr(velocity_out)))
+
+    def stream(self) -> int:
+        s = ct.c_void_p()
+        _check(self._lib.aq_batch_stream(self._h, ct.byref(s)))
+        return s.value or 0
+
+    def totals(self) -> dict:
+        c, f, p = ct.c_int64(), ct.c_int64(), ct.c_int64()
+        _check(self._lib.aq_batch_totals(self._h, ct.byref(c), ct.byref(f), ct.byref(p)))
+        return {"cells": c.value, "nodes": f.value, "particles": p.value}
+
+    def download_scene(self, scene: int, fields=None) -> dict:
+        sx, sy, sz = self.sizes[scene]
+        n = self.particle_counts[scene]
+        arrs = _abi.alloc_state(sx, sy, sz, n, fields)
+        st = _abi.make_host_state(sx, sy, sz, n, arrs)
+        _check(self._lib.aq_batch_download_scene(self._h, scene, ct.byref(st)))
+        arrs["physical_time"] = st.physical_time
+        return arrs
+
+    def solve_stats(self, scene: int) -> dict:
+        s = _abi.SolveStats()
+        _check(self._lib.aq_batch_solve_stats(self._h, scene, ct.byref(s)))
+        return _solve_stats_dict(s)
+
+    def launch_counts(self) -> tuple:
+        a, b = ct.c_int32(), ct.c_int32()
+        _check(self._lib.aq_batch_launch_counts(self._h, ct.byref(a), ct.byref(b)))
+        return a.value, b.value
+
+    def set_grid_multiple(self, multiple: int):
+        _check(self._lib.aq_batch_set_grid_multiple(self._h, multiple))
+
+    def benchmark_pressure(self, sweeps: int) -> dict:
+        ms, cells = ct.c_float(), ct.c_int64()
+        _check(self._lib.aq_batch_benchmark_pressure(self._h, sweeps, ct.byref(ms), ct.byref(cells)))
+        return {"ms": ms.value, "cells_per_sweep": cells.value}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.aq_batch_destroy(self._h)
             self._h = ct.c_void_p()
 
     def __del__(self):

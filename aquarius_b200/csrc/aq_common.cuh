@@ -70,6 +70,41 @@ struct StepParams {
   int multiphase;
 };
 
+// One scene of a batch: its grid, parameters and offsets into the batch's
+// concatenated arrays (particles, cells, nodes, activity bricks, residual
+// partial sums).
+struct SceneDesc {
+  Dims d;
+  StepParams sp;
+  int p_off, n;  // particles
+  int c_off;     // cells (and cell-table keys)
+  int f_off;     // nodes
+  int br_off;    // 8^3 bricks
+  int rp_off;    // flat residual partials
+};
+
+// Virtual-block prefix sums per kernel family over the scenes of a batch:
+// scene s owns virtual blocks [pre[s], pre[s+1]).
+struct BatchIndex {
+  const SceneDesc* scenes;
+  int n_scenes;
+  const int* particles;  // ceil(n/256)
+  const int* nodes;      // ceil(sz/32) * ceil(sy/8) * sx
+  const int* bricks;     // bx * by * bz
+  const int* slayer;     // ceil((F - C)/256)
+  const int* flat;       // ceil(sz/128) * ceil(sy/8) * sx
+};
+
+__device__ __forceinline__ int find_scene(const int* __restrict__ pre, int ns, int vb) {
+  int lo = 0, hi = ns;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(pre + mid) <= vb) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // Device-side record of the pressure solve; read back on demand.
 struct SolveState {
   int iterations;       // sweeps done in the current/last solve

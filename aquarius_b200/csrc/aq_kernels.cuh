@@ -103,6 +103,48 @@ cudaError_t launch_resid_finalize(cudaStream_t st, const double* part, int npart
                                   int sweeps_done_per_call, double tol, int max_iters,
                                   bool set_cond, unsigned long long cond_handle);
 
+// ---- batched scenes ------------------------------------------------------------
+// Each launcher runs one stage for every scene of a batch: `total` virtual
+// blocks (the last prefix sum of the stage's family in BatchIndex) walked by
+// `grid` CTAs.  A virtual block runs the single-scene kernel's body on its
+// scene's slice of the concatenated arrays, so a scene's result does not
+// depend on the other scenes.  Single-phase scenes only.
+cudaError_t launch_batch_particles_advance(cudaStream_t st, const BatchIndex& bi, int total, int grid, bool move,
+                                           Particles cur, Particles tmp, const float* u0, const float* v0,
+                                           const float* w0, const float* un, const float* vn, const float* wn,
+                                           int* key, int* slot, int* count);
+cudaError_t launch_batch_p2g(cudaStream_t st, const BatchIndex& bi, int total, int grid, bool forces, Particles cur,
+                             const int* off, float* u0, float* v0, float* w0, float* un, float* vn, float* wn,
+                             int8_t* type, float* density);
+cudaError_t launch_batch_slayer(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int8_t* type,
+                                const float* su, const float* sv, const float* sw, float* u1, float* v1, float* w1,
+                                float* u2, float* v2, float* w2);
+cudaError_t launch_batch_divergence(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* off,
+                                    const int8_t* type, const float* density, const float* un, const float* vn,
+                                    const float* wn, int* pcount, float* div, float* rhs, float* pa, float* pb,
+                                    bool zero_init, uint8_t* brick_active, double* part_b2, int* part_nf);
+// One CTA per scene: ||b||^2 and fluid count; sets live[s] = 1.
+cudaError_t launch_batch_b2_finalize(cudaStream_t st, const BatchIndex& bi, const double* part_b2, const int* part_nf,
+                                     SolveState* ss, int* live);
+cudaError_t launch_batch_project(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int8_t* type,
+                                 const float* p, const float* density, float* u, float* v, float* w, uint8_t* has);
+cudaError_t launch_batch_extrapolate(cudaStream_t st, const BatchIndex& bi, int total, int grid, const float* ui,
+                                     const float* vi, const float* wi, const uint8_t* hi, float* uo, float* vo,
+                                     float* wo, uint8_t* ho);
+// One flat Jacobi sweep of every scene with live[s] != 0 (sz % 4 == 0).
+cudaError_t launch_batch_jacobi_flat(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* live,
+                                     const float* pin, float* pout, const float* rhs, const int8_t* type,
+                                     const uint8_t* brick_active);
+cudaError_t launch_batch_resid_flat(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* live,
+                                    const float* p, const float* rhs, const int8_t* type,
+                                    const uint8_t* brick_active, double* part);
+// Per live scene: residual, stop decision (live[s] = continue).
+cudaError_t launch_batch_resid_finalize(cudaStream_t st, const BatchIndex& bi, const double* part, SolveState* ss,
+                                        int* live, int sweeps, double tol, int max_iters);
+// Loop condition of the batched solve: any scene still live.
+cudaError_t launch_batch_solve_condition(cudaStream_t st, const int* live, int n_scenes,
+                                         unsigned long long cond_handle);
+
 // ---- FP64 PCG (k_pcg.cu) ----------------------------------------------------
 cudaError_t launch_pcg_apply(cudaStream_t st, const Dims& d, const int8_t* type, const double* in,
                              double* out);  // out = A in

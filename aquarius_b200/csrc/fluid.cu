@@ -16,18 +16,13 @@
 #include <vector>
 
 #include "../../include/aquarius_b200.h"
-#include "aq_kernels.cuh"
+#include "fluid_impl.cuh"
 
 using namespace aqb;
 
 namespace {
 
 thread_local std::string g_last_error;
-
-aq_status fail(aq_status st, const std::string& msg) {
-  g_last_error = msg;
-  return st;
-}
 
 #define AQ_CUDA(call)                                                                            \
   do {                                                                                           \
@@ -154,119 +149,6 @@ aq_status aqb::set_last_error(aq_status st, const std::string& msg) {
 }
 
 // =================================================================== fluid
-struct aq_fluid {
-  aq_config cfg{};
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  cudaStream_t side = nullptr;  // body capture
-  bool own_stream = false;
-  Dims d{};
-  StepParams sp{};
-  int n = 0;
-  bool multiphase = false;
-  int phase = 0;
-  double time = 0.0;
-  int nv_cur = 2, has_cur = 2;  // which buffer holds newVelocity / has bits
-  // Stage 1 is fused with the sort; a following stage-2 call then has no work.
-  bool sorted_by_stage1 = false;
-
-  Particles cur{}, tmp{};
-  int *key = nullptr, *slot = nullptr, *perm_u = nullptr, *sort_index = nullptr;
-  int *count = nullptr, *off = nullptr, *tile_sums = nullptr;
-  float *u0 = nullptr, *v0 = nullptr, *w0 = nullptr;
-  float *un1 = nullptr, *vn1 = nullptr, *wn1 = nullptr;
-  float *un2 = nullptr, *vn2 = nullptr, *wn2 = nullptr;
-  uint8_t *h1 = nullptr, *h2 = nullptr;
-  int8_t* type = nullptr;
-  float *density = nullptr, *div = nullptr, *rhs = nullptr, *pa = nullptr, *pb = nullptr;
-  int* pcount = nullptr;
-  float4 *vf = nullptr, *nvf = nullptr, *nvf2 = nullptr;
-  uint8_t* bact = nullptr;
-  double* part_b2 = nullptr;
-  int* part_nf = nullptr;
-  int nbricks = 0;
-  double* jpart = nullptr;
-  int jpart_cap = 0;
-  SolveState* ss = nullptr;
-  SolveState* ss_host = nullptr;
-  // persistent solve
-  int* items = nullptr;
-  int* n_items = nullptr;
-  unsigned int* bar = nullptr;
-  double* ppart = nullptr;
-  int ctas = 0;
-
-  JacobiPlan plan{4, 16, 32};
-  cudaGraphExec_t exec = nullptr;
-  bool use_graph = true;
-  int graph_launches = 0;  // launches outside the residual loop
-  int body_launches = 0;   // launches per residual-loop iteration
-
-  std::vector<void*> allocs;
-  // PCG scratch (lazily allocated)
-  double *pcg_b = nullptr, *pcg_x = nullptr, *pcg_r = nullptr, *pcg_z = nullptr, *pcg_p = nullptr,
-         *pcg_q = nullptr, *pcg_part = nullptr;
-
-  ~aq_fluid() {
-    if (device >= 0) cudaSetDevice(device);
-    if (stream) cudaStreamSynchronize(stream);
-    if (exec) cudaGraphExecDestroy(exec);
-    for (void* p : allocs) cudaFree(p);
-    if (ss_host) cudaFreeHost(ss_host);
-    if (side) cudaStreamDestroy(side);
-    if (own_stream && stream) cudaStreamDestroy(stream);
-  }
-
-  template <typename T>
-  aq_status alloc(T** p, size_t count_) {
-    void* q = nullptr;
-    const size_t bytes = count_ * sizeof(T) > 0 ? count_ * sizeof(T) : 16;
-    cudaError_t e = cudaMalloc(&q, bytes);
-    if (e != cudaSuccess)
-      return fail(e == cudaErrorMemoryAllocation ? AQ_ERR_OUT_OF_MEMORY : AQ_ERR_CUDA,
-                  std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    allocs.push_back(q);
-    *p = (T*)q;
-    e = cudaMemsetAsync(q, 0, bytes, stream);
-    if (e != cudaSuccess) return fail(AQ_ERR_CUDA, cudaGetErrorString(e));
-    return AQ_OK;
-  }
-
-  float* nvx(int which) const { return which == 1 ? un1 : un2; }
-  float* nvy(int which) const { return which == 1 ? vn1 : vn2; }
-  float* nvz(int which) const { return which == 1 ? wn1 : wn2; }
-  uint8_t* hb(int which) const { return which == 1 ? h1 : h2; }
-
-  aq_status allocate();
-  aq_status seed_and_init();
-  // stage enqueues (eager or under capture)
-  aq_status enq_particles(bool move);
-  aq_status enq_p2g(bool forces);
-  aq_status enq_divergence();
-  aq_status enq_solve_fixed(int sweeps);
-  aq_status enq_solve_body(bool set_cond, unsigned long long handle, int* launches);
-  aq_status enq_solve_residual_eager();
-  aq_status enq_project();
-  aq_status enq_extrapolate();
-  aq_status enq_diffuse();
-  aq_status run_stage(int stage);
-  aq_status enq_pre_solve();
-  aq_status enq_post_solve();
-  aq_status build_graph();
-  aq_status step(int nsteps);
-  aq_status upload(const aq_host_state* s);
-  aq_status download(aq_host_state* s);
-  aq_status derive_from_state(const std::vector<int>& content, const std::vector<float>& divv,
-                              const std::vector<float>& dens);
-  int count_jacobi_launches(int sweeps) const;
-  void invalidate_graph() {
-    if (exec) {
-      cudaGraphExecDestroy(exec);
-      exec = nullptr;
-    }
-  }
-};
-
 // ------------------------------------------------------------- allocation
 aq_status aq_fluid::allocate() {
   const size_t N = (size_t)n, C = (size_t)d.C, F = (size_t)d.F;
@@ -784,6 +666,7 @@ aq_status aq_fluid::download(aq_host_state* s) {
   if (s->cell_start || s->cell_end || s->particle_hash) {
     std::vector<int> o(C + 1);
     AQ_TRY(get(o.data(), off, 4 * (C + 1)));
+    for (size_t c = 0; c <= C; ++c) o[c] -= index_base;
     for (size_t c = 0; c < C; ++c) {
       const bool occ = o[c + 1] > o[c];
       if (s->cell_start) s->cell_start[c] = occ ? o[c] : -1;
@@ -792,7 +675,11 @@ aq_status aq_fluid::download(aq_host_state* s) {
         for (int k = o[c]; k < o[c + 1]; ++k) s->particle_hash[k] = (int)c;
     }
   }
-  if (s->sort_index && N) AQ_TRY(get(s->sort_index, sort_index, 4 * N));
+  if (s->sort_index && N) {
+    AQ_TRY(get(s->sort_index, sort_index, 4 * N));
+    if (index_base)
+      for (size_t i = 0; i < N; ++i) s->sort_index[i] -= index_base;
+  }
   return AQ_OK;
 }
 

@@ -21,15 +21,15 @@ __device__ __forceinline__ float hat1(float r) { return fmaxf(0.f, 1.f - fabsf(r
 // Weights use positions in cell units, q = p/h; the reference evaluates
 // (p - face*h)/h with approximate division (-use_fast_math).
 template <bool FORCES, bool MULTI>
-__global__ void __launch_bounds__(256) k_p2g(Dims d, StepParams sp, Particles cur, const int* __restrict__ off,
-                                            float* __restrict__ u0, float* __restrict__ v0,
-                                            float* __restrict__ w0, float* __restrict__ un,
-                                            float* __restrict__ vn, float* __restrict__ wn,
-                                            int8_t* __restrict__ type, float* __restrict__ density,
-                                            float4* __restrict__ vf, float4* __restrict__ nvf) {
-  const int z = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * 8 + threadIdx.y;
-  const int x = blockIdx.z;
+__device__ __forceinline__ void p2g_body(const Dims& d, const StepParams& sp, const Particles& cur,
+                                         const int* __restrict__ off, float* __restrict__ u0, float* __restrict__ v0,
+                                         float* __restrict__ w0, float* __restrict__ un, float* __restrict__ vn,
+                                         float* __restrict__ wn, int8_t* __restrict__ type,
+                                         float* __restrict__ density, float4* __restrict__ vf,
+                                         float4* __restrict__ nvf, int bx, int by, int bz) {
+  const int z = bx * 32 + threadIdx.x;
+  const int y = by * 8 + threadIdx.y;
+  const int x = bz;
   if (z >= d.sz || y >= d.sy) return;
   const float fx = (float)x, fy = (float)y, fz = (float)z;
   const float fxh = fx + 0.5f, fyh = fy + 0.5f, fzh = fz + 0.5f;
@@ -128,16 +128,35 @@ __global__ void __launch_bounds__(256) k_p2g(Dims d, StepParams sp, Particles cu
   un[ni] = nu; vn[ni] = nv; wn[ni] = nw;
 }
 
+template <bool FORCES, bool MULTI>
+__global__ void __launch_bounds__(256) k_p2g(Dims d, StepParams sp, Particles cur, const int* __restrict__ off,
+                                            float* __restrict__ u0, float* __restrict__ v0,
+                                            float* __restrict__ w0, float* __restrict__ un,
+                                            float* __restrict__ vn, float* __restrict__ wn,
+                                            int8_t* __restrict__ type, float* __restrict__ density,
+                                            float4* __restrict__ vf, float4* __restrict__ nvf) {
+  p2g_body<FORCES, MULTI>(d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf, blockIdx.x, blockIdx.y,
+                          blockIdx.z);
+}
+
+// node-grid virtual block -> (z block, y block, x plane) of one scene
+__device__ __forceinline__ void node_block_coords(const Dims& d, int local, int& bx, int& by, int& bz) {
+  const int gz = (d.sz + 31) / 32, gy = (d.sy + 7) / 8;
+  bx = local % gz;
+  const int t = local / gz;
+  by = t % gy;
+  bz = t / gy;
+}
+
 // Nodes with a coordinate equal to s: never reset by resetCellImpl, so they
 // persist across steps; gravity reaches them only from the fluid cell below
 // along that axis and only where fixBoundary left them AIR.
-__global__ void __launch_bounds__(256) k_slayer(Dims d, StepParams sp, const int8_t* __restrict__ type,
-                                               const float* __restrict__ su, const float* __restrict__ sv,
-                                               const float* __restrict__ sw, float* __restrict__ u1,
-                                               float* __restrict__ v1, float* __restrict__ w1,
-                                               float* __restrict__ u2, float* __restrict__ v2,
-                                               float* __restrict__ w2) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void slayer_body(const Dims& d, const StepParams& sp, const int8_t* __restrict__ type,
+                                            const float* __restrict__ su, const float* __restrict__ sv,
+                                            const float* __restrict__ sw, float* __restrict__ u1,
+                                            float* __restrict__ v1, float* __restrict__ w1, float* __restrict__ u2,
+                                            float* __restrict__ v2, float* __restrict__ w2, int block) {
+  int t = block * blockDim.x + threadIdx.x;
   const int na = (d.sy + 1) * (d.sz + 1), nb = d.sx * (d.sz + 1), nc = d.sx * d.sy;
   int x, y, z;
   if (t < na) {
@@ -176,19 +195,28 @@ __global__ void __launch_bounds__(256) k_slayer(Dims d, StepParams sp, const int
   u2[ni] = u; v2[ni] = v; w2[ni] = w;
 }
 
-// One 8x8x8 brick per CTA (threads z,y,x).
-__global__ void __launch_bounds__(512) k_divergence(Dims d, const int* __restrict__ off,
-                                                   const int8_t* __restrict__ type,
-                                                   const float* __restrict__ density,
-                                                   const float* __restrict__ un, const float* __restrict__ vn,
-                                                   const float* __restrict__ wn, int* __restrict__ pcount,
-                                                   float* __restrict__ div_out, float* __restrict__ rhs,
-                                                   float* __restrict__ pa, float* __restrict__ pb, int zero_init,
-                                                   uint8_t* __restrict__ brick_active,
-                                                   double* __restrict__ part_b2, int* __restrict__ part_nf) {
-  const int z = blockIdx.x * kBrick + threadIdx.x;
-  const int y = blockIdx.y * kBrick + threadIdx.y;
-  const int x = blockIdx.z * kBrick + threadIdx.z;
+__global__ void __launch_bounds__(256) k_slayer(Dims d, StepParams sp, const int8_t* __restrict__ type,
+                                               const float* __restrict__ su, const float* __restrict__ sv,
+                                               const float* __restrict__ sw, float* __restrict__ u1,
+                                               float* __restrict__ v1, float* __restrict__ w1,
+                                               float* __restrict__ u2, float* __restrict__ v2,
+                                               float* __restrict__ w2) {
+  slayer_body(d, sp, type, su, sv, sw, u1, v1, w1, u2, v2, w2, blockIdx.x);
+}
+
+// One 8x8x8 brick per CTA (threads z,y,x); (bx,by,bz) = brick coordinates
+// along z, y, x.
+__device__ __forceinline__ void divergence_body(const Dims& d, const int* __restrict__ off,
+                                                const int8_t* __restrict__ type, const float* __restrict__ density,
+                                                const float* __restrict__ un, const float* __restrict__ vn,
+                                                const float* __restrict__ wn, int* __restrict__ pcount,
+                                                float* __restrict__ div_out, float* __restrict__ rhs,
+                                                float* __restrict__ pa, float* __restrict__ pb, int zero_init,
+                                                uint8_t* __restrict__ brick_active, double* __restrict__ part_b2,
+                                                int* __restrict__ part_nf, int bx, int by, int bz) {
+  const int z = bx * kBrick + threadIdx.x;
+  const int y = by * kBrick + threadIdx.y;
+  const int x = bz * kBrick + threadIdx.z;
   double b2 = 0.0;
   int nf = 0;
   if (x < d.sx && y < d.sy && z < d.sz) {
@@ -222,16 +250,28 @@ __global__ void __launch_bounds__(512) k_divergence(Dims d, const int* __restric
     double tb = 0.0;
     int tn = 0;
     for (int k = 0; k < 16; ++k) { tb += sb[k]; tn += sn[k]; }
-    const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    const int bid = (bz * d.by + by) * d.bz + bx;
     part_b2[bid] = tb;
     part_nf[bid] = tn;
-    brick_active[(blockIdx.z * d.by + blockIdx.y) * d.bz + blockIdx.x] = any ? 1 : 0;
+    brick_active[bid] = any ? 1 : 0;
   }
 }
 
-__global__ void __launch_bounds__(1024) k_b2_finalize(const double* __restrict__ part_b2,
-                                                     const int* __restrict__ part_nf, int nb,
-                                                     SolveState* __restrict__ ss) {
+__global__ void __launch_bounds__(512) k_divergence(Dims d, const int* __restrict__ off,
+                                                   const int8_t* __restrict__ type,
+                                                   const float* __restrict__ density,
+                                                   const float* __restrict__ un, const float* __restrict__ vn,
+                                                   const float* __restrict__ wn, int* __restrict__ pcount,
+                                                   float* __restrict__ div_out, float* __restrict__ rhs,
+                                                   float* __restrict__ pa, float* __restrict__ pb, int zero_init,
+                                                   uint8_t* __restrict__ brick_active,
+                                                   double* __restrict__ part_b2, int* __restrict__ part_nf) {
+  divergence_body(d, off, type, density, un, vn, wn, pcount, div_out, rhs, pa, pb, zero_init, brick_active, part_b2,
+                  part_nf, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+__device__ __forceinline__ void b2_finalize_body(const double* __restrict__ part_b2, const int* __restrict__ part_nf,
+                                                 int nb, SolveState* __restrict__ ss) {
   __shared__ double sb[1024];
   __shared__ int sn[1024];
   double b = 0.0;
@@ -256,14 +296,20 @@ __global__ void __launch_bounds__(1024) k_b2_finalize(const double* __restrict__
   }
 }
 
+__global__ void __launch_bounds__(1024) k_b2_finalize(const double* __restrict__ part_b2,
+                                                     const int* __restrict__ part_nf, int nb,
+                                                     SolveState* __restrict__ ss) {
+  b2_finalize_body(part_b2, part_nf, nb, ss);
+}
+
 // updateVelocityWithPressureImpl (Fluid/Fluid_3D_kernels.cu:118-207).
-__global__ void __launch_bounds__(256) k_project(Dims d, const int8_t* __restrict__ type,
-                                                const float* __restrict__ p, const float* __restrict__ dens,
-                                                float* __restrict__ u, float* __restrict__ v,
-                                                float* __restrict__ w, uint8_t* __restrict__ has) {
-  const int z = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * 8 + threadIdx.y;
-  const int x = blockIdx.z;
+__device__ __forceinline__ void project_body(const Dims& d, const int8_t* __restrict__ type,
+                                             const float* __restrict__ p, const float* __restrict__ dens,
+                                             float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+                                             uint8_t* __restrict__ has, int bx, int by, int bz) {
+  const int z = bx * 32 + threadIdx.x;
+  const int y = by * 8 + threadIdx.y;
+  const int x = bz;
   if (z >= d.sz || y >= d.sy) return;
   const int c = cell_index(d, x, y, z), ni = node_index(d, x, y, z);
   const bool t = type[c] == kFluid;
@@ -304,18 +350,25 @@ __global__ void __launch_bounds__(256) k_project(Dims d, const int8_t* __restric
   has[ni] = hb;
 }
 
+__global__ void __launch_bounds__(256) k_project(Dims d, const int8_t* __restrict__ type,
+                                                const float* __restrict__ p, const float* __restrict__ dens,
+                                                float* __restrict__ u, float* __restrict__ v,
+                                                float* __restrict__ w, uint8_t* __restrict__ has) {
+  project_body(d, type, p, dens, u, v, w, has, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // extrapolateVelocityByOne (Fluid/Fluid_3D_kernels.cu:210-422), reading the
 // previous pass only.  Neighbour order: left, down, back, right, up, front;
 // each neighbour counts if it has the component and its velocity along the
 // neighbour direction passes the epsilon test.
-__global__ void __launch_bounds__(256) k_extrapolate(Dims d, const float* __restrict__ ui,
-                                                    const float* __restrict__ vi, const float* __restrict__ wi,
-                                                    const uint8_t* __restrict__ hi, float* __restrict__ uo,
-                                                    float* __restrict__ vo, float* __restrict__ wo,
-                                                    uint8_t* __restrict__ ho) {
-  const int z = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * 8 + threadIdx.y;
-  const int x = blockIdx.z;
+__device__ __forceinline__ void extrapolate_body(const Dims& d, const float* __restrict__ ui,
+                                                 const float* __restrict__ vi, const float* __restrict__ wi,
+                                                 const uint8_t* __restrict__ hi, float* __restrict__ uo,
+                                                 float* __restrict__ vo, float* __restrict__ wo,
+                                                 uint8_t* __restrict__ ho, int bx, int by, int bz) {
+  const int z = bx * 32 + threadIdx.x;
+  const int y = by * 8 + threadIdx.y;
+  const int x = bz;
   if (z >= d.sz || y >= d.sy) return;
   const float eps = (float)(-1 + 1e-6);
   const int ni = node_index(d, x, y, z);
@@ -361,6 +414,107 @@ __global__ void __launch_bounds__(256) k_extrapolate(Dims d, const float* __rest
   ho[ni] = h;
 }
 
+__global__ void __launch_bounds__(256) k_extrapolate(Dims d, const float* __restrict__ ui,
+                                                    const float* __restrict__ vi, const float* __restrict__ wi,
+                                                    const uint8_t* __restrict__ hi, float* __restrict__ uo,
+                                                    float* __restrict__ vo, float* __restrict__ wo,
+                                                    uint8_t* __restrict__ ho) {
+  extrapolate_body(d, ui, vi, wi, hi, uo, vo, wo, ho, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// ------------------------------------------------------------------ batched
+// Each batched kernel walks the virtual blocks of all scenes (grid-stride);
+// every virtual block belongs to one scene and runs the same body as the
+// single-scene kernel on that scene's slice of the batch arrays.
+
+template <bool FORCES>
+__global__ void __launch_bounds__(256) kb_p2g(BatchIndex bi, int total, Particles cur, const int* __restrict__ off,
+                                             float* __restrict__ u0, float* __restrict__ v0, float* __restrict__ w0,
+                                             float* __restrict__ un, float* __restrict__ vn, float* __restrict__ wn,
+                                             int8_t* __restrict__ type, float* __restrict__ density) {
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    const int s = find_scene(bi.nodes, bi.n_scenes, vb);
+    const SceneDesc& S = bi.scenes[s];
+    int bx, by, bz;
+    node_block_coords(S.d, vb - bi.nodes[s], bx, by, bz);
+    p2g_body<FORCES, false>(S.d, S.sp, cur, off + S.c_off, u0 + S.f_off, v0 + S.f_off, w0 + S.f_off, un + S.f_off,
+                            vn + S.f_off, wn + S.f_off, type + S.c_off, density + S.c_off, nullptr, nullptr, bx, by,
+                            bz);
+  }
+}
+
+__global__ void __launch_bounds__(256) kb_slayer(BatchIndex bi, int total, const int8_t* __restrict__ type,
+                                                const float* __restrict__ su, const float* __restrict__ sv,
+                                                const float* __restrict__ sw, float* __restrict__ u1,
+                                                float* __restrict__ v1, float* __restrict__ w1, float* __restrict__ u2,
+                                                float* __restrict__ v2, float* __restrict__ w2) {
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    const int s = find_scene(bi.slayer, bi.n_scenes, vb);
+    const SceneDesc& S = bi.scenes[s];
+    const int o = S.f_off;
+    slayer_body(S.d, S.sp, type + S.c_off, su + o, sv + o, sw + o, u1 + o, v1 + o, w1 + o, u2 + o, v2 + o, w2 + o,
+                vb - bi.slayer[s]);
+  }
+}
+
+__global__ void __launch_bounds__(512) kb_divergence(BatchIndex bi, int total, const int* __restrict__ off,
+                                                    const int8_t* __restrict__ type, const float* __restrict__ density,
+                                                    const float* __restrict__ un, const float* __restrict__ vn,
+                                                    const float* __restrict__ wn, int* __restrict__ pcount,
+                                                    float* __restrict__ div_out, float* __restrict__ rhs,
+                                                    float* __restrict__ pa, float* __restrict__ pb, int zero_init,
+                                                    uint8_t* __restrict__ brick_active, double* __restrict__ part_b2,
+                                                    int* __restrict__ part_nf) {
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    const int s = find_scene(bi.bricks, bi.n_scenes, vb);
+    const SceneDesc& S = bi.scenes[s];
+    const int local = vb - bi.bricks[s];
+    const int bx = local % S.d.bz, by = (local / S.d.bz) % S.d.by, bz = local / (S.d.bz * S.d.by);
+    const int c = S.c_off, f = S.f_off;
+    divergence_body(S.d, off + c, type + c, density + c, un + f, vn + f, wn + f, pcount + c, div_out + c, rhs + c,
+                    pa + c, pb + c, zero_init, brick_active + S.br_off, part_b2 + S.br_off, part_nf + S.br_off, bx,
+                    by, bz);
+  }
+}
+
+// One CTA per scene; also marks every scene's pressure solve as running.
+__global__ void __launch_bounds__(1024) kb_b2_finalize(BatchIndex bi, const double* __restrict__ part_b2,
+                                                      const int* __restrict__ part_nf, SolveState* __restrict__ ss,
+                                                      int* __restrict__ live) {
+  const SceneDesc& S = bi.scenes[blockIdx.x];
+  b2_finalize_body(part_b2 + S.br_off, part_nf + S.br_off, S.d.bx * S.d.by * S.d.bz, ss + blockIdx.x);
+  if (threadIdx.x == 0) live[blockIdx.x] = 1;
+}
+
+__global__ void __launch_bounds__(256) kb_project(BatchIndex bi, int total, const int8_t* __restrict__ type,
+                                                 const float* __restrict__ p, const float* __restrict__ dens,
+                                                 float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+                                                 uint8_t* __restrict__ has) {
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    const int s = find_scene(bi.nodes, bi.n_scenes, vb);
+    const SceneDesc& S = bi.scenes[s];
+    int bx, by, bz;
+    node_block_coords(S.d, vb - bi.nodes[s], bx, by, bz);
+    project_body(S.d, type + S.c_off, p + S.c_off, dens + S.c_off, u + S.f_off, v + S.f_off, w + S.f_off,
+                 has + S.f_off, bx, by, bz);
+  }
+}
+
+__global__ void __launch_bounds__(256) kb_extrapolate(BatchIndex bi, int total, const float* __restrict__ ui,
+                                                     const float* __restrict__ vi, const float* __restrict__ wi,
+                                                     const uint8_t* __restrict__ hi, float* __restrict__ uo,
+                                                     float* __restrict__ vo, float* __restrict__ wo,
+                                                     uint8_t* __restrict__ ho) {
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    const int s = find_scene(bi.nodes, bi.n_scenes, vb);
+    const SceneDesc& S = bi.scenes[s];
+    int bx, by, bz;
+    node_block_coords(S.d, vb - bi.nodes[s], bx, by, bz);
+    const int o = S.f_off;
+    extrapolate_body(S.d, ui + o, vi + o, wi + o, hi + o, uo + o, vo + o, wo + o, ho + o, bx, by, bz);
+  }
+}
+
 // diffusionJacobiImpl (Fluid/Fluid_3D_kernels.cu:520-556), ping-pong.  Air
 // cells keep their fractions (their pressure is already 0 after the solve).
 __global__ void __launch_bounds__(256) k_diffuse(Dims d, const int8_t* __restrict__ type, float lambda,
@@ -392,7 +546,55 @@ __global__ void __launch_bounds__(256) k_diffuse(Dims d, const int8_t* __restric
 
 inline dim3 node_grid(const Dims& d) { return dim3((d.sz + 31) / 32, (d.sy + 7) / 8, d.sx); }
 
+inline int clamp_grid(int grid, int total) { return grid < total ? grid : (total > 0 ? total : 1); }
+
 }  // namespace
+
+cudaError_t launch_batch_p2g(cudaStream_t st, const BatchIndex& bi, int total, int grid, bool forces, Particles cur,
+                             const int* off, float* u0, float* v0, float* w0, float* un, float* vn, float* wn,
+                             int8_t* type, float* density) {
+  if (forces)
+    kb_p2g<true><<<clamp_grid(grid, total), dim3(32, 8), 0, st>>>(bi, total, cur, off, u0, v0, w0, un, vn, wn, type, density);
+  else
+    kb_p2g<false><<<clamp_grid(grid, total), dim3(32, 8), 0, st>>>(bi, total, cur, off, u0, v0, w0, un, vn, wn, type, density);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_slayer(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int8_t* type,
+                                const float* su, const float* sv, const float* sw, float* u1, float* v1, float* w1,
+                                float* u2, float* v2, float* w2) {
+  kb_slayer<<<clamp_grid(grid, total), 256, 0, st>>>(bi, total, type, su, sv, sw, u1, v1, w1, u2, v2, w2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_divergence(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* off,
+                                    const int8_t* type, const float* density, const float* un, const float* vn,
+                                    const float* wn, int* pcount, float* div, float* rhs, float* pa, float* pb,
+                                    bool zero_init, uint8_t* brick_active, double* part_b2, int* part_nf) {
+  kb_divergence<<<clamp_grid(grid, total), dim3(kBrick, kBrick, kBrick), 0, st>>>(
+      bi, total, off, type, density, un, vn, wn, pcount, div, rhs, pa, pb, zero_init ? 1 : 0, brick_active, part_b2,
+      part_nf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_b2_finalize(cudaStream_t st, const BatchIndex& bi, const double* part_b2, const int* part_nf,
+                                     SolveState* ss, int* live) {
+  kb_b2_finalize<<<bi.n_scenes, 1024, 0, st>>>(bi, part_b2, part_nf, ss, live);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_project(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int8_t* type,
+                                 const float* p, const float* density, float* u, float* v, float* w, uint8_t* has) {
+  kb_project<<<clamp_grid(grid, total), dim3(32, 8), 0, st>>>(bi, total, type, p, density, u, v, w, has);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_extrapolate(cudaStream_t st, const BatchIndex& bi, int total, int grid, const float* ui,
+                                     const float* vi, const float* wi, const uint8_t* hi, float* uo, float* vo,
+                                     float* wo, uint8_t* ho) {
+  kb_extrapolate<<<clamp_grid(grid, total), dim3(32, 8), 0, st>>>(bi, total, ui, vi, wi, hi, uo, vo, wo, ho);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_p2g(cudaStream_t st, const Dims& d, const StepParams& sp, bool forces, Particles cur,
                        const int* off, int n, float* u0, float* v0, float* w0, float* un, float* vn,

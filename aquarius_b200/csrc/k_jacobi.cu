@@ -185,20 +185,21 @@ __device__ __forceinline__ bool warp_active(const Dims& d, const uint8_t* __rest
 
 __device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
+__host__ __device__ __forceinline__ int resid_flat_parts_dev(const Dims& d) {
+  return ((d.sz / 4 + 31) / 32) * ((d.sy + 7) / 8) * d.sx;
+}
+
+// (bx, by, bz) = (z-quad block, row block, x-plane group) of the flat grid;
+// the caller has checked that the warp's rows hold fluid (warp_active).
 template <int XS>
-__global__ void __launch_bounds__(256) k_jacobi_flat(Dims d, const float* __restrict__ pin,
-                                                    float* __restrict__ pout, const float* __restrict__ rhs,
-                                                    const int8_t* __restrict__ type,
-                                                    const uint8_t* __restrict__ bact) {
+__device__ __forceinline__ void jacobi_flat_body(const Dims& d, const float* __restrict__ pin,
+                                                 float* __restrict__ pout, const float* __restrict__ rhs,
+                                                 const int8_t* __restrict__ type, int bx, int by, int bz) {
   const int lane = threadIdx.x;
-  const int z = (blockIdx.x * 32 + lane) * 4;
-  const int y = blockIdx.y * 8 + threadIdx.y;
-  const int x0 = blockIdx.z * XS;
+  const int z = (bx * 32 + lane) * 4;
+  const int y = by * 8 + threadIdx.y;
+  const int x0 = bz * XS;
   const int x1 = min(x0 + XS, d.sx);
-  const bool act = y < d.sy && warp_active(d, bact, x0, x1, y, blockIdx.x * 16);
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;");
-  if (!act) return;
   const bool in = z < d.sz;
   const int plane = d.sy * d.sz;
   const int col = y * d.sz + z;
@@ -254,18 +255,35 @@ __global__ void __launch_bounds__(256) k_jacobi_flat(Dims d, const float* __rest
   }
 }
 
+// Programmatic dependent launch: the activity bricks were written two or more
+// launches earlier, so only the pressure reads wait for the previous sweep.
+template <int XS>
+__global__ void __launch_bounds__(256) k_jacobi_flat(Dims d, const float* __restrict__ pin,
+                                                    float* __restrict__ pout, const float* __restrict__ rhs,
+                                                    const int8_t* __restrict__ type,
+                                                    const uint8_t* __restrict__ bact) {
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  const int x0 = blockIdx.z * XS;
+  const bool act = y < d.sy && warp_active(d, bact, x0, min(x0 + XS, d.sx), y, blockIdx.x * 16);
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  if (!act) return;
+  jacobi_flat_body<XS>(d, pin, pout, rhs, type, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // FP64 residual ||b - A p||^2 of one iterate over fluid cells, in the flat
 // layout (one x plane x 8 rows x 128 z per block); per-block partial sums in
 // a fixed order.
-__global__ void __launch_bounds__(256) k_resid_flat(Dims d, const float* __restrict__ p,
-                                                   const float* __restrict__ rhs, const int8_t* __restrict__ type,
-                                                   const uint8_t* __restrict__ bact, double* __restrict__ part) {
+__device__ __forceinline__ void resid_flat_body(const Dims& d, const float* __restrict__ p,
+                                                const float* __restrict__ rhs, const int8_t* __restrict__ type,
+                                                const uint8_t* __restrict__ bact, double* __restrict__ part, int bx,
+                                                int by, int bz) {
   const int lane = threadIdx.x;
-  const int z = (blockIdx.x * 32 + lane) * 4;
-  const int y = blockIdx.y * 8 + threadIdx.y;
-  const int x = blockIdx.z;
-  const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-  const bool act = y < d.sy && warp_active(d, bact, x, x + 1, y, blockIdx.x * 16);
+  const int z = (bx * 32 + lane) * 4;
+  const int y = by * 8 + threadIdx.y;
+  const int x = bz;
+  const int bid = (bz * ((d.sy + 7) / 8) + by) * ((d.sz / 4 + 31) / 32) + bx;
+  const bool act = y < d.sy && warp_active(d, bact, x, x + 1, y, bx * 16);
   double acc = 0.0;
   const bool in = act && z < d.sz;
   const int plane = d.sy * d.sz;
@@ -313,6 +331,12 @@ __global__ void __launch_bounds__(256) k_resid_flat(Dims d, const float* __restr
     for (int k = 0; k < 8; ++k) t += s_red[k];
     part[bid] = t;
   }
+}
+
+__global__ void __launch_bounds__(256) k_resid_flat(Dims d, const float* __restrict__ p,
+                                                   const float* __restrict__ rhs, const int8_t* __restrict__ type,
+                                                   const uint8_t* __restrict__ bact, double* __restrict__ part) {
+  resid_flat_body(d, p, rhs, type, bact, part, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 
@@ -600,10 +624,10 @@ __global__ void __launch_bounds__(1024) k_persist_solve(Dims d, float* __restric
   }
 }
 
-__global__ void __launch_bounds__(1024) k_resid_finalize(const double* __restrict__ part, int nparts,
-                                                        SolveState* __restrict__ ss, int sweeps, double tol,
-                                                        int max_iters, int set_cond,
-                                                        cudaGraphConditionalHandle handle) {
+// Returns (in thread 0) whether the solve should continue.
+__device__ __forceinline__ bool resid_finalize_body(const double* __restrict__ part, int nparts,
+                                                    SolveState* __restrict__ ss, int sweeps, double tol,
+                                                    int max_iters) {
   __shared__ double sb[1024];
   double a = 0.0;
   for (int i = threadIdx.x; i < nparts; i += 1024) a += part[i];
@@ -626,11 +650,82 @@ __global__ void __launch_bounds__(1024) k_resid_finalize(const double* __restric
     if (!finite) ss->nonfinite = 1;
     const bool conv = finite && rel <= tol;
     ss->converged = conv ? 1 : 0;
-    if (set_cond) {
-      const bool more = finite && !conv && ss->iterations < max_iters;
-      cudaGraphSetConditional(handle, more ? 1u : 0u);
-    }
+    return finite && !conv && ss->iterations < max_iters;
   }
+  return false;
+}
+
+__global__ void __launch_bounds__(1024) k_resid_finalize(const double* __restrict__ part, int nparts,
+                                                        SolveState* __restrict__ ss, int sweeps, double tol,
+                                                        int max_iters, int set_cond,
+                                                        cudaGraphConditionalHandle handle) {
+  const bool more = resid_finalize_body(part, nparts, ss, sweeps, tol, max_iters);
+  if (threadIdx.x == 0 && set_cond) cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+// ------------------------------------------------------------------- batched
+// One flat sweep over every scene whose solve is still running (live[s]);
+// a finished scene's pressure is left as it is.
+__device__ __forceinline__ void flat_block_coords(const Dims& d, int local, int& bx, int& by, int& bz) {
+  const int gz = (d.sz / 4 + 31) / 32, gy = (d.sy + 7) / 8;
+  bx = local % gz;
+  const int t = local / gz;
+  by = t % gy;
+  bz = t / gy;
+}
+
+__global__ void __launch_bounds__(256) kb_jacobi_flat(BatchIndex bi, int total, const int* __restrict__ live,
+                                                     const float* __restrict__ pin, float* __restrict__ pout,
+                                                     const float* __restrict__ rhs, const int8_t* __restrict__ type,
+                                                     const uint8_t* __restrict__ bact) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    const int s = find_scene(bi.flat, bi.n_scenes, vb);
+    if (!live[s]) continue;
+    const SceneDesc& S = bi.scenes[s];
+    int bx, by, bz;
+    flat_block_coords(S.d, vb - bi.flat[s], bx, by, bz);
+    const int y = by * 8 + threadIdx.y;
+    if (!(y < S.d.sy && warp_active(S.d, bact + S.br_off, bz, bz + 1, y, bx * 16))) continue;
+    const int c = S.c_off;
+    jacobi_flat_body<1>(S.d, pin + c, pout + c, rhs + c, type + c, bx, by, bz);
+  }
+}
+
+__global__ void __launch_bounds__(256) kb_resid_flat(BatchIndex bi, int total, const int* __restrict__ live,
+                                                    const float* __restrict__ p, const float* __restrict__ rhs,
+                                                    const int8_t* __restrict__ type, const uint8_t* __restrict__ bact,
+                                                    double* __restrict__ part) {
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    const int s = find_scene(bi.flat, bi.n_scenes, vb);
+    if (!live[s]) continue;
+    const SceneDesc& S = bi.scenes[s];
+    int bx, by, bz;
+    flat_block_coords(S.d, vb - bi.flat[s], bx, by, bz);
+    const int c = S.c_off;
+    resid_flat_body(S.d, p + c, rhs + c, type + c, bact + S.br_off, part + S.rp_off, bx, by, bz);
+    __syncthreads();  // s_red is reused by the next virtual block
+  }
+}
+
+// One CTA per scene; a finished scene keeps its record.
+__global__ void __launch_bounds__(1024) kb_resid_finalize(BatchIndex bi, const double* __restrict__ part,
+                                                         SolveState* __restrict__ ss, int* __restrict__ live,
+                                                         int sweeps, double tol, int max_iters) {
+  const int s = blockIdx.x;
+  if (!live[s]) return;
+  const SceneDesc& S = bi.scenes[s];
+  const bool more = resid_finalize_body(part + S.rp_off, resid_flat_parts_dev(S.d), ss + s, sweeps, tol, max_iters);
+  if (threadIdx.x == 0) live[s] = more ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(1024) kb_solve_condition(const int* __restrict__ live, int n_scenes,
+                                                          cudaGraphConditionalHandle handle) {
+  int any = 0;
+  for (int s = threadIdx.x; s < n_scenes; s += blockDim.x) any |= live[s];
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) cudaGraphSetConditional(handle, any ? 1u : 0u);
 }
 
 template <int L, bool RESID, int BY>
@@ -830,6 +925,45 @@ cudaError_t launch_resid_finalize(cudaStream_t st, const double* part, int npart
                                   unsigned long long cond_handle) {
   k_resid_finalize<<<1, 1024, 0, st>>>(part, nparts, ss, sweeps_done_per_call, tol, max_iters, set_cond ? 1 : 0,
                                        (cudaGraphConditionalHandle)cond_handle);
+  return cudaGetLastError();
+}
+
+}  // namespace aqb
+
+namespace aqb {
+
+cudaError_t launch_batch_jacobi_flat(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* live,
+                                     const float* pin, float* pout, const float* rhs, const int8_t* type,
+                                     const uint8_t* brick_active) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(grid < total ? grid : (total > 0 ? total : 1));
+  lc.blockDim = dim3(32, 8);
+  lc.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  return cudaLaunchKernelEx(&lc, kb_jacobi_flat, bi, total, live, pin, pout, rhs, type, brick_active);
+}
+
+cudaError_t launch_batch_resid_flat(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* live,
+                                    const float* p, const float* rhs, const int8_t* type,
+                                    const uint8_t* brick_active, double* part) {
+  kb_resid_flat<<<grid < total ? grid : (total > 0 ? total : 1), dim3(32, 8), 0, st>>>(bi, total, live, p, rhs, type,
+                                                                                     brick_active, part);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_resid_finalize(cudaStream_t st, const BatchIndex& bi, const double* part, SolveState* ss,
+                                        int* live, int sweeps, double tol, int max_iters) {
+  kb_resid_finalize<<<bi.n_scenes, 1024, 0, st>>>(bi, part, ss, live, sweeps, tol, max_iters);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_solve_condition(cudaStream_t st, const int* live, int n_scenes,
+                                         unsigned long long cond_handle) {
+  kb_solve_condition<<<1, 1024, 0, st>>>(live, n_scenes, (cudaGraphConditionalHandle)cond_handle);
   return cudaGetLastError();
 }
 

@@ -49,13 +49,16 @@ __device__ __forceinline__ float3 sample_velocity(const float* __restrict__ u, c
                      sample_node(w, d, x - 0.5f, y - 0.5f, z));
 }
 
+// Body shared by the single-scene kernel and the batched one.  Particle
+// arrays, grids and key/slot are the scene's own (pointers already offset);
+// keys are cell indices plus key_base (the scene's first cell in a batch).
 template <bool MOVE, bool MULTI>
-__global__ void __launch_bounds__(256) k_particles_advance(
-    Dims d, StepParams sp, Particles cur, Particles tmp, const float* __restrict__ u0,
+__device__ __forceinline__ void particles_advance_body(
+    const Dims& d, const StepParams& sp, const Particles& cur, const Particles& tmp, const float* __restrict__ u0,
     const float* __restrict__ v0, const float* __restrict__ w0, const float* __restrict__ un,
     const float* __restrict__ vn, const float* __restrict__ wn, const float4* __restrict__ nvf,
-    int* __restrict__ key, int* __restrict__ slot, int* __restrict__ count, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int* __restrict__ key, int* __restrict__ slot, int* __restrict__ count, int n, int key_base, int block) {
+  const int i = block * blockDim.x + threadIdx.x;
   const bool valid = i < n;
   int k = -1;
   if (valid) {
@@ -113,7 +116,7 @@ __global__ void __launch_bounds__(256) k_particles_advance(
     hx = min(max(hx, 0), d.sx - 1);
     hy = min(max(hy, 0), d.sy - 1);
     hz = min(max(hz, 0), d.sz - 1);
-    k = cell_index(d, hx, hy, hz);
+    k = key_base + cell_index(d, hx, hy, hz);
     key[i] = k;
   }
   // Warp-aggregated slot allocation: one atomic per distinct cell per warp.
@@ -125,6 +128,43 @@ __global__ void __launch_bounds__(256) k_particles_advance(
     if (lane == leader) base = atomicAdd(count + k, __popc(peers));
     base = __shfl_sync(peers, base, leader);
     slot[i] = base + __popc(peers & ((1u << lane) - 1u));
+  }
+}
+
+template <bool MOVE, bool MULTI>
+__global__ void __launch_bounds__(256) k_particles_advance(
+    Dims d, StepParams sp, Particles cur, Particles tmp, const float* __restrict__ u0,
+    const float* __restrict__ v0, const float* __restrict__ w0, const float* __restrict__ un,
+    const float* __restrict__ vn, const float* __restrict__ wn, const float4* __restrict__ nvf,
+    int* __restrict__ key, int* __restrict__ slot, int* __restrict__ count, int n) {
+  particles_advance_body<MOVE, MULTI>(d, sp, cur, tmp, u0, v0, w0, un, vn, wn, nvf, key, slot, count, n, 0,
+                                      blockIdx.x);
+}
+
+__device__ __forceinline__ Particles offset_particles(const Particles& p, int off) {
+  Particles q = p;
+  q.px += off; q.py += off; q.pz += off;
+  q.vx += off; q.vy += off; q.vz += off;
+  if (q.frac) q.frac += off;
+  return q;
+}
+
+// All scenes of a batch: grid-stride loop over virtual blocks, each block
+// belongs to one scene.
+template <bool MOVE>
+__global__ void __launch_bounds__(256) kb_particles_advance(BatchIndex bi, int total, Particles cur, Particles tmp,
+                                                           const float* __restrict__ u0, const float* __restrict__ v0,
+                                                           const float* __restrict__ w0, const float* __restrict__ un,
+                                                           const float* __restrict__ vn, const float* __restrict__ wn,
+                                                           int* __restrict__ key, int* __restrict__ slot,
+                                                           int* __restrict__ count) {
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    const int s = find_scene(bi.particles, bi.n_scenes, vb);
+    const SceneDesc S = bi.scenes[s];
+    particles_advance_body<MOVE, false>(S.d, S.sp, offset_particles(cur, S.p_off), offset_particles(tmp, S.p_off),
+                                        u0 + S.f_off, v0 + S.f_off, w0 + S.f_off, un + S.f_off, vn + S.f_off,
+                                        wn + S.f_off, nullptr, key + S.p_off, slot + S.p_off, count, S.n, S.c_off,
+                                        vb - bi.particles[s]);
   }
 }
 
@@ -274,6 +314,19 @@ cudaError_t launch_particles_advance(cudaStream_t st, const Dims& d, const StepP
     k_particles_advance<false, true><<<nb, 256, 0, st>>>(d, sp, cur, tmp, u0, v0, w0, un, vn, wn, nvf, key, slot, count, n);
   else
     k_particles_advance<false, false><<<nb, 256, 0, st>>>(d, sp, cur, tmp, u0, v0, w0, un, vn, wn, nvf, key, slot, count, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_particles_advance(cudaStream_t st, const BatchIndex& bi, int total_blocks, int grid,
+                                           bool move, Particles cur, Particles tmp, const float* u0, const float* v0,
+                                           const float* w0, const float* un, const float* vn, const float* wn,
+                                           int* key, int* slot, int* count) {
+  if (total_blocks <= 0) return cudaSuccess;
+  const int g = grid < total_blocks ? grid : total_blocks;
+  if (move)
+    kb_particles_advance<true><<<g, 256, 0, st>>>(bi, total_blocks, cur, tmp, u0, v0, w0, un, vn, wn, key, slot, count);
+  else
+    kb_particles_advance<false><<<g, 256, 0, st>>>(bi, total_blocks, cur, tmp, u0, v0, w0, un, vn, wn, key, slot, count);
   return cudaGetLastError();
 }
 

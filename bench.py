@@ -16,6 +16,13 @@ replica of the scene (the path has no data exchange): weak scaling, time =
 max over ranks.  `--impl reference` times the CPU restatement of the
 reference step (oracle/, the reference has no CPU implementation of its own)
 on the host cores, on rank 0 only.
+
+`--workload batch` measures the batch of independent scenes instead: 256
+ball-drop scenes whose sizes are drawn per axis from {24, 32, 48, 64}
+(seeded), pool depth 0.1-0.4 plus 1-2 spheres r 0.08-0.2, 8 particles per
+fluid cell (~40M particles), dt 0.01, zero-init Jacobi to relative residual
+1e-4 per scene (cap 2000); a step advances every scene once, and the value is
+batch steps/s.
 """
 from __future__ import annotations
 
@@ -37,6 +44,9 @@ UNIT = "steps/s"
 MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 JACOBI_BYTES_PER_CELL = 13  # p read 4 + p write 4 + rhs 4 + cell type 1
+BATCH_METRIC = ("batch steps/s, 256 independent scenes of sizes {24,32,48,64} per axis x 8ppc, "
+                "Jacobi to relative residual 1e-4 per scene (plain, zero-init)")
+BATCH_SEED = 2024
 
 
 def workload_config(size=128, pressure_init="zero"):
@@ -173,8 +183,45 @@ def cpu_baseline_sample(size: int, pressure_init: str, steps: int = 1) -> dict:
             "seconds": dt}
 
 
+def batch_cpu_sample(cfgs, budget_s: float = 20.0) -> dict:
+    """One step of as many scenes as fit in the budget on the CPU oracle
+    (scene init excluded), extrapolated to the whole batch by cell count."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
+    import oracle_binding  # test infrastructure: the CPU restatement of the reference step
+    total_cells = sum(c.size_x * c.size_y * c.size_z for c in cfgs)
+    spent, cells, done = 0.0, 0, 0
+    for c in cfgs:
+        o = oracle_binding.Oracle(c)
+        t0 = time.perf_counter()
+        o.step(1)
+        spent += time.perf_counter() - t0
+        o.close()
+        cells += c.size_x * c.size_y * c.size_z
+        done += 1
+        if spent > budget_s:
+            break
+    est = spent * total_cells / cells
+    return {"value": 1.0 / est, "unit": UNIT, "cores": oracle_binding.oracle_threads(), "kind": "port",
+            "sample": f"one step of scenes 0..{done - 1} ({cells} of {total_cells} cells) on the OpenMP oracle, "
+                      f"{spent:.1f}s, extrapolated to the batch by cell count", "seconds": spent}
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
+        return
+    if args.workload == "batch":
+        from aquarius_b200.scenes import batch_configs, batch_desc
+        cfgs = batch_configs(args.scenes, seed=BATCH_SEED)
+        cb = batch_cpu_sample(cfgs, budget_s=min(150.0, 20.0 * max(1, args.steps)))
+        v = cb["value"]
+        line = {"impl": "reference", "metric": BATCH_METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+                "steps": 1, "warmup": 0, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": batch_desc(args.scenes, BATCH_SEED)},
+                "cpu_baseline": dict(cb), "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                                  "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return
     # each timed step is one full CPU step of the workload; warm-up steps are
     # bounded to one, and timed steps to what fits in a few minutes
@@ -325,6 +372,108 @@ def run_ours(args, rank: int, world: int, dist):
     f.close()
 
 
+def run_batch(args, rank: int, world: int, dist):
+    import torch
+
+    import aquarius_b200 as aq
+    from aquarius_b200.scenes import batch_configs, batch_desc
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    # every rank steps its own batch (weak scaling); ranks draw different scene sets
+    cfgs = batch_configs(args.scenes, seed=BATCH_SEED + rank, device=dev)
+    t0 = time.perf_counter()
+    b = aq.Batch(cfgs)
+    t_init = time.perf_counter() - t0
+    tot = b.totals()
+    stream = torch.cuda.ExternalStream(b.stream(), device=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    b.step(args.warmup)
+    b.synchronize()
+    per_step, per_block = b.launch_counts()
+    s0 = [b.solve_stats(i) for i in range(b.scene_count)]
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.4)
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        b.step(args.steps)
+        ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = reduce_max(ms, dist, f"cuda:{dev}")
+    s1 = [b.solve_stats(i) for i in range(b.scene_count)]
+    # the solve loop runs until its slowest scene stops: loop blocks = max over scenes
+    loop_blocks = max(x["total_blocks"] - y["total_blocks"] for x, y in zip(s1, s0))
+    launches = args.steps * per_step + loop_blocks * per_block
+    value = weak_scaling_value(args.steps, world, ms_max)
+    sweeps = [x["total_sweeps"] - y["total_sweeps"] for x, y in zip(s1, s0)]
+    conv = sum(1 for x in s1 if x["converged"])
+
+    # e2e through the host-buffer entry point: all particle state in and out
+    n = tot["particles"]
+    pin_pos = torch.empty((3, n), dtype=torch.float32).pin_memory()
+    pin_vel = torch.empty((3, n), dtype=torch.float32).pin_memory()
+    pos_np, vel_np = pin_pos.numpy(), pin_vel.numpy()
+    b.step_host(0, None, None, pos_np, vel_np)
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            b.step_host(1, pos_np, vel_np, pos_np, vel_np)
+        e1.record(stream)
+    e1.synchronize()
+    e2e_ms = reduce_max(e0.elapsed_time(e1), dist, f"cuda:{dev}")
+
+    hbm_peak, peak_kind = measured_hbm_peak()
+    jb = b.benchmark_pressure(200)
+    sweep_ms = jb["ms"] / 200
+    cells = jb["cells_per_sweep"]
+    achieved = JACOBI_BYTES_PER_CELL * cells / (sweep_ms / 1000.0) / 1e9
+    line = {
+        "metric": BATCH_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": batch_desc(args.scenes, BATCH_SEED), "scenes": b.scene_count,
+                   "cells": tot["cells"], "particles": n, "launch": "one CUDA graph per step, one launch per stage",
+                   "l2": "per-step working set > 126 MB L2 (no flush needed)", "init_s": t_init},
+        "scene_steps_per_s": value * b.scene_count,
+        "e2e": {"value": weak_scaling_value(e2e_steps, world, e2e_ms), "unit": UNIT,
+                "h2d_bytes_per_step": 2 * 12 * n, "d2h_bytes_per_step": 2 * 12 * n, "steps": e2e_steps,
+                "path": "aq_batch_step_host (C ABI), pinned host particle state of all scenes in and out"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "kb_jacobi_flat (one sweep of every live scene per launch)",
+                     "achieved": achieved, "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": None,
+                     "algorithmic_bytes": f"{JACOBI_BYTES_PER_CELL} B per updated cell per sweep x {cells} cells",
+                     "sweep_us": sweep_ms * 1000.0},
+        "clocks": clk,
+        "solver": {"mean_sweeps_per_scene_step": sum(sweeps) / len(sweeps) / args.steps,
+                   "max_sweeps_per_scene_step": max(sweeps) / args.steps,
+                   "loop_blocks_per_step": loop_blocks / args.steps,
+                   "scenes_converged_last_step": conv},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = batch_cpu_sample(cfgs)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -335,6 +484,9 @@ def main():
     ap.add_argument("--pressure-init", default="zero", choices=["zero", "carry"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default Jacobi plan")
+    ap.add_argument("--workload", default="ball128", choices=["ball128", "batch"],
+                    help="ball128: the 128^3 scene; batch: 256 independent scenes of uneven sizes")
+    ap.add_argument("--scenes", type=int, default=256, help="scenes in the batch workload")
     ap.add_argument("--eager", action="store_true",
                     help="launch the step kernel by kernel instead of one CUDA graph (for launch lists)")
     args = ap.parse_args()
@@ -353,7 +505,10 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
     try:
-        run_ours(args, rank, world, dist)
+        if args.workload == "batch":
+            run_batch(args, rank, world, dist)
+        else:
+            run_ours(args, rank, world, dist)
     finally:
         if dist is not None:
             dist.destroy_process_group()

@@ -277,6 +277,53 @@ aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, in
 
 void aq_fluid_destroy(aq_fluid* f);
 
+/* ---- Batches of independent scenes ------------------------------------------
+ * No counterpart in the reference (it simulates one scene per process).  A
+ * batch steps many independent single-phase scenes, each with its own grid
+ * size, volumes and seed, in one CUDA graph per step: every stage is one
+ * launch over all scenes, and the pressure solve sweeps only the scenes whose
+ * solve is still running.  Scene s evolves exactly as an aq_fluid created
+ * from configs[s] with the default Jacobi plan would (bit for bit).
+ *
+ * Requirements: every config valid; size_z % 4 == 0; the same pressure
+ * solver settings (pressure_iterations, pressure_init, solve_mode,
+ * rel_residual, max_iterations, check_interval), device and stream in every
+ * config; in AQ_SOLVE_RESIDUAL mode an even check_interval; every scene
+ * single-phase (all its volumes carry one phase).  Totals must fit 32-bit
+ * indices (cells, nodes and particles each < 2^31). */
+typedef struct aq_batch aq_batch;
+
+aq_status aq_batch_create(const aq_config* configs, int32_t n_scenes, aq_batch** out);
+/* Enqueues n_steps steps of every scene (asynchronous on the batch stream). */
+aq_status aq_batch_step(aq_batch* b, int32_t n_steps);
+/* Host-buffer step: optionally uploads the particle state of all scenes
+ * ([3][N] float arrays, scenes concatenated in batch order, each scene in its
+ * sorted order), steps, optionally downloads it, and synchronises.  Pinned
+ * memory makes the copies asynchronous. */
+aq_status aq_batch_step_host(aq_batch* b, int32_t n_steps, const float* position_in, const float* velocity_in,
+                             float* position_out, float* velocity_out);
+aq_status aq_batch_synchronize(aq_batch* b);
+/* The cudaStream_t the batch runs on. */
+aq_status aq_batch_stream(const aq_batch* b, void** stream);
+int32_t aq_batch_scene_count(const aq_batch* b);
+/* Size and particle count of one scene. */
+aq_status aq_batch_scene_info(const aq_batch* b, int32_t scene, int32_t size_xyz[3], int64_t* particle_count);
+/* Cells, nodes and particles over all scenes. */
+aq_status aq_batch_totals(const aq_batch* b, int64_t* cells, int64_t* nodes, int64_t* particles);
+/* One scene's state in the aq_host_state layout of a fluid of that size
+ * (cell tables and sort indices relative to the scene). */
+aq_status aq_batch_download_scene(aq_batch* b, int32_t scene, aq_host_state* s);
+aq_status aq_batch_solve_stats(aq_batch* b, int32_t scene, aq_solve_stats* st);
+/* Kernel launches per step outside the residual loop, and per loop block. */
+aq_status aq_batch_launch_counts(const aq_batch* b, int32_t* per_step, int32_t* per_block);
+/* CTAs of every batched launch = multiple x SMs (default 8). */
+aq_status aq_batch_set_grid_multiple(aq_batch* b, int32_t multiple);
+/* Times `sweeps` batched Jacobi sweeps of the current pressure systems of all
+ * scenes (graph capture, one warm-up replay, one timed replay; advances the
+ * iterates).  cells_per_sweep: cells of the flat blocks holding fluid. */
+aq_status aq_batch_benchmark_pressure(aq_batch* b, int32_t sweeps, float* ms, int64_t* cells_per_sweep);
+void aq_batch_destroy(aq_batch* b);
+
 /* Largest grid (sx*sy*sz cells) aq_jacobi_sweeps_noalloc accepts. */
 #define AQ_NOALLOC_MAX_CELLS (64 * 64 * 64)
 
