@@ -101,6 +101,10 @@ def load_library() -> ct.CDLL:
         "aq_batch_solve_stats": (ct.c_int, [P, ct.c_int32, ct.POINTER(_abi.SolveStats)]),
         "aq_batch_launch_counts": (ct.c_int, [P, ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int32)]),
         "aq_batch_set_grid_multiple": (ct.c_int, [P, ct.c_int32]),
+        "aq_batch_set_sweep_plan": (ct.c_int, [P, ct.c_int32, ct.c_int32]),
+        "aq_batch_get_sweep_plan": (ct.c_int, [P, ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int32)]),
+        "aq_batch_autotune": (ct.c_int, [P, ct.c_int32, ct.POINTER(ct.c_int32), ct.POINTER(ct.c_int32),
+                                         ct.POINTER(ct.c_float)]),
         "aq_batch_benchmark_pressure": (ct.c_int, [P, ct.c_int32, ct.POINTER(ct.c_float), ct.POINTER(ct.c_int64)]),
         "aq_batch_destroy": (None, [P]),
     }
@@ -436,6 +440,20 @@ class Batch:
 
     def set_grid_multiple(self, multiple: int):
         _check(self._lib.aq_batch_set_grid_multiple(self._h, multiple))
+
+    def set_sweep_plan(self, x_planes: int, pipelined: bool = False):
+        _check(self._lib.aq_batch_set_sweep_plan(self._h, x_planes, int(pipelined)))
+
+    def sweep_plan(self) -> tuple:
+        a, b = ct.c_int32(), ct.c_int32()
+        _check(self._lib.aq_batch_get_sweep_plan(self._h, ct.byref(a), ct.byref(b)))
+        return a.value, bool(b.value)
+
+    def autotune(self, sweeps_per_trial: int = 100) -> dict:
+        """Times every batched sweep plan on the current systems and keeps the fastest."""
+        xp, pp, us = ct.c_int32(), ct.c_int32(), ct.c_float()
+        _check(self._lib.aq_batch_autotune(self._h, sweeps_per_trial, ct.byref(xp), ct.byref(pp), ct.byref(us)))
+        return {"x_planes": xp.value, "pipelined": bool(pp.value), "sweep_us": us.value}
 
     def benchmark_pressure(self, sweeps: int) -> dict:
         ms, cells = ct.c_float(), ct.c_int64()

@@ -93,6 +93,7 @@ struct BatchIndex {
   const int* bricks;     // bx * by * bz
   const int* slayer;     // ceil((F - C)/256)
   const int* flat;       // ceil(sz/128) * ceil(sy/8) * sx
+  const int* rows;       // packed-row Jacobi warp items (depends on x planes per item)
 };
 
 __device__ __forceinline__ int find_scene(const int* __restrict__ pre, int ns, int vb) {

@@ -104,6 +104,25 @@ cudaError_t launch_resid_finalize(cudaStream_t st, const double* part, int npart
                                   bool set_cond, unsigned long long cond_handle);
 
 // ---- batched scenes ------------------------------------------------------------
+// CTAs of `kernel` (with `threads` per CTA) resident on the current device at once.
+template <typename K>
+inline int resident_ctas(K kernel, int threads, size_t smem = 0) {
+  int dev = 0, sms = 0, occ = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem);
+  return sms * (occ > 0 ? occ : 1);
+}
+// Grid of a grid-stride batched launch: one resident wave at most, capped by
+// the caller's limit and by the work.
+template <typename K>
+inline int batch_grid(K kernel, int threads, int cap, int total) {
+  int g = resident_ctas(kernel, threads);
+  if (cap < g) g = cap;
+  if (total < g) g = total;
+  return g > 0 ? g : 1;
+}
+
 // Each launcher runs one stage for every scene of a batch: `total` virtual
 // blocks (the last prefix sum of the stage's family in BatchIndex) walked by
 // `grid` CTAs.  A virtual block runs the single-scene kernel's body on its
@@ -131,10 +150,16 @@ cudaError_t launch_batch_project(cudaStream_t st, const BatchIndex& bi, int tota
 cudaError_t launch_batch_extrapolate(cudaStream_t st, const BatchIndex& bi, int total, int grid, const float* ui,
                                      const float* vi, const float* wi, const uint8_t* hi, float* uo, float* vo,
                                      float* wo, uint8_t* ho);
-// One flat Jacobi sweep of every scene with live[s] != 0 (sz % 4 == 0).
-cudaError_t launch_batch_jacobi_flat(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* live,
-                                     const float* pin, float* pout, const float* rhs, const int8_t* type,
-                                     const uint8_t* brick_active);
+// One Jacobi sweep of every scene with live[s] != 0 (sz % 4 == 0), packed
+// rows: a warp item is xs x planes x 32/min(sz/4,32) rows x up to 128 z cells;
+// bi.rows must hold the prefix sums of batch_row_items(d, xs).
+int batch_row_items(const Dims& d, int xs);
+// Cells the packed-row sweep writes (items with an active brick).
+long long batch_row_cells_updated(const Dims& d, int xs, const uint8_t* bact_host);
+// pipelined (xs > 1): plane x+1's loads are issued before plane x's arithmetic.
+cudaError_t launch_batch_jacobi_rows(cudaStream_t st, const BatchIndex& bi, int total, int xs, bool pipelined,
+                                     int grid, const int* live, const float* pin, float* pout, const float* rhs,
+                                     const int8_t* type, const uint8_t* brick_active);
 cudaError_t launch_batch_resid_flat(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* live,
                                     const float* p, const float* rhs, const int8_t* type,
                                     const uint8_t* brick_active, double* part);

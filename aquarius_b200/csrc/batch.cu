@@ -63,12 +63,15 @@ struct aq_batch {
   std::vector<double> time;
   std::vector<int> phase;
   // prefix sums of virtual blocks per family, ns + 1 each
-  std::vector<int> pre_p, pre_n, pre_b, pre_s, pre_f;
+  std::vector<int> pre_p, pre_n, pre_b, pre_s, pre_f, pre_r;
   SceneDesc* scenes_d = nullptr;
   int* pre_d = nullptr;
   BatchIndex bi{};
   int N = 0, C = 0, F = 0, NB = 0, NRP = 0;
-  int sms = 148, multiple = 8;
+  int sms = 148;
+  int multiple = 64;  // cap on CTAs per SM of a batched launch (occupancy decides below it)
+  int xs = 1;         // x planes per packed-row Jacobi item
+  bool pipe = false;  // pipelined plane loads (xs > 1)
 
   Particles cur{}, tmp{};
   int *key = nullptr, *slot = nullptr, *perm_u = nullptr, *sort_index = nullptr;
@@ -115,6 +118,7 @@ struct aq_batch {
 
   int grid() const { return std::max(1, sms * multiple); }
   int grid512() const { return std::max(1, sms * std::max(1, multiple / 2)); }
+  aq_status set_sweep_plan(int planes, bool pipelined);
 
   aq_status allocate();
   aq_status add_scene(int s, aq_fluid* f);
@@ -151,10 +155,11 @@ aq_status aq_batch::allocate() {
   AQB_TRY(alloc(&rpart, (size_t)NRP));
   AQB_TRY(alloc(&ss, (size_t)ns)); AQB_TRY(alloc(&live, (size_t)ns));
   AQB_TRY(alloc(&scenes_d, (size_t)ns));
-  AQB_TRY(alloc(&pre_d, 5 * (size_t)(ns + 1)));
+  AQB_TRY(alloc(&pre_d, 6 * (size_t)(ns + 1)));
   AQB_CUDA(cudaMemcpyAsync(scenes_d, scenes.data(), sizeof(SceneDesc) * ns, cudaMemcpyHostToDevice, stream));
   std::vector<int> pre;
   for (const auto* v : {&pre_p, &pre_n, &pre_b, &pre_s, &pre_f}) pre.insert(pre.end(), v->begin(), v->end());
+  pre.resize(6 * (size_t)(ns + 1), 0);
   AQB_CUDA(cudaMemcpyAsync(pre_d, pre.data(), sizeof(int) * pre.size(), cudaMemcpyHostToDevice, stream));
   AQB_CUDA(cudaStreamSynchronize(stream));
   bi.scenes = scenes_d;
@@ -164,6 +169,24 @@ aq_status aq_batch::allocate() {
   bi.bricks = pre_d + 2 * (ns + 1);
   bi.slayer = pre_d + 3 * (ns + 1);
   bi.flat = pre_d + 4 * (ns + 1);
+  bi.rows = pre_d + 5 * (ns + 1);
+  return set_sweep_plan(xs, pipe);
+}
+
+// Packed-row Jacobi items depend on the x planes per item: rebuild their
+// prefix sums (and the step graph).
+aq_status aq_batch::set_sweep_plan(int planes, bool pipelined) {
+  if (planes != 1 && planes != 2 && planes != 4 && planes != 8)
+    return fail(AQ_ERR_INVALID_ARGUMENT, "x planes per sweep item must be 1, 2, 4 or 8");
+  if (pipelined && planes == 1) return fail(AQ_ERR_INVALID_ARGUMENT, "pipelined sweeps need x planes > 1");
+  xs = planes;
+  pipe = pipelined;
+  pre_r.assign(1, 0);
+  for (const SceneDesc& S : scenes) pre_r.push_back(pre_r.back() + batch_row_items(S.d, xs));
+  AQB_CUDA(cudaMemcpyAsync(pre_d + 5 * (ns + 1), pre_r.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice,
+                           stream));
+  AQB_CUDA(cudaStreamSynchronize(stream));
+  invalidate_graph();
   return AQ_OK;
 }
 
@@ -222,10 +245,10 @@ aq_status aq_batch::enq_pre_solve() {
 // `sweeps` sweeps of every live scene from pa; the result of an even count
 // ends in pa, of an odd count in pb.
 aq_status aq_batch::enq_sweeps(int sweeps) {
-  const int tf = pre_f[ns];
   float* bufs[2] = {pa, pb};
   for (int k = 0; k < sweeps; ++k)
-    AQB_CUDA(launch_batch_jacobi_flat(stream, bi, tf, grid(), live, bufs[k % 2], bufs[(k + 1) % 2], rhs, type, bact));
+    AQB_CUDA(launch_batch_jacobi_rows(stream, bi, pre_r[ns], xs, pipe, grid(), live, bufs[k % 2], bufs[(k + 1) % 2],
+                                      rhs, type, bact));
   return AQ_OK;
 }
 
@@ -591,6 +614,44 @@ aq_status aq_batch_set_grid_multiple(aq_batch* b, int32_t multiple) {
   return AQ_OK;
 }
 
+aq_status aq_batch_set_sweep_plan(aq_batch* b, int32_t x_planes, int32_t pipelined) {
+  if (!b) return fail(AQ_ERR_INVALID_ARGUMENT, "batch is NULL");
+  cudaSetDevice(b->device);
+  return b->set_sweep_plan(x_planes, pipelined != 0);
+}
+
+aq_status aq_batch_get_sweep_plan(const aq_batch* b, int32_t* x_planes, int32_t* pipelined) {
+  if (!b) return fail(AQ_ERR_INVALID_ARGUMENT, "batch is NULL");
+  if (x_planes) *x_planes = b->xs;
+  if (pipelined) *pipelined = b->pipe ? 1 : 0;
+  return AQ_OK;
+}
+
+aq_status aq_batch_autotune(aq_batch* b, int32_t sweeps_per_trial, int32_t* x_planes, int32_t* pipelined,
+                            float* sweep_us) {
+  if (!b || sweeps_per_trial < 2) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(b->device);
+  int best = b->xs;
+  bool best_pipe = b->pipe;
+  float best_ms = -1.f;
+  const int cand[][2] = {{1, 0}, {2, 0}, {4, 0}, {8, 0}, {2, 1}, {4, 1}, {8, 1}};
+  for (const auto& c : cand) {
+    AQB_TRY(b->set_sweep_plan(c[0], c[1] != 0));
+    float ms = 0.f;
+    AQB_TRY(aq_batch_benchmark_pressure(b, sweeps_per_trial, &ms, nullptr));
+    if (best_ms < 0.f || ms < best_ms) {
+      best_ms = ms;
+      best = c[0];
+      best_pipe = c[1] != 0;
+    }
+  }
+  AQB_TRY(b->set_sweep_plan(best, best_pipe));
+  if (x_planes) *x_planes = best;
+  if (pipelined) *pipelined = best_pipe ? 1 : 0;
+  if (sweep_us) *sweep_us = 1000.f * best_ms / (float)sweeps_per_trial;
+  return AQ_OK;
+}
+
 aq_status aq_batch_benchmark_pressure(aq_batch* b, int32_t sweeps, float* ms, int64_t* cells_per_sweep) {
   if (!b || sweeps < 1) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
   cudaSetDevice(b->device);
@@ -628,7 +689,7 @@ aq_status aq_batch_benchmark_pressure(aq_batch* b, int32_t sweeps, float* ms, in
     AQB_CUDA(cudaMemcpy(act.data(), b->bact, act.size(), cudaMemcpyDeviceToHost));
     long long cells = 0;
     for (int s = 0; s < b->ns; ++s)
-      cells += jacobi_cells_updated(b->scenes[s].d, JacobiPlan{1, 0, 1}, act.data() + b->scenes[s].br_off);
+      cells += batch_row_cells_updated(b->scenes[s].d, b->xs, act.data() + b->scenes[s].br_off);
     *cells_per_sweep = cells;
   }
   return AQ_OK;

@@ -546,24 +546,24 @@ __global__ void __launch_bounds__(256) k_diffuse(Dims d, const int8_t* __restric
 
 inline dim3 node_grid(const Dims& d) { return dim3((d.sz + 31) / 32, (d.sy + 7) / 8, d.sx); }
 
-inline int clamp_grid(int grid, int total) { return grid < total ? grid : (total > 0 ? total : 1); }
-
 }  // namespace
 
 cudaError_t launch_batch_p2g(cudaStream_t st, const BatchIndex& bi, int total, int grid, bool forces, Particles cur,
                              const int* off, float* u0, float* v0, float* w0, float* un, float* vn, float* wn,
                              int8_t* type, float* density) {
   if (forces)
-    kb_p2g<true><<<clamp_grid(grid, total), dim3(32, 8), 0, st>>>(bi, total, cur, off, u0, v0, w0, un, vn, wn, type, density);
+    kb_p2g<true><<<batch_grid(kb_p2g<true>, 256, grid, total), dim3(32, 8), 0, st>>>(bi, total, cur, off, u0, v0, w0,
+                                                                                   un, vn, wn, type, density);
   else
-    kb_p2g<false><<<clamp_grid(grid, total), dim3(32, 8), 0, st>>>(bi, total, cur, off, u0, v0, w0, un, vn, wn, type, density);
+    kb_p2g<false><<<batch_grid(kb_p2g<false>, 256, grid, total), dim3(32, 8), 0, st>>>(bi, total, cur, off, u0, v0,
+                                                                                     w0, un, vn, wn, type, density);
   return cudaGetLastError();
 }
 
 cudaError_t launch_batch_slayer(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int8_t* type,
                                 const float* su, const float* sv, const float* sw, float* u1, float* v1, float* w1,
                                 float* u2, float* v2, float* w2) {
-  kb_slayer<<<clamp_grid(grid, total), 256, 0, st>>>(bi, total, type, su, sv, sw, u1, v1, w1, u2, v2, w2);
+  kb_slayer<<<batch_grid(kb_slayer, 256, grid, total), 256, 0, st>>>(bi, total, type, su, sv, sw, u1, v1, w1, u2, v2, w2);
   return cudaGetLastError();
 }
 
@@ -571,7 +571,7 @@ cudaError_t launch_batch_divergence(cudaStream_t st, const BatchIndex& bi, int t
                                     const int8_t* type, const float* density, const float* un, const float* vn,
                                     const float* wn, int* pcount, float* div, float* rhs, float* pa, float* pb,
                                     bool zero_init, uint8_t* brick_active, double* part_b2, int* part_nf) {
-  kb_divergence<<<clamp_grid(grid, total), dim3(kBrick, kBrick, kBrick), 0, st>>>(
+  kb_divergence<<<batch_grid(kb_divergence, 512, grid, total), dim3(kBrick, kBrick, kBrick), 0, st>>>(
       bi, total, off, type, density, un, vn, wn, pcount, div, rhs, pa, pb, zero_init ? 1 : 0, brick_active, part_b2,
       part_nf);
   return cudaGetLastError();
@@ -585,14 +585,14 @@ cudaError_t launch_batch_b2_finalize(cudaStream_t st, const BatchIndex& bi, cons
 
 cudaError_t launch_batch_project(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int8_t* type,
                                  const float* p, const float* density, float* u, float* v, float* w, uint8_t* has) {
-  kb_project<<<clamp_grid(grid, total), dim3(32, 8), 0, st>>>(bi, total, type, p, density, u, v, w, has);
+  kb_project<<<batch_grid(kb_project, 256, grid, total), dim3(32, 8), 0, st>>>(bi, total, type, p, density, u, v, w, has);
   return cudaGetLastError();
 }
 
 cudaError_t launch_batch_extrapolate(cudaStream_t st, const BatchIndex& bi, int total, int grid, const float* ui,
                                      const float* vi, const float* wi, const uint8_t* hi, float* uo, float* vo,
                                      float* wo, uint8_t* ho) {
-  kb_extrapolate<<<clamp_grid(grid, total), dim3(32, 8), 0, st>>>(bi, total, ui, vi, wi, hi, uo, vo, wo, ho);
+  kb_extrapolate<<<batch_grid(kb_extrapolate, 256, grid, total), dim3(32, 8), 0, st>>>(bi, total, ui, vi, wi, hi, uo, vo, wo, ho);
   return cudaGetLastError();
 }
 

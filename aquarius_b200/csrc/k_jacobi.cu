@@ -189,6 +189,32 @@ __host__ __device__ __forceinline__ int resid_flat_parts_dev(const Dims& d) {
   return ((d.sz / 4 + 31) / 32) * ((d.sy + 7) / 8) * d.sx;
 }
 
+// One Jacobi update of 4 consecutive z cells: p' = (x+1, x-1, y+1, y-1, z+1,
+// z-1 summed in that order, + rhs) / 6 on fluid cells, 0 elsewhere.  Every
+// sweep kernel uses this function, so they agree bit for bit.
+__device__ __forceinline__ float4 jacobi_quad(const float4& xm, const float4& xp, const float4& ym, const float4& yp,
+                                              const float4& pc, float zlo, float zhi, const float4& b,
+                                              const char4& t) {
+  float4 o;
+  {
+    float s = xp.x + xm.x; s += yp.x; s += ym.x; s += pc.y; s += zlo; s += b.x;
+    o.x = t.x == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+  }
+  {
+    float s = xp.y + xm.y; s += yp.y; s += ym.y; s += pc.z; s += pc.x; s += b.y;
+    o.y = t.y == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+  }
+  {
+    float s = xp.z + xm.z; s += yp.z; s += ym.z; s += pc.w; s += pc.y; s += b.z;
+    o.z = t.z == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+  }
+  {
+    float s = xp.w + xm.w; s += yp.w; s += ym.w; s += zhi; s += pc.z; s += b.w;
+    o.w = t.w == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
+  }
+  return o;
+}
+
 // (bx, by, bz) = (z-quad block, row block, x-plane group) of the flat grid;
 // the caller has checked that the warp's rows hold fluid (warp_active).
 template <int XS>
@@ -204,54 +230,46 @@ __device__ __forceinline__ void jacobi_flat_body(const Dims& d, const float* __r
   const int plane = d.sy * d.sz;
   const int col = y * d.sz + z;
   const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-  float4 pm = zero, pc = zero, pp = zero;
+  // p at x-1, x, x+1 and the rest of plane x; with XS > 1 the loads of plane
+  // x+1 are issued before plane x's arithmetic (software pipelining along x)
+  float4 pm = zero, pc = zero, pp = zero, ym = zero, yp = zero, b = zero;
+  char4 t = make_char4(0, 0, 0, 0);
   if (in) {
-    pc = ld4(pin + x0 * plane + col);
-    pm = x0 > 0 ? ld4(pin + (x0 - 1) * plane + col) : pc;
-    pp = x0 + 1 < d.sx ? ld4(pin + (x0 + 1) * plane + col) : pc;
+    const int c = x0 * plane + col;
+    pc = ld4(pin + c);
+    pm = x0 > 0 ? ld4(pin + c - plane) : pc;
+    pp = x0 + 1 < d.sx ? ld4(pin + c + plane) : pc;
+    ym = y > 0 ? ld4(pin + c - d.sz) : pc;
+    yp = y + 1 < d.sy ? ld4(pin + c + d.sz) : pc;
+    b = ld4(rhs + c);
+    t = *reinterpret_cast<const char4*>(type + c);
   }
   for (int x = x0; x < x1; ++x) {
     const int c = x * plane + col;
-    // prefetch the plane after next before this plane's arithmetic
-    float4 pn = pp;
-    if (in && x + 2 < d.sx && x + 1 < x1) pn = ld4(pin + c + 2 * plane);
-    float4 ym = pc, yp = pc, b = zero;
-    char4 t = make_char4(0, 0, 0, 0);
-    if (in) {
-      if (y > 0) ym = ld4(pin + c - d.sz);
-      if (y + 1 < d.sy) yp = ld4(pin + c + d.sz);
-      b = ld4(rhs + c);
-      t = *reinterpret_cast<const char4*>(type + c);
+    float4 pn = pp, nym = pp, nyp = pp, nb = zero;
+    char4 nt = make_char4(0, 0, 0, 0);
+    if (in && x + 1 < x1) {
+      const int cn = c + plane;
+      if (x + 2 < d.sx) pn = ld4(pin + cn + plane);
+      if (y > 0) nym = ld4(pin + cn - d.sz);
+      if (y + 1 < d.sy) nyp = ld4(pin + cn + d.sz);
+      nb = ld4(rhs + cn);
+      nt = *reinterpret_cast<const char4*>(type + cn);
     }
     float zlo = __shfl_up_sync(0xffffffffu, pc.w, 1);
     float zhi = __shfl_down_sync(0xffffffffu, pc.x, 1);
     if (in) {
       if (lane == 0) zlo = z > 0 ? pin[c - 1] : pc.x;
       if (lane == 31 || z + 4 >= d.sz) zhi = z + 4 < d.sz ? pin[c + 4] : pc.w;
-      const float4 xm = pm, xp = pp;
-      float4 o;
-      // p' = (x+1, x-1, y+1, y-1, z+1, z-1 summed in that order, + rhs) / 6
-      {
-        float s = xp.x + xm.x; s += yp.x; s += ym.x; s += pc.y; s += zlo; s += b.x;
-        o.x = t.x == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
-      }
-      {
-        float s = xp.y + xm.y; s += yp.y; s += ym.y; s += pc.z; s += pc.x; s += b.y;
-        o.y = t.y == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
-      }
-      {
-        float s = xp.z + xm.z; s += yp.z; s += ym.z; s += pc.w; s += pc.y; s += b.z;
-        o.z = t.z == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
-      }
-      {
-        float s = xp.w + xm.w; s += yp.w; s += ym.w; s += zhi; s += pc.z; s += b.w;
-        o.w = t.w == kFluid ? __fdiv_rn(s, 6.f) : 0.f;
-      }
-      *reinterpret_cast<float4*>(pout + c) = o;
+      *reinterpret_cast<float4*>(pout + c) = jacobi_quad(pm, pp, ym, yp, pc, zlo, zhi, b, t);
     }
     pm = pc;
     pc = pp;
     pp = (x + 2 < d.sx) ? pn : pc;
+    ym = nym;
+    yp = nyp;
+    b = nb;
+    t = nt;
   }
 }
 
@@ -674,22 +692,141 @@ __device__ __forceinline__ void flat_block_coords(const Dims& d, int local, int&
   bz = t / gy;
 }
 
-__global__ void __launch_bounds__(256) kb_jacobi_flat(BatchIndex bi, int total, const int* __restrict__ live,
-                                                     const float* __restrict__ pin, float* __restrict__ pout,
-                                                     const float* __restrict__ rhs, const int8_t* __restrict__ type,
-                                                     const uint8_t* __restrict__ bact) {
+// Packed-row sweep for batches of small grids.  A warp work item is XS x
+// planes x R rows x up to 128 z cells of one scene: with zw = min(sz/4, 32)
+// z-quads per row, lane l covers row l / zw, quad l % zw, and R = 32 / zw rows
+// share the warp, so a 24-wide grid still fills 30 of 32 lanes.  Items are
+// numbered per scene as ((xg * ygroups) + yg) * zblocks + zb; a CTA's 8 warps
+// take consecutive items.  Same arithmetic as the flat kernel (jacobi_quad),
+// so results are bitwise those of the single-scene sweep.
+struct RowItem {
+  int zw, R, ygroups, zblocks;
+};
+
+__host__ __device__ __forceinline__ RowItem row_item_shape(const Dims& d) {
+  RowItem r;
+  const int zq = d.sz / 4;
+  r.zw = zq < 32 ? zq : 32;
+  r.R = 32 / r.zw;
+  r.ygroups = (d.sy + r.R - 1) / r.R;
+  r.zblocks = (zq + 31) / 32;
+  return r;
+}
+
+__host__ __device__ __forceinline__ int row_items(const Dims& d, int xs) {
+  const RowItem r = row_item_shape(d);
+  return ((d.sx + xs - 1) / xs) * r.ygroups * r.zblocks;
+}
+
+// Does any 8^3 brick under x in [x0,x1), y in [y0,y1), z in [z0,z1) hold fluid?
+__device__ __forceinline__ bool range_active(const Dims& d, const uint8_t* __restrict__ bact, int x0, int x1, int y0,
+                                             int y1, int z0, int z1) {
+  const int bx0 = x0 / kBrick, nbx = (x1 - 1) / kBrick - bx0 + 1;
+  const int by0 = y0 / kBrick, nby = (y1 - 1) / kBrick - by0 + 1;
+  const int bz0 = z0 / kBrick, nbz = (z1 - 1) / kBrick - bz0 + 1;
+  const int nb = nbx * nby * nbz;
+  int a = 0;
+  for (int k = threadIdx.x & 31; k < nb; k += 32) {
+    const int iz = k % nbz, t = k / nbz, iy = t % nby, ix = t / nby;
+    a |= bact[((bx0 + ix) * d.by + by0 + iy) * d.bz + bz0 + iz];
+  }
+  return __any_sync(0xffffffffu, a) != 0;
+}
+
+template <int XS, bool PIPE>
+__global__ void __launch_bounds__(256) kb_jacobi_rows(BatchIndex bi, int total, const int* __restrict__ live,
+                                                     const float* __restrict__ pin_all, float* __restrict__ pout_all,
+                                                     const float* __restrict__ rhs_all,
+                                                     const int8_t* __restrict__ type_all,
+                                                     const uint8_t* __restrict__ bact_all) {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;");
-  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
-    const int s = find_scene(bi.flat, bi.n_scenes, vb);
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < total; item += warps) {
+    const int s = find_scene(bi.rows, bi.n_scenes, item);
     if (!live[s]) continue;
     const SceneDesc& S = bi.scenes[s];
-    int bx, by, bz;
-    flat_block_coords(S.d, vb - bi.flat[s], bx, by, bz);
-    const int y = by * 8 + threadIdx.y;
-    if (!(y < S.d.sy && warp_active(S.d, bact + S.br_off, bz, bz + 1, y, bx * 16))) continue;
-    const int c = S.c_off;
-    jacobi_flat_body<1>(S.d, pin + c, pout + c, rhs + c, type + c, bx, by, bz);
+    const Dims& d = S.d;
+    const RowItem ri = row_item_shape(d);
+    int local = item - bi.rows[s];
+    const int zb = local % ri.zblocks;
+    local /= ri.zblocks;
+    const int yg = local % ri.ygroups;
+    const int xg = local / ri.ygroups;
+    const int x0 = xg * XS, x1 = min(x0 + XS, d.sx);
+    const int ylo = yg * ri.R, yhi = min(ylo + ri.R, d.sy);
+    const int zlo0 = zb * 128, zhi0 = min(zlo0 + 128, d.sz);
+    if (!range_active(d, bact_all + S.br_off, x0, x1, ylo, yhi, zlo0, zhi0)) continue;
+    const int r = lane / ri.zw, q = lane % ri.zw;
+    const int y = ylo + r;
+    const int z = (zb * 32 + q) * 4;
+    const bool in = r < ri.R && y < d.sy && z < d.sz;
+    const float* __restrict__ pin = pin_all + S.c_off;
+    float* __restrict__ pout = pout_all + S.c_off;
+    const float* __restrict__ rhs = rhs_all + S.c_off;
+    const int8_t* __restrict__ type = type_all + S.c_off;
+    const int plane = d.sy * d.sz;
+    const int col = y * d.sz + z;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    // p at x-1, x, x+1 and the rest of plane x.  PIPE: the loads of plane
+    // x+1 are issued before plane x's arithmetic (software pipelining along x,
+    // more registers); otherwise only p at x+2 is prefetched.
+    float4 pm = zero, pc = zero, pp = zero, ym = zero, yp = zero, b = zero;
+    char4 t = make_char4(0, 0, 0, 0);
+    if (in) {
+      const int c = x0 * plane + col;
+      pc = ld4(pin + c);
+      pm = x0 > 0 ? ld4(pin + c - plane) : pc;
+      pp = x0 + 1 < d.sx ? ld4(pin + c + plane) : pc;
+      if (PIPE) {
+        ym = y > 0 ? ld4(pin + c - d.sz) : pc;
+        yp = y + 1 < d.sy ? ld4(pin + c + d.sz) : pc;
+        b = ld4(rhs + c);
+        t = *reinterpret_cast<const char4*>(type + c);
+      }
+    }
+    for (int x = x0; x < x1; ++x) {
+      const int c = x * plane + col;
+      float4 pn = pp, nym = pp, nyp = pp, nb = zero;
+      char4 nt = make_char4(0, 0, 0, 0);
+      if (PIPE) {
+        if (in && x + 1 < x1) {
+          const int cn = c + plane;
+          if (x + 2 < d.sx) pn = ld4(pin + cn + plane);
+          if (y > 0) nym = ld4(pin + cn - d.sz);
+          if (y + 1 < d.sy) nyp = ld4(pin + cn + d.sz);
+          nb = ld4(rhs + cn);
+          nt = *reinterpret_cast<const char4*>(type + cn);
+        }
+      } else {
+        if (in && x + 2 < d.sx && x + 1 < x1) pn = ld4(pin + c + 2 * plane);
+        ym = pc;
+        yp = pc;
+        if (in) {
+          if (y > 0) ym = ld4(pin + c - d.sz);
+          if (y + 1 < d.sy) yp = ld4(pin + c + d.sz);
+          b = ld4(rhs + c);
+          t = *reinterpret_cast<const char4*>(type + c);
+        }
+      }
+      float zlo = __shfl_up_sync(0xffffffffu, pc.w, 1);
+      float zhi = __shfl_down_sync(0xffffffffu, pc.x, 1);
+      if (in) {
+        if (q == 0) zlo = z > 0 ? pin[c - 1] : pc.x;
+        if (q == ri.zw - 1 || z + 4 >= d.sz) zhi = z + 4 < d.sz ? pin[c + 4] : pc.w;
+        *reinterpret_cast<float4*>(pout + c) = jacobi_quad(pm, pp, ym, yp, pc, zlo, zhi, b, t);
+      }
+      pm = pc;
+      pc = pp;
+      pp = (x + 2 < d.sx) ? pn : pc;
+      if (PIPE) {
+        ym = nym;
+        yp = nyp;
+        b = nb;
+        t = nt;
+      }
+    }
   }
 }
 
@@ -932,26 +1069,64 @@ cudaError_t launch_resid_finalize(cudaStream_t st, const double* part, int npart
 
 namespace aqb {
 
-cudaError_t launch_batch_jacobi_flat(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* live,
-                                     const float* pin, float* pout, const float* rhs, const int8_t* type,
-                                     const uint8_t* brick_active) {
+int batch_row_items(const Dims& d, int xs) { return row_items(d, xs); }
+
+long long batch_row_cells_updated(const Dims& d, int xs, const uint8_t* bact_host) {
+  const RowItem ri = row_item_shape(d);
+  long long cells = 0;
+  for (int x0 = 0; x0 < d.sx; x0 += xs)
+    for (int y0 = 0; y0 < d.sy; y0 += ri.R)
+      for (int z0 = 0; z0 < d.sz; z0 += 128) {
+        const int x1 = std::min(x0 + xs, d.sx), y1 = std::min(y0 + ri.R, d.sy), z1 = std::min(z0 + 128, d.sz);
+        bool act = false;
+        for (int bx = x0 / kBrick; bx <= (x1 - 1) / kBrick && !act; ++bx)
+          for (int by = y0 / kBrick; by <= (y1 - 1) / kBrick && !act; ++by)
+            for (int bz = z0 / kBrick; bz <= (z1 - 1) / kBrick && !act; ++bz)
+              act = bact_host[(bx * d.by + by) * d.bz + bz] != 0;
+        if (act) cells += (long long)(x1 - x0) * (y1 - y0) * (z1 - z0);
+      }
+  return cells;
+}
+
+cudaError_t launch_batch_jacobi_rows(cudaStream_t st, const BatchIndex& bi, int total, int xs, bool pipelined,
+                                     int grid, const int* live, const float* pin, float* pout, const float* rhs,
+                                     const int8_t* type, const uint8_t* brick_active) {
   cudaLaunchConfig_t lc = {};
-  lc.gridDim = dim3(grid < total ? grid : (total > 0 ? total : 1));
-  lc.blockDim = dim3(32, 8);
+  lc.blockDim = dim3(256);
   lc.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   lc.attrs = at;
   lc.numAttrs = 1;
-  return cudaLaunchKernelEx(&lc, kb_jacobi_flat, bi, total, live, pin, pout, rhs, type, brick_active);
+  auto go = [&](auto kern) {
+    const int items_per_cta = 8;
+    const int need = (total + items_per_cta - 1) / items_per_cta;
+    lc.gridDim = dim3(std::max(1, std::min({grid, need, resident_ctas(kern, 256)})));
+    return cudaLaunchKernelEx(&lc, kern, bi, total, live, pin, pout, rhs, type, brick_active);
+  };
+  if (pipelined) {
+    switch (xs) {
+      case 2: return go(kb_jacobi_rows<2, true>);
+      case 4: return go(kb_jacobi_rows<4, true>);
+      case 8: return go(kb_jacobi_rows<8, true>);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  switch (xs) {
+    case 1: return go(kb_jacobi_rows<1, false>);
+    case 2: return go(kb_jacobi_rows<2, false>);
+    case 4: return go(kb_jacobi_rows<4, false>);
+    case 8: return go(kb_jacobi_rows<8, false>);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_batch_resid_flat(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* live,
                                     const float* p, const float* rhs, const int8_t* type,
                                     const uint8_t* brick_active, double* part) {
-  kb_resid_flat<<<grid < total ? grid : (total > 0 ? total : 1), dim3(32, 8), 0, st>>>(bi, total, live, p, rhs, type,
-                                                                                     brick_active, part);
+  const int g = std::max(1, std::min({grid, total, resident_ctas(kb_resid_flat, 256)}));
+  kb_resid_flat<<<g, dim3(32, 8), 0, st>>>(bi, total, live, p, rhs, type, brick_active, part);
   return cudaGetLastError();
 }
 

@@ -322,7 +322,8 @@ cudaError_t launch_batch_particles_advance(cudaStream_t st, const BatchIndex& bi
                                            const float* w0, const float* un, const float* vn, const float* wn,
                                            int* key, int* slot, int* count) {
   if (total_blocks <= 0) return cudaSuccess;
-  const int g = grid < total_blocks ? grid : total_blocks;
+  const int g = move ? batch_grid(kb_particles_advance<true>, 256, grid, total_blocks)
+                     : batch_grid(kb_particles_advance<false>, 256, grid, total_blocks);
   if (move)
     kb_particles_advance<true><<<g, 256, 0, st>>>(bi, total_blocks, cur, tmp, u0, v0, w0, un, vn, wn, key, slot, count);
   else

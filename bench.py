@@ -394,6 +394,13 @@ def run_batch(args, rank: int, world: int, dist):
 
     b.step(args.warmup)
     b.synchronize()
+    if args.no_tune:
+        xp, pipe = b.sweep_plan()
+        tune = {"x_planes": xp, "pipelined": pipe, "sweep_us": None}
+    else:
+        tune = b.autotune(50)
+    b.step(1)
+    b.synchronize()
     per_step, per_block = b.launch_counts()
     s0 = [b.solve_stats(i) for i in range(b.scene_count)]
 
@@ -456,7 +463,8 @@ def run_batch(args, rank: int, world: int, dist):
                 "h2d_bytes_per_step": 2 * 12 * n, "d2h_bytes_per_step": 2 * 12 * n, "steps": e2e_steps,
                 "path": "aq_batch_step_host (C ABI), pinned host particle state of all scenes in and out"},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "kb_jacobi_flat (one sweep of every live scene per launch)",
+        "roofline": {"bound": "hbm", "kernel": f"kb_jacobi_rows<{tune['x_planes']}, {'pipelined' if tune['pipelined'] else 'plain'}> "
+                               "(one sweep of every live scene per launch, packed rows)",
                      "achieved": achieved, "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": None,
                      "algorithmic_bytes": f"{JACOBI_BYTES_PER_CELL} B per updated cell per sweep x {cells} cells",
@@ -466,6 +474,8 @@ def run_batch(args, rank: int, world: int, dist):
                    "max_sweeps_per_scene_step": max(sweeps) / args.steps,
                    "loop_blocks_per_step": loop_blocks / args.steps,
                    "scenes_converged_last_step": conv},
+        "sweep_plan": {"x_planes_per_item": tune["x_planes"], "pipelined": tune["pipelined"],
+                       "tuned_sweep_us": tune["sweep_us"]},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = batch_cpu_sample(cfgs)

@@ -316,8 +316,20 @@ aq_status aq_batch_download_scene(aq_batch* b, int32_t scene, aq_host_state* s);
 aq_status aq_batch_solve_stats(aq_batch* b, int32_t scene, aq_solve_stats* st);
 /* Kernel launches per step outside the residual loop, and per loop block. */
 aq_status aq_batch_launch_counts(const aq_batch* b, int32_t* per_step, int32_t* per_block);
-/* CTAs of every batched launch = multiple x SMs (default 8). */
+/* Caps every batched launch at multiple x SMs CTAs (default 64, i.e. as many
+ * as are resident at once; a batched launch never exceeds one resident wave).
+ * Results do not depend on it. */
 aq_status aq_batch_set_grid_multiple(aq_batch* b, int32_t multiple);
+/* Shape of the batched Jacobi sweep: x planes each warp streams (1, 2, 4 or
+ * 8; default 1) and, for more than one plane, whether the next plane's loads
+ * are issued before the current plane's arithmetic.  Results do not depend
+ * on it. */
+aq_status aq_batch_set_sweep_plan(aq_batch* b, int32_t x_planes, int32_t pipelined);
+aq_status aq_batch_get_sweep_plan(const aq_batch* b, int32_t* x_planes, int32_t* pipelined);
+/* Project-written autotuner of the batched sweep: times every sweep plan on
+ * the current pressure systems (advances the iterates), keeps the fastest. */
+aq_status aq_batch_autotune(aq_batch* b, int32_t sweeps_per_trial, int32_t* x_planes, int32_t* pipelined,
+                            float* sweep_us);
 /* Times `sweeps` batched Jacobi sweeps of the current pressure systems of all
  * scenes (graph capture, one warm-up replay, one timed replay; advances the
  * iterates).  cells_per_sweep: cells of the flat blocks holding fluid. */

@@ -68,18 +68,47 @@ def test_scene_in_batch_equals_scene_alone(solver):
             assert len(set(iters)) > 1  # scenes stopped at different sweep counts
 
 
-def test_batch_grid_multiple_does_not_change_results():
-    cfgs = batch_configs(4, seed=3, sizes=(16, 24), solve_mode=_abi.SOLVE_RESIDUAL, check_interval=20,
+def test_launch_shape_does_not_change_results():
+    # sizes 12..160: one to five rows per warp, and two z blocks per row at 160
+    cfgs = batch_configs(4, seed=3, sizes=(12, 20, 24), solve_mode=_abi.SOLVE_RESIDUAL, check_interval=20,
                          max_iterations=200, rel_residual=1e-3)
+    cfgs.append(_abi.make_config((20, 12, 160), [dict(shape="box", min=(0, 0, 0), max=(1, 0.4, 1))],
+                                 timestep=0.01, solve_mode=_abi.SOLVE_RESIDUAL, check_interval=20,
+                                 max_iterations=200, rel_residual=1e-3, pressure_init=_abi.PRESSURE_ZERO))
     out = []
-    for m in (1, 8):
+    for m, planes, pipe in ((1, 1, False), (64, 2, False), (3, 4, True), (64, 8, False), (64, 8, True)):
         with aq.Batch(cfgs) as b:
             b.set_grid_multiple(m)
+            b.set_sweep_plan(planes, pipe)
+            assert b.sweep_plan() == (planes, pipe)
             b.step(3)
             out.append([b.download_scene(s, ["position", "pressure"]) for s in range(len(cfgs))])
-    for a, b in zip(*out):
-        for k in ("position", "pressure"):
-            np.testing.assert_array_equal(a[k], b[k])
+    for run in out[1:]:
+        for a, b in zip(out[0], run):
+            for k in ("position", "pressure"):
+                np.testing.assert_array_equal(a[k], b[k])
+    with aq.Fluid(cfgs[-1]) as f:
+        f.step(3)
+        np.testing.assert_array_equal(f.download_state(["pressure"])["pressure"], out[0][-1]["pressure"])
+
+
+def test_batch_autotune_keeps_results():
+    # zero-init pressure: the sweeps the tuner runs on the current systems do
+    # not carry into the next step, so the tuned batch must stay bitwise equal
+    cfgs = batch_configs(6, seed=9, sizes=(16, 24, 32), solve_mode=_abi.SOLVE_FIXED, pressure_iterations=30,
+                         pressure_init=_abi.PRESSURE_ZERO)
+    with aq.Batch(cfgs) as b, aq.Batch(cfgs) as ref:
+        b.step(1)
+        ref.step(1)
+        r = b.autotune(20)
+        assert r["x_planes"] in (1, 2, 4, 8) and r["sweep_us"] > 0
+        assert b.sweep_plan() == (r["x_planes"], r["pipelined"])
+        b.step(2)
+        ref.step(2)
+        for s in range(len(cfgs)):
+            x, y = b.download_scene(s, ["position", "pressure"]), ref.download_scene(s, ["position", "pressure"])
+            for k in ("position", "pressure"):
+                np.testing.assert_array_equal(x[k], y[k])
 
 
 def test_batch_launch_counts_and_benchmark():
