@@ -170,6 +170,18 @@ cudaError_t launch_batch_resid_finalize(cudaStream_t st, const BatchIndex& bi, c
 cudaError_t launch_batch_solve_condition(cudaStream_t st, const int* live, int n_scenes,
                                          unsigned long long cond_handle);
 
+// ---- U-Net building blocks (k_unet.cu) ---------------------------------------
+// Channels-last bf16 tensors over a grid; 3x3x3 convolution, zero padding.
+// (cin, cout) must be one of the instantiated pairs (else cudaErrorInvalidValue).
+cudaError_t launch_conv3_fwd(cudaStream_t st, int cin, int cout, bool relu, const void* in, const void* w,
+                             const float* bias, void* out, int sx, int sy, int sz);
+// dw[t][co][ci] (f32) from x (cin) and dy (cout); part: conv3_wgrad_part_floats scratch.
+cudaError_t launch_conv3_wgrad(cudaStream_t st, int cin, int cout, const void* x, const void* dy, float* part,
+                               float* dw, int sx, int sy, int sz);
+size_t conv3_wgrad_part_floats(int cin, int cout, int voxels);
+// wt[t][ci][co] = w[26-t][co][ci] (weights of the data gradient).
+cudaError_t launch_flip_transpose(cudaStream_t st, const void* w, void* wt, int cin, int cout);
+
 // ---- FP64 PCG (k_pcg.cu) ----------------------------------------------------
 cudaError_t launch_pcg_apply(cudaStream_t st, const Dims& d, const int8_t* type, const double* in,
                              double* out);  // out = A in

@@ -336,6 +336,24 @@ aq_status aq_batch_autotune(aq_batch* b, int32_t sweeps_per_trial, int32_t* x_pl
 aq_status aq_batch_benchmark_pressure(aq_batch* b, int32_t sweeps, float* ms, int64_t* cells_per_sweep);
 void aq_batch_destroy(aq_batch* b);
 
+/* ---- Learned pressure warm start: building blocks ---------------------------
+ * No counterpart in the reference.  BF16 tensors are channels-last over the
+ * cell layout ((x*sy + y)*sz + z)*C + c, all pointers device memory, work on
+ * `stream` (NULL = legacy default stream).
+ * aq_conv3_forward: out = act(bias + conv3x3x3(in, w)), zero padding,
+ *   w[27][cout][cin] bf16 (tap = (dx+1)*9 + (dy+1)*3 + (dz+1)), bias f32 or
+ *   NULL, relu 0/1.  (cin, cout) in {(16,16), (16,32), (32,32), (32,64),
+ *   (64,64), (96,32), (48,16), (32,16), (64,32), (32,96), (16,48)}.
+ * aq_conv3_weight_grad: dw[27][cout][cin] (f32) = sum over voxels of
+ *   dy[v][co] * x[v + tap offset][ci]; (cin, cout) a forward layer pair.
+ * aq_conv3_flip_transpose: wt[t][ci][co] = w[26-t][co][ci], the weights whose
+ *   forward convolution of dy is the data gradient. */
+aq_status aq_conv3_forward(int32_t cin, int32_t cout, int32_t relu, const void* in, const void* w, const float* bias,
+                           void* out, int32_t sx, int32_t sy, int32_t sz, void* stream);
+aq_status aq_conv3_weight_grad(int32_t cin, int32_t cout, const void* x, const void* dy, float* dw, int32_t sx,
+                               int32_t sy, int32_t sz, void* stream);
+aq_status aq_conv3_flip_transpose(int32_t cin, int32_t cout, const void* w, void* wt, void* stream);
+
 /* Largest grid (sx*sy*sz cells) aq_jacobi_sweeps_noalloc accepts. */
 #define AQ_NOALLOC_MAX_CELLS (64 * 64 * 64)
 
