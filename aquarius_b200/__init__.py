@@ -28,7 +28,7 @@ from . import _abi
 
 __all__ = [
     "ShapeType", "InitializationVolume", "ConfigFLIP", "FluidConfig", "Fluid", "AquariusError",
-    "library_path", "load_library", "STAGES", "Batch",
+    "library_path", "load_library", "STAGES", "Batch", "UNet", "Dataset",
 ]
 
 STAGES = _abi.STAGES
@@ -107,6 +107,23 @@ def load_library() -> ct.CDLL:
                                          ct.POINTER(ct.c_float)]),
         "aq_batch_benchmark_pressure": (ct.c_int, [P, ct.c_int32, ct.POINTER(ct.c_float), ct.POINTER(ct.c_int64)]),
         "aq_batch_destroy": (None, [P]),
+        "aq_unet_create": (ct.c_int, [ct.c_int32, ct.c_uint32, ct.POINTER(P)]),
+        "aq_unet_destroy": (None, [P]),
+        "aq_unet_parameter_count": (ct.c_int, [P, ct.POINTER(ct.c_int64)]),
+        "aq_unet_save": (ct.c_int, [P, ct.c_char_p]),
+        "aq_unet_load": (ct.c_int, [P, ct.c_char_p]),
+        "aq_unet_get_output_scale": (ct.c_int, [P, ct.POINTER(ct.c_float)]),
+        "aq_unet_predict": (ct.c_int, [P, ct.c_int32, ct.c_int32, ct.c_int32, P, P, P, P]),
+        "aq_unet_train": (ct.c_int, [P, P, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_float, ct.c_uint32, ct.c_float,
+                                     ct.POINTER(ct.c_float)]),
+        "aq_unet_evaluate": (ct.c_int, [P, P, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_double)]),
+        "aq_unet_gradients": (ct.c_int, [P, P, ct.c_int64]),
+        "aq_dataset_create": (ct.c_int, [ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.POINTER(P)]),
+        "aq_dataset_destroy": (None, [P]),
+        "aq_dataset_count": (ct.c_int32, [P]),
+        "aq_dataset_add_fluid": (ct.c_int, [P, P, ct.c_double, ct.c_int32, ct.POINTER(ct.c_int32)]),
+        "aq_dataset_target_rms": (ct.c_int, [P, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_double)]),
+        "aq_dataset_get": (ct.c_int, [P, ct.c_int32, P, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -476,3 +493,113 @@ class Batch:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class UNet:
+    """The learned pressure warm start's network (no reference counterpart):
+    a 3-level 3D U-Net in BF16 with FP32 accumulation, trained and run by the
+    library's own kernels."""
+
+    def __init__(self, device: int = 0, seed: int = 1, weights=None):
+        self._lib = load_library()
+        self._h = ct.c_void_p()
+        _check(self._lib.aq_unet_create(device, seed, ct.byref(self._h)))
+        if weights is not None:
+            self.load(weights)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def parameter_count(self) -> int:
+        n = ct.c_int64()
+        _check(self._lib.aq_unet_parameter_count(self._h, ct.byref(n)))
+        return n.value
+
+    def save(self, path):
+        _check(self._lib.aq_unet_save(self._h, str(path).encode()))
+
+    def load(self, path):
+        _check(self._lib.aq_unet_load(self._h, str(path).encode()))
+
+    def output_scale(self) -> float:
+        v = ct.c_float()
+        _check(self._lib.aq_unet_get_output_scale(self._h, ct.byref(v)))
+        return v.value
+
+    def predict(self, size, rhs_ptr: int, type_ptr: int, out_ptr: int, stream: int = 0):
+        _check(self._lib.aq_unet_predict(self._h, *size, rhs_ptr, type_ptr, out_ptr, stream or None))
+
+    def train(self, ds: "Dataset", first: int, count: int, steps: int, lr: float = 1e-3, seed: int = 1,
+              out_scale: float = 0.0) -> float:
+        loss = ct.c_float()
+        _check(self._lib.aq_unet_train(self._h, ds._h, first, count, steps, lr, seed, out_scale, ct.byref(loss)))
+        return loss.value
+
+    def evaluate(self, ds: "Dataset", first: int, count: int) -> float:
+        e = ct.c_double()
+        _check(self._lib.aq_unet_evaluate(self._h, ds._h, first, count, ct.byref(e)))
+        return e.value
+
+    def gradients(self) -> np.ndarray:
+        out = np.zeros(self.parameter_count(), np.float32)
+        _check(self._lib.aq_unet_gradients(self._h, out.ctypes.data, out.size))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.aq_unet_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Dataset:
+    """Device-resident (rhs, fluid mark) -> FP64-PCG pressure pairs of one grid size."""
+
+    def __init__(self, size, capacity: int, device: int = 0):
+        self._lib = load_library()
+        self._h = ct.c_void_p()
+        self.size = tuple(size)
+        _check(self._lib.aq_dataset_create(*self.size, capacity, device, ct.byref(self._h)))
+
+    def __len__(self):
+        return self._lib.aq_dataset_count(self._h)
+
+    def add_fluid(self, fluid: Fluid, pcg_rel_tol: float = 1e-10, pcg_max_iter: int = 100000) -> int:
+        it = ct.c_int32()
+        _check(self._lib.aq_dataset_add_fluid(self._h, fluid._h, pcg_rel_tol, pcg_max_iter, ct.byref(it)))
+        return it.value
+
+    def target_rms(self, first: int = 0, count: int = None) -> float:
+        v = ct.c_double()
+        _check(self._lib.aq_dataset_target_rms(self._h, first, len(self) - first if count is None else count,
+                                               ct.byref(v)))
+        return v.value
+
+    def get(self, i: int) -> dict:
+        n = self.size[0] * self.size[1] * self.size[2]
+        rhs, typ, tgt = np.zeros(n, np.float32), np.zeros(n, np.int8), np.zeros(n, np.float32)
+        _check(self._lib.aq_dataset_get(self._h, i, rhs.ctypes.data, typ.ctypes.data, tgt.ctypes.data))
+        return {"rhs": rhs, "type": typ, "target": tgt}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.aq_dataset_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

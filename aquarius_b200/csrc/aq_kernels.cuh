@@ -182,6 +182,34 @@ size_t conv3_wgrad_part_floats(int cin, int cout, int voxels);
 // wt[t][ci][co] = w[26-t][co][ci] (weights of the data gradient).
 cudaError_t launch_flip_transpose(cudaStream_t st, const void* w, void* wt, int cin, int cout);
 
+// U-Net glue (channels-last bf16, fine grid sx,sy,sz even; coarse = half).
+cudaError_t launch_absmax(cudaStream_t st, const float* a, int n, float* part /*>= 1024*/, float* out);
+cudaError_t launch_unet_input(cudaStream_t st, const float* rhs, const int8_t* type, const float* scale, void* out,
+                              int V);
+cudaError_t launch_pool2(cudaStream_t st, const void* in, void* out, int sx, int sy, int sz, int C);
+cudaError_t launch_pool2_bwd(cudaStream_t st, const void* dout, void* din, int sx, int sy, int sz, int C,
+                             bool accumulate);
+cudaError_t launch_upcat(cudaStream_t st, const void* coarse, const void* skip, void* out, int sx, int sy, int sz,
+                         int Cu, int Cs);
+cudaError_t launch_upcat_bwd(cudaStream_t st, const void* dout, void* dcoarse, void* dskip, int sx, int sy, int sz,
+                             int Cu, int Cs);
+cudaError_t launch_relu_bwd(cudaStream_t st, void* dy, const void* y, int n);
+int chan_sum_parts(int V);
+cudaError_t launch_chan_sum(cudaStream_t st, const void* dy, int V, int C, float* part, float* out);
+cudaError_t launch_head_fwd(cudaStream_t st, const void* h, const float* w, const float* b, float* out, int V);
+int head_parts();
+cudaError_t launch_head_loss_bwd(cudaStream_t st, const float* out, const float* target, const int8_t* type,
+                                 const void* h, const float* w, const float* nf, void* dh, int V, float* part,
+                                 float* sums);
+cudaError_t launch_adam(cudaStream_t st, float* w, const float* g, float* m, float* v, int n, float lr, float b1,
+                        float b2, float eps, int t, void* wb);
+cudaError_t launch_f32_to_bf16(cudaStream_t st, const float* a, void* b, int n);
+cudaError_t launch_unet_to_pressure(cudaStream_t st, const float* out, const float* scale, float out_scale,
+                                    const int8_t* type, float* p, int V);
+cudaError_t launch_unet_scale_copy(cudaStream_t st, const float* a, float k, float* b, int n);
+cudaError_t launch_unet_sample(cudaStream_t st, const float* rhs, const int8_t* type, const double* p,
+                               const float* scale, float* rhs_s, int8_t* type_s, float* target, int V);
+
 // ---- FP64 PCG (k_pcg.cu) ----------------------------------------------------
 cudaError_t launch_pcg_apply(cudaStream_t st, const Dims& d, const int8_t* type, const double* in,
                              double* out);  // out = A in

@@ -1336,9 +1336,11 @@ aq_status aq_fluid_autotune(aq_fluid* f, int32_t sweeps_per_trial, const char* c
   return AQ_OK;
 }
 
-aq_status aq_fluid_pcg_reference(aq_fluid* f, double rel_tol, int32_t max_iter, float* pressure_out,
-                                 double* rel_error, int32_t* iterations, double* achieved) {
-  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+}  // extern "C"
+
+// FP64 diagonal-PCG on the fluid's current pressure system; the solution is
+// left in f->pcg_x (device, FP64).
+aq_status aqb::fluid_pcg_solve(aq_fluid* f, double rel_tol, int max_iter, int* iterations, double* achieved) {
   cudaSetDevice(f->device);
   const Dims& d = f->d;
   const size_t C = (size_t)d.C;
@@ -1393,6 +1395,19 @@ aq_status aq_fluid_pcg_reference(aq_fluid* f, double rel_tol, int32_t max_iter, 
   }
   if (iterations) *iterations = it;
   if (achieved) *achieved = bn > 0 ? rn / bn : 0.0;
+  return AQ_OK;
+}
+
+extern "C" {
+
+aq_status aq_fluid_pcg_reference(aq_fluid* f, double rel_tol, int32_t max_iter, float* pressure_out,
+                                 double* rel_error, int32_t* iterations, double* achieved) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  int it_ = 0;
+  AQ_TRY(fluid_pcg_solve(f, rel_tol, max_iter, &it_, achieved));
+  if (iterations) *iterations = it_;
+  const size_t C = (size_t)f->d.C;
+  cudaStream_t s = f->stream;
   std::vector<double> x(C);
   std::vector<float> p(C);
   std::vector<int8_t> ty(C);

@@ -134,3 +134,8 @@ struct aq_fluid {
   }
 };
 
+namespace aqb {
+// FP64 diagonal-PCG on the fluid's current pressure system (as the last
+// divergence stage built it); the solution is left in f->pcg_x (device).
+aq_status fluid_pcg_solve(aq_fluid* f, double rel_tol, int max_iter, int* iterations, double* achieved);
+}  // namespace aqb

@@ -300,6 +300,236 @@ cudaError_t fwd_relu(cudaStream_t st, bool relu, bool has_bias, const bf16* in, 
               : fwd_bias<CIN, COUT, false>(st, has_bias, in, w, b, out, sx, sy, sz);
 }
 
+// ------------------------------------------------------------ U-Net glue
+// Grid-stride elementwise kernels over channels-last tensors.  Fine grid
+// (sx,sy,sz), coarse grid (sx/2,sy/2,sz/2); every size is even.
+
+__device__ __forceinline__ int coarse_of(int v, int sx, int sy, int sz) {
+  const int z = v % sz, t = v / sz, y = t % sy, x = t / sy;
+  return (((x >> 1) * (sy >> 1) + (y >> 1)) * (sz >> 1)) + (z >> 1);
+}
+
+// max |a[i]| over i < n: per-block maxima, then one block (order-independent)
+__global__ void k_absmax_part(const float* __restrict__ a, int n, float* __restrict__ part) {
+  __shared__ float sm[256];
+  float m = 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = fmaxf(m, fabsf(a[i]));
+  sm[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] = fmaxf(sm[threadIdx.x], sm[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
+}
+__global__ void k_absmax_final(const float* __restrict__ part, int n, float* __restrict__ out) {
+  __shared__ float sm[256];
+  float m = 0.f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, part[i]);
+  sm[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] = fmaxf(sm[threadIdx.x], sm[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sm[0];
+}
+
+// Network input, 16 channels: [rhs / max|rhs|, 1 on fluid cells (0 air), 0 x 14].
+__global__ void k_unet_input(const float* __restrict__ rhs, const int8_t* __restrict__ type,
+                             const float* __restrict__ scale, bf16* __restrict__ out, int V) {
+  const float s = *scale;
+  const float inv = s > 0.f ? 1.f / s : 0.f;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    __align__(16) bf16 row[16];
+    row[0] = __float2bfloat16(rhs[v] * inv);
+    row[1] = __float2bfloat16(type[v] == kFluid ? 1.f : 0.f);
+#pragma unroll
+    for (int c = 2; c < 16; ++c) row[c] = __float2bfloat16(0.f);
+    uint4* dst = reinterpret_cast<uint4*>(out + (size_t)v * 16);
+    dst[0] = reinterpret_cast<const uint4*>(row)[0];
+    dst[1] = reinterpret_cast<const uint4*>(row)[1];
+  }
+}
+
+// 2x2x2 average pooling: out (coarse) from in (fine), C channels.
+__global__ void k_pool2(const bf16* __restrict__ in, bf16* __restrict__ out, int sx, int sy, int sz, int C) {
+  const int cx = sx >> 1, cy = sy >> 1, cz = sz >> 1;
+  const int n = cx * cy * cz * C;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = i % C, V = i / C;
+    const int z = V % cz, t = V / cz, y = t % cy, x = t / cy;
+    float acc = 0.f;
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        for (int e = 0; e < 2; ++e)
+          acc += __bfloat162float(in[((size_t)(((2 * x + a) * sy + 2 * y + b) * sz + 2 * z + e)) * C + c]);
+    out[i] = __float2bfloat16(acc * 0.125f);
+  }
+}
+
+// din (fine) = [din +] dout(coarse parent) / 8
+__global__ void k_pool2_bwd(const bf16* __restrict__ dout, bf16* __restrict__ din, int sx, int sy, int sz, int C,
+                            int accumulate) {
+  const int n = sx * sy * sz * C;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = i % C, v = i / C;
+    float g = __bfloat162float(dout[(size_t)coarse_of(v, sx, sy, sz) * C + c]) * 0.125f;
+    if (accumulate) g += __bfloat162float(din[i]);
+    din[i] = __float2bfloat16(g);
+  }
+}
+
+// out (fine, Cu + Cs channels) = [coarse(parent) (Cu), skip (Cs)]
+__global__ void k_upcat(const bf16* __restrict__ coarse, const bf16* __restrict__ skip, bf16* __restrict__ out,
+                        int sx, int sy, int sz, int Cu, int Cs) {
+  const int C = Cu + Cs;
+  const int n = sx * sy * sz * C;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = i % C, v = i / C;
+    out[i] = c < Cu ? coarse[(size_t)coarse_of(v, sx, sy, sz) * Cu + c] : skip[(size_t)v * Cs + (c - Cu)];
+  }
+}
+
+// dskip = dout[:, Cu:]; dcoarse[P] = sum over the 8 children of dout[:, :Cu]
+__global__ void k_upcat_bwd_skip(const bf16* __restrict__ dout, bf16* __restrict__ dskip, int V, int Cu, int Cs) {
+  const int n = V * Cs;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = i % Cs, v = i / Cs;
+    dskip[i] = dout[(size_t)v * (Cu + Cs) + Cu + c];
+  }
+}
+__global__ void k_upcat_bwd_coarse(const bf16* __restrict__ dout, bf16* __restrict__ dcoarse, int sx, int sy, int sz,
+                                   int Cu, int Cs) {
+  const int cx = sx >> 1, cy = sy >> 1, cz = sz >> 1;
+  const int n = cx * cy * cz * Cu;
+  const int C = Cu + Cs;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = i % Cu, V = i / Cu;
+    const int z = V % cz, t = V / cz, y = t % cy, x = t / cy;
+    float acc = 0.f;
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        for (int e = 0; e < 2; ++e)
+          acc += __bfloat162float(dout[((size_t)(((2 * x + a) * sy + 2 * y + b) * sz + 2 * z + e)) * C + c]);
+    dcoarse[i] = __float2bfloat16(acc);
+  }
+}
+
+// dy = y > 0 ? dy : 0 (ReLU backward, y the layer's output)
+__global__ void k_relu_bwd(bf16* __restrict__ dy, const bf16* __restrict__ y, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (!(__bfloat162float(y[i]) > 0.f)) dy[i] = __float2bfloat16(0.f);
+}
+
+// Per-block channel sums of dy (V x C) over `rows` consecutive voxels.
+__global__ void k_chan_sum_part(const bf16* __restrict__ dy, int V, int C, int rows, float* __restrict__ part) {
+  const int v0 = blockIdx.x * rows, v1 = min(V, v0 + rows);
+  for (int c = threadIdx.x; c < C; c += blockDim.x) {
+    float s = 0.f;
+    for (int v = v0; v < v1; ++v) s += __bfloat162float(dy[(size_t)v * C + c]);
+    part[(size_t)blockIdx.x * C + c] = s;
+  }
+}
+
+// Output head: out[v] = b + sum_c w[c] h[v][c] (16 channels), f32
+__global__ void k_head_fwd(const bf16* __restrict__ h, const float* __restrict__ w, const float* __restrict__ b,
+                           float* __restrict__ out, int V) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    float s = *b;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) s += w[c] * __bfloat162float(h[(size_t)v * 16 + c]);
+    out[v] = s;
+  }
+}
+
+// Loss over fluid cells, L = sum (out - t)^2 / n_fluid, and its gradients:
+// dh[v][c] = g_v w[c] with g_v = 2 (out - t) / n_fluid (0 off fluid); per
+// block partial sums of g_v h[v][c] (16), g_v, and the loss.
+__global__ void __launch_bounds__(256) k_head_loss_bwd(const float* __restrict__ out, const float* __restrict__ target,
+                                                       const int8_t* __restrict__ type, const bf16* __restrict__ h,
+                                                       const float* __restrict__ w, const float* __restrict__ nf,
+                                                       bf16* __restrict__ dh, int V, float* __restrict__ part) {
+  __shared__ float sm[18][256];
+  float acc[18];
+#pragma unroll
+  for (int k = 0; k < 18; ++k) acc[k] = 0.f;
+  const float inv = *nf > 0.f ? 1.f / *nf : 0.f;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const bool fl = type[v] == kFluid;
+    const float e = fl ? out[v] - target[v] : 0.f;
+    const float g = 2.f * e * inv;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const float hv = __bfloat162float(h[(size_t)v * 16 + c]);
+      acc[c] += g * hv;
+      dh[(size_t)v * 16 + c] = __float2bfloat16(g * w[c]);
+    }
+    acc[16] += g;
+    acc[17] += e * e * inv;
+  }
+#pragma unroll
+  for (int k = 0; k < 18; ++k) sm[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+#pragma unroll
+      for (int k = 0; k < 18; ++k) sm[k][threadIdx.x] += sm[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x < 18) part[(size_t)blockIdx.x * 18 + threadIdx.x] = sm[threadIdx.x][0];
+}
+
+// Adam (bias-corrected) on n parameters; refreshes the bf16 copy if given.
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2,
+                       bf16* __restrict__ wb) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16(wi);
+  }
+}
+
+__global__ void k_scale_copy(const float* __restrict__ a, float k, float* __restrict__ b, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i] * k;
+}
+
+__global__ void k_f32_to_bf16(const float* __restrict__ a, bf16* __restrict__ b, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = __float2bfloat16(a[i]);
+}
+
+// Warm start: p = out * scale * out_scale on fluid cells, 0 elsewhere.
+__global__ void k_unet_to_pressure(const float* __restrict__ out, const float* __restrict__ scale, float out_scale,
+                                   const int8_t* __restrict__ type, float* __restrict__ p, int V) {
+  const float s = *scale * out_scale;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+    p[v] = type[v] == kFluid ? out[v] * s : 0.f;
+}
+
+// Dataset sample: rhs / scale, type, target p / scale.
+__global__ void k_unet_sample(const float* __restrict__ rhs, const int8_t* __restrict__ type,
+                              const double* __restrict__ p, const float* __restrict__ scale, float* __restrict__ rhs_s,
+                              int8_t* __restrict__ type_s, float* __restrict__ target, int V) {
+  const float s = *scale;
+  const float inv = s > 0.f ? 1.f / s : 0.f;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    rhs_s[v] = rhs[v] * inv;
+    type_s[v] = type[v];
+    target[v] = type[v] == kFluid ? (float)p[v] * inv : 0.f;
+  }
+}
+
+inline int ew_grid(long long n) {
+  const long long b = (n + 255) / 256;
+  return (int)std::min<long long>(std::max<long long>(b, 1), 148 * 16);
+}
+
 }  // namespace
 
 int unet_wgrad_chunk(int voxels) {
@@ -362,6 +592,94 @@ size_t conv3_wgrad_part_floats(int cin, int cout, int voxels) {
 cudaError_t launch_flip_transpose(cudaStream_t st, const void* w, void* wt, int cin, int cout) {
   const int n = 27 * cin * cout;
   k_flip_transpose<<<(n + 255) / 256, 256, 0, st>>>((const bf16*)w, (bf16*)wt, cin, cout);
+  return cudaGetLastError();
+}
+
+}  // namespace aqb
+
+namespace aqb {
+
+cudaError_t launch_absmax(cudaStream_t st, const float* a, int n, float* part /*>= 1024*/, float* out) {
+  const int g = std::min(1024, std::max(1, (n + 255) / 256));
+  k_absmax_part<<<g, 256, 0, st>>>(a, n, part);
+  k_absmax_final<<<1, 256, 0, st>>>(part, g, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_unet_input(cudaStream_t st, const float* rhs, const int8_t* type, const float* scale, void* out,
+                              int V) {
+  k_unet_input<<<ew_grid(V), 256, 0, st>>>(rhs, type, scale, (bf16*)out, V);
+  return cudaGetLastError();
+}
+cudaError_t launch_pool2(cudaStream_t st, const void* in, void* out, int sx, int sy, int sz, int C) {
+  k_pool2<<<ew_grid((long long)sx * sy * sz * C / 8), 256, 0, st>>>((const bf16*)in, (bf16*)out, sx, sy, sz, C);
+  return cudaGetLastError();
+}
+cudaError_t launch_pool2_bwd(cudaStream_t st, const void* dout, void* din, int sx, int sy, int sz, int C,
+                             bool accumulate) {
+  k_pool2_bwd<<<ew_grid((long long)sx * sy * sz * C), 256, 0, st>>>((const bf16*)dout, (bf16*)din, sx, sy, sz, C,
+                                                                    accumulate ? 1 : 0);
+  return cudaGetLastError();
+}
+cudaError_t launch_upcat(cudaStream_t st, const void* coarse, const void* skip, void* out, int sx, int sy, int sz,
+                         int Cu, int Cs) {
+  k_upcat<<<ew_grid((long long)sx * sy * sz * (Cu + Cs)), 256, 0, st>>>((const bf16*)coarse, (const bf16*)skip,
+                                                                        (bf16*)out, sx, sy, sz, Cu, Cs);
+  return cudaGetLastError();
+}
+cudaError_t launch_upcat_bwd(cudaStream_t st, const void* dout, void* dcoarse, void* dskip, int sx, int sy, int sz,
+                             int Cu, int Cs) {
+  const int V = sx * sy * sz;
+  k_upcat_bwd_skip<<<ew_grid((long long)V * Cs), 256, 0, st>>>((const bf16*)dout, (bf16*)dskip, V, Cu, Cs);
+  k_upcat_bwd_coarse<<<ew_grid((long long)V / 8 * Cu), 256, 0, st>>>((const bf16*)dout, (bf16*)dcoarse, sx, sy, sz,
+                                                                     Cu, Cs);
+  return cudaGetLastError();
+}
+cudaError_t launch_relu_bwd(cudaStream_t st, void* dy, const void* y, int n) {
+  k_relu_bwd<<<ew_grid(n), 256, 0, st>>>((bf16*)dy, (const bf16*)y, n);
+  return cudaGetLastError();
+}
+int chan_sum_parts(int V) { return std::min(1024, std::max(1, (V + 255) / 256)); }
+cudaError_t launch_chan_sum(cudaStream_t st, const void* dy, int V, int C, float* part, float* out) {
+  const int np = chan_sum_parts(V);
+  const int rows = (V + np - 1) / np;
+  k_chan_sum_part<<<np, 64, 0, st>>>((const bf16*)dy, V, C, rows, part);
+  k_sum_parts<<<(C + 255) / 256, 256, 0, st>>>(part, np, C, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_head_fwd(cudaStream_t st, const void* h, const float* w, const float* b, float* out, int V) {
+  k_head_fwd<<<ew_grid(V), 256, 0, st>>>((const bf16*)h, w, b, out, V);
+  return cudaGetLastError();
+}
+int head_parts() { return 296; }
+cudaError_t launch_head_loss_bwd(cudaStream_t st, const float* out, const float* target, const int8_t* type,
+                                 const void* h, const float* w, const float* nf, void* dh, int V, float* part,
+                                 float* sums /* 18: dw[16], db, loss */) {
+  k_head_loss_bwd<<<head_parts(), 256, 0, st>>>(out, target, type, (const bf16*)h, w, nf, (bf16*)dh, V, part);
+  k_sum_parts<<<1, 32, 0, st>>>(part, head_parts(), 18, sums);
+  return cudaGetLastError();
+}
+cudaError_t launch_adam(cudaStream_t st, float* w, const float* g, float* m, float* v, int n, float lr, float b1,
+                        float b2, float eps, int t, void* wb) {
+  const float c1 = 1.f - powf(b1, (float)t), c2 = 1.f - powf(b2, (float)t);
+  k_adam<<<ew_grid(n), 256, 0, st>>>(w, g, m, v, n, lr, b1, b2, eps, c1, c2, (bf16*)wb);
+  return cudaGetLastError();
+}
+cudaError_t launch_f32_to_bf16(cudaStream_t st, const float* a, void* b, int n) {
+  k_f32_to_bf16<<<ew_grid(n), 256, 0, st>>>(a, (bf16*)b, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_unet_to_pressure(cudaStream_t st, const float* out, const float* scale, float out_scale,
+                                    const int8_t* type, float* p, int V) {
+  k_unet_to_pressure<<<ew_grid(V), 256, 0, st>>>(out, scale, out_scale, type, p, V);
+  return cudaGetLastError();
+}
+cudaError_t launch_unet_scale_copy(cudaStream_t st, const float* a, float k, float* b, int n) {
+  k_scale_copy<<<ew_grid(n), 256, 0, st>>>(a, k, b, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_unet_sample(cudaStream_t st, const float* rhs, const int8_t* type, const double* p,
+                               const float* scale, float* rhs_s, int8_t* type_s, float* target, int V) {
+  k_unet_sample<<<ew_grid(V), 256, 0, st>>>(rhs, type, p, scale, rhs_s, type_s, target, V);
   return cudaGetLastError();
 }
 

@@ -354,6 +354,59 @@ aq_status aq_conv3_weight_grad(int32_t cin, int32_t cout, const void* x, const v
                                int32_t sy, int32_t sz, void* stream);
 aq_status aq_conv3_flip_transpose(int32_t cin, int32_t cout, const void* w, void* wt, void* stream);
 
+/* ---- Learned pressure warm start: network, dataset, training ---------------
+ * No counterpart in the reference.  A 3-level 3D U-Net (16/32/64 channels,
+ * 3x3x3 convolutions + ReLU, average pooling, upsampling with skip
+ * concatenation, 1x1x1 head), BF16 weights and activations with FP32
+ * accumulation, trained by the library's own kernels (Adam, FP32 master
+ * weights) on pressure systems labelled by the FP64 PCG.  Input: the pressure
+ * right-hand side (-divergence x density) scaled by its max-abs, and the
+ * fluid mark; output: the pressure, used to warm-start the Jacobi solve
+ * (AQ_PRESSURE_LEARNED).  Grid sizes must be divisible by 4.  A network runs
+ * on its own stream; it must not be trained while a fluid step that uses it
+ * is in flight, and fluids sharing it must not step concurrently. */
+typedef struct aq_unet aq_unet;
+typedef struct aq_dataset aq_dataset;
+
+aq_status aq_unet_create(int32_t device, uint32_t seed, aq_unet** out);
+void aq_unet_destroy(aq_unet* net);
+aq_status aq_unet_parameter_count(const aq_unet* net, int64_t* count);
+/* Weights file: magic, version, output scale, per layer (cin, cout, f32
+ * weights [27][cout][cin], f32 bias [cout]), head (16 weights, bias). */
+aq_status aq_unet_save(aq_unet* net, const char* path);
+aq_status aq_unet_load(aq_unet* net, const char* path);
+aq_status aq_unet_get_output_scale(const aq_unet* net, float* scale);
+/* Forward pass on device buffers (rhs [C] f32, type [C] int8 0 air / 1
+ * fluid): pressure [C] = warm start (0 off fluid).  stream NULL = the
+ * network's stream. */
+aq_status aq_unet_predict(aq_unet* net, int32_t sx, int32_t sy, int32_t sz, const float* rhs, const int8_t* type,
+                          float* pressure, void* stream);
+
+/* Device-resident training pairs of one grid size. */
+aq_status aq_dataset_create(int32_t sx, int32_t sy, int32_t sz, int32_t capacity, int32_t device, aq_dataset** out);
+void aq_dataset_destroy(aq_dataset* ds);
+int32_t aq_dataset_count(const aq_dataset* ds);
+/* Adds the fluid's current pressure system (as its last divergence stage
+ * built it) labelled by an FP64 PCG solve to pcg_rel_tol. */
+aq_status aq_dataset_add_fluid(aq_dataset* ds, aq_fluid* f, double pcg_rel_tol, int32_t pcg_max_iter,
+                               int32_t* pcg_iterations);
+aq_status aq_dataset_target_rms(aq_dataset* ds, int32_t first, int32_t count, double* rms);
+/* Host copy of sample i: rhs / max|rhs| [C], type [C], pressure / max|rhs| [C]
+ * (any pointer may be NULL). */
+aq_status aq_dataset_get(aq_dataset* ds, int32_t i, float* rhs, int8_t* type, float* target);
+/* `steps` Adam steps (one sample each, drawn with `seed` from samples
+ * [first, first+count)), cosine-decayed learning rate from lr.  out_scale <= 0
+ * sets the network's output scale to the targets' RMS.  mean_loss: mean MSE
+ * (over fluid cells, in output-scale units) of the last tenth of the steps. */
+aq_status aq_unet_train(aq_unet* net, aq_dataset* ds, int32_t first, int32_t count, int32_t steps, float lr,
+                        uint32_t seed, float out_scale, float* mean_loss);
+/* Mean over samples of the relative L2 error (fluid cells) of the prediction
+ * against the FP64 PCG pressure. */
+aq_status aq_unet_evaluate(aq_unet* net, aq_dataset* ds, int32_t first, int32_t count, double* mean_rel_error);
+/* The gradients of the last training step, in weights-file order (per layer
+ * weights then bias, then head weights and bias); n = parameter count. */
+aq_status aq_unet_gradients(aq_unet* net, float* out, int64_t n);
+
 /* Largest grid (sx*sy*sz cells) aq_jacobi_sweeps_noalloc accepts. */
 #define AQ_NOALLOC_MAX_CELLS (64 * 64 * 64)
 
