@@ -118,6 +118,7 @@ def load_library() -> ct.CDLL:
                                      ct.POINTER(ct.c_float)]),
         "aq_unet_evaluate": (ct.c_int, [P, P, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_double)]),
         "aq_unet_gradients": (ct.c_int, [P, P, ct.c_int64]),
+        "aq_fluid_set_warm_start": (ct.c_int, [P, P]),
         "aq_dataset_create": (ct.c_int, [ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.POINTER(P)]),
         "aq_dataset_destroy": (None, [P]),
         "aq_dataset_count": (ct.c_int32, [P]),
@@ -215,7 +216,8 @@ class FluidConfig:
             pressure_iterations=f.pressureIterations, diffusion_iterations=f.diffusionIterations,
             timestep=f.timestep, flip_coeff=f.FLIPcoeff, particle_jitter=f.particleJitter,
             domain_size=self.gridPhysicalSize, seed=self.seed,
-            pressure_init={"carry": _abi.PRESSURE_CARRY, "zero": _abi.PRESSURE_ZERO}[self.pressureInit],
+            pressure_init={"carry": _abi.PRESSURE_CARRY, "zero": _abi.PRESSURE_ZERO,
+                           "learned": _abi.PRESSURE_LEARNED}[self.pressureInit],
             solve_mode={"fixed": _abi.SOLVE_FIXED, "residual": _abi.SOLVE_RESIDUAL}[self.solveMode],
             rel_residual=self.relResidual, max_iterations=self.maxIterations,
             check_interval=self.checkInterval, device=self.device, stream=self.stream)
@@ -312,9 +314,12 @@ class Fluid:
     def solve_stats(self) -> dict:
         s = _abi.SolveStats()
         _check(self._lib.aq_fluid_solve_stats(self._h, ct.byref(s)))
-        return {"iterations": s.iterations, "rel_residual": s.rel_residual, "b_norm": s.b_norm,
-                "fluid_cells": s.fluid_cells, "converged": bool(s.converged), "blocks": s.blocks,
-                "total_sweeps": s.total_sweeps, "total_blocks": s.total_blocks}
+        return _solve_stats_dict(s)
+
+    def set_warm_start(self, net):
+        """Attaches the network AQ_PRESSURE_LEARNED ('learned') uses (None detaches)."""
+        self._net = net
+        _check(self._lib.aq_fluid_set_warm_start(self._h, None if net is None else net.handle))
 
     def pcg_reference(self, rel_tol: float = 1e-12, max_iter: int = 100000, want_pressure: bool = False):
         """FP64 PCG solve of the current pressure system; returns the relative
@@ -388,7 +393,8 @@ class Fluid:
 def _solve_stats_dict(s) -> dict:
     return {"iterations": s.iterations, "rel_residual": s.rel_residual, "b_norm": s.b_norm,
             "fluid_cells": s.fluid_cells, "converged": bool(s.converged), "blocks": s.blocks,
-            "total_sweeps": s.total_sweeps, "total_blocks": s.total_blocks}
+            "total_sweeps": s.total_sweeps, "total_blocks": s.total_blocks, "warm_start": s.warm_start,
+            "warm_rel_residual": s.warm_rel_residual, "zero_rel_residual": s.zero_rel_residual}
 
 
 class Batch:

@@ -25,6 +25,7 @@ SHAPE_SPHERE = 0
 SHAPE_SQUARE = 1
 PRESSURE_CARRY = 0
 PRESSURE_ZERO = 1
+PRESSURE_LEARNED = 2
 SOLVE_FIXED = 0
 SOLVE_RESIDUAL = 1
 
@@ -124,6 +125,9 @@ class SolveStats(ct.Structure):
         ("blocks", ct.c_int32),
         ("total_sweeps", ct.c_int64),
         ("total_blocks", ct.c_int64),
+        ("warm_start", ct.c_int32),
+        ("warm_rel_residual", ct.c_double),
+        ("zero_rel_residual", ct.c_double),
     ]
 
 

@@ -119,6 +119,9 @@ struct SolveState {
   int sync_timeout;  // the persistent solve gave up waiting at a grid barrier
   long long total_sweeps;  // cumulative over the fluid's life
   long long total_bodies;
+  int warm;                // learned warm start: 1 prediction kept, 2 zero-init fallback, 0 none
+  double warm_rel;         // relative residuals after the first 20 sweeps of each start
+  double zero_rel;
 };
 
 }  // namespace aqb

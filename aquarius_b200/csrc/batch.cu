@@ -385,6 +385,8 @@ aq_status aq_batch_create(const aq_config* configs, int32_t n_scenes, aq_batch**
     NB += (long long)cdiv(c.size_x, kBrick) * cdiv(c.size_y, kBrick) * cdiv(c.size_z, kBrick);
     NRP += (long long)((c.size_z / 4 + 31) / 32) * ((c.size_y + 7) / 8) * c.size_x;
   }
+  if (c0.pressure_init == AQ_PRESSURE_LEARNED)
+    return fail(AQ_ERR_INVALID_CONFIG, "batched scenes do not take the learned warm start");
   if (c0.solve_mode == AQ_SOLVE_RESIDUAL && c0.check_interval % 2 != 0)
     return fail(AQ_ERR_INVALID_CONFIG, "batched residual solves need an even check_interval");
   if (C + 1 >= (1LL << 31) || F >= (1LL << 31)) return fail(AQ_ERR_INVALID_CONFIG, "batch too large for 32-bit indices");
@@ -596,6 +598,9 @@ aq_status aq_batch_solve_stats(aq_batch* b, int32_t scene, aq_solve_stats* out) 
   out->blocks = s.bodies;
   out->total_sweeps = s.total_sweeps;
   out->total_blocks = s.total_bodies;
+  out->warm_start = s.warm;
+  out->warm_rel_residual = s.warm_rel;
+  out->zero_rel_residual = s.zero_rel;
   return AQ_OK;
 }
 

@@ -17,6 +17,7 @@
 
 #include "../../include/aquarius_b200.h"
 #include "fluid_impl.cuh"
+#include "unet_impl.cuh"
 
 using namespace aqb;
 
@@ -41,6 +42,55 @@ thread_local std::string g_last_error;
 __global__ void k_copy_f(const float* __restrict__ a, float* __restrict__ b, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = a[i];
+}
+
+// Sweeps run from each start of the learned warm start before they are compared.
+constexpr int kWarmSweeps = 20;
+
+// Learned warm start: compares the FP64 residuals after kWarmSweeps sweeps
+// from the network's prediction and from zero (partial sums summed in the
+// fixed order of the residual finaliser); the zero-init path wins when the
+// prediction's residual is larger (or not finite).
+__global__ void __launch_bounds__(1024) k_pick_start(const double* __restrict__ pl, const double* __restrict__ pz,
+                                                     int nparts, SolveState* __restrict__ ss, int* __restrict__ pick,
+                                                     double tol) {
+  __shared__ double sa[1024], sb[1024];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += 1024) {
+    a += pl[i];
+    b += pz[i];
+  }
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int o = 512; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sa[threadIdx.x] += sa[threadIdx.x + o];
+      sb[threadIdx.x] += sb[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double bn = ss->b2 > 0.0 ? sqrt(ss->b2) : 0.0;
+    const double rl = bn > 0.0 ? sqrt(sa[0]) / bn : 0.0, rz = bn > 0.0 ? sqrt(sb[0]) / bn : 0.0;
+    const bool zero_wins = !(rl <= rz);
+    *pick = zero_wins ? 1 : 0;
+    ss->warm = zero_wins ? 2 : 1;
+    ss->warm_rel = rl;
+    ss->zero_rel = rz;
+    const double rel = zero_wins ? rz : rl;
+    ss->iterations = kWarmSweeps;
+    ss->total_sweeps += 2 * kWarmSweeps;
+    ss->r2 = zero_wins ? sb[0] : sa[0];
+    ss->rel_residual = rel;
+    if (!isfinite(rel)) ss->nonfinite = 1;
+    ss->converged = (isfinite(rel) && rel <= tol) ? 1 : 0;
+  }
+}
+
+__global__ void k_copy_if(const int* __restrict__ pick, const float* __restrict__ a, float* __restrict__ b, int n) {
+  if (*pick == 0) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
 
 int covered_faces(int s1, int s2) {  // fixBoundary launch coverage (Fluid/Fluid_3D_common.cu:13-41)
@@ -222,7 +272,7 @@ aq_status aq_fluid::enq_p2g(bool forces) {
 aq_status aq_fluid::enq_divergence() {
   int nb = 0;
   AQ_CUDA(launch_divergence(stream, d, off, type, density, nvx(nv_cur), nvy(nv_cur), nvz(nv_cur), pcount, div,
-                            rhs, pa, pb, cfg.pressure_init == AQ_PRESSURE_ZERO, bact, part_b2, part_nf, &nb));
+                            rhs, pa, pb, cfg.pressure_init != AQ_PRESSURE_CARRY, bact, part_b2, part_nf, &nb));
   AQ_CUDA(launch_b2_finalize(stream, part_b2, part_nf, nb, ss));
   return AQ_OK;
 }
@@ -251,34 +301,62 @@ int aq_fluid::count_jacobi_launches(int sweeps) const {
 // iterate are written to jpart; the result ends in pa.  Tiled plans fuse the
 // residual into their last launch (one extra level); the flat plan computes
 // it with one residual pass over the final iterate.
-static aq_status enqueue_sweeps(aq_fluid* f, int sweeps, bool with_residual = true) {
-  const std::vector<int> parts = split_sweeps(sweeps, f->plan.levels);
-  const bool flat = f->plan.by == 0;
-  float* bufs[2] = {f->pa, f->pb};
+// The same with an explicit plan and buffer pair (result in `a`, residual
+// partials in `part`).
+static aq_status enqueue_sweeps_on(aq_fluid* f, const JacobiPlan& plan, float* a, float* b, int sweeps,
+                                   bool with_residual, double* part) {
+  const std::vector<int> parts = split_sweeps(sweeps, plan.levels);
+  const bool flat = plan.by == 0;
+  float* bufs[2] = {a, b};
   for (size_t k = 0; k < parts.size(); ++k) {
     const bool last = k + 1 == parts.size();
-    JacobiPlan p = f->plan;
+    JacobiPlan p = plan;
     p.levels = parts[k];
     int np = 0;
     AQ_CUDA(launch_jacobi(f->stream, f->d, p, last && with_residual && !flat, bufs[k % 2], bufs[(k + 1) % 2],
-                          f->rhs, f->type, f->bact, f->jpart, &np));
+                          f->rhs, f->type, f->bact, part, &np));
   }
   if (flat && with_residual && !parts.empty())
-    AQ_CUDA(launch_resid_flat(f->stream, f->d, bufs[parts.size() % 2], f->rhs, f->type, f->bact, f->jpart));
+    AQ_CUDA(launch_resid_flat(f->stream, f->d, bufs[parts.size() % 2], f->rhs, f->type, f->bact, part));
   if (parts.size() % 2 == 1) {
-    k_copy_f<<<(f->d.C + 255) / 256, 256, 0, f->stream>>>(f->pb, f->pa, f->d.C);
+    k_copy_f<<<(f->d.C + 255) / 256, 256, 0, f->stream>>>(b, a, f->d.C);
     AQ_CUDA(cudaGetLastError());
   }
   return AQ_OK;
 }
 
-static int last_parts(const aq_fluid* f, int sweeps) {
-  const std::vector<int> parts = split_sweeps(sweeps, f->plan.levels);
+static aq_status enqueue_sweeps(aq_fluid* f, int sweeps, bool with_residual = true) {
+  return enqueue_sweeps_on(f, f->plan, f->pa, f->pb, sweeps, with_residual, f->jpart);
+}
+
+static int last_parts_of(const aq_fluid* f, const JacobiPlan& plan, int sweeps) {
+  const std::vector<int> parts = split_sweeps(sweeps, plan.levels);
   if (parts.empty()) return 0;
-  if (f->plan.by == 0) return resid_flat_parts(f->d);
-  JacobiPlan p = f->plan;
+  if (plan.by == 0) return resid_flat_parts(f->d);
+  JacobiPlan p = plan;
   p.levels = parts.back();
   return jacobi_parts(f->d, p, true);
+}
+
+static int last_parts(const aq_fluid* f, int sweeps) { return last_parts_of(f, f->plan, sweeps); }
+
+int aq_fluid::solve_sweeps_done() const { return cfg.pressure_init == AQ_PRESSURE_LEARNED ? kWarmSweeps : 0; }
+
+// AQ_PRESSURE_LEARNED: pa <- network prediction; kWarmSweeps sweeps from it
+// and from zero; the solve continues in pa from the better of the two.
+aq_status aq_fluid::enq_learned_start() {
+  if (!net || !net_acts) return fail(AQ_ERR_INVALID_CONFIG, "AQ_PRESSURE_LEARNED needs a network (aq_fluid_set_warm_start)");
+  AQ_TRY(unet_predict(net, stream, net_acts, rhs, type, pa));
+  AQ_TRY(enqueue_sweeps_on(this, plan, pa, pb, kWarmSweeps, true, jpart));
+  AQ_CUDA(cudaMemsetAsync(za, 0, sizeof(float) * d.C, stream));
+  AQ_CUDA(cudaMemsetAsync(zb, 0, sizeof(float) * d.C, stream));
+  AQ_TRY(enqueue_sweeps_on(this, plan, za, zb, kWarmSweeps, true, jpart2));
+  k_pick_start<<<1, 1024, 0, stream>>>(jpart, jpart2, last_parts(this, kWarmSweeps), ss, pick,
+                                       cfg.solve_mode == AQ_SOLVE_RESIDUAL ? (double)cfg.rel_residual : 0.0);
+  AQ_CUDA(cudaGetLastError());
+  k_copy_if<<<std::min((d.C + 255) / 256, 148 * 8), 256, 0, stream>>>(pick, za, pa, d.C);
+  AQ_CUDA(cudaGetLastError());
+  return AQ_OK;
 }
 
 // The whole solve as one cooperative launch (plan.by == 1).
@@ -383,12 +461,13 @@ aq_status aq_fluid::run_stage(int stage) {
     case AQ_STAGE_P2G: return enq_p2g(true);
     case AQ_STAGE_DIVERGENCE: return enq_divergence();
     case AQ_STAGE_PRESSURE:
-      if (cfg.pressure_init == AQ_PRESSURE_ZERO) {  // done by the divergence kernel inside a step
+      if (cfg.pressure_init != AQ_PRESSURE_CARRY) {  // done by the divergence kernel inside a step
         AQ_CUDA(cudaMemsetAsync(pa, 0, sizeof(float) * d.C, stream));
         AQ_CUDA(cudaMemsetAsync(pb, 0, sizeof(float) * d.C, stream));
       }
+      if (cfg.pressure_init == AQ_PRESSURE_LEARNED) AQ_TRY(enq_learned_start());
       if (cfg.solve_mode == AQ_SOLVE_RESIDUAL) return enq_solve_residual_eager();
-      return enq_solve_fixed(cfg.pressure_iterations);
+      return enq_solve_fixed(cfg.pressure_iterations - solve_sweeps_done());
     case AQ_STAGE_PROJECT: return enq_project();
     case AQ_STAGE_EXTRAPOLATE: return enq_extrapolate();
     case AQ_STAGE_DIFFUSE:
@@ -404,6 +483,7 @@ aq_status aq_fluid::enq_pre_solve() {
   AQ_TRY(enq_particles(true));
   AQ_TRY(enq_p2g(true));
   AQ_TRY(enq_divergence());
+  if (cfg.pressure_init == AQ_PRESSURE_LEARNED) AQ_TRY(enq_learned_start());
   return AQ_OK;
 }
 
@@ -486,14 +566,17 @@ aq_status aq_fluid::build_graph() {
     st = capture(g, nullptr, 0, [&]() {
       aq_status s2 = enq_pre_solve();
       if (s2 != AQ_OK) return s2;
-      s2 = enq_solve_fixed(cfg.pressure_iterations);
+      s2 = enq_solve_fixed(cfg.pressure_iterations - solve_sweeps_done());
       if (s2 != AQ_OK) return s2;
       return enq_post_solve();
     });
-    launches += cfg.pressure_iterations > 0 ? count_jacobi_launches(cfg.pressure_iterations) : 0;
+    const int rest = cfg.pressure_iterations - solve_sweeps_done();
+    launches += rest > 0 ? count_jacobi_launches(rest) : 0;
     body_launches = 0;
   }
   if (st != AQ_OK) { cudaGraphDestroy(g); return st; }
+  if (cfg.pressure_init == AQ_PRESSURE_LEARNED)  // network, two 20-sweep starts, pick, copy
+    launches += kUNetForwardLaunches + 2 * (count_jacobi_launches(kWarmSweeps) - 1) + 2;
   launches += 1 + 3 + (multiphase ? cfg.diffusion_iterations : 0);
   graph_launches = launches;
   cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
@@ -507,7 +590,7 @@ aq_status aq_fluid::step(int nsteps) {
     for (int i = 0; i < nsteps; ++i) {
       AQ_TRY(enq_pre_solve());
       if (cfg.solve_mode == AQ_SOLVE_RESIDUAL) AQ_TRY(enq_solve_residual_eager());
-      else AQ_TRY(enq_solve_fixed(cfg.pressure_iterations));
+      else AQ_TRY(enq_solve_fixed(cfg.pressure_iterations - solve_sweeps_done()));
       AQ_TRY(enq_post_solve());
       time += (double)cfg.timestep;
     }
@@ -889,8 +972,15 @@ aq_status validate(const aq_config* c) {
   if (!std::isfinite(c->timestep) || c->timestep < 0.f) return fail(AQ_ERR_INVALID_CONFIG, "timestep must be >= 0");
   if (c->pressure_iterations < 0 || c->diffusion_iterations < 0)
     return fail(AQ_ERR_INVALID_CONFIG, "iteration counts must be >= 0");
-  if (c->pressure_init != AQ_PRESSURE_CARRY && c->pressure_init != AQ_PRESSURE_ZERO)
+  if (c->pressure_init != AQ_PRESSURE_CARRY && c->pressure_init != AQ_PRESSURE_ZERO &&
+      c->pressure_init != AQ_PRESSURE_LEARNED)
     return fail(AQ_ERR_INVALID_CONFIG, "unknown pressure_init");
+  if (c->pressure_init == AQ_PRESSURE_LEARNED) {
+    if (c->size_x % 4 || c->size_y % 4 || c->size_z % 4)
+      return fail(AQ_ERR_INVALID_CONFIG, "the learned warm start needs grid sizes divisible by 4");
+    if (c->solve_mode == AQ_SOLVE_FIXED && c->pressure_iterations < kWarmSweeps)
+      return fail(AQ_ERR_INVALID_CONFIG, "the learned warm start needs pressure_iterations >= 20");
+  }
   if (c->solve_mode != AQ_SOLVE_FIXED && c->solve_mode != AQ_SOLVE_RESIDUAL)
     return fail(AQ_ERR_INVALID_CONFIG, "unknown solve_mode");
   if (c->solve_mode == AQ_SOLVE_RESIDUAL) {
@@ -1123,6 +1213,35 @@ aq_status aq_fluid_solve_stats(const aq_fluid* f, aq_solve_stats* st) {
   st->blocks = s.bodies;
   st->total_sweeps = s.total_sweeps;
   st->total_blocks = s.total_bodies;
+  st->warm_start = s.warm;
+  st->warm_rel_residual = s.warm_rel;
+  st->zero_rel_residual = s.zero_rel;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_set_warm_start(aq_fluid* f, aq_unet* net) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  cudaSetDevice(f->device);
+  AQ_CUDA(cudaStreamSynchronize(f->stream));
+  f->invalidate_graph();
+  if (!net) {
+    f->net = nullptr;
+    f->net_acts = nullptr;
+    return AQ_OK;
+  }
+  if (net->device != f->device) return fail(AQ_ERR_INVALID_ARGUMENT, "network and fluid are on different devices");
+  aqb::UActs* acts = nullptr;
+  AQ_TRY(unet_acts(net, f->d.sx, f->d.sy, f->d.sz, false, &acts));
+  if (!f->za) {
+    AQ_TRY(f->alloc(&f->za, (size_t)f->d.C));
+    AQ_TRY(f->alloc(&f->zb, (size_t)f->d.C));
+    AQ_TRY(f->alloc(&f->jpart2, (size_t)f->jpart_cap));
+    AQ_TRY(f->alloc(&f->pick, 1));
+  }
+  if (f->plan.by == 1) f->plan = f->d.sz % 4 == 0 ? JacobiPlan{1, 0, 1} : JacobiPlan{2, 16, 16};
+  AQ_CUDA(cudaStreamSynchronize(net->stream));
+  f->net = net;
+  f->net_acts = acts;
   return AQ_OK;
 }
 
@@ -1141,6 +1260,8 @@ aq_status aq_fluid_launches_per_step(const aq_fluid* f, int32_t* launches) {
 
 aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, int32_t x_planes) {
   if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  if (rows == 1 && f->cfg.pressure_init == AQ_PRESSURE_LEARNED)
+    return fail(AQ_ERR_INVALID_ARGUMENT, "the persistent solve does not take the learned warm start");
   if (rows == 1) {  // persistent cooperative solve
     if (levels != 1 || f->d.sz % 4 != 0 || f->ctas <= 0)
       return fail(AQ_ERR_INVALID_ARGUMENT, "persistent solve needs sz % 4 == 0");

@@ -10,6 +10,7 @@
 
 namespace aqb {
 inline aq_status fail(aq_status st, const std::string& msg) { return set_last_error(st, msg); }
+struct UActs;
 }  // namespace aqb
 
 struct aq_fluid {
@@ -64,6 +65,12 @@ struct aq_fluid {
   int ctas = 0;
 
   JacobiPlan plan{4, 16, 32};
+  // learned warm start (AQ_PRESSURE_LEARNED)
+  aq_unet* net = nullptr;
+  aqb::UActs* net_acts = nullptr;
+  float *za = nullptr, *zb = nullptr;  // the zero-init path of the first sweeps
+  double* jpart2 = nullptr;
+  int* pick = nullptr;  // 1: the zero-init path won
   cudaGraphExec_t exec = nullptr;
   bool use_graph = true;
   int graph_launches = 0;  // launches outside the residual loop
@@ -113,6 +120,8 @@ struct aq_fluid {
   aq_status enq_solve_fixed(int sweeps);
   aq_status enq_solve_body(bool set_cond, unsigned long long handle, int* launches);
   aq_status enq_solve_residual_eager();
+  aq_status enq_learned_start();
+  int solve_sweeps_done() const;  // sweeps the warm start already did (0 without it)
   aq_status enq_project();
   aq_status enq_extrapolate();
   aq_status enq_diffuse();

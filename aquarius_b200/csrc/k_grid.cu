@@ -293,6 +293,9 @@ __device__ __forceinline__ void b2_finalize_body(const double* __restrict__ part
     ss->nonfinite = 0;
     ss->rel_residual = -1.0;
     ss->r2 = -1.0;
+    ss->warm = 0;
+    ss->warm_rel = -1.0;
+    ss->zero_rel = -1.0;
   }
 }
 

@@ -50,14 +50,15 @@ struct aq_unet {
   float out_scale = 1.f;  // network output x out_scale = pressure / max|rhs|
   int adam_t = 0;
   float *absmax_part = nullptr, *scale = nullptr, *nf = nullptr, *hpart = nullptr, *hsum = nullptr;
-  float* loss_log = nullptr;  // per training step loss (device), capacity loss_cap
-  int loss_cap = 0;
   std::vector<aqb::UActs*> acts;
   std::vector<void*> allocs;
   ~aq_unet();
 };
 
 namespace aqb {
+// Kernel launches of unet_predict: absmax 2, input 1, 10 convolutions, 2
+// poolings, 2 upsample-concatenations, head 1, output 1.
+constexpr int kUNetForwardLaunches = 19;
 // Activations for a grid size (allocated once per size, before any capture).
 aq_status unet_acts(aq_unet* net, int sx, int sy, int sz, bool grads, UActs** out);
 // Enqueues the forward pass on `st`: p[v] = pressure warm start on fluid

@@ -60,7 +60,16 @@ typedef enum aq_shape { AQ_SHAPE_SPHERE = 0, AQ_SHAPE_SQUARE = 1 } aq_shape;
  * CARRY: the reference behaviour — pressure persists across steps (it is only
  *        cleared when the grid is created, Fluid/MAC_Grid_3D.cu:54).
  * ZERO:  pressure is zeroed before every solve. */
-typedef enum aq_pressure_init { AQ_PRESSURE_CARRY = 0, AQ_PRESSURE_ZERO = 1 } aq_pressure_init;
+/* LEARNED: pressure is zeroed, then the warm-start network attached with
+ *        aq_fluid_set_warm_start predicts it; 20 sweeps are run from the
+ *        prediction and 20 from zero, and the solve continues from whichever
+ *        has the lower residual (zero-init Jacobi is the fallback and the
+ *        judge).  Needs sizes divisible by 4.  No counterpart in the reference. */
+typedef enum aq_pressure_init {
+  AQ_PRESSURE_CARRY = 0,
+  AQ_PRESSURE_ZERO = 1,
+  AQ_PRESSURE_LEARNED = 2
+} aq_pressure_init;
 
 /* FIXED: exactly pressure_iterations Jacobi sweeps (Fluid/Fluid_3D_common.cu:48-55).
  * RESIDUAL: sweep in blocks of check_interval until the relative residual
@@ -169,6 +178,12 @@ typedef struct aq_solve_stats {
   int32_t blocks;           /* residual-check blocks of the last solve */
   int64_t total_sweeps;     /* sweeps since creation */
   int64_t total_blocks;     /* residual-check blocks since creation */
+  /* AQ_PRESSURE_LEARNED: 1 the network's prediction was kept, 2 the zero-init
+   * fallback won, 0 no warm start this solve; the two relative residuals
+   * after the first 20 sweeps (-1 if not run). */
+  int32_t warm_start;
+  double warm_rel_residual;
+  double zero_rel_residual;
 } aq_solve_stats;
 
 /* Fills *cfg with the reference defaults (Fluid/FluidConfig.cuh:20-97):
@@ -406,6 +421,11 @@ aq_status aq_unet_evaluate(aq_unet* net, aq_dataset* ds, int32_t first, int32_t 
 /* The gradients of the last training step, in weights-file order (per layer
  * weights then bias, then head weights and bias); n = parameter count. */
 aq_status aq_unet_gradients(aq_unet* net, float* out, int64_t n);
+
+/* Attaches the network used by AQ_PRESSURE_LEARNED (NULL detaches).  The
+ * network must outlive the fluid's steps; allocate-once buffers for the
+ * fluid's grid are made here, so call it before the first step. */
+aq_status aq_fluid_set_warm_start(aq_fluid* f, aq_unet* net);
 
 /* Largest grid (sx*sy*sz cells) aq_jacobi_sweeps_noalloc accepts. */
 #define AQ_NOALLOC_MAX_CELLS (64 * 64 * 64)

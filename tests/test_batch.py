@@ -69,3 +69,18 @@ def test_create_rejects_empty_batch(built_library):
 def test_create_without_device_fails_loudly(built_library):
     st, msg = _create(batch_configs(3, seed=1, sizes=(16, 24)))
     assert _abi.STATUS_NAMES[st] == "AQ_ERR_NO_DEVICE"
+
+
+def test_learned_mode_validation(built_library):
+    from aquarius_b200.scenes import batch_configs as bc
+    lib = aq.load_library()
+    ok = _abi.make_config((16, 16, 16), None, pressure_init=_abi.PRESSURE_LEARNED, solve_mode=_abi.SOLVE_RESIDUAL)
+    assert lib.aq_config_validate(ct.byref(ok)) == 0
+    bad = _abi.make_config((18, 16, 16), None, pressure_init=_abi.PRESSURE_LEARNED)
+    assert _abi.STATUS_NAMES[lib.aq_config_validate(ct.byref(bad))] == "AQ_ERR_INVALID_CONFIG"
+    few = _abi.make_config((16, 16, 16), None, pressure_init=_abi.PRESSURE_LEARNED, solve_mode=_abi.SOLVE_FIXED,
+                           pressure_iterations=10)
+    assert _abi.STATUS_NAMES[lib.aq_config_validate(ct.byref(few))] == "AQ_ERR_INVALID_CONFIG"
+    cfgs = bc(2, seed=1, sizes=(16,), pressure_init=_abi.PRESSURE_LEARNED)
+    st, msg = _create(cfgs)
+    assert _abi.STATUS_NAMES[st] == "AQ_ERR_INVALID_CONFIG" and "learned" in msg
