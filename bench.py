@@ -365,11 +365,62 @@ def run_ours(args, rank: int, world: int, dist):
         "jacobi_plan": {"levels": tune["plan"][0], "rows": tune["plan"][1], "x_planes": tune["plan"][2],
                         "tuned_sweep_us": tune["sweep_us"]},
     }
+    plain_rel = [st1["rel_residual"], pstats["rel_residual"]]
+    f.close()
+    if not args.no_learned:
+        line["learned"] = learned_arm(args, dev, stream, max(plain_rel), ms_max / args.steps, dist)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(args.size, args.pressure_init, steps=1)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    f.close()
+
+
+def learned_arm(args, dev, stream, plain_residual: float, plain_ms: float, dist) -> dict:
+    """The same workload with the learned warm start (AQ_PRESSURE_LEARNED):
+    (a) to the same target 1e-4 (cap 2000), (b) to the residual the plain
+    step reached at its cap, i.e. at equal achieved residual."""
+    import torch
+
+    import aquarius_b200 as aq
+    from aquarius_b200 import _abi
+    wpath = ROOT / "aquarius_b200" / "weights" / f"unet_{args.size}.bin"
+    if not wpath.exists():
+        return {"unavailable": f"no trained weights for {args.size}^3 ({wpath.name})"}
+    net = aq.UNet(device=dev, weights=wpath)
+    out = {"weights": wpath.name, "parameters": net.parameter_count()}
+    for name, target in (("to_1e-4", 1e-4), ("to_plain_residual", plain_residual)):
+        cfg = workload_config(args.size, "zero")
+        cfg.pressure_init = _abi.PRESSURE_LEARNED
+        cfg.rel_residual = float(target)
+        cfg.device = dev
+        f = aq.Fluid(cfg)
+        f.set_warm_start(net)
+        f.step(args.warmup)
+        f.synchronize()
+        s0 = f.solve_stats()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lstream = torch.cuda.ExternalStream(f.stream(), device=dev)
+        with torch.cuda.stream(lstream):
+            ev0.record(lstream)
+            f.step(args.steps)
+            ev1.record(lstream)
+        ev1.synchronize()
+        ms = reduce_max(ev0.elapsed_time(ev1), dist, f"cuda:{dev}") / args.steps
+        s1 = f.solve_stats()
+        f.step(1)
+        s2 = f.solve_stats()
+        pcg = f.pcg_reference(rel_tol=1e-12, max_iter=200000)
+        out[name] = {"target_rel_residual": target, "steps_per_s": 1000.0 / ms, "ms_per_step": ms,
+                     "time_vs_plain": ms / plain_ms,
+                     "sweeps_per_step": (s1["total_sweeps"] - s0["total_sweeps"]) / args.steps,
+                     "last_rel_residual": s2["rel_residual"], "last_iterations": s2["iterations"],
+                     "converged": s2["converged"], "warm_start_kept": s2["warm_start"] == 1,
+                     "residual_after_20_sweeps": {"learned": s2["warm_rel_residual"],
+                                                  "zero_init": s2["zero_rel_residual"]},
+                     "pressure_rel_error_vs_fp64_pcg": pcg["rel_error"]}
+        f.close()
+    net.close()
+    return out
 
 
 def run_batch(args, rank: int, world: int, dist):
@@ -494,6 +545,7 @@ def main():
     ap.add_argument("--pressure-init", default="zero", choices=["zero", "carry"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default Jacobi plan")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
     ap.add_argument("--workload", default="ball128", choices=["ball128", "batch"],
                     help="ball128: the 128^3 scene; batch: 256 independent scenes of uneven sizes")
     ap.add_argument("--scenes", type=int, default=256, help="scenes in the batch workload")
