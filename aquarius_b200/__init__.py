@@ -115,7 +115,7 @@ def load_library() -> ct.CDLL:
         "aq_unet_get_output_scale": (ct.c_int, [P, ct.POINTER(ct.c_float)]),
         "aq_unet_predict": (ct.c_int, [P, ct.c_int32, ct.c_int32, ct.c_int32, P, P, P, P]),
         "aq_unet_train": (ct.c_int, [P, P, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_float, ct.c_uint32, ct.c_float,
-                                     ct.POINTER(ct.c_float)]),
+                                     ct.c_float, ct.c_int32, ct.POINTER(ct.c_float)]),
         "aq_unet_evaluate": (ct.c_int, [P, P, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_double)]),
         "aq_unet_gradients": (ct.c_int, [P, P, ct.c_int64]),
         "aq_fluid_set_warm_start": (ct.c_int, [P, P]),
@@ -537,9 +537,10 @@ class UNet:
         _check(self._lib.aq_unet_predict(self._h, *size, rhs_ptr, type_ptr, out_ptr, stream or None))
 
     def train(self, ds: "Dataset", first: int, count: int, steps: int, lr: float = 1e-3, seed: int = 1,
-              out_scale: float = 0.0) -> float:
+              out_scale: float = 0.0, residual_weight: float = 0.0, residual_sweeps: int = 20) -> float:
         loss = ct.c_float()
-        _check(self._lib.aq_unet_train(self._h, ds._h, first, count, steps, lr, seed, out_scale, ct.byref(loss)))
+        _check(self._lib.aq_unet_train(self._h, ds._h, first, count, steps, lr, seed, out_scale, residual_weight,
+                                       residual_sweeps, ct.byref(loss)))
         return loss.value
 
     def evaluate(self, ds: "Dataset", first: int, count: int) -> float:

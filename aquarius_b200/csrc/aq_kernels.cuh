@@ -179,6 +179,8 @@ cudaError_t launch_conv3_fwd(cudaStream_t st, int cin, int cout, bool relu, cons
 cudaError_t launch_conv3_wgrad(cudaStream_t st, int cin, int cout, const void* x, const void* dy, float* part,
                                float* dw, int sx, int sy, int sz);
 size_t conv3_wgrad_part_floats(int cin, int cout, int voxels);
+// Forward kernel variant: halo-tiled (true, default) or im2col streaming.
+void set_conv_tiled(bool tiled);
 // wt[t][ci][co] = w[26-t][co][ci] (weights of the data gradient).
 cudaError_t launch_flip_transpose(cudaStream_t st, const void* w, void* wt, int cin, int cout);
 
@@ -197,10 +199,16 @@ cudaError_t launch_relu_bwd(cudaStream_t st, void* dy, const void* y, int n);
 int chan_sum_parts(int V);
 cudaError_t launch_chan_sum(cudaStream_t st, const void* dy, int V, int C, float* part, float* out);
 cudaError_t launch_head_fwd(cudaStream_t st, const void* h, const float* w, const float* b, float* out, int V);
-int head_parts();
-cudaError_t launch_head_loss_bwd(cudaStream_t st, const float* out, const float* target, const int8_t* type,
-                                 const void* h, const float* w, const float* nf, void* dh, int V, float* part,
-                                 float* sums);
+// Training loss L = ||e||^2/||t||^2 + alpha ||A J^k e||^2/||A J^k t||^2 (fluid
+// cells, e = out - target, J a homogeneous Jacobi sweep, A the pressure
+// operator) and the head's backward pass: dh, head_sums = [dw 16, db, loss].
+// Scratch: e, p0..p3, g (V floats each), part (loss_parts() * 8), sums (6),
+// head_part (loss_parts() * 17).
+int loss_parts();
+cudaError_t launch_unet_loss_bwd(cudaStream_t st, const float* out, const float* target, const int8_t* type,
+                                 const void* h, const float* w, float alpha, int k, void* dh, int sx, int sy, int sz,
+                                 float* e, float* p0, float* p1, float* p2, float* p3, float* g, float* part,
+                                 float* sums, float* head_part, float* head_sums);
 cudaError_t launch_adam(cudaStream_t st, float* w, const float* g, float* m, float* v, int n, float lr, float b1,
                         float b2, float eps, int t, void* wb);
 cudaError_t launch_f32_to_bf16(cudaStream_t st, const float* a, void* b, int n);

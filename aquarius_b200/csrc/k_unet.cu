@@ -25,6 +25,9 @@ namespace {
 
 using bf16 = __nv_bfloat16;
 
+// Forward convolution variant: halo-tiled (default) or im2col streaming.
+bool g_conv_tiled = true;
+
 constexpr int kTileM = 128;  // voxels per forward CTA (4 warps x 32)
 constexpr int kRowK = 24;    // smem row of one 16-wide k chunk: 16 + 8 pad bf16 (48 B, conflict-free ldmatrix)
 
@@ -164,6 +167,112 @@ __global__ void __launch_bounds__(128) k_conv3_fwd(const bf16* __restrict__ in, 
     }
 }
 
+// Halo-tiled forward: a CTA computes a 4 (x) x 4 (y) x 16 (z) block of
+// output voxels.  The input block with its one-voxel halo (6 x 6 x 18
+// voxels x CIN channels) is staged in shared memory once (cp.async, zero
+// fill outside the grid); every tap then gathers its A fragments straight
+// from that block with ldmatrix (each lane addresses its own voxel row), so
+// the input is read ~2.5x instead of 27x.  Weights stream per tap, double
+// buffered.  8 warps; m tile j = 16 z voxels at (x, y) = (j / 4, j % 4),
+// warp w owns tiles 2w and 2w+1.  Rows are padded by 16 B (odd count of 16 B
+// chunks: ldmatrix without bank conflicts).
+constexpr int kTX = 4, kTY = 4, kTZ = 16;
+constexpr int kHX = kTX + 2, kHY = kTY + 2, kHZ = kTZ + 2, kHalo = kHX * kHY * kHZ;
+
+template <int CIN, int COUT>
+constexpr size_t fwd_tile_smem() {
+  return (size_t)kHalo * (CIN + 8) * sizeof(bf16) + (size_t)2 * COUT * (CIN + 8) * sizeof(bf16);
+}
+
+template <int CIN, int COUT, bool RELU, bool BIAS>
+__global__ void __launch_bounds__(256) k_conv3_fwd_tile(const bf16* __restrict__ in, const bf16* __restrict__ w,
+                                                       const float* __restrict__ bias, bf16* __restrict__ out,
+                                                       int sx, int sy, int sz) {
+  static_assert(CIN % 16 == 0 && COUT % 8 == 0, "channel counts");
+  constexpr int RS = CIN + 8;  // row stride (bf16)
+  constexpr int KS = CIN / 16, NT = COUT / 8, CH = CIN / 8;
+  extern __shared__ __align__(16) unsigned char ft_smem[];
+  bf16* sH = reinterpret_cast<bf16*>(ft_smem);
+  bf16* sW = sH + kHalo * RS;  // [2][COUT][RS]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int z0 = blockIdx.x * kTZ, y0 = blockIdx.y * kTY, x0 = blockIdx.z * kTX;
+  // stage the halo block
+  for (int i = tid; i < kHalo * CH; i += 256) {
+    const int c = i % CH, h = i / CH;
+    const int hz = h % kHZ, t = h / kHZ, hy = t % kHY, hx = t / kHY;
+    const int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z0 + hz - 1;
+    const bool ok = gx >= 0 && gx < sx && gy >= 0 && gy < sy && gz >= 0 && gz < sz;
+    cp_async16(sH + h * RS + c * 8, ok ? in + ((size_t)((gx * sy + gy) * sz + gz) * CIN + c * 8) : in, ok);
+  }
+  auto stage_w = [&](int tap, int buf) {
+    bf16* dst = sW + buf * COUT * RS;
+    for (int i = tid; i < COUT * CH; i += 256) {
+      const int c = i % CH, n = i / CH;
+      cp_async16(dst + n * RS + c * 8, w + ((size_t)(tap * COUT + n) * CIN + c * 8), true);
+    }
+  };
+  stage_w(0, 0);
+  cp_async_commit();
+  float acc[2][NT][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < NT; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
+  for (int tap = 0; tap < 27; ++tap) {
+    const int buf = tap & 1;
+    if (tap + 1 < 27) stage_w(tap + 1, buf ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    int dx, dy, dz;
+    tap_offset(tap, dx, dy, dz);
+    const bf16* wb = sW + buf * COUT * RS;
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) {
+      unsigned bfr[NT][2];
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) ldsm_x2(bfr[nt], wb + (nt * 8 + (lane & 7)) * RS + ks * 16 + ((lane >> 3) & 1) * 8);
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        const int j = warp * 2 + mt;
+        const int ox = j >> 2, oy = j & 3;
+        const int h = ((ox + dx + 1) * kHY + (oy + dy + 1)) * kHZ + (lane & 15) + dz + 1;
+        unsigned afr[4];
+        ldsm_x4(afr, sH + h * RS + ks * 16 + (lane >> 4) * 8);
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) mma_bf16(acc[mt][nt], afr, bfr[nt]);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    const int j = warp * 2 + mt;
+    const int gx = x0 + (j >> 2), gy = y0 + (j & 3);
+    if (gx >= sx || gy >= sy) continue;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int co = nt * 8 + (lane & 3) * 2;
+      const float b0 = BIAS ? bias[co] : 0.f, b1 = BIAS ? bias[co + 1] : 0.f;
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const int gz = z0 + (lane >> 2) + hh * 8;
+        if (gz < sz) {
+          float a = acc[mt][nt][2 * hh] + b0, c = acc[mt][nt][2 * hh + 1] + b1;
+          if (RELU) {
+            a = fmaxf(a, 0.f);
+            c = fmaxf(c, 0.f);
+          }
+          *reinterpret_cast<__nv_bfloat162*>(out + (size_t)((gx * sy + gy) * sz + gz) * COUT + co) =
+              __floats2bfloat162_rn(a, c);
+        }
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------- weight grad
 // grid (chunks, 27): one tap, `cv` voxels per CTA in tiles of 128.  A = dY^T
 // (COUT x voxels), B = x shifted by the tap (voxels x CIN); both staged with
@@ -281,6 +390,16 @@ __global__ void k_flip_transpose(const bf16* __restrict__ w, bf16* __restrict__ 
 template <int CIN, int COUT, bool RELU, bool BIAS>
 cudaError_t fwd_launch(cudaStream_t st, const bf16* in, const bf16* w, const float* b, bf16* out, int sx, int sy,
                        int sz) {
+  if (g_conv_tiled) {
+    constexpr size_t smem = fwd_tile_smem<CIN, COUT>();
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k_conv3_fwd_tile<CIN, COUT, RELU, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    if (attr != cudaSuccess) return attr;
+    const dim3 grid((sz + kTZ - 1) / kTZ, (sy + kTY - 1) / kTY, (sx + kTX - 1) / kTX);
+    k_conv3_fwd_tile<CIN, COUT, RELU, BIAS><<<grid, 256, smem, st>>>(in, w, b, out, sx, sy, sz);
+    return cudaGetLastError();
+  }
   const int V = sx * sy * sz;
   k_conv3_fwd<CIN, COUT, RELU, BIAS><<<(V + kTileM - 1) / kTileM, 128, 0, st>>>(in, w, b, out, sx, sy, sz);
   return cudaGetLastError();
@@ -443,43 +562,6 @@ __global__ void k_head_fwd(const bf16* __restrict__ h, const float* __restrict__
   }
 }
 
-// Loss over fluid cells, L = sum (out - t)^2 / n_fluid, and its gradients:
-// dh[v][c] = g_v w[c] with g_v = 2 (out - t) / n_fluid (0 off fluid); per
-// block partial sums of g_v h[v][c] (16), g_v, and the loss.
-__global__ void __launch_bounds__(256) k_head_loss_bwd(const float* __restrict__ out, const float* __restrict__ target,
-                                                       const int8_t* __restrict__ type, const bf16* __restrict__ h,
-                                                       const float* __restrict__ w, const float* __restrict__ nf,
-                                                       bf16* __restrict__ dh, int V, float* __restrict__ part) {
-  __shared__ float sm[18][256];
-  float acc[18];
-#pragma unroll
-  for (int k = 0; k < 18; ++k) acc[k] = 0.f;
-  const float inv = *nf > 0.f ? 1.f / *nf : 0.f;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-    const bool fl = type[v] == kFluid;
-    const float e = fl ? out[v] - target[v] : 0.f;
-    const float g = 2.f * e * inv;
-#pragma unroll
-    for (int c = 0; c < 16; ++c) {
-      const float hv = __bfloat162float(h[(size_t)v * 16 + c]);
-      acc[c] += g * hv;
-      dh[(size_t)v * 16 + c] = __float2bfloat16(g * w[c]);
-    }
-    acc[16] += g;
-    acc[17] += e * e * inv;
-  }
-#pragma unroll
-  for (int k = 0; k < 18; ++k) sm[k][threadIdx.x] = acc[k];
-  __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
-    if (threadIdx.x < o)
-#pragma unroll
-      for (int k = 0; k < 18; ++k) sm[k][threadIdx.x] += sm[k][threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x < 18) part[(size_t)blockIdx.x * 18 + threadIdx.x] = sm[threadIdx.x][0];
-}
-
 // Adam (bias-corrected) on n parameters; refreshes the bf16 copy if given.
 __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
                        float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2,
@@ -525,12 +607,144 @@ __global__ void k_unet_sample(const float* __restrict__ rhs, const int8_t* __res
   }
 }
 
+// ---------------------------------------------------------- training loss
+// L = ||e||^2 / ||t||^2 + alpha ||A e||^2 / ||A t||^2 over fluid cells, e = o - t,
+// with A the pressure operator the Jacobi sweeps solve ((A x)_i = 6 x_i - sum
+// of the six neighbours, a neighbour outside the grid taking x_i, air 0).
+// The second term is the prediction's relative residual: it penalises the
+// rough error that Jacobi sweeps do not remove.
+
+__device__ __forceinline__ void block_sum2(float a, float b, float* part) {
+  __shared__ float sa[256], sb[256];
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sa[threadIdx.x] += sa[threadIdx.x + o];
+      sb[threadIdx.x] += sb[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[blockIdx.x * 2] = sa[0];
+    part[blockIdx.x * 2 + 1] = sb[0];
+  }
+}
+
+// e = o - t on fluid cells (0 elsewhere); partial sums of e^2 and t^2.
+__global__ void __launch_bounds__(256) k_loss_err(const float* __restrict__ o, const float* __restrict__ t,
+                                                  const int8_t* __restrict__ type, float* __restrict__ e, int V,
+                                                  float* __restrict__ part) {
+  float se = 0.f, st = 0.f;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const bool fl = type[v] == kFluid;
+    const float ev = fl ? o[v] - t[v] : 0.f;
+    e[v] = ev;
+    se += ev * ev;
+    st += fl ? t[v] * t[v] : 0.f;
+  }
+  block_sum2(se, st, part);
+}
+
+// y = A x on fluid cells (0 elsewhere); partial sums of y^2 (and 0).
+__global__ void __launch_bounds__(256) k_apply_A(const float* __restrict__ x, const int8_t* __restrict__ type,
+                                                 float* __restrict__ y, int sx, int sy, int sz,
+                                                 float* __restrict__ part) {
+  float sq = 0.f;
+  const int V = sx * sy * sz;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    float r = 0.f;
+    if (type[v] == kFluid) {
+      const int z = v % sz, tt = v / sz, yy = tt % sy, xx = tt / sy;
+      const float c = x[v];
+      float s = xx + 1 < sx ? x[v + sy * sz] : c;
+      s += xx > 0 ? x[v - sy * sz] : c;
+      s += yy + 1 < sy ? x[v + sz] : c;
+      s += yy > 0 ? x[v - sz] : c;
+      s += z + 1 < sz ? x[v + 1] : c;
+      s += z > 0 ? x[v - 1] : c;
+      r = 6.f * c - s;
+    }
+    y[v] = r;
+    sq += r * r;
+  }
+  block_sum2(sq, 0.f, part);
+}
+
+// y = J x on fluid cells (0 elsewhere): one homogeneous Jacobi sweep, the
+// mean of the six neighbours (a neighbour outside the grid taking x_i).
+// J is symmetric, so it is its own adjoint in the gradient.
+__global__ void __launch_bounds__(256) k_apply_J(const float* __restrict__ x, const int8_t* __restrict__ type,
+                                                 float* __restrict__ y, int sx, int sy, int sz) {
+  const int V = sx * sy * sz;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    float r = 0.f;
+    if (type[v] == kFluid) {
+      const int z = v % sz, tt = v / sz, yy = tt % sy, xx = tt / sy;
+      const float c = x[v];
+      float s = xx + 1 < sx ? x[v + sy * sz] : c;
+      s += xx > 0 ? x[v - sy * sz] : c;
+      s += yy + 1 < sy ? x[v + sz] : c;
+      s += yy > 0 ? x[v - sz] : c;
+      s += z + 1 < sz ? x[v + 1] : c;
+      s += z > 0 ? x[v - 1] : c;
+      r = s * (1.f / 6.f);
+    }
+    y[v] = r;
+  }
+}
+
+// g = 2 e / ||t||^2 + 2 alpha q / ||A t||^2 on fluid cells (q = A A e);
+// sums = [||e||^2, ||t||^2, ||Ae||^2, ||At||^2]; loss written to *loss.
+__global__ void k_loss_grad(const float* __restrict__ e, const float* __restrict__ q, const int8_t* __restrict__ type,
+                            const float* __restrict__ sums, float alpha, float* __restrict__ g, int V,
+                            float* __restrict__ loss) {
+  const float st = fmaxf(sums[1], 1e-30f), sat = fmaxf(sums[3], 1e-30f);
+  const float a = 2.f / st, c = 2.f * alpha / sat;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+    g[v] = type[v] == kFluid ? a * e[v] + c * q[v] : 0.f;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *loss = sums[0] / st + alpha * sums[2] / sat;
+}
+
+// Head backward from the output gradient g: dh[v][c] = g_v w[c]; per-block
+// partial sums of g_v h[v][c] (16) and g_v.
+__global__ void __launch_bounds__(256) k_head_bwd(const float* __restrict__ g, const bf16* __restrict__ h,
+                                                  const float* __restrict__ w, bf16* __restrict__ dh, int V,
+                                                  float* __restrict__ part) {
+  __shared__ float sm[17][256];
+  float acc[17];
+#pragma unroll
+  for (int k = 0; k < 17; ++k) acc[k] = 0.f;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const float gv = g[v];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      acc[c] += gv * __bfloat162float(h[(size_t)v * 16 + c]);
+      dh[(size_t)v * 16 + c] = __float2bfloat16(gv * w[c]);
+    }
+    acc[16] += gv;
+  }
+#pragma unroll
+  for (int k = 0; k < 17; ++k) sm[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+#pragma unroll
+      for (int k = 0; k < 17; ++k) sm[k][threadIdx.x] += sm[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x < 17) part[(size_t)blockIdx.x * 17 + threadIdx.x] = sm[threadIdx.x][0];
+}
+
 inline int ew_grid(long long n) {
   const long long b = (n + 255) / 256;
   return (int)std::min<long long>(std::max<long long>(b, 1), 148 * 16);
 }
 
 }  // namespace
+
+void set_conv_tiled(bool tiled) { g_conv_tiled = tiled; }
 
 int unet_wgrad_chunk(int voxels) {
   // about 2 CTAs per SM per tap at 128^3, at least one 128-voxel tile
@@ -650,14 +864,6 @@ cudaError_t launch_head_fwd(cudaStream_t st, const void* h, const float* w, cons
   k_head_fwd<<<ew_grid(V), 256, 0, st>>>((const bf16*)h, w, b, out, V);
   return cudaGetLastError();
 }
-int head_parts() { return 296; }
-cudaError_t launch_head_loss_bwd(cudaStream_t st, const float* out, const float* target, const int8_t* type,
-                                 const void* h, const float* w, const float* nf, void* dh, int V, float* part,
-                                 float* sums /* 18: dw[16], db, loss */) {
-  k_head_loss_bwd<<<head_parts(), 256, 0, st>>>(out, target, type, (const bf16*)h, w, nf, (bf16*)dh, V, part);
-  k_sum_parts<<<1, 32, 0, st>>>(part, head_parts(), 18, sums);
-  return cudaGetLastError();
-}
 cudaError_t launch_adam(cudaStream_t st, float* w, const float* g, float* m, float* v, int n, float lr, float b1,
                         float b2, float eps, int t, void* wb) {
   const float c1 = 1.f - powf(b1, (float)t), c2 = 1.f - powf(b2, (float)t);
@@ -680,6 +886,49 @@ cudaError_t launch_unet_scale_copy(cudaStream_t st, const float* a, float k, flo
 cudaError_t launch_unet_sample(cudaStream_t st, const float* rhs, const int8_t* type, const double* p,
                                const float* scale, float* rhs_s, int8_t* type_s, float* target, int V) {
   k_unet_sample<<<ew_grid(V), 256, 0, st>>>(rhs, type, p, scale, rhs_s, type_s, target, V);
+  return cudaGetLastError();
+}
+
+}  // namespace aqb
+
+namespace aqb {
+
+int loss_parts() { return 296; }
+
+// L = ||e||^2/||t||^2 + alpha ||A J^k e||^2 / ||A J^k t||^2: the second term is
+// (residual after k Jacobi sweeps from the prediction / the same from zero)^2.
+// Scratch: e, p0..p3, g (V floats each), part (loss_parts() * 8), sums (6).
+cudaError_t launch_unet_loss_bwd(cudaStream_t st, const float* out, const float* target, const int8_t* type,
+                                 const void* h, const float* w, float alpha, int k, void* dh, int sx, int sy, int sz,
+                                 float* e, float* p0, float* p1, float* p2, float* p3, float* g, float* part,
+                                 float* sums, float* head_part, float* head_sums /* 18: dw 16, db, loss */) {
+  const int V = sx * sy * sz;
+  const int P = loss_parts();
+  // J^k x into p0/p1; returns the buffer holding the result
+  auto smooth = [&](const float* x, float* a, float* b) -> const float* {
+    const float* src = x;
+    float* bufs[2] = {a, b};
+    for (int i = 0; i < k; ++i) {
+      k_apply_J<<<P, 256, 0, st>>>(src, type, bufs[i % 2], sx, sy, sz);
+      src = bufs[i % 2];
+    }
+    return src;
+  };
+  k_loss_err<<<P, 256, 0, st>>>(out, target, type, e, V, part);
+  const float* je = smooth(e, p0, p1);
+  k_apply_A<<<P, 256, 0, st>>>(je, type, p2, sx, sy, sz, part + 2 * P);  // r = A J^k e
+  const float* jt = smooth(target, p0, p1);
+  k_apply_A<<<P, 256, 0, st>>>(jt, type, p3, sx, sy, sz, part + 4 * P);  // A J^k t (sum only)
+  k_apply_A<<<P, 256, 0, st>>>(p2, type, p3, sx, sy, sz, part + 6 * P);  // q = A r
+  const float* v = smooth(p3, p0, p1);                                    // J^k q
+  k_sum_parts<<<1, 32, 0, st>>>(part, P, 2, sums);
+  k_sum_parts<<<1, 32, 0, st>>>(part + 2 * P, P, 2, sums + 2);
+  k_sum_parts<<<1, 32, 0, st>>>(part + 4 * P, P, 2, sums + 4);
+  cudaError_t err = cudaMemcpyAsync(sums + 3, sums + 4, sizeof(float), cudaMemcpyDeviceToDevice, st);
+  if (err != cudaSuccess) return err;
+  k_loss_grad<<<ew_grid(V), 256, 0, st>>>(e, v, type, sums, alpha, g, V, head_sums + 17);
+  k_head_bwd<<<P, 256, 0, st>>>(g, (const bf16*)h, w, (bf16*)dh, V, head_part);
+  k_sum_parts<<<1, 32, 0, st>>>(head_part, P, 17, head_sums);
   return cudaGetLastError();
 }
 

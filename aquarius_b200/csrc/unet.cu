@@ -128,6 +128,11 @@ aq_status aqb::unet_acts(aq_unet* net, int sx, int sy, int sz, bool grads, UActs
       wp = std::max(wp, conv3_wgrad_part_floats(kLayerIO[l][0], kLayerIO[l][1], (int)vox[l]));
     UN_TRY(dalloc(al, &a->wpart, wp, st));
     UN_TRY(dalloc(al, &a->cpart, (size_t)chan_sum_parts((int)V) * 96, st));
+    UN_TRY(dalloc(al, &a->le, V, st)); UN_TRY(dalloc(al, &a->l0, V, st)); UN_TRY(dalloc(al, &a->l1, V, st));
+    UN_TRY(dalloc(al, &a->l2, V, st)); UN_TRY(dalloc(al, &a->l3, V, st)); UN_TRY(dalloc(al, &a->lg, V, st));
+    UN_TRY(dalloc(al, &a->lpart, (size_t)loss_parts() * 8, st));
+    UN_TRY(dalloc(al, &a->lsums, 8, st));
+    UN_TRY(dalloc(al, &a->hpart, (size_t)loss_parts() * 17, st));
   }
   *out = a;
   return AQ_OK;
@@ -173,11 +178,13 @@ aq_status conv_bwd(aq_unet* net, cudaStream_t st, UActs* a, int l, const bf16* x
   return AQ_OK;
 }
 
-aq_status backward(aq_unet* net, cudaStream_t st, UActs* a, const float* target, const int8_t* type) {
+aq_status backward(aq_unet* net, cudaStream_t st, UActs* a, const float* target, const int8_t* type, float alpha,
+                   int k) {
   const int sx = a->sx, sy = a->sy, sz = a->sz;
   const int hx = sx / 2, hy = sy / 2, hz = sz / 2, qx = sx / 4, qy = sy / 4, qz = sz / 4;
   const int V = sx * sy * sz, V2 = V / 8, V4 = V / 64;
-  UN_CUDA(launch_head_loss_bwd(st, a->out, target, type, a->d1, net->hp, net->nf, a->g_d1, V, net->hpart, net->hg));
+  UN_CUDA(launch_unet_loss_bwd(st, a->out, target, type, a->d1, net->hp, alpha, k, a->g_d1, sx, sy, sz, a->le, a->l0,
+                               a->l1, a->l2, a->l3, a->lg, a->lpart, a->lsums, a->hpart, net->hg));
   UN_CUDA(launch_relu_bwd(st, a->g_d1, a->d1, V * 16));
   UN_TRY(conv_bwd(net, st, a, 9, a->d1a, a->g_d1, a->g_d1a, sx, sy, sz));
   UN_CUDA(launch_relu_bwd(st, a->g_d1a, a->d1a, V * 16));
@@ -236,7 +243,6 @@ struct aq_dataset {
   float* rhs = nullptr;     // [cap][V] rhs / max|rhs|
   int8_t* type = nullptr;   // [cap][V]
   float* target = nullptr;  // [cap][V] FP64-PCG pressure / max|rhs| (f32)
-  std::vector<float> nfluid;
   float* scratch = nullptr;  // absmax parts + scale
   std::vector<void*> allocs;
   ~aq_dataset() {
@@ -265,6 +271,11 @@ aq_status aq_conv3_weight_grad(int32_t cin, int32_t cout, const void* x, const v
   const cudaError_t e = launch_conv3_wgrad((cudaStream_t)stream, cin, cout, x, dy, part, dw, sx, sy, sz);
   cudaFreeAsync(part, (cudaStream_t)stream);
   UN_CUDA(e);
+  return AQ_OK;
+}
+
+aq_status aq_conv3_set_tiled(int32_t tiled) {
+  set_conv_tiled(tiled != 0);
   return AQ_OK;
 }
 
@@ -324,9 +335,7 @@ aq_status aq_unet_create(int32_t device, uint32_t seed, aq_unet** out) {
   if ((s = dalloc(net->allocs, &net->hp, 17, st)) != AQ_OK || (s = dalloc(net->allocs, &net->hg, 18, st)) != AQ_OK ||
       (s = dalloc(net->allocs, &net->hm, 17, st)) != AQ_OK || (s = dalloc(net->allocs, &net->hv, 17, st)) != AQ_OK ||
       (s = dalloc(net->allocs, &net->absmax_part, 1024, st)) != AQ_OK ||
-      (s = dalloc(net->allocs, &net->scale, 1, st)) != AQ_OK || (s = dalloc(net->allocs, &net->nf, 1, st)) != AQ_OK ||
-      (s = dalloc(net->allocs, &net->hpart, (size_t)head_parts() * 18, st)) != AQ_OK ||
-      (s = dalloc(net->allocs, &net->hsum, 18, st)) != AQ_OK)
+      (s = dalloc(net->allocs, &net->scale, 1, st)) != AQ_OK)
     return bail(s);
   std::vector<float> hh(17, 0.f);
   for (int i = 0; i < 16; ++i) hh[i] = nd(rng) * 0.25f;
@@ -458,12 +467,7 @@ aq_status aq_dataset_add_fluid(aq_dataset* ds, aq_fluid* f, double pcg_rel_tol, 
   UN_CUDA(launch_absmax(f->stream, f->rhs, V, ds->scratch, ds->scratch + 1024));
   UN_CUDA(launch_unet_sample(f->stream, f->rhs, f->type, f->pcg_x, ds->scratch + 1024, ds->rhs + o, ds->type + o,
                              ds->target + o, V));
-  std::vector<int8_t> ty(V);
-  UN_CUDA(cudaMemcpyAsync(ty.data(), f->type, V, cudaMemcpyDeviceToHost, f->stream));
   UN_CUDA(cudaStreamSynchronize(f->stream));
-  int nf = 0;
-  for (int v = 0; v < V; ++v) nf += ty[v] == kFluid;
-  ds->nfluid.push_back((float)nf);
   ds->n += 1;
   return AQ_OK;
 }
@@ -504,8 +508,10 @@ aq_status aq_dataset_target_rms(aq_dataset* ds, int32_t first, int32_t count, do
 // targets are divided by out_scale (set here if out_scale <= 0: the targets'
 // RMS).  mean_loss: mean loss over the last tenth of the steps.
 aq_status aq_unet_train(aq_unet* net, aq_dataset* ds, int32_t first, int32_t count, int32_t steps, float lr,
-                        uint32_t seed, float out_scale, float* mean_loss) {
-  if (!net || !ds || first < 0 || count < 1 || first + count > ds->n || steps < 1)
+                        uint32_t seed, float out_scale, float residual_weight, int32_t residual_sweeps,
+                        float* mean_loss) {
+  if (!net || !ds || first < 0 || count < 1 || first + count > ds->n || steps < 1 || residual_sweeps < 0 ||
+      residual_sweeps > 1000)
     return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
   cudaSetDevice(net->device);
   if (out_scale <= 0.f) {
@@ -533,15 +539,14 @@ aq_status aq_unet_train(aq_unet* net, aq_dataset* ds, int32_t first, int32_t cou
     const size_t o = (size_t)i * V;
     // input from the stored scaled rhs (scale 1), target / out_scale
     if (launch_unet_input(st, ds->rhs + o, ds->type + o, one, a->in0, V) != cudaSuccess ||
-        launch_unet_scale_copy(st, ds->target + o, 1.f / out_scale, tgt, V) != cudaSuccess ||
-        cudaMemcpyAsync(net->nf, &ds->nfluid[i], sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        launch_unet_scale_copy(st, ds->target + o, 1.f / out_scale, tgt, V) != cudaSuccess) {
       status = fail(AQ_ERR_CUDA, "training step setup");
       break;
     }
     // cosine learning-rate decay to 5% of lr
     const float lr_s = lr * (0.05f + 0.95f * 0.5f * (1.f + cosf(3.14159265f * (float)s / (float)steps)));
     if ((status = forward(net, st, a)) != AQ_OK) break;
-    if ((status = backward(net, st, a, tgt, ds->type + o)) != AQ_OK) break;
+    if ((status = backward(net, st, a, tgt, ds->type + o, residual_weight, residual_sweeps)) != AQ_OK) break;
     if ((status = adam_step(net, st, lr_s)) != AQ_OK) break;
     if (cudaMemcpyAsync(losses + s, net->hg + 17, sizeof(float), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
       status = fail(AQ_ERR_CUDA, "loss copy");

@@ -34,6 +34,9 @@ struct UActs {
   float* out = nullptr;
   float* wpart = nullptr;  // weight-gradient partial sums (largest layer)
   float* cpart = nullptr;  // channel-sum partials
+  // training loss scratch: error, four work buffers, output gradient (V each)
+  float *le = nullptr, *l0 = nullptr, *l1 = nullptr, *l2 = nullptr, *l3 = nullptr, *lg = nullptr;
+  float *lpart = nullptr, *lsums = nullptr, *hpart = nullptr;
   bool grads = false;
   std::vector<void*> allocs;
 };
@@ -49,7 +52,7 @@ struct aq_unet {
   float *hp = nullptr, *hg = nullptr, *hm = nullptr, *hv = nullptr;
   float out_scale = 1.f;  // network output x out_scale = pressure / max|rhs|
   int adam_t = 0;
-  float *absmax_part = nullptr, *scale = nullptr, *nf = nullptr, *hpart = nullptr, *hsum = nullptr;
+  float *absmax_part = nullptr, *scale = nullptr;
   std::vector<aqb::UActs*> acts;
   std::vector<void*> allocs;
   ~aq_unet();

@@ -65,6 +65,23 @@ def generate(size: int, scenes: int, steps_per_scene: int, every: int, seed: int
     return ds, info
 
 
+def check_warm(net: UNet, size: int, device: int, steps: int = 4) -> list:
+    """Residuals after 20 sweeps from the prediction and from zero on the
+    ball-drop scene (pool y < 0.3, sphere r 0.12 at (0.5, 0.7, 0.5))."""
+    vols = [dict(shape="box", min=(0, 0, 0), max=(1, 0.3, 1), phase=0),
+            dict(shape="sphere", center=(0.5, 0.7, 0.5), radius=0.12, phase=0)]
+    cfg = _abi.make_config((size, size, size), vols, timestep=0.64 / size, pressure_init=_abi.PRESSURE_LEARNED,
+                           solve_mode=_abi.SOLVE_FIXED, pressure_iterations=200, device=device)
+    out = []
+    with Fluid(cfg) as f:
+        f.set_warm_start(net)
+        for _ in range(steps):
+            f.step(1)
+            s = f.solve_stats()
+            out.append([s["warm_rel_residual"], s["zero_rel_residual"]])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--size", type=int, default=64)
@@ -74,6 +91,13 @@ def main():
     ap.add_argument("--sim-sweeps", type=int, default=200, help="Jacobi sweeps of the data-generating simulation")
     ap.add_argument("--train-steps", type=int, default=6000)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--residual-weight", type=float, default=0.3,
+                    help="weight of (residual after --residual-sweeps sweeps from the prediction / from zero)^2 "
+                         "in the loss")
+    ap.add_argument("--residual-sweeps", type=int, default=20)
+    ap.add_argument("--check-warm", action="store_true",
+                    help="after training, step a 128^3-style test scene with the warm start and report "
+                         "the residuals after 20 sweeps from the prediction and from zero")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--init", type=str, default=None, help="weights file to start from (fine-tuning)")
     ap.add_argument("--out", type=str, default=None)
@@ -92,14 +116,17 @@ def main():
     net.train(ds, 0, n_train, steps=1, lr=0.0)  # output scale from the training targets
     before = net.evaluate(ds, n_train, n_test) if n_test else None
     loss = net.train(ds, 0, n_train, steps=args.train_steps, lr=args.lr, seed=args.seed,
-                     out_scale=net.output_scale())
+                     out_scale=net.output_scale(), residual_weight=args.residual_weight,
+                     residual_sweeps=args.residual_sweeps)
     train_s = time.perf_counter() - t0
     after = net.evaluate(ds, n_train, n_test) if n_test else None
     train_err = net.evaluate(ds, 0, min(n_train, 64))
     out = pathlib.Path(args.out) if args.out else WEIGHTS_DIR / f"unet_{args.size}.bin"
     out.parent.mkdir(parents=True, exist_ok=True)
     net.save(out)
-    print(json.dumps(dict(info, size=args.size, train_pairs=n_train, test_pairs=n_test,
+    warm = check_warm(net, args.size, args.device) if args.check_warm else None
+    print(json.dumps(dict(info, size=args.size, train_pairs=n_train, test_pairs=n_test, warm_check=warm,
+                          residual_weight=args.residual_weight, residual_sweeps=args.residual_sweeps,
                           train_steps=args.train_steps, train_s=train_s, final_loss=loss,
                           test_rel_error_before=before, test_rel_error_after=after,
                           train_rel_error=train_err, output_scale=net.output_scale(), weights=str(out),

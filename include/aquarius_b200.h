@@ -368,6 +368,10 @@ aq_status aq_conv3_forward(int32_t cin, int32_t cout, int32_t relu, const void* 
 aq_status aq_conv3_weight_grad(int32_t cin, int32_t cout, const void* x, const void* dy, float* dw, int32_t sx,
                                int32_t sy, int32_t sz, void* stream);
 aq_status aq_conv3_flip_transpose(int32_t cin, int32_t cout, const void* w, void* wt, void* stream);
+/* Forward kernel used by aq_conv3_forward and the network: 1 = halo-tiled
+ * (default), 0 = im2col streaming.  Process-wide; set it while no
+ * convolution is in flight.  Both compute the same sums in the same order. */
+aq_status aq_conv3_set_tiled(int32_t tiled);
 
 /* ---- Learned pressure warm start: network, dataset, training ---------------
  * No counterpart in the reference.  A 3-level 3D U-Net (16/32/64 channels,
@@ -411,10 +415,16 @@ aq_status aq_dataset_target_rms(aq_dataset* ds, int32_t first, int32_t count, do
 aq_status aq_dataset_get(aq_dataset* ds, int32_t i, float* rhs, int8_t* type, float* target);
 /* `steps` Adam steps (one sample each, drawn with `seed` from samples
  * [first, first+count)), cosine-decayed learning rate from lr.  out_scale <= 0
- * sets the network's output scale to the targets' RMS.  mean_loss: mean MSE
- * (over fluid cells, in output-scale units) of the last tenth of the steps. */
+ * sets the network's output scale to the targets' RMS.  Loss over fluid
+ * cells, e = prediction - target, A the pressure operator and J one
+ * homogeneous Jacobi sweep: ||e||^2/||t||^2 + residual_weight *
+ * ||A J^k e||^2/||A J^k t||^2 with k = residual_sweeps; the second term is the
+ * square of (residual after k sweeps from the prediction) / (the same from
+ * zero), the ratio the warm start's fallback rule compares at k = 20.
+ * mean_loss: mean loss of the last tenth of the steps. */
 aq_status aq_unet_train(aq_unet* net, aq_dataset* ds, int32_t first, int32_t count, int32_t steps, float lr,
-                        uint32_t seed, float out_scale, float* mean_loss);
+                        uint32_t seed, float out_scale, float residual_weight, int32_t residual_sweeps,
+                        float* mean_loss);
 /* Mean over samples of the relative L2 error (fluid cells) of the prediction
  * against the FP64 PCG pressure. */
 aq_status aq_unet_evaluate(aq_unet* net, aq_dataset* ds, int32_t first, int32_t count, double* mean_rel_error);

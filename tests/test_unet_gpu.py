@@ -82,6 +82,26 @@ class TorchUNet:
         return [g.detach().cpu().numpy() for g in out]
 
 
+def apply_A(torch, x, fl):
+    """The pressure operator: 6 x_i - sum of the six neighbours, a neighbour
+    outside the grid taking x_i (x is 0 off fluid); fluid rows only."""
+    xp = torch.nn.functional.pad(x[None, None], (1, 1, 1, 1, 1, 1), mode="replicate")[0, 0]
+    s = (xp[2:, 1:-1, 1:-1] + xp[:-2, 1:-1, 1:-1] + xp[1:-1, 2:, 1:-1] + xp[1:-1, :-2, 1:-1]
+         + xp[1:-1, 1:-1, 2:] + xp[1:-1, 1:-1, :-2])
+    return torch.where(fl, 6 * x - s, torch.zeros_like(x))
+
+
+def apply_J(torch, x, fl, k):
+    """k homogeneous Jacobi sweeps: the mean of the six neighbours (clamped at
+    the walls) on fluid cells, 0 elsewhere."""
+    for _ in range(k):
+        xp = torch.nn.functional.pad(x[None, None], (1, 1, 1, 1, 1, 1), mode="replicate")[0, 0]
+        s = (xp[2:, 1:-1, 1:-1] + xp[:-2, 1:-1, 1:-1] + xp[1:-1, 2:, 1:-1] + xp[1:-1, :-2, 1:-1]
+             + xp[1:-1, 1:-1, 2:] + xp[1:-1, 1:-1, :-2])
+        x = torch.where(fl, s / 6, torch.zeros_like(x))
+    return x
+
+
 def _input(torch, rhs, typ, shape):
     x = torch.zeros(1, 16, *shape, device="cuda")
     x[0, 0] = torch.tensor(rhs.reshape(shape), device="cuda").to(torch.bfloat16).float()
@@ -142,14 +162,18 @@ def test_training_gradients_match_torch(tmp_path):
     net = aq.UNet(seed=9)
     net.save(tmp_path / "w.bin")
     _, layers, head = read_weights(tmp_path / "w.bin")
-    net.train(ds, 0, 1, steps=1, lr=0.0, out_scale=1.0)
+    alpha, k = 0.5, 3
+    net.train(ds, 0, 1, steps=1, lr=0.0, out_scale=1.0, residual_weight=alpha, residual_sweeps=k)
     got = net.gradients()
     s = ds.get(0)
     ref = TorchUNet(torch, layers, head, requires_grad=True)
-    out = ref(_input(torch, s["rhs"], s["type"], shape)).flatten()
-    fl = torch.tensor(s["type"] == 1, device="cuda")
-    tgt = torch.tensor(s["target"], device="cuda")
-    loss = ((out - tgt)[fl] ** 2).sum() / fl.sum()
+    out = ref(_input(torch, s["rhs"], s["type"], shape))
+    fl = torch.tensor(s["type"] == 1, device="cuda").reshape(shape)
+    tgt = torch.tensor(s["target"], device="cuda").reshape(shape)
+    e = torch.where(fl, out - tgt, torch.zeros_like(out))
+    tz = torch.where(fl, tgt, torch.zeros_like(tgt))
+    AJ = lambda x: apply_A(torch, apply_J(torch, x, fl, k), fl)
+    loss = (e ** 2).sum() / (tgt[fl] ** 2).sum() + alpha * (AJ(e) ** 2).sum() / (AJ(tz) ** 2).sum()
     loss.backward()
     o = 0
     for i, g_ref in enumerate(ref.grads_in_file_order()):

@@ -25,6 +25,8 @@ def _lib():
     lib.aq_conv3_weight_grad.argtypes = [I, I, P, P, P, I, I, I, P]
     lib.aq_conv3_flip_transpose.restype = ct.c_int
     lib.aq_conv3_flip_transpose.argtypes = [I, I, P, P, P]
+    lib.aq_conv3_set_tiled.restype = ct.c_int
+    lib.aq_conv3_set_tiled.argtypes = [I]
     return lib
 
 
@@ -49,11 +51,13 @@ def _rel(a, b):
     return float((a - b).norm() / max(b.norm(), 1e-30))
 
 
+@pytest.mark.parametrize("tiled", [1, 0], ids=["tiled", "im2col"])
 @pytest.mark.parametrize("cin,cout", FWD_PAIRS)
-@pytest.mark.parametrize("shape", [(5, 6, 7), (12, 8, 16)])
-def test_conv3_forward_matches_torch(cin, cout, shape):
+@pytest.mark.parametrize("shape", [(5, 6, 7), (12, 8, 16), (8, 12, 36)])
+def test_conv3_forward_matches_torch(cin, cout, shape, tiled):
     torch = _torch()
     lib = _lib()
+    assert lib.aq_conv3_set_tiled(tiled) == 0
     g = torch.Generator(device="cuda").manual_seed(cin * 100 + cout)
     V = shape[0] * shape[1] * shape[2]
     x = torch.randn(V, cin, device="cuda", generator=g).to(torch.bfloat16)
@@ -69,6 +73,29 @@ def test_conv3_forward_matches_torch(cin, cout, shape):
             ref = torch.relu(ref)
         got = _to_ncdhw(out, shape)
         assert _rel(got, ref) < 8e-3  # bf16 rounding of the output
+    lib.aq_conv3_set_tiled(1)
+
+
+def test_tiled_and_im2col_agree_bitwise():
+    torch = _torch()
+    lib = _lib()
+    shape = (9, 10, 20)
+    V = shape[0] * shape[1] * shape[2]
+    g = torch.Generator(device="cuda").manual_seed(5)
+    for cin, cout in FWD_PAIRS:
+        x = torch.randn(V, cin, device="cuda", generator=g).to(torch.bfloat16)
+        w = (torch.randn(27, cout, cin, device="cuda", generator=g) * 0.1).to(torch.bfloat16)
+        b = torch.randn(cout, device="cuda", generator=g)
+        outs = []
+        for tiled in (1, 0):
+            lib.aq_conv3_set_tiled(tiled)
+            o = torch.empty(V, cout, device="cuda", dtype=torch.bfloat16)
+            assert lib.aq_conv3_forward(cin, cout, 1, x.data_ptr(), w.data_ptr(), b.data_ptr(), o.data_ptr(),
+                                        *shape, None) == 0
+            outs.append(o)
+        torch.cuda.synchronize()
+        assert torch.equal(outs[0], outs[1]), (cin, cout)
+    lib.aq_conv3_set_tiled(1)
 
 
 @pytest.mark.parametrize("cin,cout", LAYER_PAIRS)
