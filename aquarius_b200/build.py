@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo", *ARCH,
     "-Xcompiler", "-fPIC,-ffp-contract=off",
-    "-shared", "-cudart", "static",
+    "-shared", "-cudart", "static", "-Xlinker", "--no-undefined",
     f"-I{ROOT / 'include'}",
 ]
 

@@ -65,9 +65,11 @@ cudaError_t launch_diffuse(cudaStream_t st, const Dims& d, const int8_t* type, f
 // ---- pressure (k_jacobi.cu) -------------------------------------------------
 struct JacobiPlan {
   int levels;      // sweeps per launch (1,2,4,8)
-  int by;          // tile rows (y threads); 0 = flat kernel; 1 = persistent solve
-  int xc;          // x planes per CTA
+  int by;          // tile rows (y threads); 0 = flat kernel; 1 = persistent solve; 2 = cube tiles
+  int xc;          // x planes per CTA (cube: tile edge in x and y)
 };
+// Cube plans accepted by launch_jacobi (levels, tile edge).
+bool cube_plan_ok(int levels, int tx);
 
 // ---- persistent solve (k_jacobi.cu) ------------------------------------------
 // The whole pressure solve in one cooperative launch: every CTA sweeps its

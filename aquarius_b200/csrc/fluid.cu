@@ -292,7 +292,8 @@ static std::vector<int> split_sweeps(int sweeps, int levels) {
 
 int aq_fluid::count_jacobi_launches(int sweeps) const {
   const int k = (int)split_sweeps(sweeps, plan.levels).size();
-  return k + (k % 2) + 1 + (plan.by == 0 ? 1 : 0);  // sweeps, parity copy, finalize, flat residual pass
+  // sweeps, parity copy, finalize, separate residual pass (flat and cube plans)
+  return k + (k % 2) + 1 + (plan.by == 0 || plan.by == 2 ? 1 : 0);
 }
 
 // `sweeps` Jacobi sweeps from pa; the last launch also writes the residual
@@ -306,7 +307,7 @@ int aq_fluid::count_jacobi_launches(int sweeps) const {
 static aq_status enqueue_sweeps_on(aq_fluid* f, const JacobiPlan& plan, float* a, float* b, int sweeps,
                                    bool with_residual, double* part) {
   const std::vector<int> parts = split_sweeps(sweeps, plan.levels);
-  const bool flat = plan.by == 0;
+  const bool flat = plan.by == 0 || plan.by == 2;  // residual in a separate pass
   float* bufs[2] = {a, b};
   for (size_t k = 0; k < parts.size(); ++k) {
     const bool last = k + 1 == parts.size();
@@ -332,7 +333,7 @@ static aq_status enqueue_sweeps(aq_fluid* f, int sweeps, bool with_residual = tr
 static int last_parts_of(const aq_fluid* f, const JacobiPlan& plan, int sweeps) {
   const std::vector<int> parts = split_sweeps(sweeps, plan.levels);
   if (parts.empty()) return 0;
-  if (plan.by == 0) return resid_flat_parts(f->d);
+  if (plan.by == 0 || plan.by == 2) return resid_flat_parts(f->d);
   JacobiPlan p = plan;
   p.levels = parts.back();
   return jacobi_parts(f->d, p, true);
@@ -1271,6 +1272,15 @@ aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, in
     f->invalidate_graph();
     return AQ_OK;
   }
+  if (rows == 2) {  // cube tiles: `levels` sweeps per launch on x_planes-edge tiles
+    if (f->d.sz % 4 != 0 || !cube_plan_ok(levels, x_planes))
+      return fail(AQ_ERR_INVALID_ARGUMENT, "unsupported cube plan (sz % 4 == 0; edge 8 with 1-4 levels or 16 with 2/4)");
+    cudaSetDevice(f->device);
+    AQ_CUDA(cudaStreamSynchronize(f->stream));
+    f->plan = JacobiPlan{levels, 2, x_planes};
+    f->invalidate_graph();
+    return AQ_OK;
+  }
   const bool flat = rows == 0;
   if (flat ? (levels != 1 || f->d.sz % 4 != 0 || !(x_planes == 1 || x_planes == 2 || x_planes == 4 || x_planes == 8))
            : (!(levels == 1 || levels == 2 || levels == 4 || levels == 8) || !(rows == 8 || rows == 16 || rows == 32) ||
@@ -1433,7 +1443,8 @@ aq_status aq_fluid_autotune(aq_fluid* f, int32_t sweeps_per_trial, const char* c
     if (out) *out = r;
     return AQ_OK;
   }
-  const int cands[][3] = {{1, 0, 1}, {1, 0, 2}, {1, 1, 1}, {1, 16, 8}, {2, 16, 16}, {2, 32, 16}, {4, 32, 16}};
+  const int cands[][3] = {{1, 0, 1}, {1, 0, 2}, {1, 1, 1}, {1, 16, 8}, {2, 16, 16}, {2, 32, 16}, {4, 32, 16},
+                          {2, 2, 8},  {3, 2, 8},  {4, 2, 8}, {2, 2, 16}, {4, 2, 16}};
   float best = 1e30f;
   int bestp[3] = {f->plan.levels, f->plan.by, f->plan.xc};
   for (const auto& c : cands) {

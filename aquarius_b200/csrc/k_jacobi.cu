@@ -16,6 +16,7 @@
 // 1/L of a plain sweep.  With RESID an extra level evaluates the FP64
 // residual b - A p of the written iterate on the CTA's output cells.
 #include <algorithm>
+#include <type_traits>
 
 #include "aq_kernels.cuh"
 
@@ -355,6 +356,155 @@ __global__ void __launch_bounds__(256) k_resid_flat(Dims d, const float* __restr
                                                    const float* __restrict__ rhs, const int8_t* __restrict__ type,
                                                    const uint8_t* __restrict__ bact, double* __restrict__ part) {
   resid_flat_body(d, p, rhs, type, bact, part, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+
+// ------------------------------------------------------------- cube tiles
+// Temporally blocked sweep on 3D tiles held in shared memory: a CTA loads a
+// (TX+2L) x (TX+2L) x 32 block of cells (its core TX x TX x (32-2L) plus an
+// L-cell halo), runs L sweeps on it and writes the core.  Sweep s updates the
+// cells at distance >= s from the block faces, whose neighbours were all
+// updated by sweep s-1, so the core ends exactly as after L separate sweeps
+// (same arithmetic, jacobi_quad's summation order).  Warps own block rows
+// (x, y) with lanes along z: a lane keeps its cells' pressure, rhs and
+// fluid/in-grid bits in registers across the sweeps; x and y neighbours come
+// from a shared-memory ping-pong, z neighbours by warp shuffle.
+template <int L, int TX>
+struct CubeShape {
+  static constexpr int E = TX + 2 * L;  // block rows per axis (x, y)
+  static constexpr int TZ = 32 - 2 * L;  // core along z
+  static constexpr int ROWS = E * E;
+};
+
+template <int L, int TX, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_jacobi_cube(Dims d, const float* __restrict__ pin,
+                                                           float* __restrict__ pout, const float* __restrict__ rhs,
+                                                           const int8_t* __restrict__ type,
+                                                           const uint8_t* __restrict__ bact) {
+  using S = CubeShape<L, TX>;
+  constexpr int E = S::E, TZ = S::TZ, ROWS = S::ROWS;
+  constexpr int R = (ROWS + WARPS - 1) / WARPS;
+  using Mask = typename std::conditional<(R > 32), unsigned long long, unsigned>::type;
+  extern __shared__ __align__(16) float cube_smem[];  // [2][ROWS][32]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int x0 = blockIdx.z * TX, y0 = blockIdx.y * TX, z0 = blockIdx.x * TZ;
+  // skip blocks whose core holds no fluid (their cells stay 0 in both buffers)
+  int a = 0;
+  {
+    const int bx0 = x0 / kBrick, bx1 = (min(x0 + TX, d.sx) - 1) / kBrick;
+    const int by0 = y0 / kBrick, by1 = (min(y0 + TX, d.sy) - 1) / kBrick;
+    const int bz0 = z0 / kBrick, bz1 = (min(z0 + TZ, d.sz) - 1) / kBrick;
+    const int nbx = bx1 - bx0 + 1, nby = by1 - by0 + 1, nbz = bz1 - bz0 + 1;
+    for (int k = threadIdx.x; k < nbx * nby * nbz; k += WARPS * 32) {
+      const int iz = k % nbz, t = k / nbz, iy = t % nby, ix = t / nby;
+      a |= bact[((bx0 + ix) * d.by + by0 + iy) * d.bz + bz0 + iz];
+    }
+  }
+  const bool active = __syncthreads_or(a) != 0;
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  if (!active) return;
+  const int gz = z0 - L + lane;
+  const bool zin = gz >= 0 && gz < d.sz;
+  float p[R], b[R];
+  Mask fluid = 0, ing = 0;
+  float* buf0 = cube_smem;
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const int r = warp + WARPS * k;
+    p[k] = 0.f;
+    b[k] = 0.f;
+    if (r < ROWS) {
+      const int gx = x0 - L + r / E, gy = y0 - L + r % E;
+      if (zin && gx >= 0 && gx < d.sx && gy >= 0 && gy < d.sy) {
+        const int c = (gx * d.sy + gy) * d.sz + gz;
+        p[k] = pin[c];
+        b[k] = rhs[c];
+        ing |= Mask(1) << k;
+        if (type[c] == kFluid) fluid |= Mask(1) << k;
+      }
+      buf0[r * 32 + lane] = p[k];
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int s = 1; s <= L; ++s) {
+    const float* src = cube_smem + ((s - 1) & 1) * ROWS * 32;
+    float* dst = cube_smem + (s & 1) * ROWS * 32;
+    const bool zok = lane >= s && lane < 32 - s;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int r = warp + WARPS * k;
+      if (r >= ROWS) continue;
+      const int lx = r / E, ly = r % E;
+      if (lx < s || lx >= E - s || ly < s || ly >= E - s) continue;  // warp-uniform
+      const float c = p[k];
+      const float zmv = __shfl_up_sync(0xffffffffu, c, 1);
+      const float zpv = __shfl_down_sync(0xffffffffu, c, 1);
+      if (zok && ((ing >> k) & 1)) {
+        const int gx = x0 - L + lx, gy = y0 - L + ly;
+        const float xp = gx + 1 < d.sx ? src[(r + E) * 32 + lane] : c;
+        const float xm = gx > 0 ? src[(r - E) * 32 + lane] : c;
+        const float yp = gy + 1 < d.sy ? src[(r + 1) * 32 + lane] : c;
+        const float ym = gy > 0 ? src[(r - 1) * 32 + lane] : c;
+        const float zp = gz + 1 < d.sz ? zpv : c;
+        const float zm = gz > 0 ? zmv : c;
+        float sum = xp + xm;
+        sum += yp;
+        sum += ym;
+        sum += zp;
+        sum += zm;
+        sum += b[k];
+        const float v = ((fluid >> k) & 1) ? __fdiv_rn(sum, 6.f) : 0.f;
+        p[k] = v;
+        dst[r * 32 + lane] = v;
+      }
+    }
+    __syncthreads();
+  }
+  if (lane < L || lane >= L + TZ || !zin) return;
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const int r = warp + WARPS * k;
+    if (r >= ROWS) continue;
+    const int lx = r / E, ly = r % E;
+    if (lx < L || lx >= L + TX || ly < L || ly >= L + TX) continue;
+    if ((ing >> k) & 1) pout[((x0 - L + lx) * d.sy + (y0 - L + ly)) * d.sz + gz] = p[k];
+  }
+}
+
+template <int L, int TX, int WARPS>
+cudaError_t launch_cube(cudaStream_t st, const Dims& d, const float* pin, float* pout, const float* rhs,
+                        const int8_t* type, const uint8_t* bact) {
+  using S = CubeShape<L, TX>;
+  constexpr size_t smem = (size_t)2 * S::ROWS * 32 * sizeof(float);
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      k_jacobi_cube<L, TX, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (attr != cudaSuccess) return attr;
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3((d.sz + S::TZ - 1) / S::TZ, (d.sy + TX - 1) / TX, (d.sx + TX - 1) / TX);
+  lc.blockDim = dim3(WARPS * 32);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  return cudaLaunchKernelEx(&lc, k_jacobi_cube<L, TX, WARPS>, d, pin, pout, rhs, type, bact);
+}
+
+// Cube plans: (levels, TX) -> warps per CTA.
+cudaError_t dispatch_cube(cudaStream_t st, const Dims& d, int levels, int tx, const float* pin, float* pout,
+                          const float* rhs, const int8_t* type, const uint8_t* bact) {
+  if (levels == 1 && tx == 8) return launch_cube<1, 8, 4>(st, d, pin, pout, rhs, type, bact);
+  if (levels == 2 && tx == 8) return launch_cube<2, 8, 8>(st, d, pin, pout, rhs, type, bact);
+  if (levels == 3 && tx == 8) return launch_cube<3, 8, 8>(st, d, pin, pout, rhs, type, bact);
+  if (levels == 4 && tx == 8) return launch_cube<4, 8, 16>(st, d, pin, pout, rhs, type, bact);
+  if (levels == 1 && tx == 16) return launch_cube<1, 16, 16>(st, d, pin, pout, rhs, type, bact);
+  if (levels == 2 && tx == 16) return launch_cube<2, 16, 16>(st, d, pin, pout, rhs, type, bact);
+  if (levels == 4 && tx == 16) return launch_cube<4, 16, 16>(st, d, pin, pout, rhs, type, bact);
+  return cudaErrorInvalidValue;
 }
 
 
@@ -945,6 +1095,22 @@ cudaError_t jacobi_prepare() {
 }
 
 long long jacobi_cells_updated(const Dims& d, const JacobiPlan& p, const uint8_t* bact_host) {
+  if (p.by == 2) {  // cube: core cells of the tiles whose core holds fluid
+    const int tx = p.xc, tz = 32 - 2 * p.levels;
+    long long cells = 0;
+    for (int x0 = 0; x0 < d.sx; x0 += tx)
+      for (int y0 = 0; y0 < d.sy; y0 += tx)
+        for (int z0 = 0; z0 < d.sz; z0 += tz) {
+          const int x1 = std::min(x0 + tx, d.sx), y1 = std::min(y0 + tx, d.sy), z1 = std::min(z0 + tz, d.sz);
+          bool act = false;
+          for (int bx = x0 / kBrick; bx <= (x1 - 1) / kBrick && !act; ++bx)
+            for (int by = y0 / kBrick; by <= (y1 - 1) / kBrick && !act; ++by)
+              for (int bz = z0 / kBrick; bz <= (z1 - 1) / kBrick && !act; ++bz)
+                act = bact_host[(bx * d.by + by) * d.bz + bz] != 0;
+          if (act) cells += (long long)(x1 - x0) * (y1 - y0) * (z1 - z0);
+        }
+    return cells;
+  }
   if (p.by == 0) {
     long long cells = 0;  // flat: xc x planes x 8 rows (one warp per row) x 128 z per block
     for (int x0 = 0; x0 < d.sx; x0 += p.xc)
@@ -980,7 +1146,7 @@ long long jacobi_cells_updated(const Dims& d, const JacobiPlan& p, const uint8_t
 }
 
 int jacobi_parts(const Dims& d, const JacobiPlan& p, bool resid) {
-  if (p.by == 0) return resid ? -1 : 1;
+  if (p.by == 0 || p.by == 2) return resid ? -1 : 1;
   const int H = p.levels + (resid ? 1 : 0);
   const int TZ = 32 - 2 * H, TY = p.by - 2 * H;
   if (TZ <= 0 || TY <= 0 || p.xc <= 0) return -1;
@@ -1011,8 +1177,18 @@ cudaError_t launch_jacobi(cudaStream_t st, const Dims& d, const JacobiPlan& plan
       default: return cudaErrorInvalidValue;
     }
   }
+  if (plan.by == 2) {
+    // cube plan: plan.levels sweeps per launch on TX = plan.xc tiles
+    if (resid || d.sz % 4 != 0) return cudaErrorInvalidValue;
+    if (nparts_out) *nparts_out = 0;
+    return dispatch_cube(st, d, plan.levels, plan.xc, pin, pout, rhs, type, brick_active);
+  }
   if (resid) return dispatch_levels<true>(st, d, plan, pin, pout, rhs, type, brick_active, part, nparts_out);
   return dispatch_levels<false>(st, d, plan, pin, pout, rhs, type, brick_active, part, nparts_out);
+}
+
+bool cube_plan_ok(int levels, int tx) {
+  return (tx == 8 && levels >= 1 && levels <= 4) || (tx == 16 && (levels == 1 || levels == 2 || levels == 4));
 }
 
 int persist_items(const Dims& d) { return ((d.sz / 4 + 31) / 32) * ((d.sy + 7) / 8) * d.sx; }

@@ -139,6 +139,8 @@ def jacobi_kernel_name(f) -> str:
         return "k_persist_solve (whole solve in one cooperative launch)"
     if rows == 0:
         return f"k_jacobi_flat<{xplanes}> (1 sweep/launch, float4 z-quads)"
+    if rows == 2:
+        return f"k_jacobi_cube<{levels} sweeps/launch, {xplanes}x{xplanes}x{32 - 2 * levels} tiles> (shared-memory cubes)"
     return f"k_jacobi<{levels} sweeps/launch, {rows} rows, {xplanes} x-planes> (temporally blocked)"
 
 

@@ -351,7 +351,8 @@ def test_jacobi_plans_agree(mode):
         o.stage(k)
     st = o.get_state()
     results = {}
-    for plan in [(1, 0, 1), (1, 1, 1), (1, 0, 2), (2, 16, 16), (4, 32, 16)]:
+    for plan in [(1, 0, 1), (1, 1, 1), (1, 0, 2), (2, 16, 16), (4, 32, 16), (1, 2, 8), (2, 2, 8), (3, 2, 8),
+                 (4, 2, 8), (2, 2, 16), (4, 2, 16)]:
         f = aq.Fluid(cfg)
         f.set_jacobi_plan(*plan)
         f.upload_state(st)
@@ -366,6 +367,25 @@ def test_jacobi_plans_agree(mode):
     o.stage(_abi.STAGE_PRESSURE)
     assert rel_l2(p0, o.get_state(["pressure"])["pressure"]) <= TOL
     assert s0["iterations"] == o.solve_stats()["iterations"]
+
+
+@pytest.mark.parametrize("shape", [(40, 36, 52), (24, 20, 28)])
+def test_cube_plans_match_flat_on_ragged_grids(shape):
+    # tiles that overhang the grid on every axis, full steps in a graph
+    vols = [dict(shape="box", min=(0, 0, 0), max=(1, 0.35, 1)),
+            dict(shape="sphere", center=(0.45, 0.7, 0.55), radius=0.2)]
+    cfg = _abi.make_config(shape, vols, timestep=0.01, pressure_init=_abi.PRESSURE_CARRY, pressure_iterations=57)
+    ref = aq.Fluid(cfg)
+    ref.step(3)
+    a = ref.download_state(["pressure", "position", "new_velocity"])
+    ref.close()
+    for plan in [(2, 2, 8), (3, 2, 8), (4, 2, 8), (2, 2, 16), (4, 2, 16)]:
+        with aq.Fluid(cfg) as f:
+            f.set_jacobi_plan(*plan)
+            f.step(3)
+            b = f.download_state(["pressure", "position", "new_velocity"])
+        for k in ("pressure", "position", "new_velocity"):
+            np.testing.assert_array_equal(a[k], b[k], err_msg=f"{plan} {k}")
 
 
 def test_persistent_step_graph_matches_flat():
