@@ -119,6 +119,7 @@ def load_library() -> ct.CDLL:
         "aq_unet_evaluate": (ct.c_int, [P, P, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_double)]),
         "aq_unet_gradients": (ct.c_int, [P, P, ct.c_int64]),
         "aq_fluid_set_warm_start": (ct.c_int, [P, P]),
+        "aq_fluid_phase_mass": (ct.c_int, [P, ct.POINTER(ct.c_double)]),
         "aq_dataset_create": (ct.c_int, [ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.POINTER(P)]),
         "aq_dataset_destroy": (None, [P]),
         "aq_dataset_count": (ct.c_int32, [P]),
@@ -315,6 +316,12 @@ class Fluid:
         s = _abi.SolveStats()
         _check(self._lib.aq_fluid_solve_stats(self._h, ct.byref(s)))
         return _solve_stats_dict(s)
+
+    def phase_mass(self) -> list:
+        """Sum over particles of the volume fractions of each of the 4 phases."""
+        m = (ct.c_double * 4)()
+        _check(self._lib.aq_fluid_phase_mass(self._h, m))
+        return list(m)
 
     def set_warm_start(self, net):
         """Attaches the network AQ_PRESSURE_LEARNED ('learned') uses (None detaches)."""

@@ -21,6 +21,9 @@ cudaError_t launch_particles_advance(cudaStream_t st, const Dims& d, const StepP
                                      Particles cur, Particles tmp, const float* u0, const float* v0,
                                      const float* w0, const float* un, const float* vn, const float* wn,
                                      const float4* nvf, int* key, int* slot, int* count, int n);
+// Per-block FP64 sums of the particle volume fractions: part[frac_sum_parts()][4].
+int frac_sum_parts();
+cudaError_t launch_frac_sum(cudaStream_t st, const float4* frac, int n, double* part);
 // Exclusive scan of count[0..C] into off[0..C] (off[C] = N) and clears count.
 cudaError_t launch_cell_scan(cudaStream_t st, int C, int* count, int* off, int* tile_sums);
 size_t cell_scan_tiles(int C);

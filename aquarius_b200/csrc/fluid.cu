@@ -1220,6 +1220,28 @@ aq_status aq_fluid_solve_stats(const aq_fluid* f, aq_solve_stats* st) {
   return AQ_OK;
 }
 
+aq_status aq_fluid_phase_mass(aq_fluid* f, double mass[4]) {
+  if (!f || !mass) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(f->device);
+  for (int k = 0; k < 4; ++k) mass[k] = 0.0;
+  if (!f->multiphase) {
+    mass[f->phase] = (double)f->n;
+    return AQ_OK;
+  }
+  const int np = frac_sum_parts();
+  double* part = nullptr;
+  AQ_CUDA(cudaMallocAsync((void**)&part, sizeof(double) * 4 * np, f->stream));
+  cudaError_t e = launch_frac_sum(f->stream, f->cur.frac, f->n, part);
+  std::vector<double> h((size_t)4 * np);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), part, sizeof(double) * 4 * np, cudaMemcpyDeviceToHost, f->stream);
+  cudaFreeAsync(part, f->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
+  AQ_CUDA(e);
+  for (int b = 0; b < np; ++b)
+    for (int k = 0; k < 4; ++k) mass[k] += h[(size_t)b * 4 + k];
+  return AQ_OK;
+}
+
 aq_status aq_fluid_set_warm_start(aq_fluid* f, aq_unet* net) {
   if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
   cudaSetDevice(f->device);

@@ -297,7 +297,32 @@ __global__ void __launch_bounds__(256) k_rank_gather(const int* __restrict__ key
 
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
 
+// Per-block FP64 sums of the particles' volume fractions (4 phases).
+__global__ void __launch_bounds__(256) k_frac_sum(const float4* __restrict__ frac, int n, double* __restrict__ part) {
+  __shared__ double sm[4][256];
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 f = frac[i];
+    a[0] += f.x; a[1] += f.y; a[2] += f.z; a[3] += f.w;
+  }
+  for (int k = 0; k < 4; ++k) sm[k][threadIdx.x] = a[k];
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 4; ++k) sm[k][threadIdx.x] += sm[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) part[blockIdx.x * 4 + threadIdx.x] = sm[threadIdx.x][0];
+}
+
 }  // namespace
+
+int frac_sum_parts() { return 512; }
+
+cudaError_t launch_frac_sum(cudaStream_t st, const float4* frac, int n, double* part) {
+  k_frac_sum<<<frac_sum_parts(), 256, 0, st>>>(frac, n, part);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_particles_advance(cudaStream_t st, const Dims& d, const StepParams& sp, bool move,
                                      Particles cur, Particles tmp, const float* u0, const float* v0,

@@ -59,8 +59,8 @@ typedef enum aq_shape { AQ_SHAPE_SPHERE = 0, AQ_SHAPE_SQUARE = 1 } aq_shape;
 /* Pressure initial guess for each step's solve.
  * CARRY: the reference behaviour — pressure persists across steps (it is only
  *        cleared when the grid is created, Fluid/MAC_Grid_3D.cu:54).
- * ZERO:  pressure is zeroed before every solve. */
-/* LEARNED: pressure is zeroed, then the warm-start network attached with
+ * ZERO:  pressure is zeroed before every solve.
+ * LEARNED: pressure is zeroed, then the warm-start network attached with
  *        aq_fluid_set_warm_start predicts it; 20 sweeps are run from the
  *        prediction and 20 from zero, and the solve continues from whichever
  *        has the lower residual (zero-init Jacobi is the fallback and the
@@ -431,6 +431,12 @@ aq_status aq_unet_evaluate(aq_unet* net, aq_dataset* ds, int32_t first, int32_t 
 /* The gradients of the last training step, in weights-file order (per layer
  * weights then bias, then head weights and bias); n = parameter count. */
 aq_status aq_unet_gradients(aq_unet* net, float* out, int64_t n);
+
+/* Concentration mass per phase: the sum over particles of their volume
+ * fractions (FP64; single-phase fluids: the particle count in their phase).
+ * No counterpart in the reference; its change over a run is the
+ * concentration-mass conservation error of multiphase diffusion. */
+aq_status aq_fluid_phase_mass(aq_fluid* f, double mass[4]);
 
 /* Attaches the network used by AQ_PRESSURE_LEARNED (NULL detaches).  The
  * network must outlive the fluid's steps; allocate-once buffers for the
