@@ -118,6 +118,8 @@ def load_library() -> ct.CDLL:
                                      ct.c_float, ct.c_int32, ct.POINTER(ct.c_float)]),
         "aq_unet_evaluate": (ct.c_int, [P, P, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_double)]),
         "aq_unet_gradients": (ct.c_int, [P, P, ct.c_int64]),
+        "aq_unet_set_output_scale": (ct.c_int, [P, ct.c_float]),
+        "aq_unet_evaluate_warm": (ct.c_int, [P, P, ct.c_int32, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_double)]),
         "aq_fluid_set_warm_start": (ct.c_int, [P, P]),
         "aq_fluid_phase_mass": (ct.c_int, [P, ct.POINTER(ct.c_double)]),
         "aq_dataset_create": (ct.c_int, [ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.POINTER(P)]),
@@ -554,6 +556,15 @@ class UNet:
         e = ct.c_double()
         _check(self._lib.aq_unet_evaluate(self._h, ds._h, first, count, ct.byref(e)))
         return e.value
+
+    def set_output_scale(self, scale: float):
+        _check(self._lib.aq_unet_set_output_scale(self._h, scale))
+
+    def evaluate_warm(self, ds: "Dataset", first: int, count: int, sweeps: int = 20) -> float:
+        """Mean (residual after `sweeps` sweeps from the prediction) / (from zero)."""
+        r = ct.c_double()
+        _check(self._lib.aq_unet_evaluate_warm(self._h, ds._h, first, count, sweeps, ct.byref(r)))
+        return r.value
 
     def gradients(self) -> np.ndarray:
         out = np.zeros(self.parameter_count(), np.float32)

@@ -73,6 +73,13 @@ struct JacobiPlan {
 };
 // Cube plans accepted by launch_jacobi (levels, tile edge).
 bool cube_plan_ok(int levels, int tx);
+// List plan (by = 3): the warp rows (x, y, 128-wide z block) whose bricks hold
+// fluid, listed once per solve, then one sweep per launch over the list by a
+// resident wave of CTAs (sz % 4 == 0).
+int row_items_capacity(const Dims& d);
+cudaError_t launch_row_items(cudaStream_t st, const Dims& d, const uint8_t* brick_active, int* items, int* n_items);
+cudaError_t launch_jacobi_list(cudaStream_t st, const Dims& d, const float* pin, float* pout, const float* rhs,
+                               const int8_t* type, const int* items, const int* n_items);
 
 // ---- persistent solve (k_jacobi.cu) ------------------------------------------
 // The whole pressure solve in one cooperative launch: every CTA sweeps its

@@ -238,6 +238,8 @@ aq_status aq_fluid::allocate() {
     AQ_TRY(alloc(&n_items, 1));
     AQ_TRY(alloc(&bar, 1));
     AQ_TRY(alloc(&ppart, (size_t)std::max(ctas, 1)));
+    AQ_TRY(alloc(&row_items, (size_t)row_items_capacity(d)));
+    AQ_TRY(alloc(&n_row_items, 1));
   }
   // default Jacobi plan: one vectorised sweep per launch where z allows it,
   // otherwise the tiled kernel with two sweeps per launch
@@ -274,6 +276,7 @@ aq_status aq_fluid::enq_divergence() {
   AQ_CUDA(launch_divergence(stream, d, off, type, density, nvx(nv_cur), nvy(nv_cur), nvz(nv_cur), pcount, div,
                             rhs, pa, pb, cfg.pressure_init != AQ_PRESSURE_CARRY, bact, part_b2, part_nf, &nb));
   AQ_CUDA(launch_b2_finalize(stream, part_b2, part_nf, nb, ss));
+  AQ_TRY(enq_row_items());
   return AQ_OK;
 }
 
@@ -292,8 +295,8 @@ static std::vector<int> split_sweeps(int sweeps, int levels) {
 
 int aq_fluid::count_jacobi_launches(int sweeps) const {
   const int k = (int)split_sweeps(sweeps, plan.levels).size();
-  // sweeps, parity copy, finalize, separate residual pass (flat and cube plans)
-  return k + (k % 2) + 1 + (plan.by == 0 || plan.by == 2 ? 1 : 0);
+  // sweeps, parity copy, finalize, separate residual pass (flat, cube and list plans)
+  return k + (k % 2) + 1 + (plan.by == 0 || plan.by >= 2 ? 1 : 0);
 }
 
 // `sweeps` Jacobi sweeps from pa; the last launch also writes the residual
@@ -307,9 +310,14 @@ int aq_fluid::count_jacobi_launches(int sweeps) const {
 static aq_status enqueue_sweeps_on(aq_fluid* f, const JacobiPlan& plan, float* a, float* b, int sweeps,
                                    bool with_residual, double* part) {
   const std::vector<int> parts = split_sweeps(sweeps, plan.levels);
-  const bool flat = plan.by == 0 || plan.by == 2;  // residual in a separate pass
+  const bool flat = plan.by == 0 || plan.by >= 2;  // residual in a separate pass
   float* bufs[2] = {a, b};
   for (size_t k = 0; k < parts.size(); ++k) {
+    if (plan.by == 3) {
+      AQ_CUDA(launch_jacobi_list(f->stream, f->d, bufs[k % 2], bufs[(k + 1) % 2], f->rhs, f->type, f->row_items,
+                                 f->n_row_items));
+      continue;
+    }
     const bool last = k + 1 == parts.size();
     JacobiPlan p = plan;
     p.levels = parts[k];
@@ -333,13 +341,19 @@ static aq_status enqueue_sweeps(aq_fluid* f, int sweeps, bool with_residual = tr
 static int last_parts_of(const aq_fluid* f, const JacobiPlan& plan, int sweeps) {
   const std::vector<int> parts = split_sweeps(sweeps, plan.levels);
   if (parts.empty()) return 0;
-  if (plan.by == 0 || plan.by == 2) return resid_flat_parts(f->d);
+  if (plan.by == 0 || plan.by >= 2) return resid_flat_parts(f->d);
   JacobiPlan p = plan;
   p.levels = parts.back();
   return jacobi_parts(f->d, p, true);
 }
 
 static int last_parts(const aq_fluid* f, int sweeps) { return last_parts_of(f, f->plan, sweeps); }
+
+aq_status aq_fluid::enq_row_items() {
+  if (plan.by != 3) return AQ_OK;
+  AQ_CUDA(launch_row_items(stream, d, bact, row_items, n_row_items));
+  return AQ_OK;
+}
 
 int aq_fluid::solve_sweeps_done() const { return cfg.pressure_init == AQ_PRESSURE_LEARNED ? kWarmSweeps : 0; }
 
@@ -942,6 +956,7 @@ aq_status aq_fluid::upload(const aq_host_state* s) {
     AQ_CUDA(cudaMemcpy(dv.data(), div, 4 * C, cudaMemcpyDeviceToHost));
     AQ_CUDA(cudaMemcpy(dn.data(), density, 4 * C, cudaMemcpyDeviceToHost));
     AQ_TRY(derive_from_state(ct, dv, dn));
+    AQ_TRY(enq_row_items());
   }
   nv_cur = has_cur = 2;
   sorted_by_stage1 = false;
@@ -1294,6 +1309,17 @@ aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, in
     f->invalidate_graph();
     return AQ_OK;
   }
+  if (rows == 3) {  // list of active warp rows, one sweep per launch
+    if (f->d.sz % 4 != 0 || levels != 1 || x_planes != 1)
+      return fail(AQ_ERR_INVALID_ARGUMENT, "the list plan is (1, 3, 1) and needs sz % 4 == 0");
+    cudaSetDevice(f->device);
+    AQ_CUDA(cudaStreamSynchronize(f->stream));
+    f->plan = JacobiPlan{1, 3, 1};
+    AQ_TRY(f->enq_row_items());  // the current system's rows
+    AQ_CUDA(cudaStreamSynchronize(f->stream));
+    f->invalidate_graph();
+    return AQ_OK;
+  }
   if (rows == 2) {  // cube tiles: `levels` sweeps per launch on x_planes-edge tiles
     if (f->d.sz % 4 != 0 || !cube_plan_ok(levels, x_planes))
       return fail(AQ_ERR_INVALID_ARGUMENT, "unsupported cube plan (sz % 4 == 0; edge 8 with 1-4 levels or 16 with 2/4)");
@@ -1393,7 +1419,8 @@ aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, in
   if (cells_per_sweep) {
     std::vector<uint8_t> act((size_t)f->nbricks);
     AQ_CUDA(cudaMemcpy(act.data(), f->bact, act.size(), cudaMemcpyDeviceToHost));
-    *cells_per_sweep = jacobi_cells_updated(f->d, f->plan.by == 1 ? JacobiPlan{1, 0, 1} : f->plan, act.data());
+    *cells_per_sweep =
+        jacobi_cells_updated(f->d, f->plan.by == 1 || f->plan.by == 3 ? JacobiPlan{1, 0, 1} : f->plan, act.data());
   }
   return AQ_OK;
 }
@@ -1466,7 +1493,7 @@ aq_status aq_fluid_autotune(aq_fluid* f, int32_t sweeps_per_trial, const char* c
     return AQ_OK;
   }
   const int cands[][3] = {{1, 0, 1}, {1, 0, 2}, {1, 1, 1}, {1, 16, 8}, {2, 16, 16}, {2, 32, 16}, {4, 32, 16},
-                          {2, 2, 8},  {3, 2, 8},  {4, 2, 8}, {2, 2, 16}, {4, 2, 16}};
+                          {2, 2, 8},  {3, 2, 8},  {4, 2, 8}, {2, 2, 16}, {4, 2, 16}, {1, 3, 1}};
   float best = 1e30f;
   int bestp[3] = {f->plan.levels, f->plan.by, f->plan.xc};
   for (const auto& c : cands) {

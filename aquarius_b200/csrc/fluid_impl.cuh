@@ -71,6 +71,8 @@ struct aq_fluid {
   float *za = nullptr, *zb = nullptr;  // the zero-init path of the first sweeps
   double* jpart2 = nullptr;
   int* pick = nullptr;  // 1: the zero-init path won
+  // list plan: active warp rows of the current system
+  int *row_items = nullptr, *n_row_items = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool use_graph = true;
   int graph_launches = 0;  // launches outside the residual loop
@@ -122,6 +124,7 @@ struct aq_fluid {
   aq_status enq_solve_residual_eager();
   aq_status enq_learned_start();
   int solve_sweeps_done() const;  // sweeps the warm start already did (0 without it)
+  aq_status enq_row_items();       // list plan: rebuild the active-row list (no-op otherwise)
   aq_status enq_project();
   aq_status enq_extrapolate();
   aq_status enq_diffuse();

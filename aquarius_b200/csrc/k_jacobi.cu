@@ -219,12 +219,11 @@ __device__ __forceinline__ float4 jacobi_quad(const float4& xm, const float4& xp
 // (bx, by, bz) = (z-quad block, row block, x-plane group) of the flat grid;
 // the caller has checked that the warp's rows hold fluid (warp_active).
 template <int XS>
-__device__ __forceinline__ void jacobi_flat_body(const Dims& d, const float* __restrict__ pin,
-                                                 float* __restrict__ pout, const float* __restrict__ rhs,
-                                                 const int8_t* __restrict__ type, int bx, int by, int bz) {
+__device__ __forceinline__ void jacobi_row(const Dims& d, const float* __restrict__ pin, float* __restrict__ pout,
+                                           const float* __restrict__ rhs, const int8_t* __restrict__ type, int bx,
+                                           int y, int bz) {
   const int lane = threadIdx.x;
   const int z = (bx * 32 + lane) * 4;
-  const int y = by * 8 + threadIdx.y;
   const int x0 = bz * XS;
   const int x1 = min(x0 + XS, d.sx);
   const bool in = z < d.sz;
@@ -272,6 +271,74 @@ __device__ __forceinline__ void jacobi_flat_body(const Dims& d, const float* __r
     b = nb;
     t = nt;
   }
+}
+
+template <int XS>
+__device__ __forceinline__ void jacobi_flat_body(const Dims& d, const float* __restrict__ pin,
+                                                 float* __restrict__ pout, const float* __restrict__ rhs,
+                                                 const int8_t* __restrict__ type, int bx, int by, int bz) {
+  jacobi_row<XS>(d, pin, pout, rhs, type, bx, by * 8 + threadIdx.y, bz);
+}
+
+// List plan: one sweep of the warp rows (x, y, 128-wide z block) that hold
+// fluid, from a list built once per solve (k_row_items).  A resident wave of
+// CTAs walks the list, so no CTA is scheduled only to find its rows empty.
+// Same arithmetic as the flat sweep (jacobi_quad).
+__global__ void __launch_bounds__(256) k_jacobi_list(Dims d, const float* __restrict__ pin, float* __restrict__ pout,
+                                                    const float* __restrict__ rhs, const int8_t* __restrict__ type,
+                                                    const int* __restrict__ items, const int* __restrict__ n_items) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  const int n = *n_items;
+  const int gz = (d.sz / 4 + 31) / 32;
+  for (int it = blockIdx.x * 8 + threadIdx.y; it < n; it += gridDim.x * 8) {
+    const int id = __ldg(items + it);
+    const int zb = id % gz, t = id / gz;
+    jacobi_row<1>(d, pin, pout, rhs, type, zb, t % d.sy, t / d.sy);
+  }
+}
+
+// Ordered list of the active warp rows: id = (x * sy + y) * gz + zb for every
+// row whose 8^3 bricks (x/8, y/8, 16 z bricks of block zb) hold fluid.
+__global__ void __launch_bounds__(1024) k_row_items(Dims d, const uint8_t* __restrict__ bact, int* __restrict__ items,
+                                                   int* __restrict__ n_items) {
+  __shared__ int s_cnt[32], s_pre[32];
+  __shared__ int s_tot, s_base;
+  const int gz = (d.sz / 4 + 31) / 32;
+  const int total = d.sx * d.sy * gz;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_base = 0;
+  __syncthreads();
+  for (int base = 0; base < total; base += 1024) {
+    const int id = base + threadIdx.x;
+    int a = 0;
+    if (id < total) {
+      const int zb = id % gz, t = id / gz, y = t % d.sy, x = t / d.sy;
+      for (int k = 0; k < 16 && zb * 16 + k < d.bz && !a; ++k)
+        a = bact[((x / kBrick) * d.by + y / kBrick) * d.bz + zb * 16 + k] ? 1 : 0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, a);
+    const int pre = __popc(m & ((1u << lane) - 1u));
+    if (lane == 0) s_cnt[w] = __popc(m);
+    __syncthreads();
+    if (w == 0) {
+      const int v = s_cnt[lane];
+      int incl = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int tt = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += tt;
+      }
+      s_pre[lane] = incl - v;
+      if (lane == 31) s_tot = incl;
+    }
+    __syncthreads();
+    if (a) items[s_base + s_pre[w] + pre] = id;
+    __syncthreads();
+    if (threadIdx.x == 0) s_base += s_tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *n_items = s_base;
 }
 
 // Programmatic dependent launch: the activity bricks were written two or more
@@ -1316,6 +1383,33 @@ cudaError_t launch_batch_solve_condition(cudaStream_t st, const int* live, int n
                                          unsigned long long cond_handle) {
   kb_solve_condition<<<1, 1024, 0, st>>>(live, n_scenes, (cudaGraphConditionalHandle)cond_handle);
   return cudaGetLastError();
+}
+
+}  // namespace aqb
+
+namespace aqb {
+
+int row_items_capacity(const Dims& d) { return d.sx * d.sy * ((d.sz / 4 + 31) / 32); }
+
+cudaError_t launch_row_items(cudaStream_t st, const Dims& d, const uint8_t* brick_active, int* items, int* n_items) {
+  k_row_items<<<1, 1024, 0, st>>>(d, brick_active, items, n_items);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_jacobi_list(cudaStream_t st, const Dims& d, const float* pin, float* pout, const float* rhs,
+                               const int8_t* type, const int* items, const int* n_items) {
+  if (d.sz % 4 != 0) return cudaErrorInvalidValue;
+  const int need = (row_items_capacity(d) + 7) / 8;
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(std::max(1, std::min(need, resident_ctas(k_jacobi_list, 256))));
+  lc.blockDim = dim3(32, 8);
+  lc.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  return cudaLaunchKernelEx(&lc, k_jacobi_list, d, pin, pout, rhs, type, items, n_items);
 }
 
 }  // namespace aqb

@@ -613,6 +613,51 @@ aq_status aq_unet_evaluate(aq_unet* net, aq_dataset* ds, int32_t first, int32_t 
   return AQ_OK;
 }
 
+// Mean over samples of (residual after `sweeps` Jacobi sweeps from the
+// prediction) / (the same from zero), the ratio the warm start's fallback
+// rule compares: below 1 the prediction is kept.
+aq_status aq_unet_evaluate_warm(aq_unet* net, aq_dataset* ds, int32_t first, int32_t count, int32_t sweeps,
+                                double* mean_ratio) {
+  if (!net || !ds || !mean_ratio || first < 0 || count < 1 || first + count > ds->n || sweeps < 0 || sweeps > 1000)
+    return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaSetDevice(net->device);
+  UActs* a = nullptr;
+  UN_TRY(unet_acts(net, ds->sx, ds->sy, ds->sz, true, &a));
+  const int sx = ds->sx, sy = ds->sy, sz = ds->sz;
+  const size_t V = (size_t)sx * sy * sz;
+  cudaStream_t st = net->stream;
+  float* p = nullptr;
+  UN_CUDA(cudaMallocAsync((void**)&p, sizeof(float) * V, st));
+  double acc = 0.0;
+  aq_status status = AQ_OK;
+  for (int i = first; i < first + count && status == AQ_OK; ++i) {
+    const size_t o = (size_t)i * V;
+    // rhs is stored scaled (max-abs 1): p is in the targets' units
+    if ((status = unet_predict(net, st, a, ds->rhs + o, ds->type + o, p)) != AQ_OK) break;
+    float sums[6];
+    if (launch_unet_loss_bwd(st, p, ds->target + o, ds->type + o, a->d1, net->hp, 1.f, sweeps, a->g_d1, sx, sy, sz,
+                             a->le, a->l0, a->l1, a->l2, a->l3, a->lg, a->lpart, a->lsums, a->hpart,
+                             net->hg) != cudaSuccess ||
+        cudaMemcpyAsync(sums, a->lsums, sizeof(sums), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      status = fail(AQ_ERR_CUDA, "warm-start evaluation");
+      break;
+    }
+    acc += sums[3] > 0.f ? sqrt((double)sums[2] / (double)sums[3]) : 0.0;
+  }
+  cudaFreeAsync(p, st);
+  UN_CUDA(cudaStreamSynchronize(st));
+  if (status != AQ_OK) return status;
+  *mean_ratio = acc / count;
+  return AQ_OK;
+}
+
+aq_status aq_unet_set_output_scale(aq_unet* net, float scale) {
+  if (!net || !(scale > 0.f)) return fail(AQ_ERR_INVALID_ARGUMENT, "scale must be > 0");
+  net->out_scale = scale;
+  return AQ_OK;
+}
+
 aq_status aq_unet_gradients(aq_unet* net, float* out, int64_t n) {
   int64_t total = 0;
   UN_TRY(aq_unet_parameter_count(net, &total));

@@ -1,8 +1,9 @@
 """Trains the learned pressure warm start and writes its weights file.
 
-    python -m aquarius_b200.train_unet --size 64 --scenes 500 --out weights/unet_64.bin
-    python -m aquarius_b200.train_unet --size 128 --scenes 100 --init weights/unet_64.bin \
-        --out weights/unet_128.bin
+    python -m aquarius_b200.train_unet --size 64 --scenes 500 --train-steps 12000 --calibrate-scale \
+        --out aquarius_b200/weights/unet_64.bin
+    python -m aquarius_b200.train_unet --size 128 --scenes 40 --adopt aquarius_b200/weights/unet_64.bin \
+        --calibrate-scale --out aquarius_b200/weights/unet_128.bin
 
 Training pairs: seeded ball-drop scenes (a pool of random depth 0.1-0.4 under
 1-3 spheres of radius 0.08-0.2 at random positions, 8 particles per cell),
@@ -12,7 +13,13 @@ next step (rhs = -divergence x density, fluid mark) is labelled by the FP64
 PCG to relative residual 1e-10 and stored on the device.  The network is then
 trained by the library's own kernels (Adam, cosine learning rate) on 90% of
 the pairs and evaluated on the rest (mean relative L2 pressure error over
-fluid cells).  Everything runs on one GPU; a JSON summary goes to stdout.
+fluid cells).  `--adopt` skips training and takes a trained network as it is
+(the fully convolutional network applies to any grid size divisible by 4).
+`--calibrate-scale` then picks the network's output scale, among multiples
+of its current one, that minimises the mean ratio of the residuals after 20
+Jacobi sweeps from the prediction and from zero on the held-out pairs (all
+pairs with --adopt): the quantity the warm start's fallback rule compares.
+Everything runs on one GPU; a JSON summary goes to stdout.
 """
 from __future__ import annotations
 
@@ -100,6 +107,9 @@ def main():
                          "the residuals after 20 sweeps from the prediction and from zero")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--init", type=str, default=None, help="weights file to start from (fine-tuning)")
+    ap.add_argument("--adopt", type=str, default=None, help="weights file to use as it is (no training)")
+    ap.add_argument("--calibrate-scale", action="store_true",
+                    help="choose the output scale by the 20-sweep residual ratio on held-out pairs")
     ap.add_argument("--out", type=str, default=None)
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args()
@@ -107,25 +117,41 @@ def main():
     ds, info = generate(args.size, args.scenes, args.steps_per_scene, args.every, args.seed, args.sim_sweeps,
                         args.device)
     n = len(ds)
-    n_train = max(1, int(round(0.9 * n)))
-    n_test = n - n_train
     net = UNet(device=args.device, seed=args.seed)
-    if args.init:
-        net.load(args.init)
     t0 = time.perf_counter()
-    net.train(ds, 0, n_train, steps=1, lr=0.0)  # output scale from the training targets
-    before = net.evaluate(ds, n_train, n_test) if n_test else None
-    loss = net.train(ds, 0, n_train, steps=args.train_steps, lr=args.lr, seed=args.seed,
-                     out_scale=net.output_scale(), residual_weight=args.residual_weight,
-                     residual_sweeps=args.residual_sweeps)
+    if args.adopt:
+        net.load(args.adopt)
+        n_train, n_test = 0, n
+        before = net.evaluate(ds, 0, n)
+        loss, after, train_err = None, before, None
+    else:
+        n_train = max(1, int(round(0.9 * n)))
+        n_test = n - n_train
+        if args.init:
+            net.load(args.init)
+        net.train(ds, 0, n_train, steps=1, lr=0.0)  # output scale from the training targets
+        before = net.evaluate(ds, n_train, n_test) if n_test else None
+        loss = net.train(ds, 0, n_train, steps=args.train_steps, lr=args.lr, seed=args.seed,
+                         out_scale=net.output_scale(), residual_weight=args.residual_weight,
+                         residual_sweeps=args.residual_sweeps)
+        after = net.evaluate(ds, n_train, n_test) if n_test else None
+        train_err = net.evaluate(ds, 0, min(n_train, 64))
     train_s = time.perf_counter() - t0
-    after = net.evaluate(ds, n_train, n_test) if n_test else None
-    train_err = net.evaluate(ds, 0, min(n_train, 64))
+    calibration = None
+    if args.calibrate_scale and n_test:
+        base = net.output_scale()
+        calibration = []
+        for k in (0.25, 0.35, 0.5, 0.7, 1.0, 1.4, 2.0):
+            net.set_output_scale(base * k)
+            calibration.append([base * k, net.evaluate_warm(ds, n_train, n_test, args.residual_sweeps)])
+        best = min(calibration, key=lambda t: t[1])
+        net.set_output_scale(best[0])
     out = pathlib.Path(args.out) if args.out else WEIGHTS_DIR / f"unet_{args.size}.bin"
     out.parent.mkdir(parents=True, exist_ok=True)
     net.save(out)
     warm = check_warm(net, args.size, args.device) if args.check_warm else None
     print(json.dumps(dict(info, size=args.size, train_pairs=n_train, test_pairs=n_test, warm_check=warm,
+                          adopted=args.adopt, scale_calibration=calibration,
                           residual_weight=args.residual_weight, residual_sweeps=args.residual_sweeps,
                           train_steps=args.train_steps, train_s=train_s, final_loss=loss,
                           test_rel_error_before=before, test_rel_error_after=after,

@@ -395,6 +395,7 @@ aq_status aq_unet_parameter_count(const aq_unet* net, int64_t* count);
 aq_status aq_unet_save(aq_unet* net, const char* path);
 aq_status aq_unet_load(aq_unet* net, const char* path);
 aq_status aq_unet_get_output_scale(const aq_unet* net, float* scale);
+aq_status aq_unet_set_output_scale(aq_unet* net, float scale);
 /* Forward pass on device buffers (rhs [C] f32, type [C] int8 0 air / 1
  * fluid): pressure [C] = warm start (0 off fluid).  stream NULL = the
  * network's stream. */
@@ -428,6 +429,11 @@ aq_status aq_unet_train(aq_unet* net, aq_dataset* ds, int32_t first, int32_t cou
 /* Mean over samples of the relative L2 error (fluid cells) of the prediction
  * against the FP64 PCG pressure. */
 aq_status aq_unet_evaluate(aq_unet* net, aq_dataset* ds, int32_t first, int32_t count, double* mean_rel_error);
+/* Mean over samples of (relative residual after `sweeps` Jacobi sweeps from
+ * the prediction) / (the same from zero): the ratio the warm start's
+ * fallback rule compares at 20 sweeps (below 1, the prediction is kept). */
+aq_status aq_unet_evaluate_warm(aq_unet* net, aq_dataset* ds, int32_t first, int32_t count, int32_t sweeps,
+                                double* mean_ratio);
 /* The gradients of the last training step, in weights-file order (per layer
  * weights then bias, then head weights and bias); n = parameter count. */
 aq_status aq_unet_gradients(aq_unet* net, float* out, int64_t n);

@@ -352,7 +352,7 @@ def test_jacobi_plans_agree(mode):
     st = o.get_state()
     results = {}
     for plan in [(1, 0, 1), (1, 1, 1), (1, 0, 2), (2, 16, 16), (4, 32, 16), (1, 2, 8), (2, 2, 8), (3, 2, 8),
-                 (4, 2, 8), (2, 2, 16), (4, 2, 16)]:
+                 (4, 2, 8), (2, 2, 16), (4, 2, 16), (1, 3, 1)]:
         f = aq.Fluid(cfg)
         f.set_jacobi_plan(*plan)
         f.upload_state(st)
@@ -370,7 +370,7 @@ def test_jacobi_plans_agree(mode):
 
 
 @pytest.mark.parametrize("shape", [(40, 36, 52), (24, 20, 28)])
-def test_cube_plans_match_flat_on_ragged_grids(shape):
+def test_cube_and_list_plans_match_flat_on_ragged_grids(shape):
     # tiles that overhang the grid on every axis, full steps in a graph
     vols = [dict(shape="box", min=(0, 0, 0), max=(1, 0.35, 1)),
             dict(shape="sphere", center=(0.45, 0.7, 0.55), radius=0.2)]
@@ -379,7 +379,7 @@ def test_cube_plans_match_flat_on_ragged_grids(shape):
     ref.step(3)
     a = ref.download_state(["pressure", "position", "new_velocity"])
     ref.close()
-    for plan in [(2, 2, 8), (3, 2, 8), (4, 2, 8), (2, 2, 16), (4, 2, 16)]:
+    for plan in [(2, 2, 8), (3, 2, 8), (4, 2, 8), (2, 2, 16), (4, 2, 16), (1, 3, 1)]:
         with aq.Fluid(cfg) as f:
             f.set_jacobi_plan(*plan)
             f.step(3)

@@ -99,3 +99,19 @@ def test_learned_graph_equals_eager(trained_net):
     np.testing.assert_array_equal(a["pressure"], b["pressure"])
     np.testing.assert_array_equal(a["position"], b["position"])
     assert sa["iterations"] == sb["iterations"] and sa["warm_start"] == sb["warm_start"]
+
+
+def test_evaluate_warm_matches_the_step_pick(trained_net):
+    # the dataset-side ratio (J^20 applied to the prediction's error against
+    # the FP64 solution) equals the step's residual ratio after 20 sweeps
+    ds = aq.Dataset(SHAPE, capacity=1)
+    with aq.Fluid(_cfg(_abi.PRESSURE_ZERO, _abi.SOLVE_FIXED, pressure_iterations=200)) as z:
+        for stage in range(1, 5):
+            z.run_stage(stage)
+        ds.add_fluid(z, 1e-12)
+    ratio = trained_net.evaluate_warm(ds, 0, 1, 20)
+    with aq.Fluid(_cfg(_abi.PRESSURE_LEARNED)) as f:
+        f.set_warm_start(trained_net)
+        f.step(1)
+        s = f.solve_stats()
+    assert ratio == pytest.approx(s["warm_rel_residual"] / s["zero_rel_residual"], rel=2e-2)
