@@ -241,9 +241,10 @@ aq_status aq_fluid::allocate() {
     AQ_TRY(alloc(&row_items, (size_t)row_items_capacity(d)));
     AQ_TRY(alloc(&n_row_items, 1));
   }
-  // default Jacobi plan: one vectorised sweep per launch where z allows it,
-  // otherwise the tiled kernel with two sweeps per launch
-  plan = d.sz % 4 == 0 ? JacobiPlan{1, 0, 1} : JacobiPlan{2, 16, 16};
+  // default Jacobi plan: one vectorised sweep per launch over the listed
+  // active warp rows where z allows it, otherwise the tiled kernel with two
+  // sweeps per launch
+  plan = d.sz % 4 == 0 ? JacobiPlan{1, 3, 1} : JacobiPlan{2, 16, 16};
   if (d.sz % 4 == 0 && resid_flat_parts(d) > jpart_cap) {
     jpart_cap = resid_flat_parts(d);
     AQ_TRY(alloc(&jpart, (size_t)jpart_cap));

@@ -139,6 +139,8 @@ def jacobi_kernel_name(f) -> str:
         return "k_persist_solve (whole solve in one cooperative launch)"
     if rows == 0:
         return f"k_jacobi_flat<{xplanes}> (1 sweep/launch, float4 z-quads)"
+    if rows == 3:
+        return "k_jacobi_list (1 sweep/launch over the listed active warp rows, one resident wave)"
     if rows == 2:
         return f"k_jacobi_cube<{levels} sweeps/launch, {xplanes}x{xplanes}x{32 - 2 * levels} tiles> (shared-memory cubes)"
     return f"k_jacobi<{levels} sweeps/launch, {rows} rows, {xplanes} x-planes> (temporally blocked)"
@@ -368,19 +370,21 @@ def run_ours(args, rank: int, world: int, dist):
                         "tuned_sweep_us": tune["sweep_us"]},
     }
     plain_rel = [st1["rel_residual"], pstats["rel_residual"]]
+    plan = f.jacobi_plan()
     f.close()
     if not args.no_learned:
-        line["learned"] = learned_arm(args, dev, stream, max(plain_rel), ms_max / args.steps, dist)
+        line["learned"] = learned_arm(args, dev, stream, max(plain_rel), ms_max / args.steps, dist, plan)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(args.size, args.pressure_init, steps=1)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def learned_arm(args, dev, stream, plain_residual: float, plain_ms: float, dist) -> dict:
-    """The same workload with the learned warm start (AQ_PRESSURE_LEARNED):
-    (a) to the same target 1e-4 (cap 2000), (b) to the residual the plain
-    step reached at its cap, i.e. at equal achieved residual."""
+def learned_arm(args, dev, stream, plain_residual: float, plain_ms: float, dist, plan) -> dict:
+    """The same workload with the learned warm start (AQ_PRESSURE_LEARNED) and
+    the plain step's Jacobi plan: (a) to the same target 1e-4 (cap 2000), (b)
+    to the residual the plain step reached at its cap, i.e. at equal achieved
+    residual."""
     import torch
 
     import aquarius_b200 as aq
@@ -389,13 +393,15 @@ def learned_arm(args, dev, stream, plain_residual: float, plain_ms: float, dist)
     if not wpath.exists():
         return {"unavailable": f"no trained weights for {args.size}^3 ({wpath.name})"}
     net = aq.UNet(device=dev, weights=wpath)
-    out = {"weights": wpath.name, "parameters": net.parameter_count()}
+    out = {"weights": wpath.name, "parameters": net.parameter_count(), "jacobi_plan": list(plan)}
     for name, target in (("to_1e-4", 1e-4), ("to_plain_residual", plain_residual)):
         cfg = workload_config(args.size, "zero")
         cfg.pressure_init = _abi.PRESSURE_LEARNED
         cfg.rel_residual = float(target)
         cfg.device = dev
         f = aq.Fluid(cfg)
+        if plan[1] != 1:  # the persistent solve does not take the warm start
+            f.set_jacobi_plan(*plan)
         f.set_warm_start(net)
         f.step(args.warmup)
         f.synchronize()
