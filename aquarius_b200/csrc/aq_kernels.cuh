@@ -169,9 +169,14 @@ int batch_row_items(const Dims& d, int xs);
 // Cells the packed-row sweep writes (items with an active brick).
 long long batch_row_cells_updated(const Dims& d, int xs, const uint8_t* bact_host);
 // pipelined (xs > 1): plane x+1's loads are issued before plane x's arithmetic.
+// list (may be NULL): the active (scene, item) pairs from launch_batch_row_list.
 cudaError_t launch_batch_jacobi_rows(cudaStream_t st, const BatchIndex& bi, int total, int xs, bool pipelined,
                                      int grid, const int* live, const float* pin, float* pout, const float* rhs,
-                                     const int8_t* type, const uint8_t* brick_active);
+                                     const int8_t* type, const uint8_t* brick_active, const int2* list,
+                                     const int* n_list);
+// The (scene, local item) pairs whose bricks hold fluid (capacity: total).
+cudaError_t launch_batch_row_list(cudaStream_t st, const BatchIndex& bi, int total, int xs,
+                                  const uint8_t* brick_active, int2* list, int* n_list);
 cudaError_t launch_batch_resid_flat(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* live,
                                     const float* p, const float* rhs, const int8_t* type,
                                     const uint8_t* brick_active, double* part);

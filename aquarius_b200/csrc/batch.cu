@@ -72,6 +72,9 @@ struct aq_batch {
   int multiple = 64;  // cap on CTAs per SM of a batched launch (occupancy decides below it)
   int xs = 1;         // x planes per packed-row Jacobi item
   bool pipe = false;  // pipelined plane loads (xs > 1)
+  int2* row_list = nullptr;  // active (scene, item) pairs of the current systems
+  int* n_row_list = nullptr;
+  int row_list_cap = 0;
 
   Particles cur{}, tmp{};
   int *key = nullptr, *slot = nullptr, *perm_u = nullptr, *sort_index = nullptr;
@@ -119,6 +122,11 @@ struct aq_batch {
   int grid() const { return std::max(1, sms * multiple); }
   int grid512() const { return std::max(1, sms * std::max(1, multiple / 2)); }
   aq_status set_sweep_plan(int planes, bool pipelined);
+  aq_status enq_row_list() {
+    if (cudaError_t e = launch_batch_row_list(stream, bi, pre_r[ns], xs, bact, row_list, n_row_list))
+      return fail(AQ_ERR_CUDA, std::string("row list: ") + cudaGetErrorString(e));
+    return AQ_OK;
+  }
 
   aq_status allocate();
   aq_status add_scene(int s, aq_fluid* f);
@@ -156,6 +164,10 @@ aq_status aq_batch::allocate() {
   AQB_TRY(alloc(&ss, (size_t)ns)); AQB_TRY(alloc(&live, (size_t)ns));
   AQB_TRY(alloc(&scenes_d, (size_t)ns));
   AQB_TRY(alloc(&pre_d, 6 * (size_t)(ns + 1)));
+  row_list_cap = 0;
+  for (const SceneDesc& S : scenes) row_list_cap += batch_row_items(S.d, 1);  // one plane per item: the most items
+  AQB_TRY(alloc(&row_list, (size_t)row_list_cap));
+  AQB_TRY(alloc(&n_row_list, 1));
   AQB_CUDA(cudaMemcpyAsync(scenes_d, scenes.data(), sizeof(SceneDesc) * ns, cudaMemcpyHostToDevice, stream));
   std::vector<int> pre;
   for (const auto* v : {&pre_p, &pre_n, &pre_b, &pre_s, &pre_f}) pre.insert(pre.end(), v->begin(), v->end());
@@ -185,6 +197,7 @@ aq_status aq_batch::set_sweep_plan(int planes, bool pipelined) {
   for (const SceneDesc& S : scenes) pre_r.push_back(pre_r.back() + batch_row_items(S.d, xs));
   AQB_CUDA(cudaMemcpyAsync(pre_d + 5 * (ns + 1), pre_r.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice,
                            stream));
+  AQB_TRY(enq_row_list());  // items depend on the plane count
   AQB_CUDA(cudaStreamSynchronize(stream));
   invalidate_graph();
   return AQ_OK;
@@ -239,6 +252,7 @@ aq_status aq_batch::enq_pre_solve() {
   AQB_CUDA(launch_batch_divergence(stream, bi, tb, grid512(), off, type, density, un1, vn1, wn1, pcount, div, rhs,
                                    pa, pb, solver.pressure_init == AQ_PRESSURE_ZERO, bact, part_b2, part_nf));
   AQB_CUDA(launch_batch_b2_finalize(stream, bi, part_b2, part_nf, ss, live));
+  AQB_TRY(enq_row_list());
   return AQ_OK;
 }
 
@@ -248,7 +262,7 @@ aq_status aq_batch::enq_sweeps(int sweeps) {
   float* bufs[2] = {pa, pb};
   for (int k = 0; k < sweeps; ++k)
     AQB_CUDA(launch_batch_jacobi_rows(stream, bi, pre_r[ns], xs, pipe, grid(), live, bufs[k % 2], bufs[(k + 1) % 2],
-                                      rhs, type, bact));
+                                      rhs, type, bact, row_list, n_row_list));
   return AQ_OK;
 }
 
@@ -298,7 +312,7 @@ aq_status aq_batch::build_graph() {
     if (e != cudaSuccess) return fail(AQ_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
     return AQ_OK;
   };
-  const int pre_launches = (N > 0 ? 6 : 3) + 4;
+  const int pre_launches = (N > 0 ? 6 : 3) + 5;  // sort; p2g, s-layer, divergence, b2, row list
   const int post_launches = 4;
   aq_status st;
   if (solver.solve_mode == AQ_SOLVE_RESIDUAL) {
@@ -474,6 +488,7 @@ aq_status aq_batch_create(const aq_config* configs, int32_t n_scenes, aq_batch**
   b->N = (int)P;
   aq_status st = b->allocate();
   for (int s = 0; s < n_scenes && st == AQ_OK; ++s) st = b->add_scene(s, fl[s]);
+  if (st == AQ_OK) st = b->enq_row_list();  // the scenes' initial activity bricks
   if (st == AQ_OK && cudaStreamSynchronize(b->stream) != cudaSuccess)
     st = fail(AQ_ERR_CUDA, "batch initialisation failed");
   release();

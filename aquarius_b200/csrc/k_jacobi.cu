@@ -950,23 +950,34 @@ __device__ __forceinline__ bool range_active(const Dims& d, const uint8_t* __res
   return __any_sync(0xffffffffu, a) != 0;
 }
 
-template <int XS, bool PIPE>
+// LIST: walk a list of (scene, local item) pairs whose bricks hold fluid
+// (kb_row_list), built once per step, instead of every item.
+template <int XS, bool PIPE, bool LIST>
 __global__ void __launch_bounds__(256) kb_jacobi_rows(BatchIndex bi, int total, const int* __restrict__ live,
                                                      const float* __restrict__ pin_all, float* __restrict__ pout_all,
                                                      const float* __restrict__ rhs_all,
                                                      const int8_t* __restrict__ type_all,
-                                                     const uint8_t* __restrict__ bact_all) {
+                                                     const uint8_t* __restrict__ bact_all,
+                                                     const int2* __restrict__ list, const int* __restrict__ n_list) {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;");
   const int lane = threadIdx.x & 31;
   const int warps = gridDim.x * (blockDim.x >> 5);
-  for (int item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < total; item += warps) {
-    const int s = find_scene(bi.rows, bi.n_scenes, item);
+  const int n = LIST ? *n_list : total;
+  for (int item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < n; item += warps) {
+    int s, local;
+    if (LIST) {
+      const int2 e = __ldg(list + item);
+      s = e.x;
+      local = e.y;
+    } else {
+      s = find_scene(bi.rows, bi.n_scenes, item);
+      local = item - bi.rows[s];
+    }
     if (!live[s]) continue;
     const SceneDesc& S = bi.scenes[s];
     const Dims& d = S.d;
     const RowItem ri = row_item_shape(d);
-    int local = item - bi.rows[s];
     const int zb = local % ri.zblocks;
     local /= ri.zblocks;
     const int yg = local % ri.ygroups;
@@ -974,7 +985,7 @@ __global__ void __launch_bounds__(256) kb_jacobi_rows(BatchIndex bi, int total, 
     const int x0 = xg * XS, x1 = min(x0 + XS, d.sx);
     const int ylo = yg * ri.R, yhi = min(ylo + ri.R, d.sy);
     const int zlo0 = zb * 128, zhi0 = min(zlo0 + 128, d.sz);
-    if (!range_active(d, bact_all + S.br_off, x0, x1, ylo, yhi, zlo0, zhi0)) continue;
+    if (!LIST && !range_active(d, bact_all + S.br_off, x0, x1, ylo, yhi, zlo0, zhi0)) continue;
     const int r = lane / ri.zw, q = lane % ri.zw;
     const int y = ylo + r;
     const int z = (zb * 32 + q) * 4;
@@ -1044,6 +1055,43 @@ __global__ void __launch_bounds__(256) kb_jacobi_rows(BatchIndex bi, int total, 
         t = nt;
       }
     }
+  }
+}
+
+// The (scene, local item) pairs of the packed-row sweep whose bricks hold
+// fluid.  Warp-aggregated appends: the list order varies from run to run,
+// the sweep's results do not (items are independent).
+template <int XS>
+__global__ void __launch_bounds__(256) kb_row_list(BatchIndex bi, int total, const uint8_t* __restrict__ bact_all,
+                                                  int2* __restrict__ list, int* __restrict__ n_list) {
+  const int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+    const int item = base + threadIdx.x;
+    int act = 0, s = 0, local = 0;
+    if (item < total) {
+      s = find_scene(bi.rows, bi.n_scenes, item);
+      local = item - bi.rows[s];
+      const SceneDesc& S = bi.scenes[s];
+      const Dims& d = S.d;
+      const RowItem ri = row_item_shape(d);
+      int t = local;
+      const int zb = t % ri.zblocks;
+      t /= ri.zblocks;
+      const int yg = t % ri.ygroups, xg = t / ri.ygroups;
+      const int x0 = xg * XS, x1 = min(x0 + XS, d.sx);
+      const int y0 = yg * ri.R, y1 = min(y0 + ri.R, d.sy);
+      const int z0 = zb * 128, z1 = min(z0 + 128, d.sz);
+      const uint8_t* bact = bact_all + S.br_off;
+      for (int bx = x0 / kBrick; bx <= (x1 - 1) / kBrick && !act; ++bx)
+        for (int by = y0 / kBrick; by <= (y1 - 1) / kBrick && !act; ++by)
+          for (int bz = z0 / kBrick; bz <= (z1 - 1) / kBrick && !act; ++bz)
+            act = bact[(bx * d.by + by) * d.bz + bz] ? 1 : 0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, act);
+    int pos = 0;
+    if (lane == 0 && m) pos = atomicAdd(n_list, __popc(m));
+    pos = __shfl_sync(0xffffffffu, pos, 0) + __popc(m & ((1u << lane) - 1u));
+    if (act) list[pos] = make_int2(s, local);
   }
 }
 
@@ -1333,7 +1381,8 @@ long long batch_row_cells_updated(const Dims& d, int xs, const uint8_t* bact_hos
 
 cudaError_t launch_batch_jacobi_rows(cudaStream_t st, const BatchIndex& bi, int total, int xs, bool pipelined,
                                      int grid, const int* live, const float* pin, float* pout, const float* rhs,
-                                     const int8_t* type, const uint8_t* brick_active) {
+                                     const int8_t* type, const uint8_t* brick_active, const int2* list,
+                                     const int* n_list) {
   cudaLaunchConfig_t lc = {};
   lc.blockDim = dim3(256);
   lc.stream = st;
@@ -1346,23 +1395,41 @@ cudaError_t launch_batch_jacobi_rows(cudaStream_t st, const BatchIndex& bi, int 
     const int items_per_cta = 8;
     const int need = (total + items_per_cta - 1) / items_per_cta;
     lc.gridDim = dim3(std::max(1, std::min({grid, need, resident_ctas(kern, 256)})));
-    return cudaLaunchKernelEx(&lc, kern, bi, total, live, pin, pout, rhs, type, brick_active);
+    return cudaLaunchKernelEx(&lc, kern, bi, total, live, pin, pout, rhs, type, brick_active, list, n_list);
   };
+  const bool L = list != nullptr;
+#define AQ_ROWS(X, P) return L ? go(kb_jacobi_rows<X, P, true>) : go(kb_jacobi_rows<X, P, false>)
   if (pipelined) {
     switch (xs) {
-      case 2: return go(kb_jacobi_rows<2, true>);
-      case 4: return go(kb_jacobi_rows<4, true>);
-      case 8: return go(kb_jacobi_rows<8, true>);
+      case 2: AQ_ROWS(2, true);
+      case 4: AQ_ROWS(4, true);
+      case 8: AQ_ROWS(8, true);
       default: return cudaErrorInvalidValue;
     }
   }
   switch (xs) {
-    case 1: return go(kb_jacobi_rows<1, false>);
-    case 2: return go(kb_jacobi_rows<2, false>);
-    case 4: return go(kb_jacobi_rows<4, false>);
-    case 8: return go(kb_jacobi_rows<8, false>);
+    case 1: AQ_ROWS(1, false);
+    case 2: AQ_ROWS(2, false);
+    case 4: AQ_ROWS(4, false);
+    case 8: AQ_ROWS(8, false);
     default: return cudaErrorInvalidValue;
   }
+#undef AQ_ROWS
+}
+
+cudaError_t launch_batch_row_list(cudaStream_t st, const BatchIndex& bi, int total, int xs,
+                                  const uint8_t* brick_active, int2* list, int* n_list) {
+  cudaError_t e = cudaMemsetAsync(n_list, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const int g = std::max(1, std::min((total + 255) / 256, 148 * 8));
+  switch (xs) {
+    case 1: kb_row_list<1><<<g, 256, 0, st>>>(bi, total, brick_active, list, n_list); break;
+    case 2: kb_row_list<2><<<g, 256, 0, st>>>(bi, total, brick_active, list, n_list); break;
+    case 4: kb_row_list<4><<<g, 256, 0, st>>>(bi, total, brick_active, list, n_list); break;
+    case 8: kb_row_list<8><<<g, 256, 0, st>>>(bi, total, brick_active, list, n_list); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_batch_resid_flat(cudaStream_t st, const BatchIndex& bi, int total, int grid, const int* live,

@@ -152,8 +152,9 @@ def measured_traffic(f):
     try:
         d = json.loads((ROOT / "profiles" / "roofline_traffic.json").read_text())
         levels, rows, xplanes = f.jacobi_plan()
-        if rows == 0 and xplanes == 1 and "k_jacobi_flat" in d:
-            return d["k_jacobi_flat"]["bytes_per_launch"]
+        key = {(0, 1): "k_jacobi_flat", (3, 1): "k_jacobi_list"}.get((rows, xplanes))
+        if key in d:
+            return d[key]["bytes_per_launch"]
     except Exception:
         pass
     return None
@@ -609,6 +610,44 @@ def run_multiphase(args, rank: int, world: int, dist):
     f.close()
 
 
+def run_profile_case(case: str):
+    """Small, fixed cases for single-kernel ncu captures (no JSON line):
+    jacobi: the 128^3 workload's system after 3 steps, 6 sweeps of the
+    default plan; batch-rows: 32 scenes of the batch set, 6 batched sweeps;
+    conv: two U-Net inferences at 128^3 on seeded random inputs."""
+    import numpy as np
+    import torch
+
+    import aquarius_b200 as aq
+    if case == "jacobi":
+        f = aq.Fluid(workload_config(128, "zero"))
+        f.step(3)
+        f.synchronize()
+        print(f.jacobi_plan(), f.benchmark_pressure(6))
+        f.close()
+    elif case == "batch-rows":
+        from aquarius_b200.scenes import batch_configs
+        b = aq.Batch(batch_configs(32, seed=BATCH_SEED))
+        b.step(2)
+        b.synchronize()
+        b.set_sweep_plan(8, False)
+        print(b.benchmark_pressure(6))
+        b.close()
+    elif case == "conv":
+        net = aq.UNet(weights=ROOT / "aquarius_b200" / "weights" / "unet_128.bin")
+        V = 128 ** 3
+        rng = np.random.RandomState(0)
+        typ = torch.tensor((rng.rand(V) < 0.5).astype(np.int8), device="cuda")
+        rhs = torch.tensor(rng.randn(V).astype(np.float32), device="cuda")
+        out = torch.zeros(V, device="cuda")
+        torch.cuda.synchronize()
+        for _ in range(2):
+            net.predict((128, 128, 128), rhs.data_ptr(), typ.data_ptr(), out.data_ptr())
+        torch.cuda.synchronize()
+        print("conv ok")
+        net.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -620,6 +659,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default Jacobi plan")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
+    ap.add_argument("--profile-case", choices=["jacobi", "batch-rows", "conv"], default=None,
+                    help="run one small fixed case for an ncu capture and exit")
     ap.add_argument("--workload", default="ball128", choices=["ball128", "batch", "multiphase256"],
                     help="ball128: the 128^3 scene; batch: 256 independent scenes of uneven sizes; "
                          "multiphase256: two phases with diffusion at 256^3")
@@ -629,6 +670,9 @@ def main():
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.profile_case:
+        run_profile_case(args.profile_case)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -118,7 +118,7 @@ def test_batch_launch_counts_and_benchmark():
         b.step(2)
         per_step, per_block = b.launch_counts()
         assert per_block == 20 + 3
-        assert per_step == 6 + 4 + 4
+        assert per_step == 6 + 5 + 4
         r = b.benchmark_pressure(40)
         assert r["ms"] > 0
         assert 0 < r["cells_per_sweep"] <= b.totals()["cells"]
