@@ -160,6 +160,16 @@ def measured_traffic(f):
     return None
 
 
+def batch_traffic(cells: int):
+    """DRAM bytes per batched sweep: the per-updated-cell traffic of the
+    committed 32-scene capture (profiles/roofline_traffic.json) x cells."""
+    try:
+        d = json.loads((ROOT / "profiles" / "roofline_traffic.json").read_text())
+        return d["kb_jacobi_rows"]["bytes_per_updated_cell"] * cells
+    except Exception:
+        return None
+
+
 def measured_hbm_peak():
     try:
         d = json.loads(MEASURED_PEAKS.read_text())
@@ -526,7 +536,7 @@ def run_batch(args, rank: int, world: int, dist):
         "roofline": {"bound": "hbm", "kernel": f"kb_jacobi_rows<{tune['x_planes']}, {'pipelined' if tune['pipelined'] else 'plain'}> "
                                "(one sweep of every live scene per launch, packed rows)",
                      "achieved": achieved, "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None,
+                     "frac": achieved / hbm_peak, "traffic": batch_traffic(cells),
                      "algorithmic_bytes": f"{JACOBI_BYTES_PER_CELL} B per updated cell per sweep x {cells} cells",
                      "sweep_us": sweep_ms * 1000.0},
         "clocks": clk,
