@@ -122,6 +122,11 @@ def load_library() -> ct.CDLL:
         "aq_unet_evaluate_warm": (ct.c_int, [P, P, ct.c_int32, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_double)]),
         "aq_fluid_set_warm_start": (ct.c_int, [P, P]),
         "aq_fluid_phase_mass": (ct.c_int, [P, ct.POINTER(ct.c_double)]),
+        "aq_fluid_enable_ink": (ct.c_int, [P, ct.POINTER(ct.c_int32)]),
+        "aq_fluid_ink_count": (ct.c_int, [P, ct.POINTER(ct.c_int32)]),
+        "aq_fluid_download_ink": (ct.c_int, [P, P, P]),
+        "aq_fluid_upload_ink": (ct.c_int, [P, P, P]),
+        "aq_fluid_ink_advance": (ct.c_int, [P]),
         "aq_dataset_create": (ct.c_int, [ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.POINTER(P)]),
         "aq_dataset_destroy": (None, [P]),
         "aq_dataset_count": (ct.c_int32, [P]),
@@ -324,6 +329,38 @@ class Fluid:
         m = (ct.c_double * 4)()
         _check(self._lib.aq_fluid_phase_mass(self._h, m))
         return list(m)
+
+    def enable_ink(self) -> int:
+        """Seeds the ink particles (Fluid::initInkRenderer) once; every later
+        step then ends by advancing them.  Returns the ink count."""
+        n = ct.c_int32()
+        _check(self._lib.aq_fluid_enable_ink(self._h, ct.byref(n)))
+        return n.value
+
+    @property
+    def ink_count(self) -> int:
+        n = ct.c_int32()
+        _check(self._lib.aq_fluid_ink_count(self._h, ct.byref(n)))
+        return n.value
+
+    def get_ink(self) -> dict:
+        """Ink positions and velocities as [3, n] float32 arrays."""
+        n = self.ink_count
+        pos = np.zeros((3, n), np.float32)
+        vel = np.zeros((3, n), np.float32)
+        _check(self._lib.aq_fluid_download_ink(self._h, pos.ctypes.data, vel.ctypes.data))
+        return {"position": pos, "velocity": vel}
+
+    def set_ink(self, position=None, velocity=None):
+        n = self.ink_count
+        p = None if position is None else np.ascontiguousarray(position, np.float32).reshape(3, n)
+        v = None if velocity is None else np.ascontiguousarray(velocity, np.float32).reshape(3, n)
+        _check(self._lib.aq_fluid_upload_ink(self._h, None if p is None else p.ctypes.data,
+                                              None if v is None else v.ctypes.data))
+
+    def ink_advance(self):
+        """transferToInkParticles + moveInkParticles on the current grids."""
+        _check(self._lib.aq_fluid_ink_advance(self._h))
 
     def set_warm_start(self, net):
         """Attaches the network AQ_PRESSURE_LEARNED ('learned') uses (None detaches)."""

@@ -21,6 +21,10 @@ cudaError_t launch_particles_advance(cudaStream_t st, const Dims& d, const StepP
                                      Particles cur, Particles tmp, const float* u0, const float* v0,
                                      const float* w0, const float* un, const float* vn, const float* wn,
                                      const float4* nvf, int* key, int* slot, int* count, int n);
+// Ink particles: G2P with FLIP coefficient 1 and RK3 advection, in place.
+cudaError_t launch_ink_advance(cudaStream_t st, const Dims& d, float dt, Particles ink, const float* u0,
+                               const float* v0, const float* w0, const float* un, const float* vn, const float* wn,
+                               int n);
 // Per-block FP64 sums of the particle volume fractions: part[frac_sum_parts()][4].
 int frac_sum_parts();
 cudaError_t launch_frac_sum(cudaStream_t st, const float4* frac, int n, double* part);

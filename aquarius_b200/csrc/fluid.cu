@@ -112,21 +112,13 @@ struct Seeder {
   const aq_config& cfg;
   int sx, sy, sz;
   float h;
-  struct random_data rd;
-  char state[128];
+  aqb::HostRand& rng;
   std::vector<float> pos;  // xyz interleaved
   std::vector<int> phase;
 
-  Seeder(const aq_config& c, float h_) : cfg(c), sx(c.size_x), sy(c.size_y), sz(c.size_z), h(h_) {
-    memset(&rd, 0, sizeof(rd));
-    memset(state, 0, sizeof(state));
-    initstate_r(c.seed, state, sizeof(state), &rd);
-  }
-  float random0to1() {
-    int32_t v;
-    random_r(&rd, &v);
-    return (float)v / (float)RAND_MAX;
-  }
+  Seeder(const aq_config& c, float h_, aqb::HostRand& r)
+      : cfg(c), sx(c.size_x), sy(c.size_y), sz(c.size_z), h(h_), rng(r) {}
+  float random0to1() { return rng.random0to1(); }
   void at(float cx, float cy, float cz, bool sphere, float scx, float scy, float scz, float rad, float spacing,
           int ph) {
     const float jit = cfg.particle_jitter;
@@ -188,6 +180,47 @@ struct Seeder {
           center(x, y, z, cx, cy, cz);
           at(cx, cy, cz, true, scx, scy, scz, v.ball_radius, h / 2, v.phase);
         }
+  }
+  // Fluid::createSquareInk (Fluid/Fluid_3D_FLIP.cu:600-640): a lattice of
+  // the given spacing from box_min*size + spacing/2 up to box_max*size -
+  // (spacing/2 - 1e-3), loops x, y, z, each point jittered by
+  // (random0to1() - 0.5) * spacing/2 and clamped spacing/2 off the walls.
+  void square_ink(const aq_volume& v, float spacing) {
+    const float md = spacing / 2.f;
+    const float gx = (float)sx * h, gy = (float)sy * h, gz = (float)sz * h;
+    const float shrink = (float)((double)md - 1e-3);
+    const float x0 = v.box_min[0] * gx + md, y0 = v.box_min[1] * gy + md, z0 = v.box_min[2] * gz + md;
+    const float x1 = v.box_max[0] * gx - shrink, y1 = v.box_max[1] * gy - shrink, z1 = v.box_max[2] * gz - shrink;
+    const float mag = spacing / 2.f;
+    for (float x = x0; x <= x1; x += spacing)
+      for (float y = y0; y <= y1; y += spacing)
+        for (float z = z0; z <= z1; z += spacing) {
+          // (random0to1() - 0.5) is evaluated in double and stored as float
+          float jx = (float)((double)random0to1() - 0.5);
+          float jy = (float)((double)random0to1() - 0.5);
+          float jz = (float)((double)random0to1() - 0.5);
+          jx *= mag; jy *= mag; jz *= mag;
+          const float px = fminf(gx - md, fmaxf(md, x + jx));
+          const float py = fminf(gy - md, fmaxf(md, y + jy));
+          const float pz = fminf(gz - md, fmaxf(md, z + jz));
+          pos.push_back(px);
+          pos.push_back(py);
+          pos.push_back(pz);
+          phase.push_back(v.phase);
+        }
+  }
+  // Fluid::createSphereInk (Fluid/Fluid_3D_FLIP.cu:642-664): the particle
+  // seeding (8 jittered sub-points at spacing h/2, sphere filter) at every
+  // point of a lattice of the given spacing from 0, loops z, y, x.
+  void sphere_ink(const aq_volume& v, float spacing) {
+    if (!valid01(v.ball_center)) return;
+    const float scx = (v.ball_center[0] * (float)sx * h);
+    const float scy = (v.ball_center[1] * (float)sy * h);
+    const float scz = (v.ball_center[2] * (float)sz * h);
+    const float gx = (float)sx * h, gy = (float)sy * h, gz = (float)sz * h;
+    for (float z = 0; z < gz; z += spacing)
+      for (float y = 0; y < gy; y += spacing)
+        for (float x = 0; x < gx; x += spacing) at(x, y, z, true, scx, scy, scz, v.ball_radius, h / 2, v.phase);
   }
 };
 
@@ -488,6 +521,7 @@ aq_status aq_fluid::run_stage(int stage) {
     case AQ_STAGE_EXTRAPOLATE: return enq_extrapolate();
     case AQ_STAGE_DIFFUSE:
       AQ_TRY(enq_diffuse());
+      AQ_TRY(enq_ink());
       time += (double)cfg.timestep;
       return AQ_OK;
     default: return fail(AQ_ERR_INVALID_ARGUMENT, "unknown stage");
@@ -507,6 +541,48 @@ aq_status aq_fluid::enq_post_solve() {
   AQ_TRY(enq_project());
   AQ_TRY(enq_extrapolate());
   AQ_TRY(enq_diffuse());
+  return enq_ink();
+}
+
+// The step's last calls in the reference, left commented out there
+// (transferToInkParticles + moveInkParticles, Fluid/Fluid_3D_FLIP.cu:349-350):
+// the ink moves with the step's velocity (P2G) and newVelocity (after
+// extrapolation and diffusion).
+aq_status aq_fluid::enq_ink() {
+  if (!ink_on || n_ink <= 0) return AQ_OK;
+  AQ_CUDA(launch_ink_advance(stream, d, cfg.timestep, ink, u0, v0, w0, nvx(nv_cur), nvy(nv_cur), nvz(nv_cur), n_ink));
+  return AQ_OK;
+}
+
+// Fluid::initInkRenderer (Fluid/Fluid_3D_FLIP.cu:676-709), which Fluid::init
+// would run right after the particle seeding (Fluid/Fluid_3D_FLIP.cu:498):
+// spacing h/4 over the initial volumes, continuing the seeding's rand()
+// sequence; velocities start at zero.
+aq_status aq_fluid::enable_ink() {
+  if (ink_on) return AQ_OK;
+  if (!rng) return fail(AQ_ERR_INVALID_ARGUMENT, "this fluid has no seeding state");
+  Seeder s(cfg, d.h, *rng);
+  const float spacing = d.h / 4;
+  for (int i = 0; i < cfg.volume_count; ++i) {
+    const aq_volume& v = cfg.volumes[i];
+    if (v.shape == AQ_SHAPE_SQUARE) s.square_ink(v, spacing);
+    else if (v.shape == AQ_SHAPE_SPHERE) s.sphere_ink(v, spacing);
+  }
+  const size_t N = s.phase.size();
+  if (N > (size_t)INT32_MAX) return fail(AQ_ERR_INVALID_CONFIG, "too many ink particles");
+  AQ_TRY(alloc(&ink.px, N)); AQ_TRY(alloc(&ink.py, N)); AQ_TRY(alloc(&ink.pz, N));
+  AQ_TRY(alloc(&ink.vx, N)); AQ_TRY(alloc(&ink.vy, N)); AQ_TRY(alloc(&ink.vz, N));
+  ink.frac = nullptr;
+  std::vector<float> comp(N);
+  float* dst[3] = {ink.px, ink.py, ink.pz};
+  for (int k = 0; k < 3; ++k) {
+    for (size_t i = 0; i < N; ++i) comp[i] = s.pos[3 * i + k];
+    AQ_CUDA(cudaMemcpyAsync(dst[k], comp.data(), sizeof(float) * N, cudaMemcpyHostToDevice, stream));
+    AQ_CUDA(cudaStreamSynchronize(stream));
+  }
+  n_ink = (int)N;
+  ink_on = true;
+  invalidate_graph();
   return AQ_OK;
 }
 
@@ -593,7 +669,7 @@ aq_status aq_fluid::build_graph() {
   if (st != AQ_OK) { cudaGraphDestroy(g); return st; }
   if (cfg.pressure_init == AQ_PRESSURE_LEARNED)  // network, two 20-sweep starts, pick, copy
     launches += kUNetForwardLaunches + 2 * (count_jacobi_launches(kWarmSweeps) - 1) + 2;
-  launches += 1 + 3 + (multiphase ? cfg.diffusion_iterations : 0);
+  launches += 1 + 3 + (multiphase ? cfg.diffusion_iterations : 0) + (ink_on && n_ink > 0 ? 1 : 0);
   graph_launches = launches;
   cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
   cudaGraphDestroy(g);
@@ -624,7 +700,8 @@ aq_status aq_fluid::step(int nsteps) {
 
 // ------------------------------------------------------------------ init
 aq_status aq_fluid::seed_and_init() {
-  Seeder s(cfg, d.h);
+  rng.reset(new aqb::HostRand((unsigned)cfg.seed));
+  Seeder s(cfg, d.h, *rng);
   for (int i = 0; i < cfg.volume_count; ++i) {
     const aq_volume& v = cfg.volumes[i];
     if (v.shape == AQ_SHAPE_SQUARE) s.square(v);
@@ -1258,6 +1335,60 @@ aq_status aq_fluid_phase_mass(aq_fluid* f, double mass[4]) {
   return AQ_OK;
 }
 
+aq_status aq_fluid_enable_ink(aq_fluid* f, int32_t* count) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  cudaSetDevice(f->device);
+  AQ_CUDA(cudaStreamSynchronize(f->stream));
+  AQ_TRY(f->enable_ink());
+  if (count) *count = f->n_ink;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_ink_count(const aq_fluid* f, int32_t* count) {
+  if (!f || !count) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  *count = f->ink_on ? f->n_ink : 0;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_download_ink(aq_fluid* f, float* position, float* velocity) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  if (!f->ink_on) return fail(AQ_ERR_INVALID_ARGUMENT, "ink is not enabled");
+  cudaSetDevice(f->device);
+  AQ_CUDA(cudaStreamSynchronize(f->stream));
+  const size_t N = (size_t)f->n_ink;
+  const float* src[6] = {f->ink.px, f->ink.py, f->ink.pz, f->ink.vx, f->ink.vy, f->ink.vz};
+  for (int k = 0; k < 6 && N; ++k) {
+    float* dst = k < 3 ? position : velocity;
+    if (!dst) continue;
+    AQ_CUDA(cudaMemcpy(dst + (size_t)(k % 3) * N, src[k], sizeof(float) * N, cudaMemcpyDeviceToHost));
+  }
+  return AQ_OK;
+}
+
+aq_status aq_fluid_upload_ink(aq_fluid* f, const float* position, const float* velocity) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  if (!f->ink_on) return fail(AQ_ERR_INVALID_ARGUMENT, "ink is not enabled");
+  cudaSetDevice(f->device);
+  AQ_CUDA(cudaStreamSynchronize(f->stream));
+  const size_t N = (size_t)f->n_ink;
+  float* dst[6] = {f->ink.px, f->ink.py, f->ink.pz, f->ink.vx, f->ink.vy, f->ink.vz};
+  for (int k = 0; k < 6 && N; ++k) {
+    const float* src = k < 3 ? position : velocity;
+    if (!src) continue;
+    AQ_CUDA(cudaMemcpy(dst[k], src + (size_t)(k % 3) * N, sizeof(float) * N, cudaMemcpyHostToDevice));
+  }
+  return AQ_OK;
+}
+
+aq_status aq_fluid_ink_advance(aq_fluid* f) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  if (!f->ink_on) return fail(AQ_ERR_INVALID_ARGUMENT, "ink is not enabled");
+  cudaSetDevice(f->device);
+  AQ_TRY(f->enq_ink());
+  AQ_CUDA(cudaStreamSynchronize(f->stream));
+  return AQ_OK;
+}
+
 aq_status aq_fluid_set_warm_start(aq_fluid* f, aq_unet* net) {
   if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
   cudaSetDevice(f->device);
@@ -1633,6 +1764,7 @@ aq_status aq_fluid_profile_step(aq_fluid* f, float stage_ms[8]) {
   AQ_TRY(f->enq_extrapolate());
   AQ_CUDA(cudaEventRecord(ev[7], f->stream));
   AQ_TRY(f->enq_diffuse());
+  AQ_TRY(f->enq_ink());
   AQ_CUDA(cudaEventRecord(ev[8], f->stream));
   AQ_CUDA(cudaEventSynchronize(ev[8]));
   f->time += (double)f->cfg.timestep;

@@ -2,6 +2,10 @@
 // single-scene host code (fluid.cu) and the batch host code (batch.cu).
 #pragma once
 
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -11,6 +15,26 @@
 namespace aqb {
 inline aq_status fail(aq_status st, const std::string& msg) { return set_last_error(st, msg); }
 struct UActs;
+
+// The reference's random0to1() (Common/Commons.h:3-5) over glibc rand(),
+// replayed without touching the process's own rand() state: random_r over a
+// 128-byte TYPE_3 state gives the sequence of srand(seed); rand().
+struct HostRand {
+  struct random_data rd;
+  char state[128];
+  explicit HostRand(unsigned seed) {
+    memset(&rd, 0, sizeof(rd));
+    memset(state, 0, sizeof(state));
+    initstate_r(seed, state, sizeof(state), &rd);
+  }
+  HostRand(const HostRand&) = delete;
+  HostRand& operator=(const HostRand&) = delete;
+  float random0to1() {
+    int32_t v;
+    random_r(&rd, &v);
+    return (float)v / (float)RAND_MAX;
+  }
+};
 }  // namespace aqb
 
 struct aq_fluid {
@@ -73,6 +97,12 @@ struct aq_fluid {
   int* pick = nullptr;  // 1: the zero-init path won
   // list plan: active warp rows of the current system
   int *row_items = nullptr, *n_row_items = nullptr;
+  // rand() state after seeding: ink seeding continues the sequence
+  std::unique_ptr<aqb::HostRand> rng;
+  // ink particles (positions / velocities only; frac stays null)
+  Particles ink{};
+  int n_ink = 0;
+  bool ink_on = false;
   cudaGraphExec_t exec = nullptr;
   bool use_graph = true;
   int graph_launches = 0;  // launches outside the residual loop
@@ -128,6 +158,8 @@ struct aq_fluid {
   aq_status enq_project();
   aq_status enq_extrapolate();
   aq_status enq_diffuse();
+  aq_status enq_ink();     // advance the ink (no-op without ink)
+  aq_status enable_ink();  // seed and allocate the ink once
   aq_status run_stage(int stage);
   aq_status enq_pre_solve();
   aq_status enq_post_solve();

@@ -49,6 +49,40 @@ __device__ __forceinline__ float3 sample_velocity(const float* __restrict__ u, c
                      sample_node(w, d, x - 0.5f, y - 0.5f, z));
 }
 
+// transferToParticlesImpl's velocity update with FLIP coefficient c
+// (Fluid/Fluid_3D_FLIP.cu:189-227), then moveParticlesImpl
+// (Fluid/Fluid_3D_FLIP.cu:229-285): Ralston RK3 (2/9, 3/9, 4/9) in
+// newVelocity, clamped to [h/4, s*h - h/4] with the velocity component
+// reflected.  Shared by the fluid particles and the ink particles.
+__device__ __forceinline__ void g2p_move(const Dims& d, float c, float dt, const float* __restrict__ u0,
+                                         const float* __restrict__ v0, const float* __restrict__ w0,
+                                         const float* __restrict__ un, const float* __restrict__ vn,
+                                         const float* __restrict__ wn, float& px, float& py, float& pz, float& vx,
+                                         float& vy, float& vz) {
+  const float3 nv = sample_velocity(un, vn, wn, d, px, py, pz);
+  const float3 ov = sample_velocity(u0, v0, w0, d, px, py, pz);
+  const float oc = 1.0f - c;
+  vx = c * (vx + (nv.x - ov.x)) + oc * nv.x;
+  vy = c * (vy + (nv.y - ov.y)) + oc * nv.y;
+  vz = c * (vz + (nv.z - ov.z)) + oc * nv.z;
+  const float3 u1 = sample_velocity(un, vn, wn, d, px, py, pz);
+  const float3 u2 = sample_velocity(un, vn, wn, d, px + dt * u1.x / 2, py + dt * u1.y / 2, pz + dt * u1.z / 2);
+  const float3 u3 = sample_velocity(un, vn, wn, d, px + dt * u2.x * 3 / 4, py + dt * u2.y * 3 / 4,
+                                    pz + dt * u2.z * 3 / 4);
+  float qx = px + dt * (u1.x * 2 / 9 + u2.x * 3 / 9 + u3.x * 4 / 9);
+  float qy = py + dt * (u1.y * 2 / 9 + u2.y * 3 / 9 + u3.y * 4 / 9);
+  float qz = pz + dt * (u1.z * 2 / 9 + u2.z * 3 / 9 + u3.z * 4 / 9);
+  const float md = d.h / 4;
+  const float gx = (float)d.sx * d.h, gy = (float)d.sy * d.h, gz = (float)d.sz * d.h;
+  if (qx < md) { qx = md; vx *= -1.f; }
+  if (qx > gx - md) { qx = gx - md; vx *= -1.f; }
+  if (qy < md) { qy = md; vy *= -1.f; }
+  if (qy > gy - md) { qy = gy - md; vy *= -1.f; }
+  if (qz < md) { qz = md; vz *= -1.f; }
+  if (qz > gz - md) { qz = gz - md; vz *= -1.f; }
+  px = qx; py = qy; pz = qz;
+}
+
 // Body shared by the single-scene kernel and the batched one.  Particle
 // arrays, grids and key/slot are the scene's own (pointers already offset);
 // keys are cell indices plus key_base (the scene's first cell in a batch).
@@ -66,14 +100,8 @@ __device__ __forceinline__ void particles_advance_body(
     float vx = cur.vx[i], vy = cur.vy[i], vz = cur.vz[i];
     float4 fr = make_float4(0.f, 0.f, 0.f, 0.f);
     if (MOVE) {
-      // transferToParticlesImpl: FLIP/PIC blend
-      const float3 nv = sample_velocity(un, vn, wn, d, px, py, pz);
-      const float3 ov = sample_velocity(u0, v0, w0, d, px, py, pz);
-      const float c = sp.flip, oc = 1.0f - sp.flip;
-      vx = c * (vx + (nv.x - ov.x)) + oc * nv.x;
-      vy = c * (vy + (nv.y - ov.y)) + oc * nv.y;
-      vz = c * (vz + (nv.z - ov.z)) + oc * nv.z;
       if (MULTI) {
+        // transferToParticlesImpl: fractions from the cell of the unmoved particle
         int cx = (int)floorf(__fdiv_rn(px, d.h)), cy = (int)floorf(__fdiv_rn(py, d.h)),
             cz = (int)floorf(__fdiv_rn(pz, d.h));
         cx = min(max(cx, 0), d.sx - 1);
@@ -86,25 +114,7 @@ __device__ __forceinline__ void particles_advance_body(
           fr.z = __fdiv_rn(fr.z, s); fr.w = __fdiv_rn(fr.w, s);
         }
       }
-      // moveParticlesImpl: RK3 (2/9, 3/9, 4/9) in newVelocity
-      const float dt = sp.dt;
-      const float3 u1 = sample_velocity(un, vn, wn, d, px, py, pz);
-      const float3 u2 = sample_velocity(un, vn, wn, d, px + dt * u1.x / 2, py + dt * u1.y / 2,
-                                        pz + dt * u1.z / 2);
-      const float3 u3 = sample_velocity(un, vn, wn, d, px + dt * u2.x * 3 / 4, py + dt * u2.y * 3 / 4,
-                                        pz + dt * u2.z * 3 / 4);
-      float qx = px + dt * (u1.x * 2 / 9 + u2.x * 3 / 9 + u3.x * 4 / 9);
-      float qy = py + dt * (u1.y * 2 / 9 + u2.y * 3 / 9 + u3.y * 4 / 9);
-      float qz = pz + dt * (u1.z * 2 / 9 + u2.z * 3 / 9 + u3.z * 4 / 9);
-      const float md = d.h / 4;
-      const float gx = (float)d.sx * d.h, gy = (float)d.sy * d.h, gz = (float)d.sz * d.h;
-      if (qx < md) { qx = md; vx *= -1.f; }
-      if (qx > gx - md) { qx = gx - md; vx *= -1.f; }
-      if (qy < md) { qy = md; vy *= -1.f; }
-      if (qy > gy - md) { qy = gy - md; vy *= -1.f; }
-      if (qz < md) { qz = md; vz *= -1.f; }
-      if (qz > gz - md) { qz = gz - md; vz *= -1.f; }
-      px = qx; py = qy; pz = qz;
+      g2p_move(d, sp.flip, sp.dt, u0, v0, w0, un, vn, wn, px, py, pz, vx, vy, vz);
     } else if (MULTI) {
       fr = cur.frac[i];
     }
@@ -139,6 +149,22 @@ __global__ void __launch_bounds__(256) k_particles_advance(
     int* __restrict__ key, int* __restrict__ slot, int* __restrict__ count, int n) {
   particles_advance_body<MOVE, MULTI>(d, sp, cur, tmp, u0, v0, w0, un, vn, wn, nvf, key, slot, count, n, 0,
                                       blockIdx.x);
+}
+
+// Ink particles (Fluid/Fluid_3D_FLIP.cu:711-725): transferToParticlesImpl
+// with FLIP coefficient 1 and moveParticlesImpl, in place; ink is never
+// sorted or transferred to the grid.
+__global__ void __launch_bounds__(256) k_ink_advance(Dims d, float dt, Particles ink, const float* __restrict__ u0,
+                                                    const float* __restrict__ v0, const float* __restrict__ w0,
+                                                    const float* __restrict__ un, const float* __restrict__ vn,
+                                                    const float* __restrict__ wn, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float px = ink.px[i], py = ink.py[i], pz = ink.pz[i];
+  float vx = ink.vx[i], vy = ink.vy[i], vz = ink.vz[i];
+  g2p_move(d, 1.f, dt, u0, v0, w0, un, vn, wn, px, py, pz, vx, vy, vz);
+  ink.px[i] = px; ink.py[i] = py; ink.pz[i] = pz;
+  ink.vx[i] = vx; ink.vy[i] = vy; ink.vz[i] = vz;
 }
 
 __device__ __forceinline__ Particles offset_particles(const Particles& p, int off) {
@@ -339,6 +365,14 @@ cudaError_t launch_particles_advance(cudaStream_t st, const Dims& d, const StepP
     k_particles_advance<false, true><<<nb, 256, 0, st>>>(d, sp, cur, tmp, u0, v0, w0, un, vn, wn, nvf, key, slot, count, n);
   else
     k_particles_advance<false, false><<<nb, 256, 0, st>>>(d, sp, cur, tmp, u0, v0, w0, un, vn, wn, nvf, key, slot, count, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ink_advance(cudaStream_t st, const Dims& d, float dt, Particles ink, const float* u0,
+                               const float* v0, const float* w0, const float* un, const float* vn, const float* wn,
+                               int n) {
+  if (n <= 0) return cudaSuccess;
+  k_ink_advance<<<blocks_for(n, 256), 256, 0, st>>>(d, dt, ink, u0, v0, w0, un, vn, wn, n);
   return cudaGetLastError();
 }
 

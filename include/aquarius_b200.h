@@ -444,6 +444,27 @@ aq_status aq_unet_gradients(aq_unet* net, float* out, int64_t n);
  * concentration-mass conservation error of multiphase diffusion. */
 aq_status aq_fluid_phase_mass(aq_fluid* f, double mass[4]);
 
+/* Ink particles: massless tracers the reference builds but leaves switched
+ * off (its calls are commented out at Fluid/Fluid_3D_FLIP.cu:349-350 and
+ * :498).  aq_fluid_enable_ink replaces Fluid::initInkRenderer
+ * (Fluid/Fluid_3D_FLIP.cu:676-709): it seeds the ink once, at spacing h/4
+ * over the initial volumes (createSquareInk / createSphereInk,
+ * Fluid/Fluid_3D_FLIP.cu:600-664), continuing the particle seeding's rand()
+ * sequence, so the ink is the one Fluid::init would have made whenever it is
+ * called; count (may be NULL) receives the ink particle count.  From then on
+ * every step ends by advancing the ink as transferToInkParticles +
+ * moveInkParticles(timestep) would (Fluid/Fluid_3D_FLIP.cu:711-725): G2P with
+ * FLIP coefficient 1 and RK3 advection in the step's grid velocities.
+ * aq_fluid_ink_advance runs that advance alone on the current grids.
+ * Positions and velocities are [3][count] planes; either pointer may be NULL.
+ * The download / upload / advance calls fail with AQ_ERR_INVALID_ARGUMENT
+ * before aq_fluid_enable_ink. */
+aq_status aq_fluid_enable_ink(aq_fluid* f, int32_t* count);
+aq_status aq_fluid_ink_count(const aq_fluid* f, int32_t* count);
+aq_status aq_fluid_download_ink(aq_fluid* f, float* position, float* velocity);
+aq_status aq_fluid_upload_ink(aq_fluid* f, const float* position, const float* velocity);
+aq_status aq_fluid_ink_advance(aq_fluid* f);
+
 /* Attaches the network used by AQ_PRESSURE_LEARNED (NULL detaches).  The
  * network must outlive the fluid's steps; allocate-once buffers for the
  * fluid's grid are made here, so call it before the first step. */

@@ -10,6 +10,10 @@
 //   ::simulationStep(), ::physicalTime,              same names
 //   ::getCenter(), ::getContainerSize()
 //     (Fluid/Fluid.h:4-12, Fluid/Fluid_3D.cuh:7-12)
+//   ::initInkRenderer(), ::inkParticleCount          same names; the ink then
+//     (Fluid/Fluid_3D_FLIP.cu:676-709)                moves at the end of every
+//                                                    step (the reference's
+//                                                    commented-out :349-350)
 //
 // Differences: errors throw aquarius_b200::Error (the reference prints and
 // exits); draw() is a no-op (rendering is not part of this library); the
@@ -168,10 +172,26 @@ class Fluid {
     return n;
   }
   void synchronize() { check(aq_fluid_synchronize(f_), "aq_fluid_synchronize"); }
+  // Fluid::initInkRenderer (Fluid/Fluid_3D_FLIP.cu:676-709), headless: seeds
+  // the ink once; from then on every simulationStep ends with
+  // transferToInkParticles + moveInkParticles(timestep).
+  void initInkRenderer() {
+    int32_t n = 0;
+    check(aq_fluid_enable_ink(f_, &n), "aq_fluid_enable_ink");
+    inkParticleCount = n;
+  }
+  // transferToInkParticles + moveInkParticles(timestep)
+  // (Fluid/Fluid_3D_FLIP.cu:711-725) on the current grids, as one launch.
+  void advanceInk() { check(aq_fluid_ink_advance(f_), "aq_fluid_ink_advance"); }
+  // Ink positions / velocities as [3][inkParticleCount] planes (either may be NULL).
+  void downloadInk(float* position, float* velocity) {
+    check(aq_fluid_download_ink(f_, position, velocity), "aq_fluid_download_ink");
+  }
   aq_fluid* handle() const { return f_; }
   const FluidConfig& config() const { return config_; }
 
   float physicalTime = 0;  // Fluid/Fluid.h:10
+  int inkParticleCount = 0;  // Fluid/Fluid_3D_FLIP.cuh:106
 
  private:
   void release() {

@@ -21,6 +21,14 @@
 #define FLUID 1 /* CONTENT_FLUID Fluid/MAC_Grid_3D.cuh:16 */
 #define SOLID 2 /* CONTENT_SOLID Fluid/MAC_Grid_3D.cuh:17 */
 
+/* glibc rand() state; random_r with a 128-byte TYPE_3 state reproduces
+ * srand(seed); rand() exactly.  The reference uses rand() unseeded
+ * (Common/Commons.h:3-5), i.e. seed 1. */
+typedef struct {
+  struct random_data rd;
+  char state[128];
+} orc_rng;
+
 struct orc_fluid {
   aq_config cfg;
   int sx, sy, sz;
@@ -42,6 +50,10 @@ struct orc_fluid {
   int iters;
   double rel_res, b_norm;
   int fluid_cells;
+  /* rand() state after seeding (ink continues the sequence), ink particles */
+  orc_rng rng;
+  int n_ink;
+  float *ink_pos, *ink_vel; /* [3][n_ink] */
 };
 
 /* ---------------------------------------------------------------- helpers */
@@ -104,13 +116,6 @@ void orc_config_default(aq_config* c) {
 
 /* ----------------------------------------------------- particle seeding */
 
-/* glibc rand() state; random_r with a 128-byte TYPE_3 state reproduces
- * srand(seed); rand() exactly.  The reference uses rand() unseeded
- * (Common/Commons.h:3-5), i.e. seed 1. */
-typedef struct {
-  struct random_data rd;
-  char state[128];
-} orc_rng;
 
 static float random0to1(orc_rng* r) { /* Common/Commons.h:3-5 */
   int32_t v;
@@ -293,6 +298,42 @@ static inline float hat(float rx, float ry, float rz, float s) {
 
 /* ------------------------------------------------------------- stages */
 
+/* transferToParticlesImpl's velocity update (Fluid_3D_FLIP.cu:189-227) with
+ * FLIP coefficient c, then moveParticlesImpl (Fluid_3D_FLIP.cu:229-285):
+ * Ralston RK3 in newVelocity, clamped to [h/4, s*h - h/4] with the velocity
+ * component reflected. */
+static void g2p_move(const orc_fluid* o, float c, float dt, float* ppx, float* ppy, float* ppz, float* pvx,
+                     float* pvy, float* pvz) {
+  const float h = o->h;
+  float nx, ny, nz, ox, oy, oz;
+  point_velocity(o, o->new_velocity, *ppx, *ppy, *ppz, &nx, &ny, &nz);
+  point_velocity(o, o->velocity, *ppx, *ppy, *ppz, &ox, &oy, &oz);
+  float dvx = nx - ox, dvy = ny - oy, dvz = nz - oz;
+  float fx = *pvx + dvx, fy = *pvy + dvy, fz = *pvz + dvz;
+  float vx = c * fx + (1.0f - c) * nx;
+  float vy = c * fy + (1.0f - c) * ny;
+  float vz = c * fz + (1.0f - c) * nz;
+  float bx = *ppx, by = *ppy, bz = *ppz;
+  float u1x, u1y, u1z, u2x, u2y, u2z, u3x, u3y, u3z;
+  point_velocity(o, o->new_velocity, bx, by, bz, &u1x, &u1y, &u1z);
+  point_velocity(o, o->new_velocity, bx + dt * u1x / 2, by + dt * u1y / 2, bz + dt * u1z / 2, &u2x, &u2y, &u2z);
+  point_velocity(o, o->new_velocity, bx + dt * u2x * 3 / 4, by + dt * u2y * 3 / 4, bz + dt * u2z * 3 / 4, &u3x,
+                 &u3y, &u3z);
+  float dx = bx + dt * (u1x * 2 / 9 + u2x * 3 / 9 + u3x * 4 / 9);
+  float dy = by + dt * (u1y * 2 / 9 + u2y * 3 / 9 + u3y * 4 / 9);
+  float dz = bz + dt * (u1z * 2 / 9 + u2z * 3 / 9 + u3z * 4 / 9);
+  float md = h / 4;
+  float gx = (float)o->sx * h, gy = (float)o->sy * h, gz = (float)o->sz * h;
+  if (dx < md) { dx = md; vx *= -1; }
+  if (dx > gx - md) { dx = gx - md; vx *= -1; }
+  if (dy < md) { dy = md; vy *= -1; }
+  if (dy > gy - md) { dy = gy - md; vy *= -1; }
+  if (dz < md) { dz = md; vz *= -1; }
+  if (dz > gz - md) { dz = gz - md; vz *= -1; }
+  *ppx = dx; *ppy = dy; *ppz = dz;
+  *pvx = vx; *pvy = vy; *pvz = vz;
+}
+
 /* transferToParticlesImpl (Fluid_3D_FLIP.cu:189-227) then moveParticlesImpl
  * (Fluid_3D_FLIP.cu:229-285), particle by particle. */
 static void stage_g2p_advect(orc_fluid* o) {
@@ -302,15 +343,7 @@ static void stage_g2p_advect(orc_fluid* o) {
   float *vx = o->vel, *vy = o->vel + n, *vz = o->vel + 2 * n;
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < n; ++i) {
-    /* transferToParticlesImpl */
-    float nx, ny, nz, ox, oy, oz;
-    point_velocity(o, o->new_velocity, px[i], py[i], pz[i], &nx, &ny, &nz);
-    point_velocity(o, o->velocity, px[i], py[i], pz[i], &ox, &oy, &oz);
-    float dvx = nx - ox, dvy = ny - oy, dvz = nz - oz;
-    float fx = vx[i] + dvx, fy = vy[i] + dvy, fz = vz[i] + dvz;
-    vx[i] = c * fx + (1.0f - c) * nx;
-    vy[i] = c * fy + (1.0f - c) * ny;
-    vz[i] = c * fz + (1.0f - c) * nz;
+    /* transferToParticlesImpl: fractions from the cell of the unmoved particle */
     int cx = (int)floorf(px[i] / h), cy = (int)floorf(py[i] / h), cz = (int)floorf(pz[i] / h);
     cx = iclamp(cx, 0, o->sx - 1); cy = iclamp(cy, 0, o->sy - 1); cz = iclamp(cz, 0, o->sz - 1);
     int cell = cidx(o, cx, cy, cz);
@@ -318,28 +351,101 @@ static void stage_g2p_advect(orc_fluid* o) {
     float sum = f0 * 1 + f1 * 1 + f2 * 1 + f3 * 1;
     if (sum > 0) { f0 /= sum; f1 /= sum; f2 /= sum; f3 /= sum; }
     o->frac[i] = f0; o->frac[n + i] = f1; o->frac[2 * n + i] = f2; o->frac[3 * n + i] = f3;
-
-    /* moveParticlesImpl: Ralston RK3 in newVelocity */
-    float bx = px[i], by = py[i], bz = pz[i];
-    float u1x, u1y, u1z, u2x, u2y, u2z, u3x, u3y, u3z;
-    point_velocity(o, o->new_velocity, bx, by, bz, &u1x, &u1y, &u1z);
-    point_velocity(o, o->new_velocity, bx + dt * u1x / 2, by + dt * u1y / 2, bz + dt * u1z / 2,
-                   &u2x, &u2y, &u2z);
-    point_velocity(o, o->new_velocity, bx + dt * u2x * 3 / 4, by + dt * u2y * 3 / 4,
-                   bz + dt * u2z * 3 / 4, &u3x, &u3y, &u3z);
-    float dx = bx + dt * (u1x * 2 / 9 + u2x * 3 / 9 + u3x * 4 / 9);
-    float dy = by + dt * (u1y * 2 / 9 + u2y * 3 / 9 + u3y * 4 / 9);
-    float dz = bz + dt * (u1z * 2 / 9 + u2z * 3 / 9 + u3z * 4 / 9);
-    float md = h / 4;
-    float gx = (float)o->sx * h, gy = (float)o->sy * h, gz = (float)o->sz * h;
-    if (dx < md) { dx = md; vx[i] *= -1; }
-    if (dx > gx - md) { dx = gx - md; vx[i] *= -1; }
-    if (dy < md) { dy = md; vy[i] *= -1; }
-    if (dy > gy - md) { dy = gy - md; vy[i] *= -1; }
-    if (dz < md) { dz = md; vz[i] *= -1; }
-    if (dz > gz - md) { dz = gz - md; vz[i] *= -1; }
-    px[i] = dx; py[i] = dy; pz[i] = dz;
+    g2p_move(o, c, dt, &px[i], &py[i], &pz[i], &vx[i], &vy[i], &vz[i]);
   }
+}
+
+static void* xcalloc(size_t n, size_t s) {
+  void* p = calloc(n ? n : 1, s);
+  return p;
+}
+
+/* ------------------------------------------------------------------- ink
+ * Ink particles (Fluid_3D_FLIP.cu:600-725, disabled in the reference's
+ * step): massless tracers seeded at spacing h/4 over the initial volumes,
+ * continuing the fluid seeding's rand() sequence, and advected at the end of
+ * a step by transferToParticlesImpl with FLIP coefficient 1 and
+ * moveParticlesImpl on the step's grid velocities. */
+
+/* Fluid::createSquareInk (Fluid_3D_FLIP.cu:600-640): a jittered lattice. */
+static void create_square_ink(orc_fluid* o, orc_rng* rng, plist* out, const aq_volume* v, float spacing) {
+  const float md = spacing / 2.f;
+  const float gx = (float)o->sx * o->h, gy = (float)o->sy * o->h, gz = (float)o->sz * o->h;
+  const float shrink = (float)((double)md - 1e-3);
+  const float x0 = v->box_min[0] * gx + md, y0 = v->box_min[1] * gy + md, z0 = v->box_min[2] * gz + md;
+  const float x1 = v->box_max[0] * gx - shrink, y1 = v->box_max[1] * gy - shrink, z1 = v->box_max[2] * gz - shrink;
+  for (float x = x0; x <= x1; x += spacing)
+    for (float y = y0; y <= y1; y += spacing)
+      for (float z = z0; z <= z1; z += spacing) {
+        const float mag = spacing / 2.f;
+        /* (random0to1() - 0.5) is evaluated in double, then stored as float */
+        float jx = (float)((double)random0to1(rng) - 0.5);
+        float jy = (float)((double)random0to1(rng) - 0.5);
+        float jz = (float)((double)random0to1(rng) - 0.5);
+        jx *= mag; jy *= mag; jz *= mag;
+        float px = x + jx, py = y + jy, pz = z + jz;
+        px = fminf(gx - md, fmaxf(md, px));
+        py = fminf(gy - md, fmaxf(md, py));
+        pz = fminf(gz - md, fmaxf(md, pz));
+        plist_push(out, px, py, pz, v->phase);
+      }
+}
+
+/* Fluid::createSphereInk (Fluid_3D_FLIP.cu:642-664): createParticlesAt (sub-
+ * spacing h/2) at every point of a spacing lattice from 0, loops z, y, x. */
+static void create_sphere_ink(orc_fluid* o, orc_rng* rng, plist* out, const aq_volume* v, float spacing) {
+  if (!check_coord_valid(v->ball_center)) return;
+  seed_filter f;
+  f.is_sphere = 1;
+  f.cx = v->ball_center[0] * (float)o->sx * o->h;
+  f.cy = v->ball_center[1] * (float)o->sy * o->h;
+  f.cz = v->ball_center[2] * (float)o->sz * o->h;
+  f.r = v->ball_radius;
+  const float gx = (float)o->sx * o->h, gy = (float)o->sy * o->h, gz = (float)o->sz * o->h;
+  for (float z = 0; z < gz; z += spacing)
+    for (float y = 0; y < gy; y += spacing)
+      for (float x = 0; x < gx; x += spacing) create_particles_at(o, rng, out, x, y, z, &f, o->h / 2, v->phase);
+}
+
+int orc_ink_create(orc_fluid* o) {
+  if (o->ink_pos) return o->n_ink;
+  plist pl = {NULL, 0, 0};
+  const float spacing = o->h / 4;
+  for (int i = 0; i < o->cfg.volume_count; ++i) {
+    const aq_volume* v = &o->cfg.volumes[i];
+    if (v->shape == AQ_SHAPE_SQUARE) create_square_ink(o, &o->rng, &pl, v, spacing);
+    else if (v->shape == AQ_SHAPE_SPHERE) create_sphere_ink(o, &o->rng, &pl, v, spacing);
+  }
+  const int n = pl.n;
+  o->n_ink = n;
+  o->ink_pos = (float*)xcalloc(3 * (size_t)(n > 0 ? n : 1), sizeof(float));
+  o->ink_vel = (float*)xcalloc(3 * (size_t)(n > 0 ? n : 1), sizeof(float));
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) o->ink_pos[d * n + i] = pl.data[7 * (size_t)i + d];
+  free(pl.data);
+  return n;
+}
+
+int orc_ink_count(const orc_fluid* o) { return o->n_ink; }
+
+void orc_ink_advance(orc_fluid* o) {
+  const int n = o->n_ink;
+  float *p = o->ink_pos, *v = o->ink_vel;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i)
+    g2p_move(o, 1.0f, o->cfg.timestep, &p[i], &p[n + i], &p[2 * n + i], &v[i], &v[n + i], &v[2 * n + i]);
+}
+
+void orc_ink_get(const orc_fluid* o, float* pos, float* vel) {
+  const size_t n = (size_t)o->n_ink;
+  if (pos) memcpy(pos, o->ink_pos, sizeof(float) * 3 * n);
+  if (vel) memcpy(vel, o->ink_vel, sizeof(float) * 3 * n);
+}
+
+void orc_ink_set(orc_fluid* o, const float* pos, const float* vel) {
+  const size_t n = (size_t)o->n_ink;
+  if (pos) memcpy(o->ink_pos, pos, sizeof(float) * 3 * n);
+  if (vel) memcpy(o->ink_vel, vel, sizeof(float) * 3 * n);
 }
 
 /* performSpatialHashing2 (Fluid_3D_common.cuh:27-56): calcHashImpl
@@ -780,11 +886,6 @@ static void stage_diffuse(orc_fluid* o) {
 
 /* ---------------------------------------------------------- lifecycle */
 
-static void* xcalloc(size_t n, size_t s) {
-  void* p = calloc(n ? n : 1, s);
-  return p;
-}
-
 static void alloc_particles(orc_fluid* o, int n) {
   o->n = n;
   o->pos = (float*)xcalloc((size_t)3 * n, sizeof(float));
@@ -830,14 +931,13 @@ orc_fluid* orc_create(const aq_config* cfg) {
   /* Fluid::init: the grid starts all AIR/zero (createField3D + clearField3D,
    * MAC_Grid_3D.cu:43-75), then fixBoundary, seeding and transferToGrid. */
   fix_boundary(o);
-  orc_rng rng;
-  memset(&rng, 0, sizeof(rng));
-  initstate_r(cfg->seed, rng.state, sizeof(rng.state), &rng.rd);
+  memset(&o->rng, 0, sizeof(o->rng));
+  initstate_r(cfg->seed, o->rng.state, sizeof(o->rng.state), &o->rng.rd);
   plist pl = {NULL, 0, 0};
   for (int i = 0; i < cfg->volume_count; ++i) {
     const aq_volume* v = &cfg->volumes[i];
-    if (v->shape == AQ_SHAPE_SQUARE) create_square(o, &rng, &pl, v);
-    else if (v->shape == AQ_SHAPE_SPHERE) create_sphere(o, &rng, &pl, v);
+    if (v->shape == AQ_SHAPE_SQUARE) create_square(o, &o->rng, &pl, v);
+    else if (v->shape == AQ_SHAPE_SPHERE) create_sphere(o, &o->rng, &pl, v);
   }
   alloc_particles(o, pl.n);
   const int n = pl.n;
@@ -856,7 +956,7 @@ void orc_destroy(orc_fluid* o) {
   void* ptrs[] = {o->pos, o->vel, o->frac, o->pos2, o->vel2, o->frac2, o->hash, o->sort_index,
                   o->counts, o->content, o->velocity, o->new_velocity, o->nv_tmp, o->pressure,
                   o->p_tmp, o->divergence, o->density, o->pcount, o->has, o->has_tmp, o->vf,
-                  o->nvf, o->nvf_tmp, o->cstart, o->cend};
+                  o->nvf, o->nvf_tmp, o->cstart, o->cend, o->ink_pos, o->ink_vel};
   for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
   free(o);
 }
@@ -874,6 +974,9 @@ int orc_run_stage(orc_fluid* o, int stage) {
     case AQ_STAGE_EXTRAPOLATE: stage_extrapolate(o); return 0;
     case AQ_STAGE_DIFFUSE:
       stage_diffuse(o);
+      /* transferToInkParticles + moveInkParticles (Fluid_3D_FLIP.cu:349-350,
+       * commented out in the reference), once the ink exists */
+      if (o->ink_pos) orc_ink_advance(o);
       o->time += o->cfg.timestep; /* physicalTime += timestep (Fluid_3D_FLIP.cu:351) */
       return 0;
     default: return 1;

@@ -54,6 +54,17 @@ void orc_config_default(aq_config* cfg);
 /* Number of OpenMP threads the oracle uses (omp_get_max_threads). */
 int orc_threads(void);
 
+/* Ink particles (Fluid_3D_FLIP.cu:600-725): seeds them once (continuing the
+ * fluid seeding's rand() sequence; returns the count), advances them with
+ * the current grid velocities (FLIP coefficient 1, then RK3), host copies
+ * of positions / velocities ([3][n], either may be NULL).  Once seeded, the
+ * diffusion stage (the end of every step) also advances them. */
+int orc_ink_create(orc_fluid* o);
+int orc_ink_count(const orc_fluid* o);
+void orc_ink_advance(orc_fluid* o);
+void orc_ink_get(const orc_fluid* o, float* pos, float* vel);
+void orc_ink_set(orc_fluid* o, const float* pos, const float* vel);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,7 @@ using Fluid_3D_FLIP::Particle;
 
 struct RefFluid {
   Fluid_3D_FLIP::Fluid* f = nullptr;
+  bool ink = false; /* initInkRenderer ran: inkParticles is allocated */
 };
 
 template <typename T>
@@ -175,6 +176,7 @@ void* aqref_create(const aq_config* cfg) {
 void aqref_destroy(void* h) {
   RefFluid* r = (RefFluid*)h;
   if (!r) return;
+  if (r->ink) cudaFree(r->f->inkParticles);
   delete r->f;
   delete r;
 }
@@ -318,6 +320,62 @@ int aqref_set_state(void* h, const aq_host_state* s) {
     aqref_record(cudaMemcpy(f->particles, ps.data(), sizeof(Particle) * n, cudaMemcpyHostToDevice), "p", __FILE__, __LINE__);
   }
   cudaDeviceSynchronize();
+  return (int)aqref_first_error;
+}
+
+/* Ink particles, the calls the reference leaves commented out: Fluid::init
+ * would run initInkRenderer after seeding (Fluid_3D_FLIP.cu:498), so it
+ * continues the same rand() sequence when called right after aqref_create;
+ * simulationStep would end with transferToInkParticles + moveInkParticles
+ * (Fluid_3D_FLIP.cu:349-350).  Returns the ink count, or -1 on error. */
+int aqref_ink_init(void* h) {
+  RefFluid* r = (RefFluid*)h;
+  if (!r->ink) {
+    r->f->initInkRenderer();
+    cudaDeviceSynchronize();
+    r->ink = true;
+  }
+  return aqref_first_error == cudaSuccess ? r->f->inkParticleCount : -1;
+}
+
+int aqref_ink_step(void* h) {
+  RefFluid* r = (RefFluid*)h;
+  if (!r->ink) return -1;
+  r->f->transferToInkParticles();
+  r->f->moveInkParticles(r->f->timestep);
+  cudaDeviceSynchronize();
+  aqref_record(cudaGetLastError(), "ink", __FILE__, __LINE__);
+  return (int)aqref_first_error;
+}
+
+/* Ink positions / velocities as [3][n] planes (either may be NULL). */
+int aqref_ink_get(void* h, float* pos, float* vel) {
+  RefFluid* r = (RefFluid*)h;
+  if (!r->ink) return -1;
+  const int n = r->f->inkParticleCount;
+  std::vector<Fluid_3D_FLIP::Particle> ps(n);
+  aqref_record(cudaMemcpy(ps.data(), r->f->inkParticles, sizeof(Fluid_3D_FLIP::Particle) * n,
+                          cudaMemcpyDeviceToHost), "ink", __FILE__, __LINE__);
+  for (int i = 0; i < n; ++i) {
+    if (pos) { pos[i] = ps[i].position.x; pos[n + i] = ps[i].position.y; pos[2 * n + i] = ps[i].position.z; }
+    if (vel) { vel[i] = ps[i].velocity.x; vel[n + i] = ps[i].velocity.y; vel[2 * n + i] = ps[i].velocity.z; }
+  }
+  return (int)aqref_first_error;
+}
+
+int aqref_ink_set(void* h, const float* pos, const float* vel) {
+  RefFluid* r = (RefFluid*)h;
+  if (!r->ink) return -1;
+  const int n = r->f->inkParticleCount;
+  std::vector<Fluid_3D_FLIP::Particle> ps(n);
+  aqref_record(cudaMemcpy(ps.data(), r->f->inkParticles, sizeof(Fluid_3D_FLIP::Particle) * n,
+                          cudaMemcpyDeviceToHost), "ink", __FILE__, __LINE__);
+  for (int i = 0; i < n; ++i) {
+    if (pos) ps[i].position = make_float3(pos[i], pos[n + i], pos[2 * n + i]);
+    if (vel) ps[i].velocity = make_float3(vel[i], vel[n + i], vel[2 * n + i]);
+  }
+  aqref_record(cudaMemcpy(r->f->inkParticles, ps.data(), sizeof(Fluid_3D_FLIP::Particle) * n,
+                          cudaMemcpyHostToDevice), "ink", __FILE__, __LINE__);
   return (int)aqref_first_error;
 }
 

@@ -18,9 +18,12 @@ int main() {
     std::printf("init: %s\n", e.what());
     return e.status == AQ_ERR_NO_DEVICE ? 0 : 3;
   }
+  fluid.initInkRenderer();
   fluid.simulationStep();
   fluid.synchronize();
-  std::printf("particles %d time %.3f center %.1f size %.1f\n", fluid.particleCount(), fluid.physicalTime,
-              fluid.getCenter()[0], fluid.getContainerSize());
-  return fluid.physicalTime > 0 ? 0 : 4;
+  std::vector<float> ink(3 * (size_t)fluid.inkParticleCount);
+  fluid.downloadInk(ink.data(), nullptr);
+  std::printf("particles %d ink %d time %.3f center %.1f size %.1f\n", fluid.particleCount(),
+              fluid.inkParticleCount, fluid.physicalTime, fluid.getCenter()[0], fluid.getContainerSize());
+  return fluid.physicalTime > 0 && fluid.inkParticleCount > 0 ? 0 : 4;
 }

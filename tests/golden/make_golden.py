@@ -11,12 +11,20 @@ reference's own state (teacher forcing).  It also records:
     out-of-range y/z coordinates (createField3D sets only addressMode[0],
     Fluid/VolumeData.cuh:58-67);
   * the reference's run-to-run spread per stage (its Jacobi, diffusion and
-    extrapolation kernels update in place and race).
+    extrapolation kernels update in place and race);
+  * ink particles (ref_ink.npz), through the reference's own initInkRenderer /
+    transferToInkParticles / moveInkParticles, which its Fluid leaves
+    switched off: the seeded count and a SHA-256 of all seeded positions,
+    and, for a fixed sample of ink particles, the ink before and after the
+    advance that would end each step, with the grids it read.
+
+    python tests/golden/make_golden.py --out tests/golden --only ink
 """
 from __future__ import annotations
 
 import argparse
 import ctypes as ct
+import hashlib
 import json
 import pathlib
 import sys
@@ -44,6 +52,8 @@ STAGE_FIELDS = {
 }
 
 GOLDEN_SCENES = {"cfg1_16": 2, "aniso": 1, "multi_16": 1}
+INK_SCENES = {"cfg1_16": 2, "aniso": 2}
+INK_SAMPLE = 2048
 
 
 def record_scene(name: str, steps: int) -> dict:
@@ -152,6 +162,34 @@ def record_special() -> dict:
     return out
 
 
+def record_ink() -> dict:
+    out = {}
+    for name, steps in INK_SCENES.items():
+        cfg = SCENES[name]()
+        ref = RefFluid(cfg)
+        n = ref.enable_ink()  # right after init: continues the seeding's rand() sequence
+        pos = ref.get_ink()["position"]
+        idx = np.unique(np.linspace(0, n - 1, INK_SAMPLE).astype(np.int64))
+        out[f"{name}/config"] = np.frombuffer(bytes(cfg), dtype=np.uint8).copy()
+        out[f"{name}/count"] = np.int64(n)
+        out[f"{name}/init_sha256"] = np.frombuffer(hashlib.sha256(pos.tobytes()).digest(), np.uint8).copy()
+        out[f"{name}/sample"] = idx
+        out[f"{name}/init_position"] = pos[:, idx]
+        for s in range(steps):
+            ref.step(1)
+            st = ref.get_state(["velocity", "new_velocity"])
+            before = ref.get_ink()
+            ref.ink_advance()
+            after = ref.get_ink()
+            out[f"{name}/s{s}/velocity"] = st["velocity"]
+            out[f"{name}/s{s}/new_velocity"] = st["new_velocity"]
+            for k in ("position", "velocity"):
+                out[f"{name}/s{s}/in_{k}"] = before[k][:, idx]
+                out[f"{name}/s{s}/out_{k}"] = after[k][:, idx]
+        ref.close()
+    return out
+
+
 def texture_probe() -> dict:
     w, h, d = 6, 5, 4
     coords = [(2, -1, 2), (2, h, 2), (2, 2, -1), (2, 2, d), (-1, 2, 2), (w, 2, 2), (2, h - 1, 2), (2, 0, 2),
@@ -180,9 +218,14 @@ def texture_probe() -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
+    ap.add_argument("--only", choices=["all", "ink"], default="all")
     a = ap.parse_args()
     out = pathlib.Path(a.out)
     out.mkdir(parents=True, exist_ok=True)
+    np.savez_compressed(out / "ref_ink.npz", **record_ink())
+    print("ink fixtures recorded")
+    if a.only == "ink":
+        return
     probe = texture_probe()
     (out / "texture_probe.json").write_text(json.dumps(probe, indent=1))
     print("texture probe:", {k: v for k, v in probe.items() if k != "reads"})

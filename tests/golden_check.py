@@ -162,3 +162,53 @@ def replay_special(checker_factory):
             else:
                 out.append((name, f, "rel_l2", rel_l2(got[f], ref), tol))
     return out
+
+
+INK_SCENES = ["cfg1_16", "aniso"]
+
+
+def load_ink():
+    p = GOLDEN / "ref_ink.npz"
+    return dict(np.load(p)) if p.exists() else None
+
+
+def replay_ink(data: dict, scene: str, make, set_grids) -> dict:
+    """Seeds the ink of a recorded scene on a checker and replays the
+    reference's ink advances on the sampled particles, each from the
+    reference's own ink and grids (teacher forcing).
+
+    make(cfg) -> checker with enable_ink/get_ink/set_ink/ink_advance;
+    set_grids(checker, velocity, new_velocity) loads the step's grids.
+    Returns count, whether the SHA-256 of all seeded positions and the
+    sampled positions match, and per step the relative L2 errors of the
+    advanced sample's positions and velocities."""
+    import hashlib
+
+    cfg = config_from_bytes(data[f"{scene}/config"])
+    chk = make(cfg)
+    n = chk.enable_ink()
+    pos = chk.get_ink()["position"]
+    idx = data[f"{scene}/sample"]
+    out = {
+        "count": (n, int(data[f"{scene}/count"])),
+        "sha_match": hashlib.sha256(np.ascontiguousarray(pos).tobytes()).digest()
+        == bytes(data[f"{scene}/init_sha256"]),
+        "sample_equal": bool(np.array_equal(pos[:, idx], data[f"{scene}/init_position"])),
+        "steps": [],
+    }
+    s = 0
+    while f"{scene}/s{s}/velocity" in data:
+        set_grids(chk, data[f"{scene}/s{s}/velocity"], data[f"{scene}/s{s}/new_velocity"])
+        p = pos.copy()
+        v = np.zeros_like(pos)
+        p[:, idx] = data[f"{scene}/s{s}/in_position"]
+        v[:, idx] = data[f"{scene}/s{s}/in_velocity"]
+        chk.set_ink(p, v)
+        chk.ink_advance()
+        got = chk.get_ink()
+        out["steps"].append((s, rel_l2(got["position"][:, idx], data[f"{scene}/s{s}/out_position"]),
+                             rel_l2(got["velocity"][:, idx], data[f"{scene}/s{s}/out_velocity"])))
+        s += 1
+    if hasattr(chk, "close"):
+        chk.close()
+    return out

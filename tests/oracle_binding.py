@@ -47,6 +47,13 @@ def _load_oracle():
         lib.orc_pressure_residual.restype = ct.c_double
         lib.orc_pressure_residual.argtypes = [ct.c_void_p]
         lib.orc_threads.restype = ct.c_int
+        lib.orc_ink_create.restype = ct.c_int
+        lib.orc_ink_create.argtypes = [ct.c_void_p]
+        lib.orc_ink_count.restype = ct.c_int
+        lib.orc_ink_count.argtypes = [ct.c_void_p]
+        lib.orc_ink_advance.argtypes = [ct.c_void_p]
+        lib.orc_ink_get.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p]
+        lib.orc_ink_set.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p]
         _orc = lib
     return _orc
 
@@ -73,6 +80,14 @@ def _load_ref():
         lib.aqref_probe_texture.restype = ct.c_int
         lib.aqref_probe_texture.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int]
         lib.aqref_error.restype = ct.c_int
+        lib.aqref_ink_init.restype = ct.c_int
+        lib.aqref_ink_init.argtypes = [ct.c_void_p]
+        for nm in ("aqref_ink_step",):
+            getattr(lib, nm).restype = ct.c_int
+            getattr(lib, nm).argtypes = [ct.c_void_p]
+        for nm in ("aqref_ink_get", "aqref_ink_set"):
+            getattr(lib, nm).restype = ct.c_int
+            getattr(lib, nm).argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p]
         _ref = lib
     return _ref
 
@@ -81,7 +96,28 @@ def ref_available() -> bool:
     return REF_SO.exists()
 
 
-class _StateIO:
+class _InkIO:
+    """Ink particles over [3, n] numpy planes, shared by both checkers."""
+
+    n_ink: int = 0
+
+    def get_ink(self) -> dict:
+        pos = np.zeros((3, self.n_ink), np.float32)
+        vel = np.zeros((3, self.n_ink), np.float32)
+        rc = self._ink_get(pos.ctypes.data, vel.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"ink get failed: {rc}")
+        return {"position": pos, "velocity": vel}
+
+    def set_ink(self, position=None, velocity=None):
+        p = None if position is None else np.ascontiguousarray(position, np.float32).reshape(3, self.n_ink)
+        v = None if velocity is None else np.ascontiguousarray(velocity, np.float32).reshape(3, self.n_ink)
+        rc = self._ink_set(None if p is None else p.ctypes.data, None if v is None else v.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"ink set failed: {rc}")
+
+
+class _StateIO(_InkIO):
     """get_state/set_state over numpy dicts, shared by both checkers."""
 
     size: tuple
@@ -141,6 +177,21 @@ class Oracle(_StateIO):
     def pressure_residual(self) -> float:
         return self.lib.orc_pressure_residual(self.h)
 
+    def enable_ink(self) -> int:
+        self.n_ink = self.lib.orc_ink_create(self.h)
+        return self.n_ink
+
+    def ink_advance(self):
+        self.lib.orc_ink_advance(self.h)
+
+    def _ink_get(self, p, v):
+        self.lib.orc_ink_get(self.h, p, v)
+        return 0
+
+    def _ink_set(self, p, v):
+        self.lib.orc_ink_set(self.h, p, v)
+        return 0
+
     def close(self):
         if self.h:
             self.lib.orc_destroy(self.h)
@@ -179,6 +230,24 @@ class RefFluid(_StateIO):
         rc = self.lib.aqref_step(self.h, n)
         if rc != 0:
             raise RuntimeError(f"reference step failed: {rc}")
+
+    def enable_ink(self) -> int:
+        n = self.lib.aqref_ink_init(self.h)
+        if n < 0:
+            raise RuntimeError(f"reference ink init failed: {self.lib.aqref_error()}")
+        self.n_ink = n
+        return n
+
+    def ink_advance(self):
+        rc = self.lib.aqref_ink_step(self.h)
+        if rc != 0:
+            raise RuntimeError(f"reference ink step failed: {rc}")
+
+    def _ink_get(self, p, v):
+        return self.lib.aqref_ink_get(self.h, p, v)
+
+    def _ink_set(self, p, v):
+        return self.lib.aqref_ink_set(self.h, p, v)
 
     def close(self):
         if self.h:

@@ -8,7 +8,7 @@ import json
 import numpy as np
 import pytest
 
-from golden_check import GOLDEN, judge, load, replay, replay_special
+from golden_check import FLOAT_TOL, GOLDEN, INK_SCENES, judge, load, load_ink, replay, replay_ink, replay_special
 from oracle_binding import Oracle
 
 SCENES_STEPS = [("cfg1_16", 2), ("aniso", 1), ("multi_16", 1)]
@@ -55,3 +55,23 @@ def test_fixture_seeding_is_bit_exact():
         for k in st:
             if k != "physical_time":
                 np.testing.assert_array_equal(st[k], data[f"init/{k}"], err_msg=f"{scene} {k}")
+
+
+@pytest.mark.parametrize("scene", INK_SCENES)
+def test_oracle_ink_against_reference_fixtures(scene):
+    """Ink particles (the reference's switched-off initInkRenderer /
+    transferToInkParticles / moveInkParticles): seeding bit-exact, each
+    recorded advance within the float tolerance."""
+    data = load_ink()
+    if data is None:
+        pytest.skip("fixture missing")
+
+    def set_grids(o, vel, nvel):
+        o.set_state({"velocity": vel, "new_velocity": nvel})
+
+    res = replay_ink(data, scene, Oracle, set_grids)
+    assert res["count"][0] == res["count"][1]
+    assert res["sample_equal"] and res["sha_match"]
+    assert len(res["steps"]) >= 2
+    for s, ep, ev in res["steps"]:
+        assert ep <= FLOAT_TOL and ev <= FLOAT_TOL, (s, ep, ev)
