@@ -127,6 +127,10 @@ def load_library() -> ct.CDLL:
         "aq_fluid_download_ink": (ct.c_int, [P, P, P]),
         "aq_fluid_upload_ink": (ct.c_int, [P, P, P]),
         "aq_fluid_ink_advance": (ct.c_int, [P]),
+        "aq_fluid_mesh_info": (ct.c_int, [P, P]),
+        "aq_fluid_mesh": (ct.c_int, [P, P, ct.c_int64, ct.POINTER(ct.c_int32)]),
+        "aq_fluid_download_mesh": (ct.c_int, [P, P, ct.c_int64, ct.POINTER(ct.c_int32)]),
+        "aq_fluid_download_sdf": (ct.c_int, [P, P]),
         "aq_dataset_create": (ct.c_int, [ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.POINTER(P)]),
         "aq_dataset_destroy": (None, [P]),
         "aq_dataset_count": (ct.c_int32, [P]),
@@ -361,6 +365,38 @@ class Fluid:
     def ink_advance(self):
         """transferToInkParticles + moveInkParticles on the current grids."""
         _check(self._lib.aq_fluid_ink_advance(self._h))
+
+    def mesh_info(self) -> dict:
+        """Grid sizes of the surface mesher (Mesher as Fluid::init builds it)."""
+        info = _abi.MeshInfo()
+        _check(self._lib.aq_fluid_mesh_info(self._h, ct.byref(info)))
+        return {"sdf": tuple(info.sdf_size), "mesh": tuple(info.mesh_size), "h_sdf": info.sdf_cell,
+                "h_mesh": info.mesh_cell, "radius": info.particle_radius}
+
+    def download_mesh(self, capacity=None) -> np.ndarray:
+        """Meshes the current particles; the occupied-cube records, [k, 15, 6]
+        (position xyz, normal xyz per vertex slot; unused slots zero)."""
+        n = ct.c_int32()
+        if capacity is None:
+            _check(self._lib.aq_fluid_download_mesh(self._h, None, 0, ct.byref(n)))
+            capacity = n.value
+        out = np.zeros((max(int(capacity), 1), 15, 6), np.float32)
+        _check(self._lib.aq_fluid_download_mesh(self._h, out.ctypes.data, int(capacity), ct.byref(n)))
+        return out[: min(n.value, int(capacity))]
+
+    def mesh_into(self, device_ptr: int, capacity_records: int) -> int:
+        """Meshes into a device buffer of capacity_records records (the
+        reference's mesh VBO layout); returns the occupied-cube count."""
+        n = ct.c_int32()
+        _check(self._lib.aq_fluid_mesh(self._h, ct.c_void_p(device_ptr), int(capacity_records), ct.byref(n)))
+        return n.value
+
+    def download_sdf(self) -> np.ndarray:
+        """The last mesh's SDF grid, [sdf_x, sdf_y, sdf_z]."""
+        info = self.mesh_info()
+        out = np.zeros(info["sdf"], np.float32)
+        _check(self._lib.aq_fluid_download_sdf(self._h, out.ctypes.data))
+        return out
 
     def set_warm_start(self, net):
         """Attaches the network AQ_PRESSURE_LEARNED ('learned') uses (None detaches)."""

@@ -115,6 +115,17 @@ class HostState(ct.Structure):
     ]
 
 
+class MeshInfo(ct.Structure):
+    """aq_mesh_info."""
+    _fields_ = [
+        ("sdf_size", ct.c_int32 * 3),
+        ("mesh_size", ct.c_int32 * 3),
+        ("sdf_cell", ct.c_float),
+        ("mesh_cell", ct.c_float),
+        ("particle_radius", ct.c_float),
+    ]
+
+
 class SolveStats(ct.Structure):
     _fields_ = [
         ("iterations", ct.c_int32),

@@ -25,6 +25,25 @@ cudaError_t launch_particles_advance(cudaStream_t st, const Dims& d, const StepP
 cudaError_t launch_ink_advance(cudaStream_t st, const Dims& d, float dt, Particles ink, const float* u0,
                                const float* v0, const float* w0, const float* un, const float* vn, const float* wn,
                                int n);
+// Surface mesher (k_mesh.cu).  SDF grid SX*SY*SZ (cell hs), its hash grid
+// HX*HY*HZ = (SX-2)*(SY-2)*(SZ-2), marching-cubes grid MX*MY*MZ (cell hm).
+struct MeshDims {
+  int SX, SY, SZ;
+  int HX, HY, HZ;
+  int MX, MY, MZ;
+  float hs, hm, radius;
+};
+cudaError_t launch_sdf_keys(cudaStream_t st, const MeshDims& m, const float* px, const float* py, const float* pz,
+                            int* skey, int* scount, int n);
+cudaError_t launch_sdf_scatter(cudaStream_t st, const Dims& d, const float* px, const float* py, const float* pz,
+                               const int* off, const int* skey, const int* soff, float4* spos, int* bad, int n);
+cudaError_t launch_sdf(cudaStream_t st, const MeshDims& m, const int* soff, const float4* spos,
+                       cudaSurfaceObject_t surf);
+cudaError_t launch_mc_vertices(cudaStream_t st, const MeshDims& m, cudaTextureObject_t tex, float* vv);
+cudaError_t launch_mc_flags(cudaStream_t st, const MeshDims& m, const float* vv, uint8_t* ctype, int* flag);
+cudaError_t launch_mc_emit(cudaStream_t st, const MeshDims& m, cudaTextureObject_t tex, const float* vv,
+                           const uint8_t* ctype, const int* moff, float* out, long long capacity);
+cudaError_t launch_mc_tail(cudaStream_t st, const int* total, int* prev, float* out, long long capacity);
 // Per-block FP64 sums of the particle volume fractions: part[frac_sum_parts()][4].
 int frac_sum_parts();
 cudaError_t launch_frac_sum(cudaStream_t st, const float4* frac, int n, double* part);

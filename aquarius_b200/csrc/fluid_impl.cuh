@@ -15,6 +15,8 @@
 namespace aqb {
 inline aq_status fail(aq_status st, const std::string& msg) { return set_last_error(st, msg); }
 struct UActs;
+struct MeshState;                  // surface mesher buffers (mesh.cu)
+void mesh_release(MeshState* s);
 
 // The reference's random0to1() (Common/Commons.h:3-5) over glibc rand(),
 // replayed without touching the process's own rand() state: random_r over a
@@ -103,6 +105,7 @@ struct aq_fluid {
   Particles ink{};
   int n_ink = 0;
   bool ink_on = false;
+  aqb::MeshState* mesher = nullptr;  // made by the first aq_fluid_mesh call
   cudaGraphExec_t exec = nullptr;
   bool use_graph = true;
   int graph_launches = 0;  // launches outside the residual loop
@@ -117,6 +120,7 @@ struct aq_fluid {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
     if (exec) cudaGraphExecDestroy(exec);
+    if (mesher) aqb::mesh_release(mesher);
     for (void* p : allocs) cudaFree(p);
     if (ss_host) cudaFreeHost(ss_host);
     if (side) cudaStreamDestroy(side);

@@ -465,6 +465,42 @@ aq_status aq_fluid_download_ink(aq_fluid* f, float* position, float* velocity);
 aq_status aq_fluid_upload_ink(aq_fluid* f, const float* position, const float* velocity);
 aq_status aq_fluid_ink_advance(aq_fluid* f);
 
+/* Surface mesher: replaces Mesher::mesh (Rendering/Renderer3D/Mesher.cuh:
+ * 140-178, Mesher.cu:321-630) as Fluid::init builds it
+ * (Fluid/Fluid_3D_FLIP.cu:495) and draw() calls it (:404): a particle SDF on
+ * a grid of cell h/2 (computeSDF, Mesher.cuh:20-84) and marching cubes on a
+ * fixed 128^3 grid of cell size_x*h/126 spanning [-cell, 127*cell] on every
+ * axis (marchingCubes, Mesher.cu:322-425).
+ *
+ * Output layout, the reference's mesh VBO: one record per occupied cube
+ * (a cube whose type has triangles), 15 vertex slots of 6 floats (position
+ * xyz, normal xyz); slots the cube's triangles do not use are zero.  Records
+ * come in cube order (x slowest, z fastest) — the reference appends them in
+ * atomic order, so the set of records is the same, the order deterministic.
+ * Unlike the reference, the fluid's particle order is left as the step left
+ * it (the reference re-sorts the particle array by the SDF grid).
+ *
+ * aq_fluid_mesh writes into a DEVICE buffer of capacity_records records (the
+ * reference passes its mapped VBO): records past capacity are dropped,
+ * everything after the last record is zero (a buffer is cleared whole the
+ * first time it is seen); cubes (may be NULL) receives the occupied-cube
+ * count, which may exceed capacity.  aq_fluid_download_mesh does the same
+ * into HOST memory.  aq_fluid_download_sdf copies the last mesh's SDF grid,
+ * [sdf_x][sdf_y][sdf_z] with z fastest.  The particles must be sorted by
+ * cell, as any step, the init or the sort stage leaves them; otherwise the
+ * calls fail with AQ_ERR_INVALID_ARGUMENT. */
+typedef struct {
+  int32_t sdf_size[3];  /* 3 + size*h/(h/2) per axis (Mesher.cu:589-591) */
+  int32_t mesh_size[3]; /* 128 per axis (Mesher.cuh:104-106) */
+  float sdf_cell;       /* h/2 */
+  float mesh_cell;      /* size_x*h/126 */
+  float particle_radius; /* h/2 */
+} aq_mesh_info;
+aq_status aq_fluid_mesh_info(const aq_fluid* f, aq_mesh_info* info);
+aq_status aq_fluid_mesh(aq_fluid* f, float* output, int64_t capacity_records, int32_t* cubes);
+aq_status aq_fluid_download_mesh(aq_fluid* f, float* records, int64_t capacity_records, int32_t* cubes);
+aq_status aq_fluid_download_sdf(aq_fluid* f, float* sdf);
+
 /* Attaches the network used by AQ_PRESSURE_LEARNED (NULL detaches).  The
  * network must outlive the fluid's steps; allocate-once buffers for the
  * fluid's grid are made here, so call it before the first step. */

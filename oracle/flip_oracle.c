@@ -8,6 +8,7 @@
  */
 #define _DEFAULT_SOURCE
 #include "flip_oracle.h"
+#include "../aquarius_b200/csrc/mc_table.h"
 
 #include <math.h>
 #include <stdint.h>
@@ -446,6 +447,222 @@ void orc_ink_set(orc_fluid* o, const float* pos, const float* vel) {
   const size_t n = (size_t)o->n_ink;
   if (pos) memcpy(o->ink_pos, pos, sizeof(float) * 3 * n);
   if (vel) memcpy(o->ink_vel, vel, sizeof(float) * 3 * n);
+}
+
+/* ---------------------------------------------------------------- mesher
+ * The surface mesher (Rendering/Renderer3D/Mesher.cuh:20-178,
+ * Mesher.cu:321-630) as Fluid::init builds it (Fluid_3D_FLIP.cu:495):
+ * container = size * h, particle spacing h/2.  A particle SDF on a grid of
+ * cell h/2 (computeSDF: a dunfanKernel-weighted mean of the particles near a
+ * cell centre, minus the particle radius), then marching cubes on a fixed
+ * 128^3 grid spanning the container's x extent, sampling the SDF by
+ * trilinear interpolation.  Output: one record per occupied cube in cube
+ * order, 15 slots of (position, normal), unused slots zero. */
+
+void orc_mesh_dims_of(const orc_fluid* o, orc_mesh_dims* m) {
+  const float h = o->h;
+  const float cx = (float)o->sx * h, cy = (float)o->sy * h, cz = (float)o->sz * h;
+  const float spacing = h / 2; /* Mesher(containerSize, cellPhysicalSize / 2, ...) */
+  m->h_sdf = spacing;          /* Mesher.cu:583-584 */
+  m->radius = spacing;
+  m->mesh[0] = m->mesh[1] = m->mesh[2] = 128; /* Mesher.cuh:104-106 */
+  m->h_mesh = cx / (float)(128 - 2);          /* Mesher.cu:587 */
+  m->sdf[0] = (int)(3 + cx / m->h_sdf);        /* Mesher.cu:589-591 */
+  m->sdf[1] = (int)(3 + cy / m->h_sdf);
+  m->sdf[2] = (int)(3 + cz / m->h_sdf);
+}
+
+/* dunfanKernel (Fluid/WeightKernels.cuh:183-189) */
+static inline float dunfan(float rx, float ry, float rz, float support) {
+  const float r2 = rx * rx + ry * ry + rz * rz;
+  const float h2 = support * support;
+  if (r2 > h2) return 0;
+  const float t = 1.f - r2 / (h2 * 3.f);
+  return fmaxf(0.f, t * t * t);
+}
+
+/* computeSDF (Mesher.cuh:20-84) after performSpatialHashing2 on the SDF grid
+ * (Mesher.cuh:160): particles stably sorted by their SDF hash cell, then per
+ * SDF cell the 4x4x4 hash cells x-3..x (flat index, as the reference walks
+ * them) in order.  sdf: [sx][sy][sz] of the SDF grid, z fastest. */
+static void mesh_sdf(const orc_fluid* o, const orc_mesh_dims* m, float* sdf) {
+  const int n = o->n;
+  const float hs = m->h_sdf;
+  const int HX = m->sdf[0] - 2, HY = m->sdf[1] - 2, HZ = m->sdf[2] - 2;
+  const long long HC = (long long)HX * HY * HZ;
+  const int SX = m->sdf[0], SY = m->sdf[1], SZ = m->sdf[2];
+  const long long SC = (long long)SX * SY * SZ;
+  const float *px = o->pos, *py = o->pos + n, *pz = o->pos + 2 * n;
+  int* key = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  int* start = (int*)calloc((size_t)HC + 1, sizeof(int));
+  int* order = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  for (int i = 0; i < n; ++i) { /* calcHashImpl (Fluid_3D_kernels.cuh:8-27) */
+    const int x = (int)(px[i] / hs), y = (int)(py[i] / hs), z = (int)(pz[i] / hs);
+    key[i] = x * (HY * HZ) + y * HZ + z;
+    start[key[i] + 1]++;
+  }
+  for (long long c = 0; c < HC; ++c) start[c + 1] += start[c];
+  {
+    int* fill = (int*)malloc(sizeof(int) * (size_t)HC);
+    memcpy(fill, start, sizeof(int) * (size_t)HC);
+    for (int i = 0; i < n; ++i) order[fill[key[i]]++] = i; /* stable */
+    free(fill);
+  }
+  const float R = hs * 2.f;
+#pragma omp parallel for schedule(static)
+  for (long long idx = 0; idx < SC; ++idx) {
+    const int x = (int)(idx / ((long long)SY * SZ));
+    const int y = (int)((idx / SZ) % SY);
+    const int z = (int)(idx % SZ);
+    const float cx = (float)(x - 1) * hs, cy = (float)(y - 1) * hs, cz = (float)(z - 1) * hs;
+    float sw = 0, sx_ = 0, sy_ = 0, sz_ = 0;
+    for (int dx = -2; dx <= 1; ++dx)
+      for (int dy = -2; dy <= 1; ++dy)
+        for (int dz = -2; dz <= 1; ++dz) {
+          const long long cell = (long long)(x + dx - 1) * HY * HZ + (long long)(y + dy - 1) * HZ + (z + dz - 1);
+          if (cell < 0 || cell >= SC || cell >= HC) continue; /* cells past the hash grid are empty */
+          for (int j = start[cell]; j < start[cell + 1]; ++j) {
+            const int p = order[j];
+            const float w = dunfan(px[p] - cx, py[p] - cy, pz[p] - cz, R);
+            sw += w;
+            sx_ += w * px[p];
+            sy_ += w * py[p];
+            sz_ += w * pz[p];
+          }
+        }
+    float v = hs; /* "set to some positive value first" */
+    if (sw != 0) {
+      const float mx = sx_ / sw, my = sy_ / sw, mz = sz_ / sw;
+      const float ex = mx - cx, ey = my - cy, ez = mz - cz;
+      v = sqrtf(ex * ex + ey * ey + ez * ez) - m->radius;
+    }
+    sdf[((size_t)x * SY + y) * SZ + z] = v;
+  }
+  free(key);
+  free(start);
+  free(order);
+}
+
+/* tex3D on the SDF (linear filter, unnormalised coordinates, border in x,
+ * clamp in y and z; Mesher.cu:627, Fluid/VolumeData.cuh:44-76): texel
+ * centres at i + 0.5.  The texture unit filters with 8-bit fixed-point
+ * weights (CUDA Programming Guide, "Linear Filtering": 9-bit fixed point with
+ * 8 fractional bits).  The weights below are a model of what it returns,
+ * fitted to probes of the reference's own texture (tests/golden/
+ * texture_linear_probe.npz): per axis the fraction rounded half up to 1/256;
+ * per texel the x and z weights multiplied and rounded half down to 1/256,
+ * then the y weight, rounded half up.  It reproduces the probes exactly for
+ * about 92% of samples and within 1.3% of the texel range for the rest. */
+static float tex_linear(int SX, int SY, int SZ, const float* t, float cx, float cy, float cz) {
+  const float xb = cx - 0.5f, yb = cy - 0.5f, zb = cz - 0.5f;
+  const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
+  const float qa = floorf((xb - fx) * 256.f + 0.5f), qb = floorf((yb - fy) * 256.f + 0.5f),
+              qc = floorf((zb - fz) * 256.f + 0.5f);
+  const int i = (int)fx, j = (int)fy, k = (int)fz;
+  float v = 0.f;
+  for (int di = 0; di < 2; ++di)
+    for (int dj = 0; dj < 2; ++dj)
+      for (int dk = 0; dk < 2; ++dk) {
+        const int ii = i + di, jj = iclamp(j + dj, 0, SY - 1), kk = iclamp(k + dk, 0, SZ - 1);
+        const float T = (ii < 0 || ii >= SX) ? 0.f : t[((size_t)ii * SY + jj) * SZ + kk];
+        const float wx = di ? qa : 256.f - qa, wy = dj ? qb : 256.f - qb, wz = dk ? qc : 256.f - qc;
+        const float wxz = ceilf(wx * wz / 256.f - 0.5f);
+        const float w = floorf(wxz * wy / 256.f + 0.5f);
+        v += (w / 256.f) * T;
+      }
+  return v;
+}
+
+static float sdf_sample(const orc_mesh_dims* m, const float* sdf, float cx, float cy, float cz) {
+  return tex_linear(m->sdf[0], m->sdf[1], m->sdf[2], sdf, cx, cy, cz);
+}
+
+/* The same filter on any [w][h][d] field (z fastest), for the probe test. */
+void orc_tex_linear(const float* field, int w, int h, int d, const float* coords, float* out, int n) {
+  for (int q = 0; q < n; ++q) out[q] = tex_linear(w, h, d, field, coords[3 * q], coords[3 * q + 1], coords[3 * q + 2]);
+}
+
+/* getSDF on mesh vertices (Mesher.cu:294-308): 0 on the two outer layers. */
+static float mesh_vertex_sdf(const orc_mesh_dims* m, const float* sdf, int x, int y, int z) {
+  if (x == 0 || y == 0 || z == 0 || x >= m->mesh[0] - 1 || y >= m->mesh[1] - 1 || z >= m->mesh[2] - 1) return 0;
+  const float hm = m->h_mesh, hs = m->h_sdf;
+  const float px = (float)(x - 1) * hm, py = (float)(y - 1) * hm, pz = (float)(z - 1) * hm;
+  return sdf_sample(m, sdf, 1.f + px / hs, 1.f + py / hs, 1.f + pz / hs);
+}
+
+/* getSDF at a world position (Mesher.cu:312-318). */
+static float mesh_point_sdf(const orc_mesh_dims* m, const float* sdf, float px, float py, float pz) {
+  const float hs = m->h_sdf;
+  return sdf_sample(m, sdf, 1.f + px / hs, 1.f + py / hs, 1.f + pz / hs);
+}
+
+/* marchingCubes (Mesher.cu:322-425) for one cube into rec[90]. */
+static void mesh_cube(const orc_mesh_dims* m, const float* sdf, int x, int y, int z, int type, float* rec) {
+  const uint64_t row = AQ_MC_TRIANGLES[type];
+  const float hm = m->h_mesh;
+  const float bx = (float)(x - 1) * hm, by = (float)(y - 1) * hm, bz = (float)(z - 1) * hm;
+  for (int i = 0; i < 15; ++i) {
+    float* out = rec + 6 * i;
+    const int e = aq_mc_entry(row, i);
+    if (e < 0) {
+      for (int k = 0; k < 6; ++k) out[k] = 0;
+      continue;
+    }
+    const int* ca = AQ_MC_VERTEX[AQ_MC_EDGE[e][0]];
+    const int* cb = AQ_MC_VERTEX[AQ_MC_EDGE[e][1]];
+    const float sa = mesh_vertex_sdf(m, sdf, ca[0] + x, ca[1] + y, ca[2] + z);
+    const float sb = mesh_vertex_sdf(m, sdf, cb[0] + x, cb[1] + y, cb[2] + z);
+    const float f = -sa / (sb - sa);
+    const float g = 1.f - f;
+    const float px = bx + ((float)ca[0] * g + (float)cb[0] * f) * hm;
+    const float py = by + ((float)ca[1] * g + (float)cb[1] * f) * hm;
+    const float pz = bz + ((float)ca[2] * g + (float)cb[2] * f) * hm;
+    const float d = hm / 2;
+    const float l = mesh_point_sdf(m, sdf, px + -d, py, pz), r = mesh_point_sdf(m, sdf, px + d, py, pz);
+    const float u = mesh_point_sdf(m, sdf, px, py + d, pz), dn = mesh_point_sdf(m, sdf, px, py + -d, pz);
+    const float fr = mesh_point_sdf(m, sdf, px, py, pz + d), bk = mesh_point_sdf(m, sdf, px, py, pz + -d);
+    const float nx = r - l, ny = u - dn, nz = fr - bk;
+    const float inv = 1.f / sqrtf(nx * nx + ny * ny + nz * nz);
+    out[0] = px; out[1] = py; out[2] = pz;
+    out[3] = nx * inv; out[4] = ny * inv; out[5] = nz * inv;
+  }
+}
+
+int orc_mesh(orc_fluid* o, float* sdf_out, float* records, long long capacity, int* cubes) {
+  orc_mesh_dims m;
+  orc_mesh_dims_of(o, &m);
+  const size_t SCn = (size_t)m.sdf[0] * m.sdf[1] * m.sdf[2];
+  float* sdf = (float*)malloc(sizeof(float) * SCn);
+  if (!sdf) return 1;
+  mesh_sdf(o, &m, sdf);
+  const int MX = m.mesh[0], MY = m.mesh[1], MZ = m.mesh[2];
+  const int VY = MY + 1, VZ = MZ + 1;
+  const size_t NV = (size_t)(MX + 1) * VY * VZ;
+  float* vv = (float*)malloc(sizeof(float) * NV);
+  if (!vv) { free(sdf); return 1; }
+#pragma omp parallel for schedule(static)
+  for (long long idx = 0; idx < (long long)NV; ++idx) {
+    const int x = (int)(idx / ((long long)VY * VZ)), y = (int)((idx / VZ) % VY), z = (int)(idx % VZ);
+    vv[idx] = mesh_vertex_sdf(&m, sdf, x, y, z);
+  }
+  long long count = 0;
+  for (int x = 0; x < MX; ++x)
+    for (int y = 0; y < MY; ++y)
+      for (int z = 0; z < MZ; ++z) {
+        int type = 0;
+        for (int v = 0; v < 8; ++v) {
+          const int* c = AQ_MC_VERTEX[v];
+          if (vv[((size_t)(x + c[0]) * VY + (y + c[1])) * VZ + (z + c[2])] < 0) type |= 1 << v;
+        }
+        if (type == 0 || type == 255) continue; /* rows without triangles */
+        if (records && count < capacity) mesh_cube(&m, sdf, x, y, z, type, records + 90 * (size_t)count);
+        ++count;
+      }
+  if (cubes) *cubes = (int)count;
+  if (sdf_out) memcpy(sdf_out, sdf, sizeof(float) * SCn);
+  free(vv);
+  free(sdf);
+  return 0;
 }
 
 /* performSpatialHashing2 (Fluid_3D_common.cuh:27-56): calcHashImpl

@@ -65,6 +65,23 @@ void orc_ink_advance(orc_fluid* o);
 void orc_ink_get(const orc_fluid* o, float* pos, float* vel);
 void orc_ink_set(orc_fluid* o, const float* pos, const float* vel);
 
+/* Surface mesher (Rendering/Renderer3D/Mesher.cuh:20-178, Mesher.cu:321-630)
+ * on the current particles in their array order.  Grid sizes as Fluid::init
+ * builds the Mesher: SDF cell h/2 and sdf[k] = 3 + size_k * h / (h/2) cells,
+ * a 128^3 marching-cubes grid of cell size_x * h / 126. */
+typedef struct {
+  int sdf[3], mesh[3];
+  float h_sdf, h_mesh, radius;
+} orc_mesh_dims;
+void orc_mesh_dims_of(const orc_fluid* o, orc_mesh_dims* m);
+/* sdf_out ([sdf x][y][z], z fastest) and records ([capacity][15][6]) may be
+ * NULL; cubes receives the occupied-cube count (records past capacity are
+ * dropped).  Returns 0, or 1 when out of memory. */
+int orc_mesh(orc_fluid* o, float* sdf_out, float* records, long long capacity, int* cubes);
+/* The mesher's model of the texture unit's linear filter on a [w][h][d]
+ * field (z fastest) at coords ([n][3], x y z). */
+void orc_tex_linear(const float* field, int w, int h, int d, const float* coords, float* out, int n);
+
 #ifdef __cplusplus
 }
 #endif

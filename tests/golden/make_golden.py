@@ -19,6 +19,14 @@ reference's own state (teacher forcing).  It also records:
     advance that would end each step, with the grids it read.
 
     python tests/golden/make_golden.py --out tests/golden --only ink
+  * the surface mesher (ref_mesh.npz, texture_linear_probe.npz), through the
+    reference's own Mesher (oracle/_ref/libaqmesh.so) on the particles of the
+    recorded FLIP fixtures after their last sort: the SDF grid, the occupied
+    cube count and aggregates of all cube records, and a sample of records;
+    and what the SDF's texture settings (linear filter, border in x) return
+    at chosen coordinates of a random field.
+
+    python tests/golden/make_golden.py --out tests/golden --only mesh
 """
 from __future__ import annotations
 
@@ -37,8 +45,9 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
 
 from aquarius_b200 import _abi  # noqa: E402
-from oracle_binding import RefFluid, probe_texture  # noqa: E402
+from oracle_binding import RefFluid, RefMesher, probe_linear, probe_texture  # noqa: E402
 from scenes import SCENES, rel_l2  # noqa: E402
+from mesh_check import canonical_records, record_aggregates  # noqa: E402
 
 STAGE_FIELDS = {
     1: ["position", "velocity_p", "fractions"],
@@ -190,6 +199,47 @@ def record_ink() -> dict:
     return out
 
 
+MESH_SCENES = {"cfg1_16": "s1/k2/position", "aniso": "s0/k2/position"}
+MESH_SAMPLE = 1024
+
+
+def record_mesh() -> dict:
+    out = {}
+    for name, key in MESH_SCENES.items():
+        fx = np.load(HERE / f"ref_{name}.npz")
+        cfg = SCENES[name]()
+        pos = fx[key]
+        h = float(np.float32(cfg.domain_size) / np.float32(cfg.size_y))  # Fluid_3D_FLIP.cu:444
+        m = RefMesher((cfg.size_x, cfg.size_y, cfg.size_z), h, pos.shape[1])
+        r = m.mesh(pos)
+        recs = canonical_records(r["records"])
+        idx = np.unique(np.linspace(0, len(recs) - 1, MESH_SAMPLE).astype(np.int64))
+        out[f"{name}/input"] = np.array(key)
+        out[f"{name}/sdf_size"] = np.array(m.sdf_size)
+        out[f"{name}/mesh_size"] = np.array(m.mesh_size)
+        out[f"{name}/cell"] = np.array([m.h_sdf, m.h_mesh], np.float32)
+        out[f"{name}/sdf"] = r["sdf"]
+        out[f"{name}/cubes"] = np.int64(r["cubes"])
+        for k, v in record_aggregates(r["records"]).items():
+            out[f"{name}/agg/{k}"] = np.asarray(v)
+        out[f"{name}/sample"] = recs[idx]
+        m.close()
+        print(name, "mesh:", r["cubes"], "cubes, sdf", m.sdf_size)
+    return out
+
+
+def record_linear_probe() -> dict:
+    rng = np.random.default_rng(11)
+    w, h, d = 7, 6, 5
+    vals = rng.uniform(-1, 1, (d, h, w)).astype(np.float32)
+    rnd = np.stack([rng.uniform(-1.5, w + 1.5, 3000), rng.uniform(-1.5, h + 1.5, 3000),
+                    rng.uniform(-1.5, d + 1.5, 3000)], 1)
+    t = 1.0 + np.arange(2048) / 2048.0  # x fractions at 1/2048 steps: pins the weight quantisation
+    sweep = np.stack([t, np.full_like(t, 2.5), np.full_like(t, 2.5)], 1)
+    coords = np.concatenate([rnd, sweep]).astype(np.float32)
+    return {"values": vals, "coords": coords, "out": probe_linear(vals, coords)}
+
+
 def texture_probe() -> dict:
     w, h, d = 6, 5, 4
     coords = [(2, -1, 2), (2, h, 2), (2, 2, -1), (2, 2, d), (-1, 2, 2), (w, 2, 2), (2, h - 1, 2), (2, 0, 2),
@@ -218,13 +268,18 @@ def texture_probe() -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
-    ap.add_argument("--only", choices=["all", "ink"], default="all")
+    ap.add_argument("--only", choices=["all", "ink", "mesh"], default="all")
     a = ap.parse_args()
     out = pathlib.Path(a.out)
     out.mkdir(parents=True, exist_ok=True)
-    np.savez_compressed(out / "ref_ink.npz", **record_ink())
-    print("ink fixtures recorded")
-    if a.only == "ink":
+    if a.only in ("all", "mesh"):
+        np.savez_compressed(out / "texture_linear_probe.npz", **record_linear_probe())
+        np.savez_compressed(out / "ref_mesh.npz", **record_mesh())
+        print("mesh fixtures recorded")
+    if a.only in ("all", "ink"):
+        np.savez_compressed(out / "ref_ink.npz", **record_ink())
+        print("ink fixtures recorded")
+    if a.only != "all":
         return
     probe = texture_probe()
     (out / "texture_probe.json").write_text(json.dumps(probe, indent=1))

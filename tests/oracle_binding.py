@@ -3,6 +3,8 @@
 * ``Oracle``: the CPU restatement, oracle/liborc.so (flip_oracle.c).
 * ``RefFluid``: the reference's own kernels built headless, oracle/_ref/libaqref.so
   (needs a GPU; present only where oracle/Makefile's ``ref`` target was built).
+* ``RefMesher``: the reference's own surface mesher, oracle/_ref/libaqmesh.so
+  (target ``mesh``; needs a GPU).
 """
 from __future__ import annotations
 
@@ -18,9 +20,11 @@ from aquarius_b200 import _abi
 ROOT = pathlib.Path(__file__).resolve().parent.parent
 ORACLE_SO = ROOT / "oracle" / "liborc.so"
 REF_SO = ROOT / "oracle" / "_ref" / "libaqref.so"
+MESH_SO = ROOT / "oracle" / "_ref" / "libaqmesh.so"
 
 _orc = None
 _ref = None
+_mesh = None
 
 
 def _load_oracle():
@@ -54,6 +58,10 @@ def _load_oracle():
         lib.orc_ink_advance.argtypes = [ct.c_void_p]
         lib.orc_ink_get.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p]
         lib.orc_ink_set.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p]
+        lib.orc_mesh_dims_of.argtypes = [ct.c_void_p, ct.c_void_p]
+        lib.orc_tex_linear.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int]
+        lib.orc_mesh.restype = ct.c_int
+        lib.orc_mesh.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_longlong, ct.POINTER(ct.c_int)]
         _orc = lib
     return _orc
 
@@ -94,6 +102,93 @@ def _load_ref():
 
 def ref_available() -> bool:
     return REF_SO.exists()
+
+
+def mesh_ref_available() -> bool:
+    return MESH_SO.exists()
+
+
+def _load_mesh():
+    global _mesh
+    if _mesh is None:
+        if not MESH_SO.exists():
+            raise FileNotFoundError(str(MESH_SO))
+        lib = ct.CDLL(str(MESH_SO))
+        lib.aqmesh_create.restype = ct.c_void_p
+        lib.aqmesh_create.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_float, ct.c_int]
+        lib.aqmesh_destroy.argtypes = [ct.c_void_p]
+        lib.aqmesh_sizes.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]
+        lib.aqmesh_run.restype = ct.c_int
+        lib.aqmesh_run.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_longlong, ct.POINTER(ct.c_int),
+                                   ct.c_void_p, ct.c_void_p]
+        lib.aqmesh_probe_linear.restype = ct.c_int
+        lib.aqmesh_probe_linear.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                            ct.c_int]
+        lib.aqmesh_error.restype = ct.c_int
+        _mesh = lib
+    return _mesh
+
+
+class RefMesher:
+    """The reference's Mesher (Rendering/Renderer3D/Mesher.cu) on the GPU,
+    built as Fluid::init builds it for an sx*sy*sz grid of cell size h."""
+
+    def __init__(self, size, h: float, n: int):
+        self.lib = _load_mesh()
+        self.n = n
+        self.h = self.lib.aqmesh_create(size[0], size[1], size[2], h, n)
+        if not self.h:
+            raise RuntimeError(f"reference mesher init failed: {self.lib.aqmesh_error()}")
+        sdf = (ct.c_int * 3)()
+        mesh = (ct.c_int * 3)()
+        cell = (ct.c_float * 2)()
+        self.lib.aqmesh_sizes(self.h, sdf, mesh, cell)
+        self.sdf_size = tuple(sdf)
+        self.mesh_size = tuple(mesh)
+        self.h_sdf, self.h_mesh = cell[0], cell[1]
+
+    def mesh(self, position: np.ndarray, capacity_cubes: int = 1 << 18, want_sdf=True, want_order=False) -> dict:
+        pos = np.ascontiguousarray(position, np.float32).reshape(3, self.n)
+        out = np.zeros(capacity_cubes * 90, np.float32)
+        cubes = ct.c_int()
+        sx, sy, sz = self.sdf_size
+        sdf = np.zeros(sx * sy * sz, np.float32) if want_sdf else None
+        after = np.zeros((3, self.n), np.float32) if want_order else None
+        rc = self.lib.aqmesh_run(self.h, pos.ctypes.data, out.ctypes.data, out.size, ct.byref(cubes),
+                                 None if sdf is None else sdf.ctypes.data, None if after is None else after.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"reference mesh failed: {rc}")
+        res = {"cubes": cubes.value, "records": out[: cubes.value * 90].reshape(-1, 15, 6)}
+        if sdf is not None:
+            res["sdf"] = sdf.reshape(sz, sy, sx)  # x fastest
+        if after is not None:
+            res["position_after"] = after
+        return res
+
+    def close(self):
+        if self.h:
+            self.lib.aqmesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def probe_linear(values: np.ndarray, coords) -> np.ndarray:
+    """Reads a [d, h, w] float field through the reference's linear-filtered,
+    x-border texture (the mesher's SDF settings) at coords ([k, 3], x y z)."""
+    lib = _load_mesh()
+    v = np.ascontiguousarray(values, np.float32)
+    d, h, w = v.shape
+    c = np.ascontiguousarray(np.asarray(coords, dtype=np.float32))
+    out = np.zeros(len(c), np.float32)
+    rc = lib.aqmesh_probe_linear(w, h, d, v.ctypes.data, c.ctypes.data, out.ctypes.data, len(c))
+    if rc != 0:
+        raise RuntimeError(f"probe failed {rc}")
+    return out
 
 
 class _InkIO:
@@ -176,6 +271,25 @@ class Oracle(_StateIO):
 
     def pressure_residual(self) -> float:
         return self.lib.orc_pressure_residual(self.h)
+
+    def mesh_dims(self) -> dict:
+        buf = (ct.c_byte * 64)()  # orc_mesh_dims: int sdf[3], mesh[3]; float h_sdf, h_mesh, radius
+        self.lib.orc_mesh_dims_of(self.h, buf)
+        ints = np.frombuffer(bytes(buf)[:24], np.int32)
+        fl = np.frombuffer(bytes(buf)[24:36], np.float32)
+        return {"sdf": tuple(int(v) for v in ints[:3]), "mesh": tuple(int(v) for v in ints[3:6]),
+                "h_sdf": float(fl[0]), "h_mesh": float(fl[1]), "radius": float(fl[2])}
+
+    def mesh(self) -> dict:
+        """SDF grid ([x][y][z]) and the occupied-cube records ([k, 15, 6])."""
+        d = self.mesh_dims()
+        cubes = ct.c_int()
+        self.lib.orc_mesh(self.h, None, None, 0, ct.byref(cubes))
+        sdf = np.zeros(d["sdf"], np.float32)
+        rec = np.zeros((max(cubes.value, 1), 15, 6), np.float32)
+        if self.lib.orc_mesh(self.h, sdf.ctypes.data, rec.ctypes.data, cubes.value, ct.byref(cubes)) != 0:
+            raise MemoryError("oracle mesh")
+        return {"sdf": sdf, "records": rec[: cubes.value], "cubes": cubes.value, "dims": d}
 
     def enable_ink(self) -> int:
         self.n_ink = self.lib.orc_ink_create(self.h)
@@ -274,3 +388,15 @@ def probe_texture(w, h, d, coords) -> np.ndarray:
 
 def oracle_threads() -> int:
     return _load_oracle().orc_threads()
+
+
+def oracle_tex_linear(values: np.ndarray, coords) -> np.ndarray:
+    """The oracle's model of the linear-filtered, x-border texture on a
+    [d, h, w] field (as probe_linear takes it) at coords ([k, 3], x y z)."""
+    lib = _load_oracle()
+    v = np.ascontiguousarray(np.asarray(values, np.float32).transpose(2, 1, 0))  # -> [w][h][d], z fastest
+    w, h, d = v.shape
+    c = np.ascontiguousarray(np.asarray(coords, dtype=np.float32))
+    out = np.zeros(len(c), np.float32)
+    lib.orc_tex_linear(v.ctypes.data, w, h, d, c.ctypes.data, out.ctypes.data, len(c))
+    return out

@@ -37,6 +37,7 @@ def test_struct_sizes_match_c(built_library):
     assert ct.sizeof(_abi.Volume) == 4 * 12
     assert _abi.Config.stream.offset % 8 == 0
     assert ct.sizeof(_abi.HostState) == 8 * 3 + 8 * 17
+    assert ct.sizeof(_abi.MeshInfo) == 4 * 9
 
 
 def test_config_default_matches_reference(built_library):

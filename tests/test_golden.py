@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from golden_check import FLOAT_TOL, GOLDEN, INK_SCENES, judge, load, load_ink, replay, replay_ink, replay_special
-from oracle_binding import Oracle
+from oracle_binding import Oracle, oracle_tex_linear
 
 SCENES_STEPS = [("cfg1_16", 2), ("aniso", 1), ("multi_16", 1)]
 
@@ -75,3 +75,65 @@ def test_oracle_ink_against_reference_fixtures(scene):
     assert len(res["steps"]) >= 2
     for s, ep, ev in res["steps"]:
         assert ep <= FLOAT_TOL and ev <= FLOAT_TOL, (s, ep, ev)
+
+
+def test_texture_filter_model_against_reference_probe():
+    """The mesher samples its SDF through the texture unit (linear filter,
+    x border).  Along one axis the weight is the fraction rounded half up to
+    1/256, exactly; in 3D the oracle's model of the per-texel weight rounding
+    reproduces the probe for most samples."""
+    p = np.load(GOLDEN / "texture_linear_probe.npz")
+    vals, coords, out = p["values"], p["coords"].astype(np.float64), p["out"]
+    sweep = coords[:, 1] == 2.5
+    sweep &= coords[:, 2] == 2.5
+    x = coords[sweep, 0] - 0.5
+    i = np.floor(x).astype(int)
+    a = np.floor((x - i) * 256 + 0.5) / 256
+    row = vals[2, 2].astype(np.float64)
+    pred = (1 - a) * row[i] + a * row[np.minimum(i + 1, row.size - 1)]
+    assert np.abs(pred - out[sweep]).max() < 1e-6
+    got = oracle_tex_linear(vals, coords)
+    err = np.abs(got - out)
+    assert (err <= 1e-6).mean() >= 0.9
+    assert err.max() <= 0.02
+
+
+MESH_SCENES = [("cfg1_16", "ref_cfg1_16"), ("aniso", "ref_aniso")]
+
+
+@pytest.mark.parametrize("scene,fixture", MESH_SCENES)
+def test_oracle_mesh_against_reference_fixtures(scene, fixture):
+    """Surface mesher (the reference's Mesher run on the recorded particles):
+    the SDF within float rounding, the same occupied cubes, and the sampled
+    records matched vertex by vertex (the texture unit's weights are only
+    modelled, so a few vertices move by up to a tenth of a mesh cell)."""
+    from mesh_check import match_records, record_aggregates, used_slots
+    from scenes import SCENES, rel_l2
+
+    mz = np.load(GOLDEN / "ref_mesh.npz")
+    pos = np.load(GOLDEN / f"{fixture}.npz")[str(mz[f"{scene}/input"])]
+    o = Oracle(SCENES[scene]())
+    o.set_state({"position": pos})
+    r = o.mesh()
+    d = r["dims"]
+    assert tuple(mz[f"{scene}/sdf_size"]) == d["sdf"] and tuple(mz[f"{scene}/mesh_size"]) == d["mesh"]
+    assert np.allclose(mz[f"{scene}/cell"], [d["h_sdf"], d["h_mesh"]], rtol=0, atol=0)
+    ref_sdf = mz[f"{scene}/sdf"].transpose(2, 1, 0)
+    assert rel_l2(r["sdf"], ref_sdf) <= 1e-5
+    assert np.abs(r["sdf"] - ref_sdf).max() <= 1e-4 * d["h_sdf"]
+    cubes = int(mz[f"{scene}/cubes"])
+    assert abs(r["cubes"] - cubes) <= 5e-4 * cubes
+    agg = record_aggregates(r["records"])
+    assert abs(agg["vertices"] - int(mz[f"{scene}/agg/vertices"])) <= 5e-4 * agg["vertices"]
+    sample = mz[f"{scene}/sample"]
+    pairs, un_a, _ = match_records(sample, r["records"], 0.25 * d["h_mesh"])
+    assert len(pairs) >= 0.99 * len(sample)
+    ra, rb = sample[pairs[:, 0]], r["records"][pairs[:, 1]]
+    u = used_slots(ra)
+    dp = np.abs(ra[..., :3] - rb[..., :3]).max(-1)[u] / d["h_mesh"]
+    assert np.percentile(dp, 50) <= 1e-4 and np.percentile(dp, 99) <= 0.02 and dp.max() <= 0.1
+    # Normals are central differences of the filtered SDF half a mesh cell
+    # apart; where the SDF is flat (inside the fluid, on the mesh grid's
+    # clipping faces) they follow the filter's rounding and may point anywhere.
+    dn = np.abs(ra[..., 3:] - rb[..., 3:]).max(-1)[u]
+    assert (dn <= 0.05).mean() >= 0.95
