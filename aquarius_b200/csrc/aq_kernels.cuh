@@ -35,8 +35,9 @@ struct MeshDims {
 };
 cudaError_t launch_sdf_keys(cudaStream_t st, const MeshDims& m, const float* px, const float* py, const float* pz,
                             int* skey, int* scount, int n);
-cudaError_t launch_sdf_scatter(cudaStream_t st, const Dims& d, const float* px, const float* py, const float* pz,
-                               const int* off, const int* skey, const int* soff, float4* spos, int* bad, int n);
+cudaError_t launch_sdf_scatter(cudaStream_t st, const MeshDims& m, const Dims& d, const float* px, const float* py,
+                               const float* pz, const int* off, const int* skey, const int* soff, float4* spos,
+                               int* bad, int n);
 cudaError_t launch_sdf(cudaStream_t st, const MeshDims& m, const int* soff, const float4* spos,
                        cudaSurfaceObject_t surf);
 cudaError_t launch_mc_vertices(cudaStream_t st, const MeshDims& m, cudaTextureObject_t tex, float* vv);

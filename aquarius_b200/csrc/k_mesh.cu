@@ -56,8 +56,9 @@ __global__ void __launch_bounds__(256) k_sdf_keys(MeshDims m, const float* __res
 // Stable placement: the rank of particle i among the particles of its fluid
 // cell segment [off[c], off[c+1]) that share its SDF key and precede it.
 // Particles must be sorted by fluid cell (as every step leaves them); a
-// particle outside its cell's segment sets *bad and is not placed.
-__global__ void __launch_bounds__(256) k_sdf_scatter(Dims d, const float* __restrict__ px,
+// particle outside its cell's segment sets *bad and is not placed.  The
+// placed float4 carries the particle's hash z in w.
+__global__ void __launch_bounds__(256) k_sdf_scatter(MeshDims m, Dims d, const float* __restrict__ px,
                                                     const float* __restrict__ py, const float* __restrict__ pz,
                                                     const int* __restrict__ off, const int* __restrict__ skey,
                                                     const int* __restrict__ soff, float4* __restrict__ spos,
@@ -82,7 +83,7 @@ __global__ void __launch_bounds__(256) k_sdf_scatter(Dims d, const float* __rest
     atomicOr(bad, 1);
     return;
   }
-  spos[soff[k] + rank] = make_float4(x, y, z, 0.f);
+  spos[soff[k] + rank] = make_float4(x, y, z, __int_as_float(k % m.HZ));
 }
 
 // dunfanKernel (Fluid/WeightKernels.cuh:183-189), rounded as written.
@@ -94,49 +95,71 @@ __device__ __forceinline__ float dunfan(float rx, float ry, float rz, float supp
   return fmaxf(0.f, __fmul_rn(__fmul_rn(t, t), t));
 }
 
-// computeSDF (Mesher.cuh:20-84): one thread per SDF cell, z fastest.  Hash
-// cells x-3..x, y-3..y, z-3..z in the reference's loop order; those outside
-// the hash grid are skipped (the reference reaches them only through its
-// flat index, whose far cells carry zero weight).
+// computeSDF (Mesher.cuh:20-84).  A thread computes ZT consecutive SDF cells
+// along z: for each (a, b) hash row it walks the particles of the union of
+// their hash-cell windows once (contiguous in SDF order) and adds each
+// particle to the cells whose window holds its hash cell, so every cell sums
+// its particles in the reference's order (rows a, b, then c, then particle).
+// Hash cells outside the hash grid are skipped (the reference reaches them
+// only through its flat index, whose far cells carry zero weight).
+template <int ZT>
 __global__ void __launch_bounds__(256) k_sdf(MeshDims m, const int* __restrict__ soff,
                                             const float4* __restrict__ spos, cudaSurfaceObject_t surf) {
+  const int nzq = (m.SZ + ZT - 1) / ZT;
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long total = (long long)m.SX * m.SY * m.SZ;
-  if (idx >= total) return;
-  const int z = (int)(idx % m.SZ);
-  const int y = (int)((idx / m.SZ) % m.SY);
-  const int x = (int)(idx / ((long long)m.SY * m.SZ));
-  const float cx = __fmul_rn((float)(x - 1), m.hs), cy = __fmul_rn((float)(y - 1), m.hs),
-              cz = __fmul_rn((float)(z - 1), m.hs);
+  if (idx >= (long long)m.SX * m.SY * nzq) return;
+  const int zq = (int)(idx % nzq);
+  const int y = (int)((idx / nzq) % m.SY);
+  const int x = (int)(idx / ((long long)m.SY * nzq));
+  const int z0 = zq * ZT;
+  const float cx = __fmul_rn((float)(x - 1), m.hs), cy = __fmul_rn((float)(y - 1), m.hs);
+  float cz[ZT];
+#pragma unroll
+  for (int k = 0; k < ZT; ++k) cz[k] = __fmul_rn((float)(z0 + k - 1), m.hs);
   const float R = __fmul_rn(m.hs, 2.f);
-  float sw = 0.f, sx = 0.f, sy = 0.f, sz = 0.f;
+  float sw[ZT], sx[ZT], sy[ZT], sz[ZT];
+#pragma unroll
+  for (int k = 0; k < ZT; ++k) sw[k] = sx[k] = sy[k] = sz[k] = 0.f;
   const int a0 = max(x - 3, 0), a1 = min(x, m.HX - 1);
   const int b0 = max(y - 3, 0), b1 = min(y, m.HY - 1);
-  const int c0 = max(z - 3, 0), c1 = min(z, m.HZ - 1);
-  for (int a = a0; a <= a1; ++a)
-    for (int b = b0; b <= b1; ++b) {
-      const int row = (a * m.HY + b) * m.HZ;
-      for (int c = c0; c <= c1; ++c) {
-        const int j0 = __ldg(soff + row + c), j1 = __ldg(soff + row + c + 1);
+  const int c0 = max(z0 - 3, 0), c1 = min(z0 + ZT - 1, m.HZ - 1);
+  if (c0 <= c1) {
+    for (int a = a0; a <= a1; ++a)
+      for (int b = b0; b <= b1; ++b) {
+        const int row = (a * m.HY + b) * m.HZ;
+        const int j0 = __ldg(soff + row + c0), j1 = __ldg(soff + row + c1 + 1);
         for (int j = j0; j < j1; ++j) {
           const float4 p = __ldg(spos + j);
-          const float w = dunfan(__fsub_rn(p.x, cx), __fsub_rn(p.y, cy), __fsub_rn(p.z, cz), R);
-          sw = __fadd_rn(sw, w);
-          sx = __fadd_rn(sx, __fmul_rn(w, p.x));
-          sy = __fadd_rn(sy, __fmul_rn(w, p.y));
-          sz = __fadd_rn(sz, __fmul_rn(w, p.z));
+          const int c = __float_as_int(p.w);  // the particle's hash z
+          const float rx = __fsub_rn(p.x, cx), ry = __fsub_rn(p.y, cy);
+#pragma unroll
+          for (int k = 0; k < ZT; ++k) {
+            if (c < z0 + k - 3 || c > z0 + k) continue;
+            const float w = dunfan(rx, ry, __fsub_rn(p.z, cz[k]), R);
+            sw[k] = __fadd_rn(sw[k], w);
+            sx[k] = __fadd_rn(sx[k], __fmul_rn(w, p.x));
+            sy[k] = __fadd_rn(sy[k], __fmul_rn(w, p.y));
+            sz[k] = __fadd_rn(sz[k], __fmul_rn(w, p.z));
+          }
         }
       }
-    }
-  float v = m.hs;  // "set to some positive value first"
-  if (sw != 0.f) {
-    const float ex = __fsub_rn(__fdiv_rn(sx, sw), cx), ey = __fsub_rn(__fdiv_rn(sy, sw), cy),
-                ez = __fsub_rn(__fdiv_rn(sz, sw), cz);
-    v = __fsub_rn(__fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez))),
-                  m.radius);
   }
-  surf3Dwrite(v, surf, x * (int)sizeof(float), y, z);
+#pragma unroll
+  for (int k = 0; k < ZT; ++k) {
+    const int z = z0 + k;
+    if (z >= m.SZ) break;
+    float v = m.hs;  // "set to some positive value first"
+    if (sw[k] != 0.f) {
+      const float ex = __fsub_rn(__fdiv_rn(sx[k], sw[k]), cx), ey = __fsub_rn(__fdiv_rn(sy[k], sw[k]), cy),
+                  ez = __fsub_rn(__fdiv_rn(sz[k], sw[k]), cz[k]);
+      v = __fsub_rn(__fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez))),
+                    m.radius);
+    }
+    surf3Dwrite(v, surf, x * (int)sizeof(float), y, z);
+  }
 }
+
+constexpr int kSdfZ = 4;
 
 // getSDF at a world position (Mesher.cu:312-318): texture coordinate
 // 1 + position / h_sdf, filtered by the texture unit.
@@ -255,16 +278,18 @@ cudaError_t launch_sdf_keys(cudaStream_t st, const MeshDims& m, const float* px,
   return cudaGetLastError();
 }
 
-cudaError_t launch_sdf_scatter(cudaStream_t st, const Dims& d, const float* px, const float* py, const float* pz,
-                               const int* off, const int* skey, const int* soff, float4* spos, int* bad, int n) {
+cudaError_t launch_sdf_scatter(cudaStream_t st, const MeshDims& m, const Dims& d, const float* px, const float* py,
+                               const float* pz, const int* off, const int* skey, const int* soff, float4* spos,
+                               int* bad, int n) {
   if (n <= 0) return cudaSuccess;
-  k_sdf_scatter<<<blocks(n, 256), 256, 0, st>>>(d, px, py, pz, off, skey, soff, spos, bad, n);
+  k_sdf_scatter<<<blocks(n, 256), 256, 0, st>>>(m, d, px, py, pz, off, skey, soff, spos, bad, n);
   return cudaGetLastError();
 }
 
 cudaError_t launch_sdf(cudaStream_t st, const MeshDims& m, const int* soff, const float4* spos,
                        cudaSurfaceObject_t surf) {
-  k_sdf<<<blocks((long long)m.SX * m.SY * m.SZ, 256), 256, 0, st>>>(m, soff, spos, surf);
+  const long long nzq = (m.SZ + kSdfZ - 1) / kSdfZ;
+  k_sdf<kSdfZ><<<blocks((long long)m.SX * m.SY * nzq, 256), 256, 0, st>>>(m, soff, spos, surf);
   return cudaGetLastError();
 }
 

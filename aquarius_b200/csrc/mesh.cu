@@ -164,7 +164,7 @@ aq_status mesh_front(aq_fluid* f) {
   AQM_CUDA(cudaMemsetAsync(s->bad, 0, sizeof(int), st));
   AQM_CUDA(launch_sdf_keys(st, m, f->cur.px, f->cur.py, f->cur.pz, s->skey, s->scount, f->n));
   AQM_CUDA(launch_cell_scan(st, (int)s->hash_cells(), s->scount, s->soff, s->stiles));
-  AQM_CUDA(launch_sdf_scatter(st, f->d, f->cur.px, f->cur.py, f->cur.pz, f->off, s->skey, s->soff, s->spos, s->bad,
+  AQM_CUDA(launch_sdf_scatter(st, m, f->d, f->cur.px, f->cur.py, f->cur.pz, f->off, s->skey, s->soff, s->spos, s->bad,
                               f->n));
   AQM_CUDA(launch_sdf(st, m, s->soff, s->spos, s->surf));
   AQM_CUDA(launch_mc_vertices(st, m, s->tex, s->vv));

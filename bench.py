@@ -380,6 +380,7 @@ def run_ours(args, rank: int, world: int, dist):
         "jacobi_plan": {"levels": tune["plan"][0], "rows": tune["plan"][1], "x_planes": tune["plan"][2],
                         "tuned_sweep_us": tune["sweep_us"]},
     }
+    line["mesh"] = mesh_timing(f, stream)
     plain_rel = [st1["rel_residual"], pstats["rel_residual"]]
     plan = f.jacobi_plan()
     f.close()
@@ -389,6 +390,35 @@ def run_ours(args, rank: int, world: int, dist):
         line["cpu_baseline"] = cpu_baseline_sample(args.size, args.pressure_init, steps=1)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def mesh_timing(f, stream, reps: int = 10) -> dict:
+    """The surface mesher (Mesher::mesh) on the workload's particles after
+    its steps: SDF on the h/2 grid and marching cubes on the 128^3 grid into
+    a device buffer, timed with CUDA events on the fluid's stream over reps
+    calls (each call ends with a host read of the cube count)."""
+    import torch
+
+    info = f.mesh_info()
+    cap = 1 << 19
+    buf = torch.empty((cap * 90,), dtype=torch.float32, device="cuda")
+    cubes = 0
+    for _ in range(2):
+        cubes = f.mesh_into(buf.data_ptr(), cap)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(reps):
+            f.mesh_into(buf.data_ptr(), cap)
+        e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    vertices = int((buf[: cubes * 90].view(cubes, 15, 6).abs().sum(dim=2) != 0).sum().item())
+    del buf
+    return {"ms_per_mesh": ms, "cubes": cubes, "triangles": vertices // 3, "sdf_grid": list(info["sdf"]),
+            "mesh_grid": list(info["mesh"]), "reps": reps,
+            "path": "aq_fluid_mesh into a device buffer (the reference's VBO layout)"}
 
 
 def learned_arm(args, dev, stream, plain_residual: float, plain_ms: float, dist, plan) -> dict:
@@ -624,7 +654,8 @@ def run_profile_case(case: str):
     """Small, fixed cases for single-kernel ncu captures (no JSON line):
     jacobi: the 128^3 workload's system after 3 steps, 6 sweeps of the
     default plan; batch-rows: 32 scenes of the batch set, 6 batched sweeps;
-    conv: two U-Net inferences at 128^3 on seeded random inputs."""
+    conv: two U-Net inferences at 128^3 on seeded random inputs; mesh: two
+    surface meshes of the 128^3 workload after 3 steps."""
     import numpy as np
     import torch
 
@@ -643,6 +674,13 @@ def run_profile_case(case: str):
         b.set_sweep_plan(8, False)
         print(b.benchmark_pressure(6))
         b.close()
+    elif case == "mesh":
+        f = aq.Fluid(workload_config(128, "zero"))
+        f.step(3)
+        f.synchronize()
+        for _ in range(2):
+            print(len(f.download_mesh(1 << 19)))
+        f.close()
     elif case == "conv":
         net = aq.UNet(weights=ROOT / "aquarius_b200" / "weights" / "unet_128.bin")
         V = 128 ** 3
@@ -669,7 +707,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default Jacobi plan")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
-    ap.add_argument("--profile-case", choices=["jacobi", "batch-rows", "conv"], default=None,
+    ap.add_argument("--profile-case", choices=["jacobi", "batch-rows", "conv", "mesh"], default=None,
                     help="run one small fixed case for an ncu capture and exit")
     ap.add_argument("--workload", default="ball128", choices=["ball128", "batch", "multiphase256"],
                     help="ball128: the 128^3 scene; batch: 256 independent scenes of uneven sizes; "

@@ -101,17 +101,28 @@ void aqmesh_sizes(void* h, int* sdf, int* mesh, float* cell) {
 
 /* Loads particles (positions [3][n]; velocity 0, phase 0), runs mesh(), and
  * copies back: the occupied-cube count, up to `capacity` floats of the output
- * buffer, the SDF grid (x fastest, may be NULL) and the particles' positions
- * in the order mesh() left them ([3][n], may be NULL). */
+ * buffer, the SDF grid (x fastest, may be NULL), the particles' positions
+ * in the order mesh() left them ([3][n], may be NULL) and the time mesh()
+ * took between CUDA events on either side of it (may be NULL). */
 int aqmesh_run(void* h, const float* pos, float* out, long long capacity, int* cubes, float* sdf,
-               float* pos_after) {
+               float* pos_after, float* ms) {
   MeshRun* r = (MeshRun*)h;
   const int n = r->n;
   std::vector<Particle> ps(n);
   for (int i = 0; i < n; ++i) ps[i] = Particle(make_float3(pos[i], pos[n + i], pos[2 * n + i]), 0);
   aqref_record(cudaMemcpy(r->particles, ps.data(), sizeof(Particle) * n, cudaMemcpyHostToDevice), "p", __FILE__,
                __LINE__);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaDeviceSynchronize();
+  cudaEventRecord(e0);
   r->m->mesh(r->particles, r->copy, r->hashes, r->indices, r->output);
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  if (ms) cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   cudaDeviceSynchronize();
   unsigned int count = 0;
   aqref_record(cudaMemcpy(&count, r->m->occupiedCellIndex, sizeof(count), cudaMemcpyDeviceToHost), "count",

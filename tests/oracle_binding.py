@@ -120,7 +120,7 @@ def _load_mesh():
         lib.aqmesh_sizes.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]
         lib.aqmesh_run.restype = ct.c_int
         lib.aqmesh_run.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_longlong, ct.POINTER(ct.c_int),
-                                   ct.c_void_p, ct.c_void_p]
+                                   ct.c_void_p, ct.c_void_p, ct.POINTER(ct.c_float)]
         lib.aqmesh_probe_linear.restype = ct.c_int
         lib.aqmesh_probe_linear.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                             ct.c_int]
@@ -154,11 +154,14 @@ class RefMesher:
         sx, sy, sz = self.sdf_size
         sdf = np.zeros(sx * sy * sz, np.float32) if want_sdf else None
         after = np.zeros((3, self.n), np.float32) if want_order else None
+        ms = ct.c_float()
         rc = self.lib.aqmesh_run(self.h, pos.ctypes.data, out.ctypes.data, out.size, ct.byref(cubes),
-                                 None if sdf is None else sdf.ctypes.data, None if after is None else after.ctypes.data)
+                                 None if sdf is None else sdf.ctypes.data, None if after is None else after.ctypes.data,
+                                 ct.byref(ms))
         if rc != 0:
             raise RuntimeError(f"reference mesh failed: {rc}")
-        res = {"cubes": cubes.value, "records": out[: cubes.value * 90].reshape(-1, 15, 6)}
+        res = {"cubes": cubes.value, "records": out[: min(cubes.value, capacity_cubes) * 90].reshape(-1, 15, 6),
+               "ms": ms.value}
         if sdf is not None:
             res["sdf"] = sdf.reshape(sz, sy, sx)  # x fastest
         if after is not None:

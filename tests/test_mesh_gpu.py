@@ -175,3 +175,46 @@ def test_mesh_against_live_reference(scene, steps):
     u = used_slots(ra)
     dp = np.abs(ra[..., :3] - rb[..., :3]).max(-1)[u] / m.h_mesh
     assert np.percentile(dp, 99) <= 1e-3, np.percentile(dp, [50, 99, 100])
+
+
+@pytest.mark.skipif(not mesh_ref_available(), reason="reference mesher build (oracle/_ref) not present")
+def test_mesh_time_vs_reference_mesher(capsys):
+    """The 128^3 ball drop after 3 steps (5.2M particles, SDF 259^3, mesh
+    128^3) on the same GPU: ours into a device buffer (CUDA events around the
+    calls, each ending with a host read of the count) against the reference's
+    Mesher::mesh (CUDA events around the call, its own syncs included)."""
+    import bench
+    torch = pytest.importorskip("torch")
+
+    f = aq.Fluid(bench.workload_config(128, "zero"))
+    f.step(3)
+    f.synchronize()
+    pos = f.download_state(["position"])["position"]
+    cap = 1 << 19
+    buf = torch.empty((cap * 90,), dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        cubes = f.mesh_into(buf.data_ptr(), cap)
+    reps = 5
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        f.mesh_into(buf.data_ptr(), cap)
+    e1.record()
+    e1.synchronize()
+    ours = e0.elapsed_time(e1) / reps
+    del buf
+    h = float(np.float32(10.0) / np.float32(128))
+    m = RefMesher((128, 128, 128), h, pos.shape[1])
+    ref = []
+    for i in range(reps + 1):
+        r = m.mesh(pos, capacity_cubes=1, want_sdf=False)
+        if i:
+            ref.append(r["ms"])
+    m.close()
+    ref = float(np.mean(ref))
+    with capsys.disabled():
+        print(f"\nmesh 128^3 workload: ours {ours:.3f} ms/mesh, reference Mesher::mesh {ref:.3f} ms, "
+              f"cubes {cubes} vs {r['cubes']}")
+    assert abs(cubes - r["cubes"]) <= 2e-4 * r["cubes"]
+    assert ours < ref
