@@ -86,15 +86,6 @@ __global__ void __launch_bounds__(256) k_sdf_scatter(MeshDims m, Dims d, const f
   spos[soff[k] + rank] = make_float4(x, y, z, __int_as_float(k % m.HZ));
 }
 
-// dunfanKernel (Fluid/WeightKernels.cuh:183-189), rounded as written.
-__device__ __forceinline__ float dunfan(float rx, float ry, float rz, float support) {
-  const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry)), __fmul_rn(rz, rz));
-  const float h2 = __fmul_rn(support, support);
-  if (r2 > h2) return 0.f;
-  const float t = __fsub_rn(1.f, __fdiv_rn(r2, __fmul_rn(h2, 3.f)));
-  return fmaxf(0.f, __fmul_rn(__fmul_rn(t, t), t));
-}
-
 // computeSDF (Mesher.cuh:20-84).  A thread computes ZT consecutive SDF cells
 // along z: for each (a, b) hash row it walks the particles of the union of
 // their hash-cell windows once (contiguous in SDF order) and adds each
@@ -117,6 +108,7 @@ __global__ void __launch_bounds__(256) k_sdf(MeshDims m, const int* __restrict__
 #pragma unroll
   for (int k = 0; k < ZT; ++k) cz[k] = __fmul_rn((float)(z0 + k - 1), m.hs);
   const float R = __fmul_rn(m.hs, 2.f);
+  const float h2 = __fmul_rn(R, R), h2x3 = __fmul_rn(h2, 3.f);
   float sw[ZT], sx[ZT], sy[ZT], sz[ZT];
 #pragma unroll
   for (int k = 0; k < ZT; ++k) sw[k] = sx[k] = sy[k] = sz[k] = 0.f;
@@ -132,10 +124,18 @@ __global__ void __launch_bounds__(256) k_sdf(MeshDims m, const int* __restrict__
           const float4 p = __ldg(spos + j);
           const int c = __float_as_int(p.w);  // the particle's hash z
           const float rx = __fsub_rn(p.x, cx), ry = __fsub_rn(p.y, cy);
+          const float rxy = __fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry));
 #pragma unroll
           for (int k = 0; k < ZT; ++k) {
             if (c < z0 + k - 3 || c > z0 + k) continue;
-            const float w = dunfan(rx, ry, __fsub_rn(p.z, cz[k]), R);
+            // dunfanKernel (Fluid/WeightKernels.cuh:183-189), rounded as
+            // written.  Outside the support the weight is 0 and adding it
+            // (and 0 * p) leaves every sum unchanged, so those are skipped.
+            const float rz = __fsub_rn(p.z, cz[k]);
+            const float r2 = __fadd_rn(rxy, __fmul_rn(rz, rz));
+            if (r2 > h2) continue;
+            const float t = __fsub_rn(1.f, __fdiv_rn(r2, h2x3));
+            const float w = fmaxf(0.f, __fmul_rn(__fmul_rn(t, t), t));
             sw[k] = __fadd_rn(sw[k], w);
             sx[k] = __fadd_rn(sx[k], __fmul_rn(w, p.x));
             sy[k] = __fadd_rn(sy[k], __fmul_rn(w, p.y));

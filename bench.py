@@ -655,7 +655,7 @@ def run_profile_case(case: str):
     jacobi: the 128^3 workload's system after 3 steps, 6 sweeps of the
     default plan; batch-rows: 32 scenes of the batch set, 6 batched sweeps;
     conv: two U-Net inferences at 128^3 on seeded random inputs; mesh: two
-    surface meshes of the 128^3 workload after 3 steps."""
+    surface meshes of the 128^3 workload's initial particles."""
     import numpy as np
     import torch
 
@@ -676,7 +676,6 @@ def run_profile_case(case: str):
         b.close()
     elif case == "mesh":
         f = aq.Fluid(workload_config(128, "zero"))
-        f.step(3)
         f.synchronize()
         for _ in range(2):
             print(len(f.download_mesh(1 << 19)))
