@@ -266,3 +266,121 @@ def make_config(size=(50, 50, 50), volumes=None, **kw) -> Config:
         else:
             setattr(cfg, k, val)
     return cfg
+
+
+# ------------------------------------------------------------ SPH solvers
+SPH_PBF = 0
+SPH_PCISPH = 1
+
+
+class SphConfig(ct.Structure):
+    """aq_sph_config: FluidConfig + ConfigPBF / ConfigPCISPH."""
+    _fields_ = [
+        ("method", ct.c_int32),
+        ("volume_count", ct.c_int32),
+        ("volumes", Volume * AQ_MAX_VOLUMES),
+        ("gravity", ct.c_float * 3),
+        ("timestep", ct.c_float),
+        ("substeps", ct.c_int32),
+        ("iterations", ct.c_int32),
+        ("max_particle_count", ct.c_int32),
+        ("particle_jitter", ct.c_float),
+        ("stiffness", ct.c_float),
+        ("seed", ct.c_uint32),
+        ("device", ct.c_int32),
+        ("stream", ct.c_void_p),
+    ]
+
+
+class SphState(ct.Structure):
+    """aq_sph_state: planar host copies of the particle fields."""
+    _fields_ = [
+        ("particle_count", ct.c_int32),
+        ("physical_time", ct.c_double),
+        ("position", ct.c_void_p),
+        ("velocity", ct.c_void_p),
+        ("density", ct.c_void_p),
+        ("rest_density", ct.c_void_p),
+        ("last_position", ct.c_void_p),
+        ("lambda_", ct.c_void_p),
+        ("pressure", ct.c_void_p),
+        ("pressure_force", ct.c_void_p),
+        ("predicted_position", ct.c_void_p),
+        ("predicted_velocity", ct.c_void_p),
+    ]
+
+
+class SphInfo(ct.Structure):
+    _fields_ = [
+        ("particle_count", ct.c_int32),
+        ("particle_spacing", ct.c_float),
+        ("kernel_radius", ct.c_float),
+        ("grid_size", ct.c_int32 * 3),
+        ("container_size", ct.c_float),
+    ]
+
+
+# field name -> components (3: [3][n] plane, 1: [n])
+SPH_FIELDS = {
+    "position": 3, "velocity": 3, "density": 1, "rest_density": 1, "last_position": 3, "lambda": 1,
+    "pressure": 1, "pressure_force": 3, "predicted_position": 3, "predicted_velocity": 3,
+}
+
+
+def sph_config(method=SPH_PBF, volumes=None, **kw) -> SphConfig:
+    """aq_sph_config with the reference defaults for the method
+    (Fluid/FluidConfig.cuh:52-66, the default volumes and gravity),
+    overridden by keyword arguments; volumes as in make_config."""
+    c = SphConfig()
+    c.method = method
+    c.volume_count = 2
+    c.volumes[0].shape = SHAPE_SQUARE
+    c.volumes[1].shape = SHAPE_SPHERE
+    for v in (c.volumes[0], c.volumes[1]):
+        v.box_min[:] = [0.0, 0.0, 0.0]
+        v.box_max[:] = [1.0, 0.1875, 1.0]
+        v.ball_center[:] = [0.5, 0.75, 0.5]
+        v.ball_radius = 0.125
+    c.gravity[:] = [0.0, -9.8, 0.0]
+    if method == SPH_PBF:
+        c.timestep, c.substeps, c.iterations = 0.033, 4, 2
+    else:
+        c.timestep, c.substeps, c.iterations = 0.005, 1, 4
+    c.max_particle_count = 300000
+    c.particle_jitter = 0.05
+    c.stiffness = 15.0
+    c.seed = 1
+    if volumes is not None:
+        c.volume_count = len(volumes)
+        for i, vd in enumerate(volumes):
+            v = c.volumes[i]
+            v.shape = SHAPE_SPHERE if vd.get("shape") == "sphere" else SHAPE_SQUARE
+            v.box_min[:] = list(vd.get("min", (0.0, 0.0, 0.0)))
+            v.box_max[:] = list(vd.get("max", (1.0, 0.1875, 1.0)))
+            v.ball_center[:] = list(vd.get("center", (0.5, 0.75, 0.5)))
+            v.ball_radius = float(vd.get("radius", 0.125))
+    for k, val in kw.items():
+        if k == "gravity":
+            c.gravity[:] = list(val)
+        elif not hasattr(c, k):
+            raise AttributeError(k)
+        else:
+            setattr(c, k, val)
+    return c
+
+
+def make_sph_state(n: int, arrays: dict, time: float = 0.0) -> SphState:
+    st = SphState()
+    st.particle_count = n
+    st.physical_time = time
+    for name, comps in SPH_FIELDS.items():
+        a = arrays.get(name)
+        if a is not None:
+            assert a.dtype == np.float32 and a.size == comps * n and a.flags["C_CONTIGUOUS"], name
+            setattr(st, "lambda_" if name == "lambda" else name, a.ctypes.data)
+    return st
+
+
+def alloc_sph_state(n: int, fields=None) -> dict:
+    names = SPH_FIELDS.keys() if fields is None else fields
+    return {k: np.zeros((SPH_FIELDS[k], n) if SPH_FIELDS[k] == 3 else (n,), np.float32) for k in names}

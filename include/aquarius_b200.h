@@ -537,6 +537,76 @@ const char* aq_last_error(void);
 /* Library ABI version (AQ_ABI_VERSION). */
 int32_t aq_abi_version(void);
 
+/* ------------------------------------------------------------ SPH solvers
+ * The reference's two particle-only solvers, which share the FLIP path's
+ * spatial hash and stable sort: position-based fluids
+ * (Fluid_3D_PBF::Fluid, Fluid/Fluid_3D_PBF.cuh:49-133, Fluid_3D_PBF.cu)
+ * and predictive-corrective SPH (Fluid_3D_PCISPH::Fluid,
+ * Fluid/Fluid_3D_PCISPH.cuh:47-124, Fluid_3D_PCISPH.cu).  Both run in the
+ * reference's fixed 10 x 10 x 10 container (gridPhysicalSize), with a
+ * particle spacing derived from max_particle_count and a hash grid of cell
+ * = kernel radius.  aq_sph_create = make_shared<Fluid>() + init(config)
+ * (main.cu:158-170); aq_sph_step = simulationStep(). */
+typedef enum aq_sph_method { AQ_SPH_PBF = 0, AQ_SPH_PCISPH = 1 } aq_sph_method;
+
+/* FluidConfig + ConfigPBF / ConfigPCISPH (Fluid/FluidConfig.cuh:52-66). */
+typedef struct aq_sph_config {
+  int32_t method;              /* aq_sph_method */
+  int32_t volume_count;
+  aq_volume volumes[AQ_MAX_VOLUMES]; /* phase is ignored */
+  float gravity[3];
+  float timestep;              /* ConfigPBF 0.033 / ConfigPCISPH 0.005 */
+  int32_t substeps;            /* 4 / 1 */
+  int32_t iterations;          /* 2 / 4 */
+  int32_t max_particle_count;  /* 3e5 / 3e5: sets the particle spacing */
+  float particle_jitter;       /* PBF only, 0.05 */
+  float stiffness;             /* PCISPH only, 15 (read but unused by the reference) */
+  uint32_t seed;               /* glibc rand() seed of the seeding jitter (reference: 1) */
+  int32_t device;
+  void* stream;                /* cudaStream_t; NULL = library-owned stream */
+} aq_sph_config;
+
+/* Reference defaults for the method, with the default volumes and gravity. */
+aq_status aq_sph_config_default(int32_t method, aq_sph_config* cfg);
+
+/* Host copy of the particle state, [3][n] planes or [n]; any pointer may be
+ * NULL.  The reference's Particle structs (Fluid/Fluid_3D_PBF.cuh:23-44,
+ * Fluid/Fluid_3D_PCISPH.cuh:20-45) in planar form. */
+typedef struct aq_sph_state {
+  int32_t particle_count;       /* must match */
+  double physical_time;
+  float* position;              /* [3][n] */
+  float* velocity;              /* [3][n] velosity */
+  float* density;               /* [n] */
+  float* rest_density;          /* [n] restDensity */
+  float* last_position;         /* [3][n] PBF lastPosition */
+  float* lambda;                /* [n]    PBF */
+  float* pressure;              /* [n]    PCISPH */
+  float* pressure_force;        /* [3][n] PCISPH pressureForces */
+  float* predicted_position;    /* [3][n] PCISPH predictedPosition */
+  float* predicted_velocity;    /* [3][n] PCISPH predictedVelocity */
+} aq_sph_state;
+
+typedef struct aq_sph_info {
+  int32_t particle_count;
+  float particle_spacing;       /* particleSpacing */
+  float kernel_radius;          /* kernelRadius = spacing * 2.01 (PBF) / 2 (PCISPH) */
+  int32_t grid_size[3];         /* hash grid, ceil(10 / kernelRadius) per axis */
+  float container_size;         /* gridPhysicalSize, 10 */
+} aq_sph_info;
+
+typedef struct aq_sph aq_sph;
+
+aq_status aq_sph_create(const aq_sph_config* cfg, aq_sph** out);
+void aq_sph_destroy(aq_sph* s);
+aq_status aq_sph_info_get(const aq_sph* s, aq_sph_info* info);
+aq_status aq_sph_step(aq_sph* s, int32_t nsteps);
+aq_status aq_sph_synchronize(aq_sph* s);
+aq_status aq_sph_download_state(aq_sph* s, aq_sph_state* st);
+/* Replaces fields; positions are kept in the container.  Uploaded particles
+ * need not be sorted: every step starts with the spatial hash. */
+aq_status aq_sph_upload_state(aq_sph* s, const aq_sph_state* st);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,11 @@ reference's own state (teacher forcing).  It also records:
     at chosen coordinates of a random field.
 
     python tests/golden/make_golden.py --out tests/golden --only mesh
+  * the particle-only solvers (ref_sph.npz), through the reference's own
+    Fluid_3D_PBF / Fluid_3D_PCISPH (oracle/_ref/libaqsph.so) on small
+    seeded configs: the state after init and after each of three steps.
+
+    python tests/golden/make_golden.py --out tests/golden --only sph
 """
 from __future__ import annotations
 
@@ -45,7 +50,7 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
 
 from aquarius_b200 import _abi  # noqa: E402
-from oracle_binding import RefFluid, RefMesher, probe_linear, probe_texture  # noqa: E402
+from oracle_binding import RefFluid, RefMesher, RefSph, probe_linear, probe_texture  # noqa: E402
 from scenes import SCENES, rel_l2  # noqa: E402
 from mesh_check import canonical_records, record_aggregates  # noqa: E402
 
@@ -228,6 +233,34 @@ def record_mesh() -> dict:
     return out
 
 
+SPH_STEPS = 3
+
+
+def sph_scenes() -> dict:
+    """Small seeded configs of the two solvers (about 1,700 particles)."""
+    return {"pbf": _abi.sph_config(_abi.SPH_PBF, max_particle_count=8000),
+            "pcisph": _abi.sph_config(_abi.SPH_PCISPH, max_particle_count=8000)}
+
+
+def record_sph() -> dict:
+    out = {}
+    for name, cfg in sph_scenes().items():
+        ref = RefSph(cfg)
+        out[f"{name}/config"] = np.frombuffer(bytes(cfg), dtype=np.uint8).copy()
+        out[f"{name}/info"] = np.array([ref.spacing, ref.kernel_radius], np.float32)
+        out[f"{name}/grid"] = np.array(ref.grid)
+        for s in range(SPH_STEPS + 1):
+            if s:
+                ref.step(1)
+            st = ref.get_state()
+            for k, v in st.items():
+                if k != "physical_time":
+                    out[f"{name}/s{s}/{k}"] = v
+        print(name, "sph:", ref.n, "particles")
+        ref.close()
+    return out
+
+
 def record_linear_probe() -> dict:
     rng = np.random.default_rng(11)
     w, h, d = 7, 6, 5
@@ -268,7 +301,7 @@ def texture_probe() -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
-    ap.add_argument("--only", choices=["all", "ink", "mesh"], default="all")
+    ap.add_argument("--only", choices=["all", "ink", "mesh", "sph"], default="all")
     a = ap.parse_args()
     out = pathlib.Path(a.out)
     out.mkdir(parents=True, exist_ok=True)
@@ -276,6 +309,9 @@ def main():
         np.savez_compressed(out / "texture_linear_probe.npz", **record_linear_probe())
         np.savez_compressed(out / "ref_mesh.npz", **record_mesh())
         print("mesh fixtures recorded")
+    if a.only in ("all", "sph"):
+        np.savez_compressed(out / "ref_sph.npz", **record_sph())
+        print("sph fixtures recorded")
     if a.only in ("all", "ink"):
         np.savez_compressed(out / "ref_ink.npz", **record_ink())
         print("ink fixtures recorded")

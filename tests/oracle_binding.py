@@ -21,10 +21,12 @@ ROOT = pathlib.Path(__file__).resolve().parent.parent
 ORACLE_SO = ROOT / "oracle" / "liborc.so"
 REF_SO = ROOT / "oracle" / "_ref" / "libaqref.so"
 MESH_SO = ROOT / "oracle" / "_ref" / "libaqmesh.so"
+SPH_SO = ROOT / "oracle" / "_ref" / "libaqsph.so"
 
 _orc = None
 _ref = None
 _mesh = None
+_sph = None
 
 
 def _load_oracle():
@@ -59,6 +61,18 @@ def _load_oracle():
         lib.orc_ink_get.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p]
         lib.orc_ink_set.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p]
         lib.orc_mesh_dims_of.argtypes = [ct.c_void_p, ct.c_void_p]
+        lib.orc_sph_create.restype = ct.c_void_p
+        lib.orc_sph_create.argtypes = [ct.POINTER(_abi.SphConfig)]
+        lib.orc_sph_destroy.argtypes = [ct.c_void_p]
+        lib.orc_sph_count.restype = ct.c_int
+        lib.orc_sph_count.argtypes = [ct.c_void_p]
+        lib.orc_sph_info.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]
+        lib.orc_sph_step.restype = ct.c_int
+        lib.orc_sph_step.argtypes = [ct.c_void_p, ct.c_int]
+        lib.orc_sph_get.restype = ct.c_int
+        lib.orc_sph_get.argtypes = [ct.c_void_p, ct.POINTER(_abi.SphState)]
+        lib.orc_sph_set.restype = ct.c_int
+        lib.orc_sph_set.argtypes = [ct.c_void_p, ct.POINTER(_abi.SphState)]
         lib.orc_tex_linear.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int]
         lib.orc_mesh.restype = ct.c_int
         lib.orc_mesh.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_longlong, ct.POINTER(ct.c_int)]
@@ -403,3 +417,125 @@ def oracle_tex_linear(values: np.ndarray, coords) -> np.ndarray:
     out = np.zeros(len(c), np.float32)
     lib.orc_tex_linear(v.ctypes.data, w, h, d, c.ctypes.data, out.ctypes.data, len(c))
     return out
+
+
+class _SphStateIO:
+    """aq_sph_state exchange over numpy dicts, shared by the SPH checkers."""
+
+    n: int
+
+    def get_state(self, fields=None) -> dict:
+        arrs = _abi.alloc_sph_state(self.n, fields)
+        st = _abi.make_sph_state(self.n, arrs)
+        rc = self._get(ct.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"get_state failed: {rc}")
+        arrs["physical_time"] = st.physical_time
+        return arrs
+
+    def set_state(self, state: dict):
+        arrs = {k: np.ascontiguousarray(v, np.float32) for k, v in state.items() if k in _abi.SPH_FIELDS}
+        st = _abi.make_sph_state(self.n, arrs, float(state.get("physical_time", 0.0)))
+        rc = self._set(ct.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"set_state failed: {rc}")
+
+
+class SphOracle(_SphStateIO):
+    """CPU restatement of the reference's PBF / PCISPH solvers (test infrastructure)."""
+
+    def __init__(self, cfg: _abi.SphConfig):
+        self.lib = _load_oracle()
+        self.cfg = cfg
+        self.h = self.lib.orc_sph_create(ct.byref(cfg))
+        if not self.h:
+            raise ValueError("oracle rejected the config")
+        self.n = self.lib.orc_sph_count(self.h)
+        sp, kr = ct.c_float(), ct.c_float()
+        g = (ct.c_int * 3)()
+        self.lib.orc_sph_info(self.h, ct.byref(sp), ct.byref(kr), g)
+        self.spacing, self.kernel_radius, self.grid = sp.value, kr.value, tuple(g)
+
+    def _get(self, p):
+        return self.lib.orc_sph_get(self.h, p)
+
+    def _set(self, p):
+        return self.lib.orc_sph_set(self.h, p)
+
+    def step(self, n: int = 1):
+        self.lib.orc_sph_step(self.h, n)
+
+    def close(self):
+        if self.h:
+            self.lib.orc_sph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def sph_ref_available() -> bool:
+    return SPH_SO.exists()
+
+
+def _load_sph():
+    global _sph
+    if _sph is None:
+        if not SPH_SO.exists():
+            raise FileNotFoundError(str(SPH_SO))
+        lib = ct.CDLL(str(SPH_SO))
+        lib.aqsph_create.restype = ct.c_void_p
+        lib.aqsph_create.argtypes = [ct.POINTER(_abi.SphConfig)]
+        lib.aqsph_destroy.argtypes = [ct.c_void_p]
+        lib.aqsph_count.restype = ct.c_int
+        lib.aqsph_count.argtypes = [ct.c_void_p]
+        lib.aqsph_error.restype = ct.c_int
+        lib.aqsph_step.restype = ct.c_int
+        lib.aqsph_step.argtypes = [ct.c_void_p, ct.c_int]
+        lib.aqsph_get.restype = ct.c_int
+        lib.aqsph_get.argtypes = [ct.c_void_p, ct.POINTER(_abi.SphState)]
+        lib.aqsph_set.restype = ct.c_int
+        lib.aqsph_set.argtypes = [ct.c_void_p, ct.POINTER(_abi.SphState)]
+        lib.aqsph_info.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]
+        _sph = lib
+    return _sph
+
+
+class RefSph(_SphStateIO):
+    """The reference's Fluid_3D_PBF / Fluid_3D_PCISPH::Fluid on the GPU (test infrastructure)."""
+
+    def __init__(self, cfg: _abi.SphConfig):
+        self.lib = _load_sph()
+        self.h = self.lib.aqsph_create(ct.byref(cfg))
+        if not self.h:
+            raise RuntimeError(f"reference init failed: cuda error {self.lib.aqsph_error()}")
+        self.n = self.lib.aqsph_count(self.h)
+        sp, kr = ct.c_float(), ct.c_float()
+        g = (ct.c_int * 3)()
+        self.lib.aqsph_info(self.h, ct.byref(sp), ct.byref(kr), g)
+        self.spacing, self.kernel_radius, self.grid = sp.value, kr.value, tuple(g)
+
+    def _get(self, p):
+        return self.lib.aqsph_get(self.h, p)
+
+    def _set(self, p):
+        return self.lib.aqsph_set(self.h, p)
+
+    def step(self, n: int = 1):
+        rc = self.lib.aqsph_step(self.h, n)
+        if rc != 0:
+            raise RuntimeError(f"reference step failed: {rc}")
+
+    def close(self):
+        if self.h:
+            self.lib.aqsph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -137,3 +137,29 @@ def test_oracle_mesh_against_reference_fixtures(scene, fixture):
     # clipping faces) they follow the filter's rounding and may point anywhere.
     dn = np.abs(ra[..., 3:] - rb[..., 3:]).max(-1)[u]
     assert (dn <= 0.05).mean() >= 0.95
+
+
+@pytest.mark.parametrize("method", ["pbf", "pcisph"])
+def test_sph_oracle_against_reference_fixtures(method):
+    """Particle-only solvers: seeding and the init's stable sort bit for bit,
+    rest densities to float rounding, and every recorded step teacher-forced
+    from the reference's own state (judge_sph_step's bounds)."""
+    from golden_check import judge_sph_step, load_sph, sph_config_from_bytes, sph_fixture_state
+    from oracle_binding import SphOracle
+    from scenes import rel_l2
+
+    data = load_sph()
+    if data is None:
+        pytest.skip("fixture missing")
+    o = SphOracle(sph_config_from_bytes(data[f"{method}/config"]))
+    assert (o.spacing, o.kernel_radius) == tuple(float(v) for v in data[f"{method}/info"])
+    assert o.grid == tuple(int(v) for v in data[f"{method}/grid"])
+    st = o.get_state()
+    s0 = sph_fixture_state(data, method, 0)
+    assert st["position"].shape == s0["position"].shape
+    np.testing.assert_array_equal(st["position"], s0["position"])
+    assert rel_l2(st["rest_density"], s0["rest_density"]) <= 1e-6
+    for s in range(3):
+        o.set_state(sph_fixture_state(data, method, s))
+        o.step(1)
+        assert judge_sph_step(method, o.get_state(), sph_fixture_state(data, method, s + 1)) == [], s
