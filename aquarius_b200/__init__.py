@@ -127,6 +127,15 @@ def load_library() -> ct.CDLL:
         "aq_fluid_download_ink": (ct.c_int, [P, P, P]),
         "aq_fluid_upload_ink": (ct.c_int, [P, P, P]),
         "aq_fluid_ink_advance": (ct.c_int, [P]),
+        "aq_sph_config_default": (ct.c_int, [ct.c_int32, P]),
+        "aq_sph_create": (ct.c_int, [P, ct.POINTER(P)]),
+        "aq_sph_destroy": (None, [P]),
+        "aq_sph_info_get": (ct.c_int, [P, P]),
+        "aq_sph_step": (ct.c_int, [P, ct.c_int32]),
+        "aq_sph_synchronize": (ct.c_int, [P]),
+        "aq_sph_launches_per_step": (ct.c_int, [P, ct.POINTER(ct.c_int32)]),
+        "aq_sph_download_state": (ct.c_int, [P, P]),
+        "aq_sph_upload_state": (ct.c_int, [P, P]),
         "aq_fluid_mesh_info": (ct.c_int, [P, P]),
         "aq_fluid_mesh": (ct.c_int, [P, P, ct.c_int64, ct.POINTER(ct.c_int32)]),
         "aq_fluid_download_mesh": (ct.c_int, [P, P, ct.c_int64, ct.POINTER(ct.c_int32)]),
@@ -477,6 +486,70 @@ def _solve_stats_dict(s) -> dict:
             "fluid_cells": s.fluid_cells, "converged": bool(s.converged), "blocks": s.blocks,
             "total_sweeps": s.total_sweeps, "total_blocks": s.total_blocks, "warm_start": s.warm_start,
             "warm_rel_residual": s.warm_rel_residual, "zero_rel_residual": s.zero_rel_residual}
+
+
+class Sph:
+    """Fluid_3D_PBF::Fluid / Fluid_3D_PCISPH::Fluid: init(config) then
+    simulationStep() per frame (aq_sph_* in include/aquarius_b200.h)."""
+
+    PBF = _abi.SPH_PBF
+    PCISPH = _abi.SPH_PCISPH
+
+    def __init__(self, config: _abi.SphConfig):
+        self._lib = load_library()
+        self._h = ct.c_void_p()
+        self._cfg = config
+        _check(self._lib.aq_sph_create(ct.byref(config), ct.byref(self._h)))
+        info = _abi.SphInfo()
+        _check(self._lib.aq_sph_info_get(self._h, ct.byref(info)))
+        self.n = info.particle_count
+        self.particleCount = info.particle_count
+        self.spacing = info.particle_spacing
+        self.kernel_radius = info.kernel_radius
+        self.grid = tuple(info.grid_size)
+
+    @staticmethod
+    def default_config(method: int) -> _abi.SphConfig:
+        c = _abi.SphConfig()
+        _check(load_library().aq_sph_config_default(method, ct.byref(c)))
+        return c
+
+    def simulationStep(self):
+        _check(self._lib.aq_sph_step(self._h, 1))
+
+    def step(self, n: int = 1):
+        _check(self._lib.aq_sph_step(self._h, int(n)))
+
+    def synchronize(self):
+        _check(self._lib.aq_sph_synchronize(self._h))
+
+    def launches_per_step(self) -> int:
+        v = ct.c_int32()
+        _check(self._lib.aq_sph_launches_per_step(self._h, ct.byref(v)))
+        return v.value
+
+    def get_state(self, fields=None) -> dict:
+        arrs = _abi.alloc_sph_state(self.n, fields)
+        st = _abi.make_sph_state(self.n, arrs)
+        _check(self._lib.aq_sph_download_state(self._h, ct.byref(st)))
+        arrs["physical_time"] = st.physical_time
+        return arrs
+
+    def set_state(self, state: dict):
+        arrs = {k: np.ascontiguousarray(v, np.float32) for k, v in state.items() if k in _abi.SPH_FIELDS}
+        st = _abi.make_sph_state(self.n, arrs, float(state.get("physical_time", 0.0)))
+        _check(self._lib.aq_sph_upload_state(self._h, ct.byref(st)))
+
+    def close(self):
+        if self._h:
+            self._lib.aq_sph_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Batch:

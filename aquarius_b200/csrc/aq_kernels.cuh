@@ -25,6 +25,37 @@ cudaError_t launch_particles_advance(cudaStream_t st, const Dims& d, const StepP
 cudaError_t launch_ink_advance(cudaStream_t st, const Dims& d, float dt, Particles ink, const float* u0,
                                const float* v0, const float* w0, const float* un, const float* vn, const float* wn,
                                int n);
+// Particle-only solvers (k_sph.cu).  Constants of one solver; dt is the
+// substep's.
+struct SphParams {
+  float dt;
+  float3 g;                 // gravity
+  float md, size;           // particleSpacing / 2, gridPhysicalSize
+  float kr, kr2, kr6, kr9;  // kernelRadius and its powers
+  int gx, gy, gz;           // hash grid
+  float s_corr_den, s_corr_k, leave;  // PBF: cubic_spline_kernel(0), 1e-6, wall leave speed
+};
+constexpr int kSphArrays = 6;
+struct SphArrays {
+  float4* a[kSphArrays];  // null entries are skipped
+};
+cudaError_t launch_sph_keys(cudaStream_t st, const SphParams& p, const float4* pos, int* key, int* slot, int* count,
+                            int n);
+cudaError_t launch_sph_gather(cudaStream_t st, const int* key, const int* off, const int* perm_u, const SphArrays& src,
+                              const SphArrays& dst, int n);
+cudaError_t launch_pbf_predict(cudaStream_t st, const SphParams& p, float4* P, const float4* L, float4* V, int n);
+cudaError_t launch_pbf_lambda(cudaStream_t st, const SphParams& p, const int* off, float4* P, float4* V, float4* Q,
+                              bool set_rest, int n);
+cudaError_t launch_pbf_delta(cudaStream_t st, const SphParams& p, const int* off, const float4* Q, float4* P, int n);
+cudaError_t launch_pbf_update(cudaStream_t st, const SphParams& p, const float4* P, float4* L, float4* V, int n);
+cudaError_t launch_pci_init(cudaStream_t st, float4* W, float4* F, int n);
+cudaError_t launch_pci_predict(cudaStream_t st, const SphParams& p, float4* P, float4* V, float4* Q, float4* W,
+                               const float4* F, bool actual, int n);
+cudaError_t launch_pci_density(cudaStream_t st, const SphParams& p, const int* off, float4* P, float4* V,
+                               const float4* Q, float4* W, float4* R, bool set_rest, int n);
+cudaError_t launch_pci_force(cudaStream_t st, const SphParams& p, const int* off, const float4* P, const float4* R,
+                             float4* F, int n);
+
 // Surface mesher (k_mesh.cu).  SDF grid SX*SY*SZ (cell hs), its hash grid
 // HX*HY*HZ = (SX-2)*(SY-2)*(SZ-2), marching-cubes grid MX*MY*MZ (cell hm).
 struct MeshDims {

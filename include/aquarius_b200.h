@@ -602,6 +602,8 @@ void aq_sph_destroy(aq_sph* s);
 aq_status aq_sph_info_get(const aq_sph* s, aq_sph_info* info);
 aq_status aq_sph_step(aq_sph* s, int32_t nsteps);
 aq_status aq_sph_synchronize(aq_sph* s);
+/* Kernel launches in one step (the step runs as one CUDA graph). */
+aq_status aq_sph_launches_per_step(const aq_sph* s, int32_t* launches);
 aq_status aq_sph_download_state(aq_sph* s, aq_sph_state* st);
 /* Replaces fields; positions are kept in the container.  Uploaded particles
  * need not be sorted: every step starts with the spatial hash. */

@@ -112,3 +112,14 @@ def test_create_without_gpu_fails_cleanly(built_library):
     with pytest.raises(aq.AquariusError) as e:
         aq.Fluid(aq.FluidConfig())
     assert e.value.status == 7  # AQ_ERR_NO_DEVICE
+
+
+def test_sph_config_default_matches_reference(built_library):
+    import aquarius_b200 as aq
+    lib = aq.load_library()
+    for method in (_abi.SPH_PBF, _abi.SPH_PCISPH):
+        c = _abi.SphConfig()
+        assert lib.aq_sph_config_default(method, ct.byref(c)) == 0
+        assert bytes(c) == bytes(_abi.sph_config(method))
+    assert ct.sizeof(_abi.SphState) == 8 + 8 + 8 * 10
+    assert ct.sizeof(_abi.SphInfo) == 4 * 7
