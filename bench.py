@@ -584,6 +584,116 @@ def run_batch(args, rank: int, world: int, dist):
     b.close()
 
 
+def sph_cpu_sample(cfg, budget_s: float = 15.0) -> dict:
+    """The CPU oracle stepping the same solver on the host cores, on a
+    smaller particle budget (a bounded sample); steps/s scaled to the
+    workload's particle count (per-particle cost is constant)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_binding import SphOracle, oracle_threads
+    from aquarius_b200 import _abi
+    import ctypes as ct
+    small = _abi.SphConfig()
+    ct.memmove(ct.byref(small), ct.byref(cfg), ct.sizeof(cfg))
+    small.max_particle_count = 300000
+    small.stream = None
+    o = SphOracle(small)
+    t0 = time.perf_counter()
+    steps = 0
+    while time.perf_counter() - t0 < budget_s and steps < 50:
+        o.step(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"particles": o.n, "steps": steps, "seconds": dt, "threads": oracle_threads()}
+
+
+def run_sph(args, rank: int, world: int, dist):
+    """The reference's particle-only solvers (PBF or PCISPH, reference
+    defaults otherwise) with a particle budget of args.particles (default
+    3e7: about 5.6M particles in the default pool + ball scene), one CUDA
+    graph per step.  Reports steps/s; the e2e arm uploads positions and
+    velocities from pinned host memory, steps and downloads positions."""
+    import ctypes as ct
+
+    import numpy as np
+    import torch
+
+    import aquarius_b200 as aq
+    from aquarius_b200 import _abi
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    method = _abi.SPH_PBF if args.workload == "pbf" else _abi.SPH_PCISPH
+    stream = torch.cuda.Stream(device=dev)
+    cfg = _abi.sph_config(method, max_particle_count=int(args.particles), device=dev)
+    cfg.stream = stream.cuda_stream
+    t0 = time.perf_counter()
+    s = aq.Sph(cfg)
+    t_init = time.perf_counter() - t0
+    s.step(args.warmup)
+    s.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.4)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    s.step(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = reduce_max(ev0.elapsed_time(ev1), dist, f"cuda:{dev}")
+    value = weak_scaling_value(args.steps, world, ms)
+    # e2e: state in from pinned host buffers, one step, positions out
+    n = s.n
+    pin_p = torch.empty((3, n), dtype=torch.float32).pin_memory()
+    pin_v = torch.empty((3, n), dtype=torch.float32).pin_memory()
+    st0 = s.get_state(["position", "velocity"])
+    pin_p.numpy()[:] = st0["position"]
+    pin_v.numpy()[:] = st0["velocity"]
+    e2e_steps = max(1, min(args.steps, 5))
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sst = _abi.make_sph_state(n, {"position": pin_p.numpy(), "velocity": pin_v.numpy()})
+        aq._check(s._lib.aq_sph_upload_state(s._h, ct.byref(sst)))
+        s.step(1)
+        out = _abi.make_sph_state(n, {"position": pin_p.numpy()})
+        aq._check(s._lib.aq_sph_download_state(s._h, ct.byref(out)))
+    e2e_s = time.perf_counter() - t1
+    name = "PBF" if method == _abi.SPH_PBF else "PCISPH"
+    line = {
+        "metric": f"{name} steps/s, reference defaults, particle budget {int(args.particles)}",
+        "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{name}: pool y<0.1875 + ball r=0.125 in the 10^3 container, "
+                               f"timestep {cfg.timestep}, {cfg.substeps} substeps, {cfg.iterations} iterations",
+                   "particles": n, "spacing": s.spacing, "kernel_radius": s.kernel_radius, "grid": list(s.grid),
+                   "launch": "one CUDA graph per step", "init_s": t_init,
+                   "l2": "per-step working set > 126 MB L2 (no flush needed)" if n * 96 > 126e6 else "fits L2"},
+        "e2e": {"value": e2e_steps / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": 24 * n,
+                "d2h_bytes_per_step": 12 * n, "steps": e2e_steps,
+                "path": "aq_sph_upload_state + aq_sph_step + aq_sph_download_state (C ABI), wall clock"},
+        "gpu_launches": int(s.launches_per_step() * args.steps),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = sph_cpu_sample(cfg)
+        line["cpu_baseline"] = {"value": cpu["steps"] / cpu["seconds"] * cpu["particles"] / n, "unit": "steps/s",
+                                "cores": cpu["threads"], "kind": "port",
+                                "sample": f"{cpu['steps']} oracle steps of the same solver at budget 3e5 "
+                                          f"({cpu['particles']} particles) in {cpu['seconds']:.1f} s, "
+                                          f"scaled by particle count"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    s.close()
+
+
 def run_multiphase(args, rank: int, world: int, dist):
     """Multiphase FLIP with diffusion at 256^3: a phase-0 pool (concentration
     c = 0) fills y < 0.35, a phase-1 sphere (c = 1) of radius 0.12 sits at
@@ -708,9 +818,11 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
     ap.add_argument("--profile-case", choices=["jacobi", "batch-rows", "conv", "mesh"], default=None,
                     help="run one small fixed case for an ncu capture and exit")
-    ap.add_argument("--workload", default="ball128", choices=["ball128", "batch", "multiphase256"],
+    ap.add_argument("--workload", default="ball128", choices=["ball128", "batch", "multiphase256", "pbf", "pcisph"],
                     help="ball128: the 128^3 scene; batch: 256 independent scenes of uneven sizes; "
-                         "multiphase256: two phases with diffusion at 256^3")
+                         "multiphase256: two phases with diffusion at 256^3; pbf / pcisph: the "
+                         "particle-only solvers")
+    ap.add_argument("--particles", type=float, default=3e7, help="particle budget of the pbf / pcisph workloads")
     ap.add_argument("--scenes", type=int, default=256, help="scenes in the batch workload")
     ap.add_argument("--eager", action="store_true",
                     help="launch the step kernel by kernel instead of one CUDA graph (for launch lists)")
@@ -737,6 +849,8 @@ def main():
             run_batch(args, rank, world, dist)
         elif args.workload == "multiphase256":
             run_multiphase(args, rank, world, dist)
+        elif args.workload in ("pbf", "pcisph"):
+            run_sph(args, rank, world, dist)
         else:
             run_ours(args, rank, world, dist)
     finally:

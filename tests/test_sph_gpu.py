@@ -116,3 +116,32 @@ def test_against_live_reference(method):
         s.step(1)
         assert judge_sph_step(method, s.get_state(), r.get_state()) == [], k
     r.close()
+
+
+@pytest.mark.skipif(not sph_ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("method", ["pbf", "pcisph"])
+def test_step_time_vs_reference(method, capsys):
+    """Budget 3e6 (about 560k particles) on the same GPU: host wall time per
+    simulationStep, ours (one graph launch, then a synchronize) against the
+    reference's (its kernels and its own synchronisations)."""
+    import time
+
+    cfg = _abi.sph_config(METHODS[method], max_particle_count=3000000)
+    s = aq.Sph(cfg)
+    s.step(2)
+    s.synchronize()
+    reps = 5
+    t0 = time.perf_counter()
+    s.step(reps)
+    s.synchronize()
+    ours = (time.perf_counter() - t0) / reps
+    r = RefSph(cfg)
+    r.step(2)
+    t0 = time.perf_counter()
+    r.step(reps)
+    ref = (time.perf_counter() - t0) / reps
+    r.close()
+    with capsys.disabled():
+        print(f"\n{method} budget 3e6 ({s.n} particles): ours {ours * 1e3:.2f} ms/step, "
+              f"reference {ref * 1e3:.2f} ms/step")
+    assert ours < ref
