@@ -34,6 +34,7 @@ struct SphParams {
   float kr, kr2, kr6, kr9;  // kernelRadius and its powers
   int gx, gy, gz;           // hash grid
   float s_corr_den, s_corr_k, leave;  // PBF: cubic_spline_kernel(0), 1e-6, wall leave speed
+  float skip_r2;            // pairs with r^2 above it are outside both kernels' support
 };
 constexpr int kSphArrays = 6;
 struct SphArrays {

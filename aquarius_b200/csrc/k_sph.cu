@@ -37,6 +37,13 @@ __device__ __forceinline__ float clampw(float v, float lo, float hi) { return fm
 
 __device__ __forceinline__ float dot3(float x, float y, float z) { return add(add(mul(x, x), mul(y, y)), mul(z, z)); }
 
+// Neighbour pairs with r2 > p.skip_r2 lie outside both kernels' support:
+// poly6 is 0 (r2 > h2) and spikey_grad is the zero vector (sqrt(r2) > h).
+// Adding their zero terms changes no sum (at most the sign of a zero that is
+// then squared or added to a nonzero value), so the passes skip them; about
+// 85% of the 27-cell candidates are such pairs.
+__device__ __forceinline__ bool outside(float r2, const SphParams& p) { return r2 > p.skip_r2; }
+
 // poly6 (Fluid/WeightKernels.cuh:13-26)
 __device__ __forceinline__ float poly6(float vx, float vy, float vz, const SphParams& p) {
   const float r2 = dot3(vx, vy, vz);
@@ -162,6 +169,7 @@ __global__ void __launch_bounds__(256) k_pbf_lambda(SphParams p, const int* __re
   for_neighbours(p, cell_of(p, me.x, me.y, me.z), off, [&](int j) {
     const float4 o = __ldg(P + j);
     const float dx = sub(me.x, o.x), dy = sub(me.y, o.y), dz = sub(me.z, o.z);
+    if (outside(dot3(dx, dy, dz), p)) return;
     density = add(density, poly6(dx, dy, dz, p));
     const float3 w = spikey(dx, dy, dz, p);
     gx = add(gx, w.x);
@@ -192,6 +200,7 @@ __global__ void __launch_bounds__(256) k_pbf_delta(SphParams p, const int* __res
   for_neighbours(p, cell_of(p, me.x, me.y, me.z), off, [&](int j) {
     const float4 o = __ldg(Q + j);
     const float dx = sub(me.x, o.x), dy = sub(me.y, o.y), dz = sub(me.z, o.z);
+    if (outside(dot3(dx, dy, dz), p)) return;
     const float3 w = spikey(dx, dy, dz, p);
     const float t = dvd(poly6(dx, dy, dz, p), p.s_corr_den);
     const float t2 = mul(t, t);
@@ -276,7 +285,9 @@ __global__ void __launch_bounds__(256) k_pci_density(SphParams p, const int* __r
   float density = 0.f;
   for_neighbours(p, cell_of(p, me.x, me.y, me.z), off, [&](int j) {
     const float4 o = __ldg(Q + j);
-    density = add(density, poly6(sub(pq.x, o.x), sub(pq.y, o.y), sub(pq.z, o.z), p));
+    const float dx = sub(pq.x, o.x), dy = sub(pq.y, o.y), dz = sub(pq.z, o.z);
+    if (outside(dot3(dx, dy, dz), p)) return;
+    density = add(density, poly6(dx, dy, dz, p));
   });
   const float err = sub(density, me.w);
   const float pressure = add(W[i].w, mul(50.0f, err));
@@ -297,7 +308,9 @@ __global__ void __launch_bounds__(256) k_pci_force(SphParams p, const int* __res
   float fx = 0.f, fy = 0.f, fz = 0.f;
   for_neighbours(p, cell_of(p, me.x, me.y, me.z), off, [&](int j) {
     const float4 o = __ldg(R + j);
-    const float3 w = spikey(sub(r.x, o.x), sub(r.y, o.y), sub(r.z, o.z), p);
+    const float dx = sub(r.x, o.x), dy = sub(r.y, o.y), dz = sub(r.z, o.z);
+    if (outside(dot3(dx, dy, dz), p)) return;
+    const float3 w = spikey(dx, dy, dz, p);
     const float s = add(o.w, r.w);
     fx = sub(fx, mul(w.x, s));
     fy = sub(fy, mul(w.y, s));

@@ -314,6 +314,13 @@ aq_status aq_sph_create(const aq_sph_config* cfg, aq_sph** out) {
   p.s_corr_den = cubic_spline(0, kr, kr3);
   p.s_corr_k = 1e-6f;
   p.leave = (float)((double)p.md / ((double)p.dt * 1e2));
+  {
+    // the largest r^2 whose IEEE square root is still <= kernelRadius
+    float x = kr2;
+    while (std::sqrt(std::nextafter(x, INFINITY)) <= kr) x = std::nextafter(x, INFINITY);
+    while (std::sqrt(x) > kr) x = std::nextafter(x, -INFINITY);
+    p.skip_r2 = std::fmax(kr2, x);
+  }
   if ((long long)p.gx * p.gy * p.gz >= (1ll << 31)) return bail(fail(AQ_ERR_INVALID_CONFIG, "hash grid too large"));
   s->cells = p.gx * p.gy * p.gz;
   HostRand rng(cfg->seed);
