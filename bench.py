@@ -765,7 +765,8 @@ def run_profile_case(case: str):
     jacobi: the 128^3 workload's system after 3 steps, 6 sweeps of the
     default plan; batch-rows: 32 scenes of the batch set, 6 batched sweeps;
     conv: two U-Net inferences at 128^3 on seeded random inputs; mesh: two
-    surface meshes of the 128^3 workload's initial particles."""
+    surface meshes of the 128^3 workload's initial particles; pbf / pcisph:
+    one step of the solver at particle budget 3e6 (593k particles)."""
     import numpy as np
     import torch
 
@@ -784,6 +785,14 @@ def run_profile_case(case: str):
         b.set_sweep_plan(8, False)
         print(b.benchmark_pressure(6))
         b.close()
+    elif case in ("pbf", "pcisph"):
+        from aquarius_b200 import _abi
+        m = _abi.SPH_PBF if case == "pbf" else _abi.SPH_PCISPH
+        s = aq.Sph(_abi.sph_config(m, max_particle_count=3000000))
+        s.step(1)
+        s.synchronize()
+        print(case, s.n)
+        s.close()
     elif case == "mesh":
         f = aq.Fluid(workload_config(128, "zero"))
         f.synchronize()
@@ -816,7 +825,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default Jacobi plan")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
-    ap.add_argument("--profile-case", choices=["jacobi", "batch-rows", "conv", "mesh"], default=None,
+    ap.add_argument("--profile-case", choices=["jacobi", "batch-rows", "conv", "mesh", "pbf", "pcisph"], default=None,
                     help="run one small fixed case for an ncu capture and exit")
     ap.add_argument("--workload", default="ball128", choices=["ball128", "batch", "multiphase256", "pbf", "pcisph"],
                     help="ball128: the 128^3 scene; batch: 256 independent scenes of uneven sizes; "
