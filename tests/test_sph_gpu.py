@@ -121,9 +121,9 @@ def test_against_live_reference(method):
 @pytest.mark.skipif(not sph_ref_available(), reason="reference build (oracle/_ref) not present")
 @pytest.mark.parametrize("method", ["pbf", "pcisph"])
 def test_step_time_vs_reference(method, capsys):
-    """Budget 3e6 (about 560k particles) on the same GPU: host wall time per
-    simulationStep, ours (one graph launch, then a synchronize) against the
-    reference's (its kernels and its own synchronisations)."""
+    """Budget 3e6 (about 590k particles) on the same GPU: the best host wall
+    time of five single steps, ours (one graph launch, then a synchronize)
+    against the reference's (its kernels and its own synchronisations)."""
     import time
 
     cfg = _abi.sph_config(METHODS[method], max_particle_count=3000000)
@@ -131,15 +131,19 @@ def test_step_time_vs_reference(method, capsys):
     s.step(2)
     s.synchronize()
     reps = 5
-    t0 = time.perf_counter()
-    s.step(reps)
-    s.synchronize()
-    ours = (time.perf_counter() - t0) / reps
+
+    def best(step):
+        times = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            step()
+            times.append(time.perf_counter() - t0)
+        return min(times)
+
+    ours = best(lambda: (s.step(1), s.synchronize()))
     r = RefSph(cfg)
     r.step(2)
-    t0 = time.perf_counter()
-    r.step(reps)
-    ref = (time.perf_counter() - t0) / reps
+    ref = best(lambda: r.step(1))  # the harness synchronises after the step
     r.close()
     with capsys.disabled():
         print(f"\n{method} budget 3e6 ({s.n} particles): ours {ours * 1e3:.2f} ms/step, "
