@@ -135,7 +135,8 @@ bool cube_plan_ok(int levels, int tx);
 int row_items_capacity(const Dims& d);
 cudaError_t launch_row_items(cudaStream_t st, const Dims& d, const uint8_t* brick_active, int* items, int* n_items);
 cudaError_t launch_jacobi_list(cudaStream_t st, const Dims& d, const float* pin, float* pout, const float* rhs,
-                               const int8_t* type, const int* items, const int* n_items);
+                               const int8_t* type, const int* items, const int* n_items,
+                               bool early);
 
 // ---- persistent solve (k_jacobi.cu) ------------------------------------------
 // The whole pressure solve in one cooperative launch: every CTA sweeps its

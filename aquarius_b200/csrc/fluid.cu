@@ -349,7 +349,7 @@ static aq_status enqueue_sweeps_on(aq_fluid* f, const JacobiPlan& plan, float* a
   for (size_t k = 0; k < parts.size(); ++k) {
     if (plan.by == 3) {
       AQ_CUDA(launch_jacobi_list(f->stream, f->d, bufs[k % 2], bufs[(k + 1) % 2], f->rhs, f->type, f->row_items,
-                                 f->n_row_items));
+                                 f->n_row_items, k > 0));
       continue;
     }
     const bool last = k + 1 == parts.size();

@@ -286,13 +286,25 @@ __device__ __forceinline__ void jacobi_flat_body(const Dims& d, const float* __r
 // Same arithmetic as the flat sweep (jacobi_quad).
 __global__ void __launch_bounds__(256) k_jacobi_list(Dims d, const float* __restrict__ pin, float* __restrict__ pout,
                                                     const float* __restrict__ rhs, const int8_t* __restrict__ type,
-                                                    const int* __restrict__ items, const int* __restrict__ n_items) {
+                                                    const int* __restrict__ items, const int* __restrict__ n_items,
+                                                    int early) {
+  const int W = blockDim.y;
+  const int gz = (d.sz / 4 + 31) / 32;
+  int it = blockIdx.x * W + threadIdx.y;
+  int n = 0, id0 = -1;
+  // early (every sweep of a block but the first): the list was written before
+  // the previous sweep was launched, so the warp's first row id is loaded
+  // before waiting for that sweep (one L2 round trip off the critical path)
+  if (early) {
+    n = *n_items;
+    if (it < n) id0 = __ldg(items + it);
+  }
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;");
-  const int n = *n_items;
-  const int gz = (d.sz / 4 + 31) / 32;
-  for (int it = blockIdx.x * 8 + threadIdx.y; it < n; it += gridDim.x * 8) {
-    const int id = __ldg(items + it);
+  if (!early) n = *n_items;
+  for (; it < n; it += gridDim.x * W) {
+    const int id = id0 >= 0 ? id0 : __ldg(items + it);
+    id0 = -1;
     const int zb = id % gz, t = id / gz;
     jacobi_row<1>(d, pin, pout, rhs, type, zb, t % d.sy, t / d.sy);
   }
@@ -1464,19 +1476,22 @@ cudaError_t launch_row_items(cudaStream_t st, const Dims& d, const uint8_t* bric
 }
 
 cudaError_t launch_jacobi_list(cudaStream_t st, const Dims& d, const float* pin, float* pout, const float* rhs,
-                               const int8_t* type, const int* items, const int* n_items) {
+                               const int8_t* type, const int* items, const int* n_items, bool early) {
   if (d.sz % 4 != 0) return cudaErrorInvalidValue;
-  const int need = (row_items_capacity(d) + 7) / 8;
+  // 8 warps per CTA, one resident wave (4 to 32 warps per CTA and fewer,
+  // fatter waves measured the same or slower at 128^3)
+  const int wy = 8;
+  const int need = (row_items_capacity(d) + wy - 1) / wy;
   cudaLaunchConfig_t lc = {};
-  lc.gridDim = dim3(std::max(1, std::min(need, resident_ctas(k_jacobi_list, 256))));
-  lc.blockDim = dim3(32, 8);
+  lc.gridDim = dim3(std::max(1, std::min(need, resident_ctas(k_jacobi_list, 32 * wy))));
+  lc.blockDim = dim3(32, wy);
   lc.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   lc.attrs = at;
   lc.numAttrs = 1;
-  return cudaLaunchKernelEx(&lc, k_jacobi_list, d, pin, pout, rhs, type, items, n_items);
+  return cudaLaunchKernelEx(&lc, k_jacobi_list, d, pin, pout, rhs, type, items, n_items, early ? 1 : 0);
 }
 
 }  // namespace aqb
