@@ -280,6 +280,31 @@ __device__ __forceinline__ void jacobi_flat_body(const Dims& d, const float* __r
   jacobi_row<XS>(d, pin, pout, rhs, type, bx, by * 8 + threadIdx.y, bz);
 }
 
+// jacobi_row<1> of row (x, y, z block zb) with its rhs and types loaded.
+__device__ __forceinline__ void jacobi_row_pre(const Dims& d, const float* __restrict__ pin, float* __restrict__ pout,
+                                               int x, int y, int zb, const float4& b, const char4& t) {
+  const int lane = threadIdx.x;
+  const int z = (zb * 32 + lane) * 4;
+  const bool in = z < d.sz;
+  const int plane = d.sy * d.sz;
+  const int c = (x * d.sy + y) * d.sz + z;
+  float4 pc = make_float4(0.f, 0.f, 0.f, 0.f), pm = pc, pp = pc, ym = pc, yp = pc;
+  if (in) {
+    pc = ld4(pin + c);
+    pm = x > 0 ? ld4(pin + c - plane) : pc;
+    pp = x + 1 < d.sx ? ld4(pin + c + plane) : pc;
+    ym = y > 0 ? ld4(pin + c - d.sz) : pc;
+    yp = y + 1 < d.sy ? ld4(pin + c + d.sz) : pc;
+  }
+  float zlo = __shfl_up_sync(0xffffffffu, pc.w, 1);
+  float zhi = __shfl_down_sync(0xffffffffu, pc.x, 1);
+  if (in) {
+    if (lane == 0) zlo = z > 0 ? pin[c - 1] : pc.x;
+    if (lane == 31 || z + 4 >= d.sz) zhi = z + 4 < d.sz ? pin[c + 4] : pc.w;
+    *reinterpret_cast<float4*>(pout + c) = jacobi_quad(pm, pp, ym, yp, pc, zlo, zhi, b, t);
+  }
+}
+
 // List plan: one sweep of the warp rows (x, y, 128-wide z block) that hold
 // fluid, from a list built once per solve (k_row_items).  A resident wave of
 // CTAs walks the list, so no CTA is scheduled only to find its rows empty.
@@ -291,20 +316,40 @@ __global__ void __launch_bounds__(256) k_jacobi_list(Dims d, const float* __rest
   const int W = blockDim.y;
   const int gz = (d.sz / 4 + 31) / 32;
   int it = blockIdx.x * W + threadIdx.y;
-  int n = 0, id0 = -1;
-  // early (every sweep of a block but the first): the list was written before
-  // the previous sweep was launched, so the warp's first row id is loaded
-  // before waiting for that sweep (one L2 round trip off the critical path)
+  int n = 0;
+  // early (every sweep of a block but the first): the list, rhs and types
+  // were written before the previous sweep was launched, so the warp's first
+  // row is decoded and its rhs and types loaded before waiting for that sweep
+  bool pre = false;
+  int x0 = 0, y0 = 0, zb0 = 0;
+  float4 b0 = make_float4(0.f, 0.f, 0.f, 0.f);
+  char4 t0 = make_char4(0, 0, 0, 0);
   if (early) {
     n = *n_items;
-    if (it < n) id0 = __ldg(items + it);
+    if (it < n) {
+      const int id = __ldg(items + it);
+      zb0 = id % gz;
+      const int t = id / gz;
+      y0 = t % d.sy;
+      x0 = t / d.sy;
+      const int z = (zb0 * 32 + threadIdx.x) * 4;
+      if (z < d.sz) {
+        const int c = (x0 * d.sy + y0) * d.sz + z;
+        b0 = ld4(rhs + c);
+        t0 = *reinterpret_cast<const char4*>(type + c);
+      }
+      pre = true;
+    }
   }
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;");
   if (!early) n = *n_items;
+  if (pre) {
+    jacobi_row_pre(d, pin, pout, x0, y0, zb0, b0, t0);
+    it += gridDim.x * W;
+  }
   for (; it < n; it += gridDim.x * W) {
-    const int id = id0 >= 0 ? id0 : __ldg(items + it);
-    id0 = -1;
+    const int id = __ldg(items + it);
     const int zb = id % gz, t = id / gz;
     jacobi_row<1>(d, pin, pout, rhs, type, zb, t % d.sy, t / d.sy);
   }
