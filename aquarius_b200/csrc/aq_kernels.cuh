@@ -168,6 +168,12 @@ cudaError_t launch_resid_flat(cudaStream_t st, const Dims& d, const float* p, co
 int resid_flat_parts(const Dims& d);
 // Sums residual partials; updates ss; in a conditional loop body it also
 // sets the loop's condition (continue while not converged and under cap).
+// The flat residual pass and the residual check in one launch (a last-block
+// ticket; ticket starts at 0 and is left at 0).
+cudaError_t launch_resid_flat_fin(cudaStream_t st, const Dims& d, const float* p, const float* rhs,
+                                  const int8_t* type, const uint8_t* brick_active, double* part, unsigned int* ticket,
+                                  SolveState* ss, int sweeps, double tol, int max_iters, bool set_cond,
+                                  unsigned long long cond_handle);
 cudaError_t launch_resid_finalize(cudaStream_t st, const double* part, int nparts, SolveState* ss,
                                   int sweeps_done_per_call, double tol, int max_iters,
                                   bool set_cond, unsigned long long cond_handle);

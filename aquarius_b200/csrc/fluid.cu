@@ -273,6 +273,7 @@ aq_status aq_fluid::allocate() {
     AQ_TRY(alloc(&ppart, (size_t)std::max(ctas, 1)));
     AQ_TRY(alloc(&row_items, (size_t)row_items_capacity(d)));
     AQ_TRY(alloc(&n_row_items, 1));
+    AQ_TRY(alloc(&resid_ticket, 1));
   }
   // default Jacobi plan: one vectorised sweep per launch over the listed
   // active warp rows where z allows it, otherwise the tiled kernel with two
@@ -427,6 +428,14 @@ aq_status aq_fluid::enq_solve_fixed(int sweeps) {
 
 aq_status aq_fluid::enq_solve_body(bool set_cond, unsigned long long handle, int* launches) {
   const int m = cfg.check_interval;
+  if ((plan.by == 0 || plan.by >= 2) && d.sz % 4 == 0) {
+    // plans whose residual is a separate flat pass: pass and check in one launch
+    AQ_TRY(enqueue_sweeps(this, m, false));
+    AQ_CUDA(launch_resid_flat_fin(stream, d, pa, rhs, type, bact, jpart, resid_ticket, ss, m,
+                                  (double)cfg.rel_residual, cfg.max_iterations, set_cond, handle));
+    if (launches) *launches = count_jacobi_launches(m) - 1;
+    return AQ_OK;
+  }
   AQ_TRY(enqueue_sweeps(this, m));
   AQ_CUDA(launch_resid_finalize(stream, jpart, last_parts(this, m), ss, m, (double)cfg.rel_residual,
                                 cfg.max_iterations, set_cond, handle));

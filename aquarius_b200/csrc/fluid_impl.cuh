@@ -99,6 +99,7 @@ struct aq_fluid {
   int* pick = nullptr;  // 1: the zero-init path won
   // list plan: active warp rows of the current system
   int *row_items = nullptr, *n_row_items = nullptr;
+  unsigned int* resid_ticket = nullptr;  // last-block ticket of the fused residual check
   // rand() state after seeding: ink seeding continues the sequence
   std::unique_ptr<aqb::HostRand> rng;
   // ink particles (positions / velocities only; frac stays null)

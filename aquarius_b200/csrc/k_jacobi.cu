@@ -916,6 +916,10 @@ __global__ void __launch_bounds__(1024) k_persist_solve(Dims d, float* __restric
   }
 }
 
+// The solve state after a residual check of r2; whether the solve goes on.
+__device__ __forceinline__ bool finalize_state(double r2, SolveState* __restrict__ ss, int sweeps, double tol,
+                                               int max_iters);
+
 // Returns (in thread 0) whether the solve should continue.
 __device__ __forceinline__ bool resid_finalize_body(const double* __restrict__ part, int nparts,
                                                     SolveState* __restrict__ ss, int sweeps, double tol,
@@ -929,22 +933,24 @@ __device__ __forceinline__ bool resid_finalize_body(const double* __restrict__ p
     if (threadIdx.x < o) sb[threadIdx.x] += sb[threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    const double r2 = sb[0];
-    ss->iterations += sweeps;
-    ss->bodies += 1;
-    ss->total_sweeps += sweeps;
-    ss->total_bodies += 1;
-    ss->r2 = r2;
-    const double rel = ss->b2 > 0.0 ? sqrt(r2) / sqrt(ss->b2) : 0.0;
-    ss->rel_residual = rel;
-    const bool finite = isfinite(rel);
-    if (!finite) ss->nonfinite = 1;
-    const bool conv = finite && rel <= tol;
-    ss->converged = conv ? 1 : 0;
-    return finite && !conv && ss->iterations < max_iters;
-  }
+  if (threadIdx.x == 0) return finalize_state(sb[0], ss, sweeps, tol, max_iters);
   return false;
+}
+
+__device__ __forceinline__ bool finalize_state(double r2, SolveState* __restrict__ ss, int sweeps, double tol,
+                                               int max_iters) {
+  ss->iterations += sweeps;
+  ss->bodies += 1;
+  ss->total_sweeps += sweeps;
+  ss->total_bodies += 1;
+  ss->r2 = r2;
+  const double rel = ss->b2 > 0.0 ? sqrt(r2) / sqrt(ss->b2) : 0.0;
+  ss->rel_residual = rel;
+  const bool finite = isfinite(rel);
+  if (!finite) ss->nonfinite = 1;
+  const bool conv = finite && rel <= tol;
+  ss->converged = conv ? 1 : 0;
+  return finite && !conv && ss->iterations < max_iters;
 }
 
 __global__ void __launch_bounds__(1024) k_resid_finalize(const double* __restrict__ part, int nparts,
@@ -953,6 +959,54 @@ __global__ void __launch_bounds__(1024) k_resid_finalize(const double* __restric
                                                         cudaGraphConditionalHandle handle) {
   const bool more = resid_finalize_body(part, nparts, ss, sweeps, tol, max_iters);
   if (threadIdx.x == 0 && set_cond) cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+// k_resid_flat and k_resid_finalize in one launch: the last block to write
+// its partial (a ticket counter) sums the partials exactly as
+// k_resid_finalize does (1024 strided sums, then the same pairwise tree,
+// here four sums per thread), so the solve state and the loop decision are
+// the same, with one launch fewer per residual check.
+__global__ void __launch_bounds__(256) k_resid_flat_fin(Dims d, const float* __restrict__ p,
+                                                       const float* __restrict__ rhs,
+                                                       const int8_t* __restrict__ type,
+                                                       const uint8_t* __restrict__ bact, double* __restrict__ part,
+                                                       unsigned int* __restrict__ ticket, SolveState* __restrict__ ss,
+                                                       int sweeps, double tol, int max_iters, int set_cond,
+                                                       cudaGraphConditionalHandle handle) {
+  resid_flat_body(d, p, rhs, type, bact, part, blockIdx.x, blockIdx.y, blockIdx.z);
+  __shared__ bool s_last;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+  if (tid == 0) {
+    __threadfence();  // this block's partial before its ticket
+    s_last = atomicAdd(ticket, 1u) == nblocks - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  __shared__ double sb[1024];
+  const int nparts = (int)nblocks;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int v = tid + 256 * q;
+    double a = 0.0;
+    for (int i = v; i < nparts; i += 1024) a += __ldcg(part + i);
+    sb[v] = a;
+  }
+  __syncthreads();
+  for (int o = 512; o > 0; o >>= 1) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int v = tid + 256 * q;
+      if (v < o) sb[v] += sb[v + o];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    *ticket = 0u;
+    const bool more = finalize_state(sb[0], ss, sweeps, tol, max_iters);
+    if (set_cond) cudaGraphSetConditional(handle, more ? 1u : 0u);
+  }
 }
 
 // ------------------------------------------------------------------- batched
@@ -1402,6 +1456,17 @@ cudaError_t launch_resid_flat(cudaStream_t st, const Dims& d, const float* p, co
   if (d.sz % 4 != 0) return cudaErrorInvalidValue;
   k_resid_flat<<<dim3((d.sz / 4 + 31) / 32, (d.sy + 7) / 8, d.sx), dim3(32, 8), 0, st>>>(d, p, rhs, type,
                                                                                         brick_active, part);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_resid_flat_fin(cudaStream_t st, const Dims& d, const float* p, const float* rhs,
+                                  const int8_t* type, const uint8_t* brick_active, double* part, unsigned int* ticket,
+                                  SolveState* ss, int sweeps, double tol, int max_iters, bool set_cond,
+                                  unsigned long long cond_handle) {
+  if (d.sz % 4 != 0) return cudaErrorInvalidValue;
+  k_resid_flat_fin<<<dim3((d.sz / 4 + 31) / 32, (d.sy + 7) / 8, d.sx), dim3(32, 8), 0, st>>>(
+      d, p, rhs, type, brick_active, part, ticket, ss, sweeps, tol, max_iters, set_cond ? 1 : 0,
+      (cudaGraphConditionalHandle)cond_handle);
   return cudaGetLastError();
 }
 
