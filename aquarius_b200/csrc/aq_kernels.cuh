@@ -174,6 +174,12 @@ cudaError_t launch_resid_flat_fin(cudaStream_t st, const Dims& d, const float* p
                                   const int8_t* type, const uint8_t* brick_active, double* part, unsigned int* ticket,
                                   SolveState* ss, int sweeps, double tol, int max_iters, bool set_cond,
                                   unsigned long long cond_handle);
+// The same for the list plan: residual of the listed rows, per-CTA partials
+// (at most row_items_capacity / 8 of them).
+cudaError_t launch_resid_list_fin(cudaStream_t st, const Dims& d, const float* p, const float* rhs,
+                                  const int8_t* type, const int* items, const int* n_items, double* part,
+                                  unsigned int* ticket, SolveState* ss, int sweeps, double tol, int max_iters,
+                                  bool set_cond, unsigned long long cond_handle);
 cudaError_t launch_resid_finalize(cudaStream_t st, const double* part, int nparts, SolveState* ss,
                                   int sweeps_done_per_call, double tol, int max_iters,
                                   bool set_cond, unsigned long long cond_handle);

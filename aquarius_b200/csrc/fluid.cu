@@ -429,10 +429,14 @@ aq_status aq_fluid::enq_solve_fixed(int sweeps) {
 aq_status aq_fluid::enq_solve_body(bool set_cond, unsigned long long handle, int* launches) {
   const int m = cfg.check_interval;
   if ((plan.by == 0 || plan.by >= 2) && d.sz % 4 == 0) {
-    // plans whose residual is a separate flat pass: pass and check in one launch
+    // plans whose residual is a separate pass: pass and check in one launch
     AQ_TRY(enqueue_sweeps(this, m, false));
-    AQ_CUDA(launch_resid_flat_fin(stream, d, pa, rhs, type, bact, jpart, resid_ticket, ss, m,
-                                  (double)cfg.rel_residual, cfg.max_iterations, set_cond, handle));
+    if (plan.by == 3)
+      AQ_CUDA(launch_resid_list_fin(stream, d, pa, rhs, type, row_items, n_row_items, jpart, resid_ticket, ss, m,
+                                    (double)cfg.rel_residual, cfg.max_iterations, set_cond, handle));
+    else
+      AQ_CUDA(launch_resid_flat_fin(stream, d, pa, rhs, type, bact, jpart, resid_ticket, ss, m,
+                                    (double)cfg.rel_residual, cfg.max_iterations, set_cond, handle));
     if (launches) *launches = count_jacobi_launches(m) - 1;
     return AQ_OK;
   }

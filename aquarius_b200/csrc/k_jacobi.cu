@@ -961,6 +961,112 @@ __global__ void __launch_bounds__(1024) k_resid_finalize(const double* __restric
   if (threadIdx.x == 0 && set_cond) cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
 
+// The residual check of the list plan in one launch: each warp sums the
+// FP64 residual of its listed rows (in list order), each CTA its warps in
+// order, and the last CTA to finish (a ticket) sums the CTA partials as
+// k_resid_finalize does and updates the solve state.
+__device__ __forceinline__ double resid_row(const Dims& d, const float* __restrict__ p, const float* __restrict__ rhs,
+                                            const int8_t* __restrict__ type, int x, int y, int zb) {
+  const int lane = threadIdx.x;
+  const int z = (zb * 32 + lane) * 4;
+  const bool in = z < d.sz;
+  const int plane = d.sy * d.sz;
+  const int c = x * plane + y * d.sz + z;
+  float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (in) pc = ld4(p + c);
+  float zlo = __shfl_up_sync(0xffffffffu, pc.w, 1);
+  float zhi = __shfl_down_sync(0xffffffffu, pc.x, 1);
+  double acc = 0.0;
+  if (in) {
+    if (lane == 0) zlo = z > 0 ? p[c - 1] : pc.x;
+    if (lane == 31 || z + 4 >= d.sz) zhi = z + 4 < d.sz ? p[c + 4] : pc.w;
+    const float4 xm = x > 0 ? ld4(p + c - plane) : pc;
+    const float4 xp = x + 1 < d.sx ? ld4(p + c + plane) : pc;
+    const float4 ym = y > 0 ? ld4(p + c - d.sz) : pc;
+    const float4 yp = y + 1 < d.sy ? ld4(p + c + d.sz) : pc;
+    const float4 b = ld4(rhs + c);
+    const char4 t = *reinterpret_cast<const char4*>(type + c);
+    const float self[4] = {pc.x, pc.y, pc.z, pc.w};
+    const float zp[4] = {pc.y, pc.z, pc.w, zhi};
+    const float zm[4] = {zlo, pc.x, pc.y, pc.z};
+    const float vxp[4] = {xp.x, xp.y, xp.z, xp.w}, vxm[4] = {xm.x, xm.y, xm.z, xm.w};
+    const float vyp[4] = {yp.x, yp.y, yp.z, yp.w}, vym[4] = {ym.x, ym.y, ym.z, ym.w};
+    const float vb[4] = {b.x, b.y, b.z, b.w};
+    const signed char vt[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (vt[k] != kFluid) continue;
+      double s = (double)vxp[k];
+      s += (double)vxm[k];
+      s += (double)vyp[k];
+      s += (double)vym[k];
+      s += (double)zp[k];
+      s += (double)zm[k];
+      const double r = (double)vb[k] + s - 6.0 * (double)self[k];
+      acc += r * r;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc;
+}
+
+__global__ void __launch_bounds__(256) k_resid_list_fin(Dims d, const float* __restrict__ p,
+                                                       const float* __restrict__ rhs,
+                                                       const int8_t* __restrict__ type,
+                                                       const int* __restrict__ items, const int* __restrict__ n_items,
+                                                       double* __restrict__ part, unsigned int* __restrict__ ticket,
+                                                       SolveState* __restrict__ ss, int sweeps, double tol,
+                                                       int max_iters, int set_cond,
+                                                       cudaGraphConditionalHandle handle) {
+  const int n = *n_items;
+  const int gz = (d.sz / 4 + 31) / 32;
+  double wsum = 0.0;
+  for (int it = blockIdx.x * 8 + threadIdx.y; it < n; it += gridDim.x * 8) {
+    const int id = __ldg(items + it);
+    const int zb = id % gz, t = id / gz;
+    wsum += resid_row(d, p, rhs, type, t / d.sy, t % d.sy, zb);
+  }
+  __shared__ double s_red[8];
+  __shared__ bool s_last;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  if (threadIdx.x == 0) s_red[threadIdx.y] = wsum;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int k = 0; k < 8; ++k) t += s_red[k];
+    part[blockIdx.x] = t;
+    __threadfence();  // the partial before the ticket
+    s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  __shared__ double sb[1024];
+  const int nparts = (int)gridDim.x;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int v = tid + 256 * q;
+    double a = 0.0;
+    for (int i = v; i < nparts; i += 1024) a += __ldcg(part + i);
+    sb[v] = a;
+  }
+  __syncthreads();
+  for (int o = 512; o > 0; o >>= 1) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int v = tid + 256 * q;
+      if (v < o) sb[v] += sb[v + o];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    *ticket = 0u;
+    const bool more = finalize_state(sb[0], ss, sweeps, tol, max_iters);
+    if (set_cond) cudaGraphSetConditional(handle, more ? 1u : 0u);
+  }
+}
+
 // k_resid_flat and k_resid_finalize in one launch: the last block to write
 // its partial (a ticket counter) sums the partials exactly as
 // k_resid_finalize does (1024 strided sums, then the same pairwise tree,
@@ -1467,6 +1573,18 @@ cudaError_t launch_resid_flat_fin(cudaStream_t st, const Dims& d, const float* p
   k_resid_flat_fin<<<dim3((d.sz / 4 + 31) / 32, (d.sy + 7) / 8, d.sx), dim3(32, 8), 0, st>>>(
       d, p, rhs, type, brick_active, part, ticket, ss, sweeps, tol, max_iters, set_cond ? 1 : 0,
       (cudaGraphConditionalHandle)cond_handle);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_resid_list_fin(cudaStream_t st, const Dims& d, const float* p, const float* rhs,
+                                  const int8_t* type, const int* items, const int* n_items, double* part,
+                                  unsigned int* ticket, SolveState* ss, int sweeps, double tol, int max_iters,
+                                  bool set_cond, unsigned long long cond_handle) {
+  if (d.sz % 4 != 0) return cudaErrorInvalidValue;
+  const int need = (row_items_capacity(d) + 7) / 8;
+  const int grid = std::max(1, std::min(need, resident_ctas(k_resid_list_fin, 256)));
+  k_resid_list_fin<<<grid, dim3(32, 8), 0, st>>>(d, p, rhs, type, items, n_items, part, ticket, ss, sweeps, tol,
+                                                 max_iters, set_cond ? 1 : 0, (cudaGraphConditionalHandle)cond_handle);
   return cudaGetLastError();
 }
 
