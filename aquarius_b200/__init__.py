@@ -28,7 +28,7 @@ from . import _abi
 
 __all__ = [
     "ShapeType", "InitializationVolume", "ConfigFLIP", "FluidConfig", "Fluid", "AquariusError",
-    "library_path", "load_library", "STAGES", "Batch", "UNet", "Dataset",
+    "library_path", "load_library", "STAGES", "Batch", "UNet", "Dataset", "Renderer", "draw_command_default",
 ]
 
 STAGES = _abi.STAGES
@@ -146,6 +146,18 @@ def load_library() -> ct.CDLL:
         "aq_dataset_add_fluid": (ct.c_int, [P, P, ct.c_double, ct.c_int32, ct.POINTER(ct.c_int32)]),
         "aq_dataset_target_rms": (ct.c_int, [P, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_double)]),
         "aq_dataset_get": (ct.c_int, [P, ct.c_int32, P, P, P]),
+        "aq_draw_command_default": (ct.c_int, [P, ct.c_int32, ct.c_int32, ct.c_float, ct.c_int32]),
+        "aq_fluid_points_vbo": (ct.c_int, [P, P]),
+        "aq_renderer_create": (ct.c_int, [ct.c_int32, P, ct.POINTER(P)]),
+        "aq_renderer_destroy": (None, [P]),
+        "aq_renderer_set_skybox": (ct.c_int, [P, P, ct.c_int32]),
+        "aq_renderer_set_logo": (ct.c_int, [P, P, ct.c_int32, ct.c_int32]),
+        "aq_renderer_draw": (ct.c_int, [P, P, P, ct.c_int32, P, ct.c_int64, P]),
+        "aq_renderer_synchronize": (ct.c_int, [P]),
+        "aq_renderer_download_phase_thickness": (ct.c_int, [P, P]),
+        "aq_renderer_download_image": (ct.c_int, [P, P]),
+        "aq_renderer_launches": (ct.c_int, [P, ct.POINTER(ct.c_int32)]),
+        "aq_fluid_draw": (ct.c_int, [P, P, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -400,6 +412,18 @@ class Fluid:
         _check(self._lib.aq_fluid_mesh(self._h, ct.c_void_p(device_ptr), int(capacity_records), ct.byref(n)))
         return n.value
 
+    def points_vbo_into(self, device_ptr: int):
+        """updatePositionsAndPhasesVBO: 7 floats per particle into a device buffer."""
+        _check(self._lib.aq_fluid_points_vbo(self._h, ct.c_void_p(device_ptr)))
+
+    def draw(self, renderer: "Renderer", command: _abi.DrawCommand, device_ptr: Optional[int] = None):
+        """Fluid::draw(drawCommand): mesh (mesh modes), point VBO and one
+        frame; into device_ptr (W*H*4 bytes) or, when None, the renderer's own
+        image (renderer.image() downloads it)."""
+        _check(self._lib.aq_fluid_draw(self._h, renderer._h, ct.byref(command),
+                                       None if device_ptr is None else ct.c_void_p(device_ptr)))
+        renderer._last = (command.window_height, command.window_width)
+
     def download_sdf(self) -> np.ndarray:
         """The last mesh's SDF grid, [sdf_x, sdf_y, sdf_z]."""
         info = self.mesh_info()
@@ -543,6 +567,86 @@ class Sph:
     def close(self):
         if self._h:
             self._lib.aq_sph_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def draw_command_default(width: int, height: int, domain_size: float, size_y: int) -> _abi.DrawCommand:
+    """main.cu's first-frame DrawCommand for a fluid of physical size
+    domain_size with size_y cells along y (aq_draw_command_default)."""
+    dc = _abi.DrawCommand()
+    _check(load_library().aq_draw_command_default(ct.byref(dc), int(width), int(height), float(domain_size),
+                                                  int(size_y)))
+    return dc
+
+
+class Renderer:
+    """The headless frame of the reference's renderer (aq_renderer_* in
+    include/aquarius_b200.h): Skybox, Container, PointSprites and
+    FluidMeshRenderer draws as CUDA kernels writing an RGBA8 image, row 0 at
+    the bottom."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load_library()
+        self._h = ct.c_void_p()
+        _check(self._lib.aq_renderer_create(int(device), None, ct.byref(self._h)))
+        self._last = None
+
+    def set_skybox(self, faces: Optional[np.ndarray]):
+        """faces: uint8 [6, F, F, 3] in the order posx, negx, posy, negy, posz, negz."""
+        if faces is None:
+            _check(self._lib.aq_renderer_set_skybox(self._h, None, 0))
+            return
+        f = np.ascontiguousarray(faces, np.uint8)
+        assert f.ndim == 4 and f.shape[0] == 6 and f.shape[1] == f.shape[2] and f.shape[3] == 3
+        _check(self._lib.aq_renderer_set_skybox(self._h, f.ctypes.data, f.shape[1]))
+
+    def set_logo(self, img: Optional[np.ndarray]):
+        """img: uint8 [H, W, 3], first row at t = 0."""
+        if img is None:
+            _check(self._lib.aq_renderer_set_logo(self._h, None, 0, 0))
+            return
+        a = np.ascontiguousarray(img, np.uint8)
+        _check(self._lib.aq_renderer_set_logo(self._h, a.ctypes.data, a.shape[1], a.shape[0]))
+
+    def draw(self, command: _abi.DrawCommand, points_ptr: int = 0, n_points: int = 0, mesh_ptr: int = 0,
+             n_vertices: int = 0, rgba_ptr: Optional[int] = None):
+        """One frame from device VBOs into a device image (or the renderer's own)."""
+        _check(self._lib.aq_renderer_draw(self._h, ct.byref(command), ct.c_void_p(points_ptr) if points_ptr else None,
+                                          int(n_points), ct.c_void_p(mesh_ptr) if mesh_ptr else None,
+                                          int(n_vertices), None if rgba_ptr is None else ct.c_void_p(rgba_ptr)))
+        self._last = (command.window_height, command.window_width)
+
+    def synchronize(self):
+        _check(self._lib.aq_renderer_synchronize(self._h))
+
+    def image(self) -> np.ndarray:
+        """The last frame, uint8 [H, W, 4], row 0 at the bottom."""
+        h, w = self._last
+        out = np.empty((h, w, 4), np.uint8)
+        _check(self._lib.aq_renderer_download_image(self._h, out.ctypes.data))
+        return out
+
+    def phase_thickness(self) -> np.ndarray:
+        """The last frame's phase-thickness texture, float32 [H, W, 4]."""
+        h, w = self._last
+        out = np.empty((h, w, 4), np.float32)
+        _check(self._lib.aq_renderer_download_phase_thickness(self._h, out.ctypes.data))
+        return out
+
+    def launches(self) -> int:
+        v = ct.c_int32()
+        _check(self._lib.aq_renderer_launches(self._h, ct.byref(v)))
+        return v.value
+
+    def close(self):
+        if self._h:
+            self._lib.aq_renderer_destroy(self._h)
             self._h = ct.c_void_p()
 
     def __del__(self):

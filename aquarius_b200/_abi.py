@@ -384,3 +384,32 @@ def make_sph_state(n: int, arrays: dict, time: float = 0.0) -> SphState:
 def alloc_sph_state(n: int, fields=None) -> dict:
     names = SPH_FIELDS.keys() if fields is None else fields
     return {k: np.zeros((SPH_FIELDS[k], n) if SPH_FIELDS[k] == 3 else (n,), np.float32) for k in names}
+
+
+# ------------------------------------------------------------ headless frame
+RENDER_MULTIPHASE_MESH, RENDER_WATER_MESH, RENDER_FLAT_MESH, RENDER_NORMAL_MESH, RENDER_MIRROR_MESH = 0, 1, 2, 3, 4
+RENDER_REFRACT_MESH, RENDER_PHASE0_MESH, RENDER_PHASE1_MESH, RENDER_PARTICLES, RENDER_NONE = 5, 6, 7, 8, 9
+ENV_SKYBOX, ENV_CORNELL_BOX, ENV_CHESS_BOARD = 0, 1, 2
+
+
+class DrawCommand(ct.Structure):
+    """aq_draw_command: DrawCommand (Rendering/DrawCommand.h:37-59) plus what
+    Fluid::draw passes along.  Matrices are column-major (glm layout)."""
+    _fields_ = [
+        ("view", ct.c_float * 16),
+        ("projection", ct.c_float * 16),
+        ("camera_position", ct.c_float * 3),
+        ("window_width", ct.c_int32),
+        ("window_height", ct.c_int32),
+        ("fov", ct.c_float),
+        ("near_plane", ct.c_float),
+        ("far_plane", ct.c_float),
+        ("render_mode", ct.c_int32),
+        ("environment_mode", ct.c_int32),
+        ("light_position", ct.c_float * 3),
+        ("container_size", ct.c_float),
+        ("cornell_box_size", ct.c_float),
+        ("point_radius", ct.c_float),
+        ("phase_count", ct.c_int32),
+        ("phase_colors", (ct.c_float * 4) * 4),
+    ]

@@ -316,4 +316,57 @@ cudaError_t launch_pcg_xpby(cudaStream_t st, int C, const double* xv, double bet
 cudaError_t launch_pcg_init(cudaStream_t st, const Dims& d, const int8_t* type, const float* rhs,
                             double* b, double* x);
 
+
+// ------------------------------------------------------------ headless frame
+constexpr int kRenderTile = 16;  // screen tile edge in pixels (one CTA per tile)
+
+struct RenderParams {
+  int W, H, tiles_x, tiles_y;
+  int mode, env, use_phase;
+  float pv[16];    // projection * view (column-major)
+  float view[16];
+  float proj[16];
+  float model[16]; // container model
+  float cmvp[16];  // (projection * view) * container model
+  int ntri_container;
+  float cam[3], light[3];
+  float container, cornell;
+  float radius, tan_half;
+  int phase_count;
+  float phase_colors[16];
+  const uint8_t* sky;
+  int face;
+  const uint8_t* logo;
+  int lw, lh;
+};
+
+// A triangle in window space, counter-clockwise: vertices snapped to 1/256
+// pixel, window depth, 1/w and 8 varyings per vertex (world position, ndc xy,
+// normal), twice the area in 1/256^2 units, top-left flags of its edges.
+struct RenderTri {
+  int X[3], Y[3];
+  float z[3], iw[3];
+  float a[3][8];
+  long long area;
+  int tl;
+};
+
+cudaError_t launch_sprite_setup(cudaStream_t st, const RenderParams& P, const float* pts, int n, float4* spr,
+                                float4* frac, int* cnt, unsigned long long* total);
+cudaError_t launch_sprite_emit(cudaStream_t st, const RenderParams& P, const float4* spr, const int* off, int n,
+                               unsigned* keys, int* vals);
+cudaError_t launch_tri_setup(cudaStream_t st, const RenderParams& P, const float* mesh, int ntri, RenderTri* tris,
+                             int* cnt, unsigned long long* total);
+cudaError_t launch_tri_emit(cudaStream_t st, const RenderParams& P, const RenderTri* tris, const int* off, int ntri,
+                            unsigned* keys, int* vals);
+cudaError_t launch_container_setup(cudaStream_t st, const RenderParams& P, RenderTri* tris, int* live);
+// range[key] = [first, last+1) of each key's run in sorted keys[0..n)
+cudaError_t launch_tile_ranges(cudaStream_t st, const unsigned* keys, int n, int2* range);
+cudaError_t launch_phase(cudaStream_t st, const RenderParams& P, const int2* range, const int* vals,
+                         const float4* spr, const float4* frac, float4* phase);
+cudaError_t launch_frame(cudaStream_t st, const RenderParams& P, const RenderTri* ctris, const int* clive,
+                         const int2* trange, const int* tvals, const RenderTri* tris, const int2* srange,
+                         const int* svals, const float4* spr, const float4* phase, uchar4* rgba);
+cudaError_t launch_points_vbo(cudaStream_t st, Particles cur, int n, int phase, float* vbo);
+
 }  // namespace aqb

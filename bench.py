@@ -381,6 +381,7 @@ def run_ours(args, rank: int, world: int, dist):
                         "tuned_sweep_us": tune["sweep_us"]},
     }
     line["mesh"] = mesh_timing(f, stream)
+    line["render"] = render_timing(f, args.size)
     plain_rel = [st1["rel_residual"], pstats["rel_residual"]]
     plan = f.jacobi_plan()
     f.close()
@@ -419,6 +420,55 @@ def mesh_timing(f, stream, reps: int = 10) -> dict:
     return {"ms_per_mesh": ms, "cubes": cubes, "triangles": vertices // 3, "sdf_grid": list(info["sdf"]),
             "mesh_grid": list(info["mesh"]), "reps": reps,
             "path": "aq_fluid_mesh into a device buffer (the reference's VBO layout)"}
+
+
+def render_timing(f, size: int, reps: int = 10, width: int = 1728, height: int = 864) -> dict:
+    """The headless frame of the reference's renderer (main.cu's first frame:
+    skybox, container floor, phase-thickness sprites, the fluid mesh shaded
+    with reflection/refraction) on the workload's particles, in the window
+    main.cu opens on a 1920-wide screen.  Fluid::draw as aq_fluid_draw (mesh +
+    point VBO + frame) and the frame alone (aq_renderer_draw from resident
+    VBOs), host wall clock per call with a synchronize after each (the draw
+    reads its primitive-tile pair counts back to the host once per frame)."""
+    import time
+
+    import numpy as np
+    import torch
+
+    import aquarius_b200 as aq
+    rng = np.random.default_rng(11)
+    r = aq.Renderer(torch.cuda.current_device())
+    r.set_skybox(rng.integers(0, 256, (6, 256, 256, 3), dtype=np.uint8))
+    dc = aq.draw_command_default(width, height, f.getContainerSize(), size)
+    img = torch.empty((height * width * 4,), dtype=torch.uint8, device="cuda")
+
+    def best(fn):
+        for _ in range(2):
+            fn()
+        r.synchronize()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            r.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return 1e3 * float(np.median(ts))
+
+    full_ms = best(lambda: f.draw(r, dc, img.data_ptr()))
+    recs = f.download_mesh()
+    mesh = torch.from_numpy(np.ascontiguousarray(recs.reshape(-1, 6))).cuda()
+    pts = torch.empty((f.particleCount * 7,), dtype=torch.float32, device="cuda")
+    f.points_vbo_into(pts.data_ptr())
+    torch.cuda.synchronize()
+    frame_ms = best(lambda: r.draw(dc, pts.data_ptr(), f.particleCount, mesh.data_ptr(), mesh.shape[0],
+                                   img.data_ptr()))
+    out = {"ms_per_frame": frame_ms, "ms_per_fluid_draw": full_ms, "window": [width, height],
+           "render_mode": "multiphase mesh", "environment": "skybox", "particles": f.particleCount,
+           "mesh_vertices": int(mesh.shape[0]), "launches": r.launches(), "reps": reps,
+           "path": "aq_renderer_draw (frame from resident VBOs) / aq_fluid_draw (Fluid::draw)",
+           "reference": "unavailable on this box (GL)"}
+    r.close()
+    return out
 
 
 def learned_arm(args, dev, stream, plain_residual: float, plain_ms: float, dist, plan) -> dict:
@@ -766,7 +816,9 @@ def run_profile_case(case: str):
     default plan; batch-rows: 32 scenes of the batch set, 6 batched sweeps;
     conv: two U-Net inferences at 128^3 on seeded random inputs; mesh: two
     surface meshes of the 128^3 workload's initial particles; pbf / pcisph:
-    one step of the solver at particle budget 3e6 (593k particles)."""
+    one step of the solver at particle budget 3e6 (593k particles); render:
+    two headless frames (Fluid::draw) of the 128^3 workload's initial
+    particles at 1728x864."""
     import numpy as np
     import torch
 
@@ -799,6 +851,18 @@ def run_profile_case(case: str):
         for _ in range(2):
             print(len(f.download_mesh(1 << 19)))
         f.close()
+    elif case == "render":
+        f = aq.Fluid(workload_config(128, "zero"))
+        f.synchronize()
+        r = aq.Renderer(torch.cuda.current_device())
+        r.set_skybox(np.random.default_rng(11).integers(0, 256, (6, 256, 256, 3), dtype=np.uint8))
+        dc = aq.draw_command_default(1728, 864, f.getContainerSize(), 128)
+        for _ in range(2):
+            f.draw(r, dc)
+        r.synchronize()
+        print("render ok", r.launches())
+        r.close()
+        f.close()
     elif case == "conv":
         net = aq.UNet(weights=ROOT / "aquarius_b200" / "weights" / "unet_128.bin")
         V = 128 ** 3
@@ -825,7 +889,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default Jacobi plan")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
-    ap.add_argument("--profile-case", choices=["jacobi", "batch-rows", "conv", "mesh", "pbf", "pcisph"], default=None,
+    ap.add_argument("--profile-case", choices=["jacobi", "batch-rows", "conv", "mesh", "pbf", "pcisph", "render"],
+                    default=None,
                     help="run one small fixed case for an ncu capture and exit")
     ap.add_argument("--workload", default="ball128", choices=["ball128", "batch", "multiphase256", "pbf", "pcisph"],
                     help="ball128: the 128^3 scene; batch: 256 independent scenes of uneven sizes; "

@@ -609,6 +609,138 @@ aq_status aq_sph_download_state(aq_sph* s, aq_sph_state* st);
  * need not be sorted: every step starts with the spatial hash. */
 aq_status aq_sph_upload_state(aq_sph* s, const aq_sph_state* st);
 
+
+/* ---------------------------------------------------------------- frames
+ * Headless frame of the reference's renderer: the GL draw calls of one frame
+ * (main.cu:111-145: glClear, Skybox::draw, Container::drawFace, Fluid::draw)
+ * restated as CUDA kernels that write an RGBA8 image into a DEVICE buffer,
+ * with no graphics API.  The shading is the arithmetic of the reference's
+ * shaders (resources/Shaders/Skybox_fs.glsl, Container_face_fs.glsl,
+ * RayTraceEnvironment.glsl, PointSprites_points_vs.glsl,
+ * PointSprites_phase_fs.glsl, PointSprites_simple_fs.glsl,
+ * FluidMeshRenderer_vs.glsl, FluidMeshRenderer_fs.glsl); the fixed-function
+ * GL stages (clipping, point and triangle rasterisation, the 24-bit depth
+ * test GL_LESS, blending into an RGBA8 framebuffer) follow the GL rules as
+ * restated in the frame kernels' header comment.
+ *
+ *   reference                                            replacement
+ *   ---------------------------------------------------  ------------------------
+ *   DrawCommand (Rendering/DrawCommand.h:37-59)          aq_draw_command
+ *   Camera(center) + glm::lookAt / glm::perspective      aq_draw_command_default
+ *     (Rendering/Renderer3D/camera.h:65-125, main.cu:115-133)
+ *   updatePositionsAndPhasesVBO                          aq_fluid_points_vbo
+ *     (Fluid/Fluid_3D_kernels.cuh:69-91)
+ *   Skybox / Container / PointSprites /                  aq_renderer_create,
+ *     FluidMeshRenderer construction and textures          aq_renderer_set_skybox,
+ *     (Skybox.cu:5-58, Container.cu:8-40)                  aq_renderer_set_logo
+ *   Fluid::draw (Fluid/Fluid_3D_FLIP.cu:396-430)         aq_fluid_draw
+ *   the frame's draws (main.cu:136-143,                  aq_renderer_draw
+ *     FluidMeshRenderer.cu:56-126, PointSprites.cu:196-256,
+ *     Container.cu:71-120, Skybox.cu:60-78)
+ *
+ * The image is row-major with row 0 at the BOTTOM of the window (the order
+ * glReadPixels returns), 4 bytes per pixel. */
+typedef enum aq_render_mode {  /* RenderMode (Rendering/DrawCommand.h:5-19) */
+  AQ_RENDER_MULTIPHASE_MESH = 0,
+  AQ_RENDER_WATER_MESH = 1,
+  AQ_RENDER_FLAT_MESH = 2,
+  AQ_RENDER_NORMAL_MESH = 3,
+  AQ_RENDER_MIRROR_MESH = 4,
+  AQ_RENDER_REFRACT_MESH = 5,
+  AQ_RENDER_PHASE0_MESH = 6,
+  AQ_RENDER_PHASE1_MESH = 7,
+  AQ_RENDER_PARTICLES = 8,
+  AQ_RENDER_NONE = 9
+} aq_render_mode;
+
+typedef enum aq_environment_mode {  /* EnvironmentMode (Rendering/DrawCommand.h:21-26) */
+  AQ_ENV_SKYBOX = 0,
+  AQ_ENV_CORNELL_BOX = 1,
+  AQ_ENV_CHESS_BOARD = 2
+} aq_environment_mode;
+
+typedef struct aq_draw_command {
+  /* DrawCommand */
+  float view[16];        /* column-major (glm layout): element (row r, col c) at [c*4 + r] */
+  float projection[16];
+  float camera_position[3];
+  int32_t window_width, window_height;
+  float fov;             /* Camera::FOV (45); the projection above already holds it */
+  float near_plane, far_plane;
+  int32_t render_mode;   /* aq_render_mode */
+  int32_t environment_mode; /* aq_environment_mode */
+  float light_position[3];
+  float container_size;
+  float cornell_box_size;
+  /* what Fluid::draw passes along (Fluid/Fluid_3D_FLIP.cu:396-430) */
+  float point_radius;    /* phase-thickness sprites: cellPhysicalSize; AQ_RENDER_PARTICLES: renderRadius */
+  int32_t phase_count;   /* FluidConfig::phaseCount */
+  float phase_colors[4][4]; /* FluidConfig::phaseColors, rgba */
+} aq_draw_command;
+
+/* The first frame's DrawCommand of main.cu for a fluid of physical size
+ * domain_size with size_y cells along y and particles_per_cell particles per
+ * cell: Camera(center) as constructed (yaw 180, pitch -30, global yaw 0,
+ * global pitch 30, radius 18, looking at the centre), glm::lookAt,
+ * glm::perspective(45, width/height, 0.1, 1000) (45 taken as radians, as
+ * glm 0.9.9 does), light (cx, 15, cy), container size domain_size, Cornell
+ * box 4x that, render mode AQ_RENDER_MULTIPHASE_MESH, environment
+ * AQ_ENV_SKYBOX, point radius cellPhysicalSize, the default phase colours. */
+aq_status aq_draw_command_default(aq_draw_command* dc, int32_t width, int32_t height, float domain_size,
+                                  int32_t size_y);
+
+/* Fills the reference's point-sprite VBO: 7 floats per particle (position
+ * xyz, volume fractions xyzw) into a DEVICE buffer of 7*N floats, in the
+ * fluid's particle order. */
+aq_status aq_fluid_points_vbo(aq_fluid* f, float* vbo);
+
+typedef struct aq_renderer aq_renderer;
+
+/* stream: cudaStream_t (NULL: a renderer-owned stream). */
+aq_status aq_renderer_create(int32_t device, void* stream, aq_renderer** out);
+void aq_renderer_destroy(aq_renderer* r);
+
+/* Skybox cube map: six face_size x face_size RGB8 images in the order posx,
+ * negx, posy, negy, posz, negz (Skybox.cu:24-44), each row-major with its
+ * first row at t = 0, as glTexImage2D receives them.  Sampled with linear
+ * filtering, clamped to the edge.  NULL clears it (samples are black). */
+aq_status aq_renderer_set_skybox(aq_renderer* r, const uint8_t* faces_rgb, int32_t face_size);
+
+/* The Cornell box's logo texture (Container::loadOxLogo, Container.cu:16-40):
+ * width x height RGB8, first row at t = 0; linear, clamped.  NULL clears it. */
+aq_status aq_renderer_set_logo(aq_renderer* r, const uint8_t* rgb, int32_t width, int32_t height);
+
+/* One frame.  points: DEVICE point-sprite VBO (7 floats per point) or NULL
+ * when n_points is 0; mesh: DEVICE mesh VBO (6 floats per vertex, position
+ * and normal, triangles of 3 consecutive vertices; aq_fluid_mesh writes 90
+ * floats per record = 15 vertices) or NULL when n_vertices is 0; rgba:
+ * DEVICE buffer of window_width*window_height*4 bytes, or NULL for the
+ * renderer's own image buffer.  The mesh modes use
+ * the points only for the phase thickness (modes 0, 5, 6, 7).  Enqueued on
+ * the renderer's stream; aq_renderer_synchronize waits for it. */
+aq_status aq_renderer_draw(aq_renderer* r, const aq_draw_command* dc, const float* points, int32_t n_points,
+                           const float* mesh, int64_t n_vertices, uint8_t* rgba);
+aq_status aq_renderer_synchronize(aq_renderer* r);
+
+/* Fluid::draw(drawCommand) (Fluid/Fluid_3D_FLIP.cu:396-430): meshes the
+ * current particles (mesh modes; the reference re-meshes whenever the
+ * simulation is not paused), fills the point-sprite VBO and draws, all into
+ * renderer-owned buffers, the image into rgba (DEVICE, W*H*4 bytes) or, when
+ * rgba is NULL, into a renderer-owned image that aq_renderer_download_image
+ * copies out. */
+aq_status aq_fluid_draw(aq_fluid* f, aq_renderer* r, const aq_draw_command* dc, uint8_t* rgba);
+
+/* The last frame's image (W*H*4 bytes, row 0 at the bottom) into HOST memory. */
+aq_status aq_renderer_download_image(aq_renderer* r, uint8_t* host);
+
+/* The last frame's phase-thickness texture (PointSprites::phaseThicknessTexture):
+ * window_width*window_height*4 floats, row 0 at the bottom, into HOST memory.
+ * Zero when the last frame had no phase pass. */
+aq_status aq_renderer_download_phase_thickness(aq_renderer* r, float* host);
+
+/* Kernel launches of the last aq_renderer_draw. */
+aq_status aq_renderer_launches(const aq_renderer* r, int32_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,6 +5,7 @@
   (needs a GPU; present only where oracle/Makefile's ``ref`` target was built).
 * ``RefMesher``: the reference's own surface mesher, oracle/_ref/libaqmesh.so
   (target ``mesh``; needs a GPU).
+* ``RenderOracle``: the CPU restatement of the headless frame (render_oracle.c).
 """
 from __future__ import annotations
 
@@ -76,6 +77,15 @@ def _load_oracle():
         lib.orc_tex_linear.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int]
         lib.orc_mesh.restype = ct.c_int
         lib.orc_mesh.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_longlong, ct.POINTER(ct.c_int)]
+        P = ct.c_void_p
+        lib.orc_render_frame.restype = ct.c_int
+        lib.orc_render_frame.argtypes = [P, P, ct.c_int32, P, ct.c_int64, P, ct.c_int32, P, ct.c_int32, ct.c_int32,
+                                         P, P]
+        lib.orc_trace_environment.argtypes = [P, P, ct.c_int32, P, ct.c_int32, ct.c_int32, P, P, P]
+        lib.orc_shade_mesh.argtypes = [P, P, ct.c_int32, P, ct.c_int32, ct.c_int32, P, P, P, P]
+        lib.orc_sample_cube.argtypes = [P, ct.c_int32, P, P]
+        lib.orc_sample_2d.argtypes = [P, ct.c_int32, ct.c_int32, ct.c_float, ct.c_float, P]
+        lib.orc_draw_command_default.argtypes = [P, ct.c_int32, ct.c_int32, ct.c_float, ct.c_int32]
         _orc = lib
     return _orc
 
@@ -539,3 +549,57 @@ class RefSph(_SphStateIO):
             self.close()
         except Exception:
             pass
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class RenderOracle:
+    """render_oracle.c: one frame drawn GL-style on the CPU (test infrastructure)."""
+
+    def __init__(self, sky=None, logo=None):
+        self.lib = _load_oracle()
+        self.sky = None if sky is None else np.ascontiguousarray(sky, np.uint8)
+        self.logo = None if logo is None else np.ascontiguousarray(logo, np.uint8)
+        self.face = 0 if self.sky is None else int(self.sky.shape[1])
+        self.lw = 0 if self.logo is None else int(self.logo.shape[1])
+        self.lh = 0 if self.logo is None else int(self.logo.shape[0])
+
+    def frame(self, dc, points=None, mesh=None):
+        """points: float32 [N, 7]; mesh: float32 [V, 6].  Returns (rgba [H, W, 4], phase [H, W, 4])."""
+        h, w = dc.window_height, dc.window_width
+        rgba = np.zeros((h, w, 4), np.uint8)
+        phase = np.zeros((h, w, 4), np.float32)
+        pts = None if points is None else np.ascontiguousarray(points, np.float32).reshape(-1, 7)
+        msh = None if mesh is None else np.ascontiguousarray(mesh, np.float32).reshape(-1, 6)
+        rc = self.lib.orc_render_frame(ct.byref(dc), _ptr(pts), 0 if pts is None else pts.shape[0], _ptr(msh),
+                                       0 if msh is None else msh.shape[0], _ptr(self.sky), self.face,
+                                       _ptr(self.logo), self.lw, self.lh, rgba.ctypes.data, phase.ctypes.data)
+        if rc != 0:
+            raise ValueError("orc_render_frame rejected its arguments")
+        return rgba, phase
+
+    def trace(self, dc, origin, direction):
+        o = np.ascontiguousarray(origin, np.float32)
+        d = np.ascontiguousarray(direction, np.float32)
+        out = np.zeros(4, np.float32)
+        self.lib.orc_trace_environment(ct.byref(dc), _ptr(self.sky), self.face, _ptr(self.logo), self.lw, self.lh,
+                                       o.ctypes.data, d.ctypes.data, out.ctypes.data)
+        return out
+
+    def shade_mesh(self, dc, frag_pos, frag_normal, texel):
+        p = np.ascontiguousarray(frag_pos, np.float32)
+        n = np.ascontiguousarray(frag_normal, np.float32)
+        t = np.ascontiguousarray(texel, np.float32)
+        out = np.zeros(4, np.float32)
+        self.lib.orc_shade_mesh(ct.byref(dc), _ptr(self.sky), self.face, _ptr(self.logo), self.lw, self.lh,
+                                p.ctypes.data, n.ctypes.data, t.ctypes.data, out.ctypes.data)
+        return out
+
+    @staticmethod
+    def draw_command_default(width, height, domain_size, size_y):
+        dc = _abi.DrawCommand()
+        _load_oracle().orc_draw_command_default(ct.byref(dc), int(width), int(height), float(domain_size),
+                                                int(size_y))
+        return dc
