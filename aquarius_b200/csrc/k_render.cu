@@ -34,6 +34,7 @@ namespace aqb {
 namespace {
 
 constexpr int kT = kRenderTile;  // tile edge in pixels
+static_assert(kT == 16, "a warp holds two 16-pixel rows of a tile");
 
 // Container::bottomData (Rendering/Renderer3D/Container.h:41-90): the unit
 // cube's six faces as 12 triangles, floor first.
@@ -512,14 +513,39 @@ __global__ void __launch_bounds__(1024) k_tile_ranges(const unsigned* __restrict
 }
 
 // drawPhaseThickness: per tile, the sprites in submission order, summed.
+// Each warp owns an 8x4 pixel block of the 16x16 tile; per batch of 32
+// sprites it ballots which reach its block (the coverage test's own bounds)
+// and visits only those, lowest index first, so every pixel still sums in
+// submission order.  Inside a sprite's square, the disc test
+// sqrt(cx^2 + cy^2) >= 1 of PointSprites_phase_fs.glsl is decided from the
+// squared distance to the centre when that lies outside a +-2e-5 relative
+// band around the radius (the rounding of the exact path is below 1e-6
+// relative there), and by the exact gl_PointCoord arithmetic inside it: the
+// same fragments survive as in sprite_fragment.
+__device__ __forceinline__ bool sprite_disc(const float4& s, float px, float py) {
+  const float h = fm(s.z, 0.5f);
+  if (!(px >= fs(s.x, h) && px < fa(s.x, h) && py >= fs(s.y, h) && py < fa(s.y, h))) return false;
+  const float dx = fs(px, s.x), dy = fs(py, s.y);
+  const float r2 = fa(fm(dx, dx), fm(dy, dy)), R2 = fm(h, h);
+  if (r2 < fm(R2, 0.99998f)) return true;
+  if (r2 > fm(R2, 1.00002f)) return false;
+  const float ps = fa(fd(dx, s.z), 0.5f), pt = fa(fd(dy, s.z), 0.5f);
+  const float x = fs(fm(ps, 2.0f), 1.0f), y = fs(fm(pt, 2.0f), 1.0f);
+  return fsq(fa(fm(x, x), fm(y, y))) < 1.0f;
+}
+
 __global__ void __launch_bounds__(kT * kT) k_phase(RenderParams P, const int2* __restrict__ range,
                                                    const int* __restrict__ vals, const float4* __restrict__ spr,
                                                    const float4* __restrict__ frac, float4* __restrict__ phase) {
   __shared__ float4 s_spr[kT * kT], s_frac[kT * kT];
   const int tile = blockIdx.x;
   const int tx = tile % P.tiles_x, ty = tile / P.tiles_x;
-  const int i = tx * kT + (threadIdx.x % kT), j = ty * kT + (threadIdx.x / kT);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int bx = tx * kT + (warp & 1) * 8, by = ty * kT + (warp >> 1) * 4;  // the warp's 8x4 block
+  const int i = bx + (lane & 7), j = by + (lane >> 3);
   const float px = fa((float)i, 0.5f), py = fa((float)j, 0.5f);
+  const float bx0 = fa((float)bx, 0.5f), bx1 = fa((float)(bx + 7), 0.5f);
+  const float by0 = fa((float)by, 0.5f), by1 = fa((float)(by + 3), 0.5f);
   const int2 r = range[tile];
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   for (int b = r.x; b < r.y; b += kT * kT) {
@@ -531,11 +557,22 @@ __global__ void __launch_bounds__(kT * kT) k_phase(RenderParams P, const int2* _
       s_frac[threadIdx.x] = frac[id];
     }
     __syncthreads();
-    for (int k = 0; k < m; ++k) {
-      float cx, cy;
-      if (!sprite_fragment(s_spr[k], px, py, cx, cy)) continue;
-      const float4 f = s_frac[k];
-      acc.x = fa(acc.x, f.x); acc.y = fa(acc.y, f.y); acc.z = fa(acc.z, f.z); acc.w = fa(acc.w, f.w);
+    for (int k0 = 0; k0 < m; k0 += 32) {
+      const int k = k0 + lane;
+      bool hit = false;
+      if (k < m) {
+        const float4 sk = s_spr[k];
+        const float h = fm(sk.z, 0.5f);
+        hit = bx1 >= fs(sk.x, h) && bx0 < fa(sk.x, h) && by1 >= fs(sk.y, h) && by0 < fa(sk.y, h);
+      }
+      unsigned mask = __ballot_sync(0xffffffffu, hit);
+      while (mask) {
+        const int q = k0 + __ffs(mask) - 1;
+        mask &= mask - 1;
+        if (!sprite_disc(s_spr[q], px, py)) continue;
+        const float4 f = s_frac[q];
+        acc.x = fa(acc.x, f.x); acc.y = fa(acc.y, f.y); acc.z = fa(acc.z, f.z); acc.w = fa(acc.w, f.w);
+      }
     }
   }
   if (i < P.W && j < P.H) phase[(size_t)j * P.W + i] = acc;
@@ -605,14 +642,27 @@ __global__ void __launch_bounds__(kT * kT) k_frame(RenderParams P, const RenderT
     } else if (P.mode == AQ_RENDER_PARTICLES) {
       const int2 r = srange[tile];
       const float px = fa((float)i, 0.5f), py = fa((float)j, 0.5f);
+      const int jw = ty * kT + (threadIdx.x / 32) * 2;  // the warp's first row
+      const float row0 = fa((float)jw, 0.5f), row1 = fa((float)(jw + 1), 0.5f);
       const float* Pm = P.proj;
       for (int b = r.x; b < r.y; b += kT * kT) {
         const int m = min(kT * kT, r.y - b);
         __syncthreads();
         if ((int)threadIdx.x < m) s_spr[threadIdx.x] = spr[svals[b + threadIdx.x]];
         __syncthreads();
-        if (!inside) continue;
-        for (int k = 0; k < m; ++k) {
+        for (int k0 = 0; k0 < m; k0 += 32) {
+          const int kk = k0 + (threadIdx.x & 31);
+          bool hit = false;
+          if (kk < m) {
+            const float4 sk = s_spr[kk];
+            const float h = fm(sk.z, 0.5f), ly = fs(sk.y, h), hy = fa(sk.y, h);
+            hit = (row0 >= ly && row0 < hy) || (row1 >= ly && row1 < hy);
+          }
+          unsigned mask = __ballot_sync(0xffffffffu, hit);
+          if (!inside) continue;
+          while (mask) {
+          const int k = k0 + __ffs(mask) - 1;
+          mask &= mask - 1;
           float cx, cy;
           const float4 s = s_spr[k];
           if (!sprite_fragment(s, px, py, cx, cy)) continue;
@@ -627,6 +677,7 @@ __global__ void __launch_bounds__(kT * kT) k_frame(RenderParams P, const RenderT
           if (!(d < depth)) continue;
           depth = d;
           color = blend(color, mk4(fm(diffuse, 0.0f), fm(diffuse, 0.0f), fm(diffuse, 1.0f), 1.0f));
+          }
         }
       }
     }
