@@ -522,22 +522,15 @@ __global__ void __launch_bounds__(1024) k_tile_ranges(const unsigned* __restrict
 // band around the radius (the rounding of the exact path is below 1e-6
 // relative there), and by the exact gl_PointCoord arithmetic inside it: the
 // same fragments survive as in sprite_fragment.
-__device__ __forceinline__ bool sprite_disc(const float4& s, float px, float py) {
-  const float h = fm(s.z, 0.5f);
-  if (!(px >= fs(s.x, h) && px < fa(s.x, h) && py >= fs(s.y, h) && py < fa(s.y, h))) return false;
-  const float dx = fs(px, s.x), dy = fs(py, s.y);
-  const float r2 = fa(fm(dx, dx), fm(dy, dy)), R2 = fm(h, h);
-  if (r2 < fm(R2, 0.99998f)) return true;
-  if (r2 > fm(R2, 1.00002f)) return false;
-  const float ps = fa(fd(dx, s.z), 0.5f), pt = fa(fd(dy, s.z), 0.5f);
-  const float x = fs(fm(ps, 2.0f), 1.0f), y = fs(fm(pt, 2.0f), 1.0f);
-  return fsq(fa(fm(x, x), fm(y, y))) < 1.0f;
-}
-
 __global__ void __launch_bounds__(kT * kT) k_phase(RenderParams P, const int2* __restrict__ range,
                                                    const int* __restrict__ vals, const float4* __restrict__ spr,
                                                    const float4* __restrict__ frac, float4* __restrict__ phase) {
-  __shared__ float4 s_spr[kT * kT], s_frac[kT * kT];
+  // Warps run independently (no CTA barrier: their blocks take unequal
+  // work).  Each stages 32 sprites at a time in its own shared slice: the
+  // square [lx, hx) x [ly, hy), centre, squared-radius band, size and (for
+  // sprites that reach the block) the fractions.
+  __shared__ float4 s_box[8][32], s_ctr[8][32], s_frac[8][32];
+  __shared__ float s_size[8][32];
   const int tile = blockIdx.x;
   const int tx = tile % P.tiles_x, ty = tile / P.tiles_x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -546,33 +539,48 @@ __global__ void __launch_bounds__(kT * kT) k_phase(RenderParams P, const int2* _
   const float px = fa((float)i, 0.5f), py = fa((float)j, 0.5f);
   const float bx0 = fa((float)bx, 0.5f), bx1 = fa((float)(bx + 7), 0.5f);
   const float by0 = fa((float)by, 0.5f), by1 = fa((float)(by + 3), 0.5f);
+  float4* box = s_box[warp];
+  float4* ctr = s_ctr[warp];
+  float4* fr = s_frac[warp];
+  float* sz = s_size[warp];
   const int2 r = range[tile];
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (int b = r.x; b < r.y; b += kT * kT) {
-    const int m = min(kT * kT, r.y - b);
-    __syncthreads();
-    if ((int)threadIdx.x < m) {
-      const int id = vals[b + threadIdx.x];
-      s_spr[threadIdx.x] = spr[id];
-      s_frac[threadIdx.x] = frac[id];
+  for (int b = r.x; b < r.y; b += 32) {
+    const int k = b + lane;
+    bool hit = false;
+    __syncwarp();
+    if (k < r.y) {
+      const int id = __ldg(vals + k);
+      const float4 sp = __ldg(spr + id);
+      const float h = fm(sp.z, 0.5f), R2 = fm(h, h);
+      const float4 bk = make_float4(fs(sp.x, h), fa(sp.x, h), fs(sp.y, h), fa(sp.y, h));
+      hit = bx1 >= bk.x && bx0 < bk.y && by1 >= bk.z && by0 < bk.w;
+      if (hit) {
+        box[lane] = bk;
+        ctr[lane] = make_float4(sp.x, sp.y, fm(R2, 0.99998f), fm(R2, 1.00002f));
+        sz[lane] = sp.z;
+        fr[lane] = __ldg(frac + id);
+      }
     }
-    __syncthreads();
-    for (int k0 = 0; k0 < m; k0 += 32) {
-      const int k = k0 + lane;
-      bool hit = false;
-      if (k < m) {
-        const float4 sk = s_spr[k];
-        const float h = fm(sk.z, 0.5f);
-        hit = bx1 >= fs(sk.x, h) && bx0 < fa(sk.x, h) && by1 >= fs(sk.y, h) && by0 < fa(sk.y, h);
+    unsigned mask = __ballot_sync(0xffffffffu, hit);
+    __syncwarp();
+    while (mask) {
+      const int q = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const float4 bq = box[q];
+      if (!(px >= bq.x && px < bq.y && py >= bq.z && py < bq.w)) continue;
+      const float4 c = ctr[q];
+      const float dx = fs(px, c.x), dy = fs(py, c.y);
+      const float r2 = fa(fm(dx, dx), fm(dy, dy));
+      if (r2 > c.w) continue;
+      if (!(r2 < c.z)) {  // the band: the exact gl_PointCoord arithmetic
+        const float S = sz[q];
+        const float ps = fa(fd(dx, S), 0.5f), pt = fa(fd(dy, S), 0.5f);
+        const float x = fs(fm(ps, 2.0f), 1.0f), y = fs(fm(pt, 2.0f), 1.0f);
+        if (!(fsq(fa(fm(x, x), fm(y, y))) < 1.0f)) continue;
       }
-      unsigned mask = __ballot_sync(0xffffffffu, hit);
-      while (mask) {
-        const int q = k0 + __ffs(mask) - 1;
-        mask &= mask - 1;
-        if (!sprite_disc(s_spr[q], px, py)) continue;
-        const float4 f = s_frac[q];
-        acc.x = fa(acc.x, f.x); acc.y = fa(acc.y, f.y); acc.z = fa(acc.z, f.z); acc.w = fa(acc.w, f.w);
-      }
+      const float4 f = fr[q];
+      acc.x = fa(acc.x, f.x); acc.y = fa(acc.y, f.y); acc.z = fa(acc.z, f.z); acc.w = fa(acc.w, f.w);
     }
   }
   if (i < P.W && j < P.H) phase[(size_t)j * P.W + i] = acc;
