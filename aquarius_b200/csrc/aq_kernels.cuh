@@ -318,10 +318,12 @@ cudaError_t launch_pcg_init(cudaStream_t st, const Dims& d, const int8_t* type, 
 
 
 // ------------------------------------------------------------ headless frame
-constexpr int kRenderTile = 16;  // screen tile edge in pixels (one CTA per tile)
+constexpr int kRenderTile = 16;  // screen tile edge in pixels (one CTA per tile; triangle lists)
+constexpr int kSpriteTile = 8;   // point-sprite lists are kept per 8x8 pixels
 
 struct RenderParams {
   int W, H, tiles_x, tiles_y;
+  int stiles_x, stiles_y;  // 8x8 sprite tiles
   int mode, env, use_phase;
   float pv[16];    // projection * view (column-major)
   float view[16];
@@ -362,8 +364,11 @@ cudaError_t launch_tri_emit(cudaStream_t st, const RenderParams& P, const Render
 cudaError_t launch_container_setup(cudaStream_t st, const RenderParams& P, RenderTri* tris, int* live);
 // range[key] = [first, last+1) of each key's run in sorted keys[0..n)
 cudaError_t launch_tile_ranges(cudaStream_t st, const unsigned* keys, int n, int2* range);
-cudaError_t launch_phase(cudaStream_t st, const RenderParams& P, const int2* range, const int* vals,
-                         const float4* spr, const float4* frac, float4* phase);
+// The phase-thickness pass over the 8x8 sprite tiles, in the given order.
+cudaError_t launch_phase(cudaStream_t st, const RenderParams& P, const int2* range, const int* order,
+                         const int* vals, const float4* spr, const float4* frac, float4* phase);
+// load[t] = list length of sprite tile t, ids[t] = t
+cudaError_t launch_tile_load(cudaStream_t st, const int2* range, int n, unsigned* load, int* ids);
 cudaError_t launch_frame(cudaStream_t st, const RenderParams& P, const RenderTri* ctris, const int* clive,
                          const int2* trange, const int* tvals, const RenderTri* tris, const int2* srange,
                          const int* svals, const float4* spr, const float4* phase, uchar4* rgba);

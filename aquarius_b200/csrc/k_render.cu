@@ -34,7 +34,7 @@ namespace aqb {
 namespace {
 
 constexpr int kT = kRenderTile;  // tile edge in pixels
-static_assert(kT == 16, "a warp holds two 16-pixel rows of a tile");
+static_assert(kT == 16, "a CTA of 8 warps covers a 16x16 region as 8x4 blocks");
 
 // Container::bottomData (Rendering/Renderer3D/Container.h:41-90): the unit
 // cube's six faces as 12 triangles, floor first.
@@ -407,9 +407,17 @@ __device__ __forceinline__ bool sprite_fragment(const float4& s, float px, float
   return true;
 }
 
+template <int T>
 __device__ __forceinline__ int tiles_of(int i0, int i1, int j0, int j1) {
-  return (i1 / kT - i0 / kT + 1) * (j1 / kT - j0 / kT + 1);
+  return (i1 / T - i0 / T + 1) * (j1 / T - j0 / T + 1);
 }
+
+constexpr int kS = kSpriteTile;
+static_assert(kT == 2 * kS, "a 16x16 CTA region holds 2x2 sprite tiles, one per pair of 8x4 warp blocks");
+
+// The 8x4 pixel block of warp w in the 16x16 region of CTA tile (tx, ty).
+__device__ __forceinline__ int block_x(int tx, int warp) { return tx * kT + (warp & 1) * 8; }
+__device__ __forceinline__ int block_y(int ty, int warp) { return ty * kT + (warp >> 1) * 4; }
 
 // ---------------------------------------------------------------- kernels
 __global__ void __launch_bounds__(256) k_sprite_setup(RenderParams P, const float* __restrict__ pts, int n,
@@ -422,7 +430,7 @@ __global__ void __launch_bounds__(256) k_sprite_setup(RenderParams P, const floa
     float4 s;
     int i0, i1, j0, j1;
     if (sprite_setup(P, p, s) && sprite_pixels(s, P.W, P.H, i0, i1, j0, j1)) {
-      c = tiles_of(i0, i1, j0, j1);
+      c = tiles_of<kS>(i0, i1, j0, j1);
       spr[i] = s;
       frac[i] = make_float4(p[3], p[4], p[5], p[6]);
     }
@@ -444,9 +452,9 @@ __global__ void __launch_bounds__(256) k_sprite_emit(RenderParams P, const float
   int i0, i1, j0, j1;
   sprite_pixels(spr[i], P.W, P.H, i0, i1, j0, j1);
   int k = 0;
-  for (int ty = j0 / kT; ty <= j1 / kT; ++ty)
-    for (int tx = i0 / kT; tx <= i1 / kT; ++tx) {
-      keys[base + k] = (unsigned)(ty * P.tiles_x + tx);
+  for (int ty = j0 / kS; ty <= j1 / kS; ++ty)
+    for (int tx = i0 / kS; tx <= i1 / kS; ++tx) {
+      keys[base + k] = (unsigned)(ty * P.stiles_x + tx);
       vals[base + k] = i;
       ++k;
     }
@@ -464,7 +472,7 @@ __global__ void __launch_bounds__(256) k_tri_setup(RenderParams P, const float* 
     int i0, i1, j0, j1;
     if (tri_setup(P.pv, ident, q, q + 6, q + 12, q + 3, q + 9, q + 15, P.W, P.H, tr) &&
         tri_pixels(tr, P.W, P.H, i0, i1, j0, j1)) {
-      c = tiles_of(i0, i1, j0, j1);
+      c = tiles_of<kT>(i0, i1, j0, j1);
       tris[t] = tr;
     }
     cnt[t] = c;
@@ -522,19 +530,21 @@ __global__ void __launch_bounds__(1024) k_tile_ranges(const unsigned* __restrict
 // band around the radius (the rounding of the exact path is below 1e-6
 // relative there), and by the exact gl_PointCoord arithmetic inside it: the
 // same fragments survive as in sprite_fragment.
-__global__ void __launch_bounds__(kT * kT) k_phase(RenderParams P, const int2* __restrict__ range,
-                                                   const int* __restrict__ vals, const float4* __restrict__ spr,
-                                                   const float4* __restrict__ frac, float4* __restrict__ phase) {
-  // Warps run independently (no CTA barrier: their blocks take unequal
-  // work).  Each stages 32 sprites at a time in its own shared slice: the
-  // square [lx, hx) x [ly, hy), centre, squared-radius band, size and (for
-  // sprites that reach the block) the fractions.
-  __shared__ float4 s_box[8][32], s_ctr[8][32], s_frac[8][32];
-  __shared__ float s_size[8][32];
-  const int tile = blockIdx.x;
-  const int tx = tile % P.tiles_x, ty = tile / P.tiles_x;
+__global__ void __launch_bounds__(64) k_phase(RenderParams P, const int2* __restrict__ range,
+                                              const int* __restrict__ order, const int* __restrict__ vals,
+                                              const float4* __restrict__ spr, const float4* __restrict__ frac,
+                                              float4* __restrict__ phase) {
+  // One CTA of two warps per 8x8 sprite tile, the tiles taken longest list
+  // first (order).  The warps run independently, each staging 32 sprites at
+  // a time in its own shared slice: the square [lx, hx) x [ly, hy), centre,
+  // squared-radius band, size and the fractions of the sprites that reach
+  // its 8x4 block.
+  __shared__ float4 s_box[2][32], s_ctr[2][32], s_frac[2][32];
+  __shared__ float s_size[2][32];
+  const int st = order[blockIdx.x];
+  const int sx = st % P.stiles_x, sy = st / P.stiles_x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int bx = tx * kT + (warp & 1) * 8, by = ty * kT + (warp >> 1) * 4;  // the warp's 8x4 block
+  const int bx = sx * kS, by = sy * kS + warp * 4;  // the warp's 8x4 block
   const int i = bx + (lane & 7), j = by + (lane >> 3);
   const float px = fa((float)i, 0.5f), py = fa((float)j, 0.5f);
   const float bx0 = fa((float)bx, 0.5f), bx1 = fa((float)(bx + 7), 0.5f);
@@ -543,7 +553,7 @@ __global__ void __launch_bounds__(kT * kT) k_phase(RenderParams P, const int2* _
   float4* ctr = s_ctr[warp];
   float4* fr = s_frac[warp];
   float* sz = s_size[warp];
-  const int2 r = range[tile];
+  const int2 r = range[st];
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   for (int b = r.x; b < r.y; b += 32) {
     const int k = b + lane;
@@ -586,6 +596,16 @@ __global__ void __launch_bounds__(kT * kT) k_phase(RenderParams P, const int2* _
   if (i < P.W && j < P.H) phase[(size_t)j * P.W + i] = acc;
 }
 
+// Sprite-tile list lengths (sort keys for the longest-first order) and tile ids.
+__global__ void __launch_bounds__(256) k_tile_load(const int2* __restrict__ range, int n, unsigned* __restrict__ load,
+                                                   int* __restrict__ ids) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int2 r = range[t];
+  load[t] = (unsigned)(r.y - r.x);
+  ids[t] = t;
+}
+
 // The frame: background, container faces, then the mesh or the shaded sprites.
 __global__ void __launch_bounds__(kT * kT) k_frame(RenderParams P, const RenderTri* __restrict__ ctris,
                                                    const int* __restrict__ clive, const int2* __restrict__ trange,
@@ -593,10 +613,12 @@ __global__ void __launch_bounds__(kT * kT) k_frame(RenderParams P, const RenderT
                                                    const int2* __restrict__ srange, const int* __restrict__ svals,
                                                    const float4* __restrict__ spr, const float4* __restrict__ phase,
                                                    uchar4* __restrict__ rgba) {
-  __shared__ float4 s_spr[kT * kT];
+  __shared__ float4 s_spr[8][32];
   const int tile = blockIdx.x;
   const int tx = tile % P.tiles_x, ty = tile / P.tiles_x;
-  const int i = tx * kT + (threadIdx.x % kT), j = ty * kT + (threadIdx.x / kT);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int bx = block_x(tx, warp), by = block_y(ty, warp);  // the warp's 8x4 block
+  const int i = bx + (lane & 7), j = by + (lane >> 3);
   const bool inside = i < P.W && j < P.H;
   uint32_t color = 0xff000000u;  // (0,0,0,1)
   uint32_t depth = 16777215u;
@@ -648,31 +670,33 @@ __global__ void __launch_bounds__(kT * kT) k_frame(RenderParams P, const RenderT
           color = blend(color, shade_mesh(P, mk3(a[0], a[1], a[2]), mk3(a[5], a[6], a[7]), tex));
         }
     } else if (P.mode == AQ_RENDER_PARTICLES) {
-      const int2 r = srange[tile];
+      // the warp walks its sprite tile's list, 32 sprites at a time, visiting
+      // those that reach its block lowest index first
+      const int sx = bx / kS, sy = by / kS;
+      const int2 r = (sx < P.stiles_x && sy < P.stiles_y) ? srange[sy * P.stiles_x + sx] : make_int2(0, 0);
       const float px = fa((float)i, 0.5f), py = fa((float)j, 0.5f);
-      const int jw = ty * kT + (threadIdx.x / 32) * 2;  // the warp's first row
-      const float row0 = fa((float)jw, 0.5f), row1 = fa((float)(jw + 1), 0.5f);
+      const float bx0 = fa((float)bx, 0.5f), bx1 = fa((float)(bx + 7), 0.5f);
+      const float by0 = fa((float)by, 0.5f), by1 = fa((float)(by + 3), 0.5f);
       const float* Pm = P.proj;
-      for (int b = r.x; b < r.y; b += kT * kT) {
-        const int m = min(kT * kT, r.y - b);
-        __syncthreads();
-        if ((int)threadIdx.x < m) s_spr[threadIdx.x] = spr[svals[b + threadIdx.x]];
-        __syncthreads();
-        for (int k0 = 0; k0 < m; k0 += 32) {
-          const int kk = k0 + (threadIdx.x & 31);
-          bool hit = false;
-          if (kk < m) {
-            const float4 sk = s_spr[kk];
-            const float h = fm(sk.z, 0.5f), ly = fs(sk.y, h), hy = fa(sk.y, h);
-            hit = (row0 >= ly && row0 < hy) || (row1 >= ly && row1 < hy);
-          }
-          unsigned mask = __ballot_sync(0xffffffffu, hit);
-          if (!inside) continue;
-          while (mask) {
-          const int k = k0 + __ffs(mask) - 1;
+      float4* ws = s_spr[warp];
+      for (int b = r.x; b < r.y; b += 32) {
+        const int kk = b + lane;
+        bool hit = false;
+        __syncwarp();
+        if (kk < r.y) {
+          const float4 sk = __ldg(spr + __ldg(svals + kk));
+          const float h = fm(sk.z, 0.5f);
+          hit = bx1 >= fs(sk.x, h) && bx0 < fa(sk.x, h) && by1 >= fs(sk.y, h) && by0 < fa(sk.y, h);
+          if (hit) ws[lane] = sk;
+        }
+        unsigned mask = __ballot_sync(0xffffffffu, hit);
+        __syncwarp();
+        if (!inside) continue;
+        while (mask) {
+          const int q = __ffs(mask) - 1;
           mask &= mask - 1;
           float cx, cy;
-          const float4 s = s_spr[k];
+          const float4 s = ws[q];
           if (!sprite_fragment(s, px, py, cx, cy)) continue;
           const float zs = fsq(fs(fs(1.0f, fm(cx, cx)), fm(cy, cy)));
           float diffuse = gmax(0.0f, fa(fa(fm(0.0f, cx), fm(1.0f, cy)), fm(0.0f, zs)));
@@ -685,7 +709,6 @@ __global__ void __launch_bounds__(kT * kT) k_frame(RenderParams P, const RenderT
           if (!(d < depth)) continue;
           depth = d;
           color = blend(color, mk4(fm(diffuse, 0.0f), fm(diffuse, 0.0f), fm(diffuse, 1.0f), 1.0f));
-          }
         }
       }
     }
@@ -745,9 +768,15 @@ cudaError_t launch_tile_ranges(cudaStream_t st, const unsigned* keys, int n, int
   return cudaGetLastError();
 }
 
-cudaError_t launch_phase(cudaStream_t st, const RenderParams& P, const int2* range, const int* vals,
-                         const float4* spr, const float4* frac, float4* phase) {
-  k_phase<<<P.tiles_x * P.tiles_y, kT * kT, 0, st>>>(P, range, vals, spr, frac, phase);
+cudaError_t launch_phase(cudaStream_t st, const RenderParams& P, const int2* range, const int* order,
+                         const int* vals, const float4* spr, const float4* frac, float4* phase) {
+  k_phase<<<P.stiles_x * P.stiles_y, 64, 0, st>>>(P, range, order, vals, spr, frac, phase);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tile_load(cudaStream_t st, const int2* range, int n, unsigned* load, int* ids) {
+  if (n <= 0) return cudaSuccess;
+  k_tile_load<<<(n + 255) / 256, 256, 0, st>>>(range, n, load, ids);
   return cudaGetLastError();
 }
 

@@ -119,6 +119,8 @@ struct aq_renderer {
   DevBuf<unsigned> skeys, skeys2, tkeys, tkeys2;
   DevBuf<int> svals, svals2, tvals, tvals2;
   DevBuf<int2> srange, trange;
+  DevBuf<unsigned> tload, tload2;  // sprite-tile list lengths (longest-first order)
+  DevBuf<int> tids, torder;
   DevBuf<unsigned long long> totals;
   DevBuf<unsigned char> cub_tmp;
   DevBuf<uchar4> image;          // the image when the caller passes none
@@ -138,6 +140,7 @@ struct aq_renderer {
     skeys.release(); skeys2.release(); tkeys.release(); tkeys2.release();
     srange.release(); trange.release(); totals.release(); cub_tmp.release();
     image.release(); points_vbo.release(); mesh_vbo.release();
+    tload.release(); tload2.release(); tids.release(); torder.release();
     if (sky) cudaFree(sky);
     if (logo) cudaFree(logo);
     if (totals_host) cudaFreeHost(totals_host);
@@ -299,6 +302,8 @@ aq_status aq_renderer_draw(aq_renderer* r, const aq_draw_command* dc, const floa
   P.H = dc->window_height;
   P.tiles_x = (P.W + kRenderTile - 1) / kRenderTile;
   P.tiles_y = (P.H + kRenderTile - 1) / kRenderTile;
+  P.stiles_x = (P.W + kSpriteTile - 1) / kSpriteTile;
+  P.stiles_y = (P.H + kSpriteTile - 1) / kSpriteTile;
   P.mode = dc->render_mode;
   P.env = dc->environment_mode;
   mat_mul(dc->projection, dc->view, P.pv);
@@ -343,20 +348,20 @@ aq_status aq_renderer_draw(aq_renderer* r, const aq_draw_command* dc, const floa
   const bool need_tri = ntri > 0;
   P.use_phase = (mesh_mode && multiphase && n_points > 0) ? 1 : 0;
 
-  const int ntiles = P.tiles_x * P.tiles_y;
+  const int ntiles = P.tiles_x * P.tiles_y, nstiles = P.stiles_x * P.stiles_y;
   const size_t npx = (size_t)P.W * P.H;
   if (!rgba) {
     AQR_TRY(r->image.ensure(npx));
     rgba = reinterpret_cast<uint8_t*>(r->image.p);
   }
   AQR_TRY(r->phase.ensure(npx));
-  AQR_TRY(r->srange.ensure((size_t)ntiles));
+  AQR_TRY(r->srange.ensure((size_t)nstiles));
   AQR_TRY(r->trange.ensure((size_t)ntiles));
   AQR_TRY(r->ctris.ensure(12));
   AQR_TRY(r->clive.ensure(12));
   AQR_TRY(r->totals.ensure(2));
   AQR_CUDA(cudaMemsetAsync(r->totals.p, 0, 2 * sizeof(unsigned long long), st));
-  AQR_CUDA(cudaMemsetAsync(r->srange.p, 0, sizeof(int2) * ntiles, st));
+  AQR_CUDA(cudaMemsetAsync(r->srange.p, 0, sizeof(int2) * nstiles, st));
   AQR_CUDA(cudaMemsetAsync(r->trange.p, 0, sizeof(int2) * ntiles, st));
   if (need_spr) {
     const size_t n = (size_t)n_points;
@@ -399,7 +404,7 @@ aq_status aq_renderer_draw(aq_renderer* r, const aq_draw_command* dc, const floa
     AQR_TRY(r->svals.ensure(np)); AQR_TRY(r->svals2.ensure(np));
     AQR_CUDA(launch_sprite_emit(st, P, r->spr.p, r->soff.p, n_points, r->skeys.p, r->svals.p));
     ++r->launches;
-    AQR_TRY(r->sort_pairs(r->skeys, r->skeys2, r->svals, r->svals2, np, ntiles, r->srange));
+    AQR_TRY(r->sort_pairs(r->skeys, r->skeys2, r->svals, r->svals2, np, nstiles, r->srange));
   }
   if (need_tri && r->totals_host[1] > 0) {
     const int np = (int)r->totals_host[1];
@@ -410,8 +415,18 @@ aq_status aq_renderer_draw(aq_renderer* r, const aq_draw_command* dc, const floa
     AQR_TRY(r->sort_pairs(r->tkeys, r->tkeys2, r->tvals, r->tvals2, np, ntiles, r->trange));
   }
   if (P.use_phase) {
-    AQR_CUDA(launch_phase(st, P, r->srange.p, r->svals2.p, r->spr.p, r->frac.p, r->phase.p));
-    ++r->launches;
+    // sprite tiles longest list first, so the heaviest start in the first wave
+    AQR_TRY(r->tload.ensure(nstiles)); AQR_TRY(r->tload2.ensure(nstiles));
+    AQR_TRY(r->tids.ensure(nstiles)); AQR_TRY(r->torder.ensure(nstiles));
+    AQR_CUDA(launch_tile_load(st, r->srange.p, nstiles, r->tload.p, r->tids.p));
+    size_t bytes = 0;
+    AQR_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, r->tload.p, r->tload2.p, r->tids.p,
+                                                       r->torder.p, nstiles, 0, 32, st));
+    AQR_TRY(r->cub_tmp.ensure(bytes));
+    AQR_CUDA(cub::DeviceRadixSort::SortPairsDescending(r->cub_tmp.p, bytes, r->tload.p, r->tload2.p, r->tids.p,
+                                                       r->torder.p, nstiles, 0, 32, st));
+    AQR_CUDA(launch_phase(st, P, r->srange.p, r->torder.p, r->svals2.p, r->spr.p, r->frac.p, r->phase.p));
+    r->launches += 2;
   } else {
     AQR_CUDA(cudaMemsetAsync(r->phase.p, 0, sizeof(float4) * npx, st));
   }
