@@ -32,6 +32,14 @@ reference's own state (teacher forcing).  It also records:
     seeded configs: the state after init and after each of three steps.
 
     python tests/golden/make_golden.py --out tests/golden --only sph
+  * the shading of the headless frame (ref_shade.npz), through the
+    reference's own fragment shaders and camera compiled as C++ on the CPU
+    (oracle/_ref/libaqshade.so, `make -C oracle shade`; no GPU): the default
+    camera's matrices for several windows, and seeded fragments of
+    FluidMeshRenderer_fs (every mesh mode and environment),
+    RayTraceEnvironment and Container_face_fs with their outputs.
+
+    python tests/golden/make_golden.py --out tests/golden --only shade
 """
 from __future__ import annotations
 
@@ -298,10 +306,69 @@ def texture_probe() -> dict:
     return res
 
 
+SHADE_WINDOWS = [(1728, 864, 10.0), (320, 160, 10.0), (97, 31, 3.5), (1000, 1000, 7.25)]
+
+
+def record_shade() -> dict:
+    from oracle_binding import RenderOracle
+    lib = ct.CDLL(str(ROOT / "oracle" / "_ref" / "libaqshade.so"))
+    P, I = ct.c_void_p, ct.c_int32
+    lib.aqshade_camera.argtypes = [I, I, ct.c_float, P, P, P]
+    lib.aqshade_mesh.argtypes = [P, P, I, P, I, I, P, P, P, P]
+    lib.aqshade_trace.argtypes = [P, P, I, P, I, I, P, P, P]
+    lib.aqshade_container.argtypes = [P, P, I, P, I, I, P, P]
+    rng = np.random.default_rng(2024)
+    sky = rng.integers(0, 256, (6, 16, 16, 3), dtype=np.uint8)
+    logo = rng.integers(0, 256, (12, 20, 3), dtype=np.uint8)
+    res = {"sky": sky, "logo": logo, "windows": np.array(SHADE_WINDOWS, np.float32)}
+    views, projs, eyes = [], [], []
+    for w, h, size in SHADE_WINDOWS:
+        v, p, e = np.zeros(16, np.float32), np.zeros(16, np.float32), np.zeros(3, np.float32)
+        lib.aqshade_camera(int(w), int(h), float(size), v.ctypes.data, p.ctypes.data, e.ctypes.data)
+        views.append(v); projs.append(p); eyes.append(e)
+    res.update(cam_view=np.array(views), cam_projection=np.array(projs), cam_eye=np.array(eyes))
+    dc = RenderOracle.draw_command_default(320, 160, 10.0, 32)
+    n = 128
+    mesh_in, mesh_out, trace_in, trace_out, cont_in, cont_out = [], [], [], [], [], []
+    for env in range(3):
+        dc.environment_mode = env
+        for mode in range(8):
+            dc.render_mode = mode
+            for _ in range(n):
+                pos = rng.uniform(-2, 12, 3).astype(np.float32)
+                nrm = rng.normal(size=3).astype(np.float32)
+                tex = (rng.uniform(0, 60, 4) * (rng.random(4) < 0.7)).astype(np.float32)
+                out = np.zeros(4, np.float32)
+                lib.aqshade_mesh(ct.addressof(dc), sky.ctypes.data, 16, logo.ctypes.data, 20, 12, pos.ctypes.data,
+                                 nrm.ctypes.data, tex.ctypes.data, out.ctypes.data)
+                mesh_in.append(np.concatenate([[env, mode], pos, nrm, tex]).astype(np.float32))
+                mesh_out.append(out)
+        for k in range(4 * n):
+            org = rng.uniform(-10, 20, 3).astype(np.float32)
+            d = rng.normal(size=3).astype(np.float32)
+            if k % 7 == 0:
+                d[rng.integers(3)] = 0
+            out = np.zeros(4, np.float32)
+            lib.aqshade_trace(ct.addressof(dc), sky.ctypes.data, 16, logo.ctypes.data, 20, 12, org.ctypes.data,
+                              d.ctypes.data, out.ctypes.data)
+            trace_in.append(np.concatenate([[env], org, d]).astype(np.float32))
+            trace_out.append(out)
+        for _ in range(n):
+            pos = rng.uniform(-15, 25, 3).astype(np.float32)
+            out = np.zeros(4, np.float32)
+            lib.aqshade_container(ct.addressof(dc), sky.ctypes.data, 16, logo.ctypes.data, 20, 12, pos.ctypes.data,
+                                  out.ctypes.data)
+            cont_in.append(np.concatenate([[env], pos]).astype(np.float32))
+            cont_out.append(out)
+    res.update(mesh_in=np.array(mesh_in), mesh_out=np.array(mesh_out), trace_in=np.array(trace_in),
+               trace_out=np.array(trace_out), container_in=np.array(cont_in), container_out=np.array(cont_out))
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
-    ap.add_argument("--only", choices=["all", "ink", "mesh", "sph"], default="all")
+    ap.add_argument("--only", choices=["all", "ink", "mesh", "sph", "shade"], default="all")
     a = ap.parse_args()
     out = pathlib.Path(a.out)
     out.mkdir(parents=True, exist_ok=True)
@@ -312,6 +379,9 @@ def main():
     if a.only in ("all", "sph"):
         np.savez_compressed(out / "ref_sph.npz", **record_sph())
         print("sph fixtures recorded")
+    if a.only in ("all", "shade"):
+        np.savez_compressed(out / "ref_shade.npz", **record_shade())
+        print("shade fixtures recorded")
     if a.only in ("all", "ink"):
         np.savez_compressed(out / "ref_ink.npz", **record_ink())
         print("ink fixtures recorded")

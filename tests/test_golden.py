@@ -163,3 +163,49 @@ def test_sph_oracle_against_reference_fixtures(method):
         o.set_state(sph_fixture_state(data, method, s))
         o.step(1)
         assert judge_sph_step(method, o.get_state(), sph_fixture_state(data, method, s + 1)) == [], s
+
+
+# ------------------------------------------------------------ frame shading
+def _shade_fixture():
+    return np.load(GOLDEN / "ref_shade.npz")
+
+
+def test_default_camera_matches_reference_camera():
+    """aq_draw_command_default against the reference's Camera + glm::lookAt /
+    glm::perspective compiled from its own sources (bit for bit)."""
+    import aquarius_b200 as aq
+    from oracle_binding import RenderOracle
+    g = _shade_fixture()
+    for (w, h, size), v, p, e in zip(g["windows"], g["cam_view"], g["cam_projection"], g["cam_eye"]):
+        for dc in (aq.draw_command_default(int(w), int(h), float(size), 32),
+                   RenderOracle.draw_command_default(int(w), int(h), float(size), 32)):
+            np.testing.assert_array_equal(np.array(dc.view, np.float32).view(np.uint32), v.view(np.uint32))
+            np.testing.assert_array_equal(np.array(dc.projection, np.float32).view(np.uint32), p.view(np.uint32))
+            np.testing.assert_array_equal(np.array(dc.camera_position, np.float32).view(np.uint32), e.view(np.uint32))
+
+
+def test_shading_matches_reference_shaders():
+    """The oracle's shading (FluidMeshRenderer_fs, RayTraceEnvironment,
+    Container_face_fs restated in render_oracle.c) against the reference's own
+    GLSL compiled as C++ (oracle/shade_harness.cpp), bit for bit, in every mesh
+    mode and environment."""
+    from oracle_binding import RenderOracle
+    g = _shade_fixture()
+    o = RenderOracle(sky=g["sky"], logo=g["logo"])
+    dc = RenderOracle.draw_command_default(320, 160, 10.0, 32)
+    for row, want in zip(g["mesh_in"], g["mesh_out"]):
+        dc.environment_mode, dc.render_mode = int(row[0]), int(row[1])
+        got = o.shade_mesh(dc, row[2:5], row[5:8], row[8:12])
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32), err_msg=str(row))
+    for row, want in zip(g["trace_in"], g["trace_out"]):
+        dc.environment_mode = int(row[0])
+        got = o.trace(dc, row[1:4], row[4:7])
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32), err_msg=str(row))
+    cam = np.array(dc.camera_position, np.float32)
+    for row, want in zip(g["container_in"], g["container_out"]):
+        dc.environment_mode = int(row[0])
+        d = (row[1:4] - cam).astype(np.float32)
+        dd = np.float32(np.float32(d[0] * d[0] + d[1] * d[1]) + np.float32(d[2] * d[2]))
+        d = (d * np.float32(np.float32(1.0) / np.sqrt(dd))).astype(np.float32)  # GLSL normalize
+        got = o.trace(dc, cam, d)
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32), err_msg=str(row))
