@@ -25,8 +25,9 @@ namespace {
 
 using bf16 = __nv_bfloat16;
 
-// Forward convolution variant: halo-tiled (default) or im2col streaming.
-bool g_conv_tiled = true;
+// Forward convolution variant: 1 = halo-tiled mma.sync (default, the
+// fastest measured), 2 = tcgen05 UMMA, 0 = im2col streaming mma.sync.
+int g_conv_impl = 1;
 
 constexpr int kTileM = 128;  // voxels per forward CTA (4 warps x 32)
 constexpr int kRowK = 24;    // smem row of one 16-wide k chunk: 16 + 8 pad bf16 (48 B, conflict-free ldmatrix)
@@ -273,6 +274,246 @@ __global__ void __launch_bounds__(256) k_conv3_fwd_tile(const bf16* __restrict__
   }
 }
 
+// ------------------------------------------------- forward on tcgen05 (TMEM)
+// The same 4 (x) x 4 (y) x 16 (z) output block and staged input halo as
+// k_conv3_fwd_tile, as two M = 128 tiles (x pairs) of a UMMA implicit GEMM:
+// per tap, every thread copies its voxel's shifted input row from the halo
+// into the A tile of its M tile, in the canonical K-major no-swizzle layout
+// (8-row x 16-byte core matrices: +16 B per row, +128 B per 8 channels,
+// +256 B per 8 rows, +4 KB per 16 channels); the tap's weights (B, N = COUT
+// rows, same layout) arrive by cp.async; one thread issues
+// tcgen05.mma.cta_group::1.kind::f16 (bf16 x bf16 -> f32) for both tiles over
+// the tap's CIN/16 k-steps into TMEM and commits to the buffer's mbarrier.
+// Up to D = 4 taps' MMAs are in flight (A and weight slots in rings, one
+// mbarrier per tap slot) and the weights of the next P <= 8 taps are loading.  The epilogue reads each thread's row back
+// with tcgen05.ld (warp w: TMEM lanes 32 (w % 4) ..., tile w / 4).  Every
+// mbarrier wait is bounded: on a timeout the kernel records it in
+// g_umma_timeout and carries on to free its TMEM.
+// Measured against k_conv3_fwd_tile on B200 (16->16 at 128^3: 329 vs 173 us;
+// 64->64 at 32^3: 34 vs 30 us), so it is not the default: ncu shows the
+// tensor pipe 4% busy, the time going to the per-tap A copy out of the halo,
+// its proxy fence and CTA barrier, at 3 CTAs per SM against 7.  Pointing the
+// descriptors straight into a chunk-major halo needs the transposed product
+// (M = COUT, N = a 16-voxel z run), which the shapes here (COUT 16 / 32)
+// would have to pad to M = 64.
+__device__ int g_umma_timeout;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: start, leading (K) and stride (M/N) byte
+// offsets of the core matrices, the fixed version bits 46-47 = 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+         (1ull << 46);
+}
+
+// Instruction descriptor, kind::f16: D f32, A and B bf16, both K-major, N, M.
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(mbar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n.reg .pred P1;\nmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\nselp.b32 %0, 1, 0, P1;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(mbar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait on an mbarrier phase; false (and the timeout recorded) if it
+// does not complete within the limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+  for (int i = 0; i < (1 << 22); ++i)
+    if (mbar_try_wait(mbar, parity)) return true;
+  atomicExch(&g_umma_timeout, 1);
+  return false;
+}
+
+template <int N>
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__host__ __device__ constexpr int tmem_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : 256; }
+
+// Pipeline shape: D taps whose MMAs may be in flight (A slots and mbarriers
+// per tap slot) and the weights of the next P taps loading (D + P weight
+// slots).  The first (D, P) of the list below that still lets two CTAs share
+// an SM, else the first that fits.
+template <int CIN, int COUT>
+__host__ __device__ constexpr size_t umma_smem_for(int d, int p) {
+  return (size_t)kHalo * (CIN + 8) * 2 + (size_t)d * (2 * CIN * 256) + (size_t)(d + p) * COUT * CIN * 2 + 1024;
+}
+
+template <int CIN, int COUT>
+__host__ __device__ constexpr int umma_shape() {  // D * 16 + P
+  constexpr int cand[8][2] = {{4, 8}, {2, 8}, {4, 4}, {2, 4}, {1, 8}, {1, 4}, {2, 2}, {1, 2}};
+  for (int pass = 0; pass < 2; ++pass)
+    for (int i = 0; i < 8; ++i)
+      if (umma_smem_for<CIN, COUT>(cand[i][0], cand[i][1]) <= (pass == 0 ? 113u : 220u) * 1024u)
+        return cand[i][0] * 16 + cand[i][1];
+  return 1 * 16 + 2;
+}
+
+template <int CIN, int COUT>
+constexpr size_t fwd_umma_smem() {
+  return umma_smem_for<CIN, COUT>(umma_shape<CIN, COUT>() / 16, umma_shape<CIN, COUT>() % 16);
+}
+
+template <int CIN, int COUT, bool RELU, bool BIAS>
+__global__ void __launch_bounds__(256) k_conv3_fwd_umma(const bf16* __restrict__ in, const bf16* __restrict__ w,
+                                                       const float* __restrict__ bias, bf16* __restrict__ out,
+                                                       int sx, int sy, int sz) {
+  static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 128, "UMMA shapes: M = 128, N = COUT");
+  constexpr int RS = CIN + 8, CH = CIN / 8, KS = CIN / 16;
+  constexpr int D = umma_shape<CIN, COUT>() / 16, P = umma_shape<CIN, COUT>() % 16;
+  constexpr int DB = D + P;                // weight slots
+  constexpr int A_TILE = CIN * 256;        // one M tile: 128 rows x CIN bf16
+  constexpr int A_BYTES = 2 * A_TILE;      // two M tiles
+  constexpr int B_BYTES = COUT * CIN * 2;  // N rows x CIN bf16
+  constexpr int COLS = tmem_cols(2 * COUT);
+  constexpr uint32_t IDESC = umma_idesc(128, COUT);
+  extern __shared__ __align__(1024) unsigned char um_smem[];
+  bf16* sH = reinterpret_cast<bf16*>(um_smem);
+  unsigned char* sA = um_smem + (size_t)kHalo * RS * 2;  // [D][A_BYTES]
+  unsigned char* sB = sA + D * A_BYTES;                  // [DB][B_BYTES]
+  __shared__ __align__(8) uint64_t s_mbar[4];            // MMAs of tap slot t % D
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int z0 = blockIdx.x * kTZ, y0 = blockIdx.y * kTY, x0 = blockIdx.z * kTX;
+  // this thread's output voxel: M tile j = tid / 128, row r = tid % 128
+  const int j = tid >> 7, r = tid & 127;
+  const int ox = j * 2 + (r >> 6), oy = (r >> 4) & 3, oz = r & 15;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&s_tmem)),
+                 "r"(COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int q = 0; q < D; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&s_mbar[q])), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  // the tap's weights: B row n = w[tap][n][0..CIN), chunk c of 8 channels
+  auto stage_b = [&](int tap) {
+    unsigned char* B = sB + (tap % DB) * B_BYTES;
+    for (int i = tid; i < COUT * CH; i += 256) {
+      const int c = i % CH, n = i / CH;
+      cp_async16(B + (c >> 1) * (COUT * 32) + (n >> 3) * 256 + (c & 1) * 128 + (n & 7) * 16,
+                 w + ((size_t)(tap * COUT + n) * CIN + c * 8), true);
+    }
+  };
+  // group 0: the halo block with tap 0's weights; groups 1..P-1: the next taps
+  for (int i = tid; i < kHalo * CH; i += 256) {
+    const int c = i % CH, h = i / CH;
+    const int hz = h % kHZ, t = h / kHZ, hy = t % kHY, hx = t / kHY;
+    const int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z0 + hz - 1;
+    const bool ok = gx >= 0 && gx < sx && gy >= 0 && gy < sy && gz >= 0 && gz < sz;
+    cp_async16(sH + h * RS + c * 8, ok ? in + ((size_t)((gx * sy + gy) * sz + gz) * CIN + c * 8) : in, ok);
+  }
+  stage_b(0);
+  cp_async_commit();
+#pragma unroll
+  for (int q = 1; q < P; ++q) {
+    stage_b(q);
+    cp_async_commit();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  bool ok_wait = true;
+  for (int tap = 0; tap < 27; ++tap) {
+    // tap slot tap % D is free once the MMAs of tap - D are done; so is the
+    // weight slot (tap + P) % DB, last read by those MMAs
+    if (tap >= D) ok_wait &= mbar_wait(&s_mbar[tap % D], (uint32_t)(((tap - D) / D) & 1));
+    if (tap + P < 27) stage_b(tap + P);
+    cp_async_commit();
+    // this thread's copies of the tap's weights (and, first, of the halo)
+    cp_async_wait<P>();
+    if (tap == 0) __syncthreads();
+    // this thread's A row for the tap, from the halo
+    unsigned char* A = sA + (tap % D) * A_BYTES;
+    int dx, dy, dz;
+    tap_offset(tap, dx, dy, dz);
+    const int h = ((ox + dx + 1) * kHY + (oy + dy + 1)) * kHZ + (oz + dz + 1);
+    const uint4* src = reinterpret_cast<const uint4*>(sH + h * RS);
+    unsigned char* arow = A + j * A_TILE + (r >> 3) * 256 + (r & 7) * 16;
+#pragma unroll
+    for (int c = 0; c < CH; ++c) *reinterpret_cast<uint4*>(arow + (c >> 1) * 4096 + (c & 1) * 128) = src[c];
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const unsigned char* B = sB + (tap % DB) * B_BYTES;
+#pragma unroll
+      for (int t = 0; t < 2; ++t)
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+          const uint64_t ad = umma_desc(smem_u32(A + t * A_TILE + ks * 4096), 128, 256);
+          const uint64_t bd = umma_desc(smem_u32(B + ks * (COUT * 32)), 128, 256);
+          umma_f16(tmem + (uint32_t)(t * COUT), ad, bd, IDESC, (tap > 0 || ks > 0) ? 1u : 0u);
+        }
+      umma_commit(&s_mbar[tap % D]);
+    }
+  }
+  // all MMAs done: the last commit covers every earlier one
+  ok_wait &= mbar_wait(&s_mbar[26 % D], (uint32_t)((26 / D) & 1));
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const int gx = x0 + ox, gy = y0 + oy, gz = z0 + oz;
+  const bool store = ok_wait && gx < sx && gy < sy && gz < sz;
+  const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(j * COUT);
+  bf16* dst = out + (size_t)((gx * sy + gy) * sz + gz) * COUT;
+#pragma unroll
+  for (int c0 = 0; c0 < COUT; c0 += 16) {
+    float v[16];
+    tmem_ld16<16>(trow + (uint32_t)c0, v);
+    if (store) {
+      __align__(16) __nv_bfloat162 pk[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        float a = v[2 * q] + (BIAS ? bias[c0 + 2 * q] : 0.f), b = v[2 * q + 1] + (BIAS ? bias[c0 + 2 * q + 1] : 0.f);
+        if (RELU) {
+          a = fmaxf(a, 0.f);
+          b = fmaxf(b, 0.f);
+        }
+        pk[q] = __floats2bfloat162_rn(a, b);
+      }
+      uint4* d4 = reinterpret_cast<uint4*>(dst + c0);
+      d4[0] = reinterpret_cast<const uint4*>(pk)[0];
+      d4[1] = reinterpret_cast<const uint4*>(pk)[1];
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(COLS));
+  }
+}
+
 // ------------------------------------------------------------- weight grad
 // grid (chunks, 27): one tap, `cv` voxels per CTA in tiles of 128.  A = dY^T
 // (COUT x voxels), B = x shifted by the tap (voxels x CIN); both staged with
@@ -390,7 +631,18 @@ __global__ void k_flip_transpose(const bf16* __restrict__ w, bf16* __restrict__ 
 template <int CIN, int COUT, bool RELU, bool BIAS>
 cudaError_t fwd_launch(cudaStream_t st, const bf16* in, const bf16* w, const float* b, bf16* out, int sx, int sy,
                        int sz) {
-  if (g_conv_tiled) {
+  if constexpr (COUT % 16 == 0 && COUT <= 128) {
+    if (g_conv_impl == 2) {
+      constexpr size_t smem = fwd_umma_smem<CIN, COUT>();
+      static const cudaError_t attr = cudaFuncSetAttribute(
+          k_conv3_fwd_umma<CIN, COUT, RELU, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (attr != cudaSuccess) return attr;
+      const dim3 grid((sz + kTZ - 1) / kTZ, (sy + kTY - 1) / kTY, (sx + kTX - 1) / kTX);
+      k_conv3_fwd_umma<CIN, COUT, RELU, BIAS><<<grid, 256, smem, st>>>(in, w, b, out, sx, sy, sz);
+      return cudaGetLastError();
+    }
+  }
+  if (g_conv_impl >= 1) {
     constexpr size_t smem = fwd_tile_smem<CIN, COUT>();
     static const cudaError_t attr =
         cudaFuncSetAttribute(k_conv3_fwd_tile<CIN, COUT, RELU, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -744,7 +996,13 @@ inline int ew_grid(long long n) {
 
 }  // namespace
 
-void set_conv_tiled(bool tiled) { g_conv_tiled = tiled; }
+void set_conv_impl(int impl) { g_conv_impl = impl; }
+
+int conv_umma_timeouts() {
+  int v = 0;
+  cudaMemcpyFromSymbol(&v, g_umma_timeout, sizeof(int));
+  return v;
+}
 
 int unet_wgrad_chunk(int voxels) {
   // about 2 CTAs per SM per tap at 128^3, at least one 128-voxel tile

@@ -275,7 +275,14 @@ aq_status aq_conv3_weight_grad(int32_t cin, int32_t cout, const void* x, const v
 }
 
 aq_status aq_conv3_set_tiled(int32_t tiled) {
-  set_conv_tiled(tiled != 0);
+  if (tiled < 0 || tiled > 2) return fail(AQ_ERR_INVALID_ARGUMENT, "conv variant must be 0, 1 or 2");
+  set_conv_impl(tiled);
+  return AQ_OK;
+}
+
+aq_status aq_conv3_umma_status(int32_t* timeouts) {
+  if (!timeouts) return fail(AQ_ERR_INVALID_ARGUMENT, "NULL");
+  *timeouts = conv_umma_timeouts();
   return AQ_OK;
 }
 

@@ -369,9 +369,15 @@ aq_status aq_conv3_weight_grad(int32_t cin, int32_t cout, const void* x, const v
                                int32_t sy, int32_t sz, void* stream);
 aq_status aq_conv3_flip_transpose(int32_t cin, int32_t cout, const void* w, void* wt, void* stream);
 /* Forward kernel used by aq_conv3_forward and the network: 1 = halo-tiled
- * (default), 0 = im2col streaming.  Process-wide; set it while no
- * convolution is in flight.  Both compute the same sums in the same order. */
+ * mma.sync (default), 2 = tcgen05 UMMA with TMEM accumulators (pairs with
+ * cout a multiple of 16; others fall back to 1), 0 = im2col streaming
+ * mma.sync.  Process-wide;
+ * set it while no convolution is in flight.  1 and 0 compute the same sums
+ * in the same order; 2 sums the same products in the tensor core's order.
+ * aq_conv3_umma_status: nonzero *timeouts if a tcgen05 convolution ever
+ * gave up waiting for its MMAs (its output is then not written). */
 aq_status aq_conv3_set_tiled(int32_t tiled);
+aq_status aq_conv3_umma_status(int32_t* timeouts);
 
 /* ---- Learned pressure warm start: network, dataset, training ---------------
  * No counterpart in the reference.  A 3-level 3D U-Net (16/32/64 channels,

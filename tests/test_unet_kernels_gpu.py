@@ -1,7 +1,9 @@
 """The U-Net's hand-written BF16 convolution kernels against PyTorch's FP32
 conv3d (the test oracle for these kernels): forward, data gradient (forward
 on the flipped, transposed weights) and weight gradient, on odd grid sizes
-(partial tiles, every boundary) and for every channel pair the network uses."""
+(partial tiles, every boundary) and for every channel pair the network uses.
+The forward runs in three variants: halo-tiled mma.sync (the default),
+tcgen05 UMMA with TMEM accumulators and im2col mma.sync."""
 import ctypes as ct
 
 import numpy as np
@@ -27,7 +29,15 @@ def _lib():
     lib.aq_conv3_flip_transpose.argtypes = [I, I, P, P, P]
     lib.aq_conv3_set_tiled.restype = ct.c_int
     lib.aq_conv3_set_tiled.argtypes = [I]
+    lib.aq_conv3_umma_status.restype = ct.c_int
+    lib.aq_conv3_umma_status.argtypes = [ct.POINTER(I)]
     return lib
+
+
+def _no_umma_timeouts(lib):
+    v = ct.c_int32(-1)
+    assert lib.aq_conv3_umma_status(ct.byref(v)) == 0
+    assert v.value == 0, "a tcgen05 convolution gave up waiting for its MMAs"
 
 
 def _torch():
@@ -51,7 +61,7 @@ def _rel(a, b):
     return float((a - b).norm() / max(b.norm(), 1e-30))
 
 
-@pytest.mark.parametrize("tiled", [1, 0], ids=["tiled", "im2col"])
+@pytest.mark.parametrize("tiled", [2, 1, 0], ids=["umma", "tiled", "im2col"])
 @pytest.mark.parametrize("cin,cout", FWD_PAIRS)
 @pytest.mark.parametrize("shape", [(5, 6, 7), (12, 8, 16), (8, 12, 36)])
 def test_conv3_forward_matches_torch(cin, cout, shape, tiled):
@@ -73,6 +83,7 @@ def test_conv3_forward_matches_torch(cin, cout, shape, tiled):
             ref = torch.relu(ref)
         got = _to_ncdhw(out, shape)
         assert _rel(got, ref) < 8e-3  # bf16 rounding of the output
+    _no_umma_timeouts(lib)
     lib.aq_conv3_set_tiled(1)
 
 
@@ -129,3 +140,29 @@ def test_unsupported_pair_is_an_error():
     lib = _lib()
     buf = torch.zeros(1024, device="cuda", dtype=torch.bfloat16)
     assert lib.aq_conv3_forward(8, 16, 0, buf.data_ptr(), buf.data_ptr(), None, buf.data_ptr(), 2, 2, 2, None) != 0
+
+
+def test_umma_and_mma_sync_networks_agree():
+    """The network's prediction through the tcgen05 variant against the
+    default mma.sync variant (the same products; f32 sums in the tensor
+    core's order)."""
+    torch = _torch()
+    lib = _lib()
+    import pathlib
+    wpath = pathlib.Path(aq.__file__).resolve().parent / "weights" / "unet_64.bin"
+    net = aq.UNet(weights=wpath)
+    V = 64 ** 3
+    g = torch.Generator(device="cuda").manual_seed(9)
+    typ = (torch.rand(V, device="cuda", generator=g) < 0.5).to(torch.int8)
+    rhs = torch.randn(V, device="cuda", generator=g)
+    outs = []
+    for impl in (1, 2):
+        lib.aq_conv3_set_tiled(impl)
+        o = torch.zeros(V, device="cuda")
+        net.predict((64, 64, 64), rhs.data_ptr(), typ.data_ptr(), o.data_ptr())
+        torch.cuda.synchronize()
+        outs.append(o)
+    lib.aq_conv3_set_tiled(1)
+    _no_umma_timeouts(lib)
+    assert _rel(outs[1], outs[0]) < 1e-3
+    net.close()
