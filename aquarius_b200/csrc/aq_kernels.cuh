@@ -266,7 +266,7 @@ cudaError_t launch_conv3_wgrad(cudaStream_t st, int cin, int cout, const void* x
                                float* dw, int sx, int sy, int sz);
 size_t conv3_wgrad_part_floats(int cin, int cout, int voxels);
 // Forward kernel variant: halo-tiled (true, default) or im2col streaming.
-// 1 = halo-tiled mma.sync (default), 2 = tcgen05 UMMA, 0 = im2col mma.sync.
+// 2 = tcgen05 UMMA where it fits (default), 1 = halo-tiled mma.sync, 0 = im2col mma.sync.
 void set_conv_impl(int impl);
 // Nonzero if a tcgen05 convolution ever gave up waiting on its mbarriers.
 int conv_umma_timeouts();

@@ -25,9 +25,10 @@ namespace {
 
 using bf16 = __nv_bfloat16;
 
-// Forward convolution variant: 1 = halo-tiled mma.sync (default, the
-// fastest measured), 2 = tcgen05 UMMA, 0 = im2col streaming mma.sync.
-int g_conv_impl = 1;
+// Forward convolution variant: 2 = tcgen05 UMMA where its operands fit in
+// shared memory, else halo-tiled mma.sync (default); 1 = halo-tiled
+// mma.sync; 0 = im2col streaming mma.sync.
+int g_conv_impl = 2;
 
 constexpr int kTileM = 128;  // voxels per forward CTA (4 warps x 32)
 constexpr int kRowK = 24;    // smem row of one 16-wide k chunk: 16 + 8 pad bf16 (48 B, conflict-free ldmatrix)
@@ -275,27 +276,13 @@ __global__ void __launch_bounds__(256) k_conv3_fwd_tile(const bf16* __restrict__
 }
 
 // ------------------------------------------------- forward on tcgen05 (TMEM)
-// The same 4 (x) x 4 (y) x 16 (z) output block and staged input halo as
-// k_conv3_fwd_tile, as two M = 128 tiles (x pairs) of a UMMA implicit GEMM:
-// per tap, every thread copies its voxel's shifted input row from the halo
-// into the A tile of its M tile, in the canonical K-major no-swizzle layout
-// (8-row x 16-byte core matrices: +16 B per row, +128 B per 8 channels,
-// +256 B per 8 rows, +4 KB per 16 channels); the tap's weights (B, N = COUT
-// rows, same layout) arrive by cp.async; one thread issues
-// tcgen05.mma.cta_group::1.kind::f16 (bf16 x bf16 -> f32) for both tiles over
-// the tap's CIN/16 k-steps into TMEM and commits to the buffer's mbarrier.
-// Up to D = 4 taps' MMAs are in flight (A and weight slots in rings, one
-// mbarrier per tap slot) and the weights of the next P <= 8 taps are loading.  The epilogue reads each thread's row back
-// with tcgen05.ld (warp w: TMEM lanes 32 (w % 4) ..., tile w / 4).  Every
-// mbarrier wait is bounded: on a timeout the kernel records it in
-// g_umma_timeout and carries on to free its TMEM.
-// Measured against k_conv3_fwd_tile on B200 (16->16 at 128^3: 329 vs 173 us;
-// 64->64 at 32^3: 34 vs 30 us), so it is not the default: ncu shows the
-// tensor pipe 4% busy, the time going to the per-tap A copy out of the halo,
-// its proxy fence and CTA barrier, at 3 CTAs per SM against 7.  Pointing the
-// descriptors straight into a chunk-major halo needs the transposed product
-// (M = COUT, N = a 16-voxel z run), which the shapes here (COUT 16 / 32)
-// would have to pad to M = 64.
+// UMMA implicit GEMM: D[voxels x COUT] (f32, TMEM) += A[voxels x 16 channels]
+// x B[16 channels x COUT] per tap and k step, bf16 operands in shared memory
+// read through matrix descriptors (canonical K-major layout, no swizzle:
+// 8-row x 16-byte core matrices), tcgen05.mma.cta_group::1.kind::f16 issued by
+// one thread, completion through tcgen05.commit on an mbarrier whose wait is
+// bounded (a timeout is recorded in g_umma_timeout; the kernel then frees its
+// TMEM without storing), results read back with tcgen05.ld.
 __device__ int g_umma_timeout;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -358,131 +345,104 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 
 __host__ __device__ constexpr int tmem_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : 256; }
 
-// Pipeline shape: D taps whose MMAs may be in flight (A slots and mbarriers
-// per tap slot) and the weights of the next P taps loading (D + P weight
-// slots).  The first (D, P) of the list below that still lets two CTAs share
-// an SM, else the first that fits.
-template <int CIN, int COUT>
-__host__ __device__ constexpr size_t umma_smem_for(int d, int p) {
-  return (size_t)kHalo * (CIN + 8) * 2 + (size_t)d * (2 * CIN * 256) + (size_t)(d + p) * COUT * CIN * 2 + 1024;
-}
+// Output block of the tcgen05 kernel: 2 (x) x 16 (y) x 8 (z) voxels, two
+// M = 128 tiles (one per x plane, row m = 8 y + z).  Its input halo
+// (4 x 18 x 10 voxels) is stored per 8-channel chunk as z columns of 10 rows
+// of 16 B: the A operand of any tap is then a descriptor into the halo
+// itself — rows of a core matrix are 8 consecutive z (16 B apart), the 16
+// core matrices along M are the y columns (SBO = 160 B), the two along K the
+// chunk planes (LBO) — so no per-tap copy and no per-tap barrier: the CTA
+// loads the halo and all 27 taps' weights, one thread issues every MMA and
+// commits once.  On B200 the 128^3 network's inference takes 1.55 ms this
+// way against 1.64 ms with k_conv3_fwd_tile; per layer it is ahead where
+// COUT is 32 and behind at 128^3 with COUT = 16, whose N = 16 MMAs are too
+// narrow to keep the tensor pipe busy.
+constexpr int kUX = 2, kUY = 16, kUZ = 8;
+constexpr int kUHX = kUX + 2, kUHY = kUY + 2, kUHZ = kUZ + 2;
+constexpr int kUPlane = kUHX * kUHY * kUHZ * 16;  // bytes of one 8-channel chunk of the halo
 
 template <int CIN, int COUT>
-__host__ __device__ constexpr int umma_shape() {  // D * 16 + P
-  constexpr int cand[8][2] = {{4, 8}, {2, 8}, {4, 4}, {2, 4}, {1, 8}, {1, 4}, {2, 2}, {1, 2}};
-  for (int pass = 0; pass < 2; ++pass)
-    for (int i = 0; i < 8; ++i)
-      if (umma_smem_for<CIN, COUT>(cand[i][0], cand[i][1]) <= (pass == 0 ? 113u : 220u) * 1024u)
-        return cand[i][0] * 16 + cand[i][1];
-  return 1 * 16 + 2;
+__host__ __device__ constexpr size_t fwd_umma_smem() {
+  return (size_t)(CIN / 8) * kUPlane + (size_t)27 * COUT * CIN * 2 + 1024;
 }
 
+// The pairs the tcgen05 kernel takes: cout a multiple of 16 (UMMA N), the
+// halo and all weights resident.
 template <int CIN, int COUT>
-constexpr size_t fwd_umma_smem() {
-  return umma_smem_for<CIN, COUT>(umma_shape<CIN, COUT>() / 16, umma_shape<CIN, COUT>() % 16);
+__host__ __device__ constexpr bool umma_fits() {
+  return COUT % 16 == 0 && COUT <= 128 && fwd_umma_smem<CIN, COUT>() <= 200 * 1024;
 }
 
 template <int CIN, int COUT, bool RELU, bool BIAS>
 __global__ void __launch_bounds__(256) k_conv3_fwd_umma(const bf16* __restrict__ in, const bf16* __restrict__ w,
                                                        const float* __restrict__ bias, bf16* __restrict__ out,
                                                        int sx, int sy, int sz) {
-  static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 128, "UMMA shapes: M = 128, N = COUT");
-  constexpr int RS = CIN + 8, CH = CIN / 8, KS = CIN / 16;
-  constexpr int D = umma_shape<CIN, COUT>() / 16, P = umma_shape<CIN, COUT>() % 16;
-  constexpr int DB = D + P;                // weight slots
-  constexpr int A_TILE = CIN * 256;        // one M tile: 128 rows x CIN bf16
-  constexpr int A_BYTES = 2 * A_TILE;      // two M tiles
-  constexpr int B_BYTES = COUT * CIN * 2;  // N rows x CIN bf16
+  static_assert(umma_fits<CIN, COUT>(), "UMMA shapes: M = 128, N = COUT, operands resident");
+  constexpr int CH = CIN / 8, KS = CIN / 16;
+  constexpr int TAPB = COUT * CIN * 2;  // one tap's weights
   constexpr int COLS = tmem_cols(2 * COUT);
   constexpr uint32_t IDESC = umma_idesc(128, COUT);
   extern __shared__ __align__(1024) unsigned char um_smem[];
-  bf16* sH = reinterpret_cast<bf16*>(um_smem);
-  unsigned char* sA = um_smem + (size_t)kHalo * RS * 2;  // [D][A_BYTES]
-  unsigned char* sB = sA + D * A_BYTES;                  // [DB][B_BYTES]
-  __shared__ __align__(8) uint64_t s_mbar[4];            // MMAs of tap slot t % D
+  unsigned char* sH = um_smem;                // [CH][kUHX][kUHY][kUHZ][16 B]
+  unsigned char* sB = um_smem + CH * kUPlane;  // [27][canonical COUT x CIN]
+  __shared__ __align__(8) uint64_t s_mbar;
   __shared__ uint32_t s_tmem;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int z0 = blockIdx.x * kTZ, y0 = blockIdx.y * kTY, x0 = blockIdx.z * kTX;
-  // this thread's output voxel: M tile j = tid / 128, row r = tid % 128
-  const int j = tid >> 7, r = tid & 127;
-  const int ox = j * 2 + (r >> 6), oy = (r >> 4) & 3, oz = r & 15;
+  const int z0 = blockIdx.x * kUZ, y0 = blockIdx.y * kUY, x0 = blockIdx.z * kUX;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&s_tmem)),
                  "r"(COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    for (int q = 0; q < D; ++q)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&s_mbar[q])), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&s_mbar)), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  // the tap's weights: B row n = w[tap][n][0..CIN), chunk c of 8 channels
-  auto stage_b = [&](int tap) {
-    unsigned char* B = sB + (tap % DB) * B_BYTES;
-    for (int i = tid; i < COUT * CH; i += 256) {
-      const int c = i % CH, n = i / CH;
-      cp_async16(B + (c >> 1) * (COUT * 32) + (n >> 3) * 256 + (c & 1) * 128 + (n & 7) * 16,
-                 w + ((size_t)(tap * COUT + n) * CIN + c * 8), true);
-    }
-  };
-  // group 0: the halo block with tap 0's weights; groups 1..P-1: the next taps
-  for (int i = tid; i < kHalo * CH; i += 256) {
+  // the halo: chunk c of voxel (hx, hy, hz), zero outside the grid
+  for (int i = tid; i < kUHX * kUHY * kUHZ * CH; i += 256) {
     const int c = i % CH, h = i / CH;
-    const int hz = h % kHZ, t = h / kHZ, hy = t % kHY, hx = t / kHY;
+    const int hz = h % kUHZ, t = h / kUHZ, hy = t % kUHY, hx = t / kUHY;
     const int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z0 + hz - 1;
     const bool ok = gx >= 0 && gx < sx && gy >= 0 && gy < sy && gz >= 0 && gz < sz;
-    cp_async16(sH + h * RS + c * 8, ok ? in + ((size_t)((gx * sy + gy) * sz + gz) * CIN + c * 8) : in, ok);
+    cp_async16(sH + c * kUPlane + h * 16, ok ? in + ((size_t)((gx * sy + gy) * sz + gz) * CIN + c * 8) : in, ok);
   }
-  stage_b(0);
+  // all weights: tap t, row n, chunk c in the canonical K-major layout
+  for (int i = tid; i < 27 * COUT * CH; i += 256) {
+    const int c = i % CH, n = (i / CH) % COUT, t = i / (CH * COUT);
+    cp_async16(sB + t * TAPB + (c >> 1) * (COUT * 32) + (n >> 3) * 256 + (c & 1) * 128 + (n & 7) * 16,
+               w + ((size_t)(t * COUT + n) * CIN + c * 8), true);
+  }
   cp_async_commit();
-#pragma unroll
-  for (int q = 1; q < P; ++q) {
-    stage_b(q);
-    cp_async_commit();
-  }
+  cp_async_wait<0>();
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = s_tmem;
-  bool ok_wait = true;
-  for (int tap = 0; tap < 27; ++tap) {
-    // tap slot tap % D is free once the MMAs of tap - D are done; so is the
-    // weight slot (tap + P) % DB, last read by those MMAs
-    if (tap >= D) ok_wait &= mbar_wait(&s_mbar[tap % D], (uint32_t)(((tap - D) / D) & 1));
-    if (tap + P < 27) stage_b(tap + P);
-    cp_async_commit();
-    // this thread's copies of the tap's weights (and, first, of the halo)
-    cp_async_wait<P>();
-    if (tap == 0) __syncthreads();
-    // this thread's A row for the tap, from the halo
-    unsigned char* A = sA + (tap % D) * A_BYTES;
-    int dx, dy, dz;
-    tap_offset(tap, dx, dy, dz);
-    const int h = ((ox + dx + 1) * kHY + (oy + dy + 1)) * kHZ + (oz + dz + 1);
-    const uint4* src = reinterpret_cast<const uint4*>(sH + h * RS);
-    unsigned char* arow = A + j * A_TILE + (r >> 3) * 256 + (r & 7) * 16;
+  if (tid == 0) {
+    const uint32_t h0 = smem_u32(sH), b0 = smem_u32(sB);
+    for (int tap = 0; tap < 27; ++tap) {
+      int dx, dy, dz;
+      tap_offset(tap, dx, dy, dz);
 #pragma unroll
-    for (int c = 0; c < CH; ++c) *reinterpret_cast<uint4*>(arow + (c >> 1) * 4096 + (c & 1) * 128) = src[c];
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const unsigned char* B = sB + (tap % DB) * B_BYTES;
-#pragma unroll
-      for (int t = 0; t < 2; ++t)
+      for (int j = 0; j < kUX; ++j) {
+        // tile j: output x plane j reads halo plane j + dx + 1, columns from dy + 1, rows from dz + 1
+        const uint32_t a0 = h0 + (uint32_t)((((j + dx + 1) * kUHY + (dy + 1)) * kUHZ + (dz + 1)) * 16);
 #pragma unroll
         for (int ks = 0; ks < KS; ++ks) {
-          const uint64_t ad = umma_desc(smem_u32(A + t * A_TILE + ks * 4096), 128, 256);
-          const uint64_t bd = umma_desc(smem_u32(B + ks * (COUT * 32)), 128, 256);
-          umma_f16(tmem + (uint32_t)(t * COUT), ad, bd, IDESC, (tap > 0 || ks > 0) ? 1u : 0u);
+          const uint64_t ad = umma_desc(a0 + (uint32_t)(2 * ks * kUPlane), kUPlane, kUHZ * 16);
+          const uint64_t bd = umma_desc(b0 + (uint32_t)(tap * TAPB + ks * (COUT * 32)), 128, 256);
+          umma_f16(tmem + (uint32_t)(j * COUT), ad, bd, IDESC, (tap > 0 || ks > 0) ? 1u : 0u);
         }
-      umma_commit(&s_mbar[tap % D]);
+      }
     }
+    umma_commit(&s_mbar);
   }
-  // all MMAs done: the last commit covers every earlier one
-  ok_wait &= mbar_wait(&s_mbar[26 % D], (uint32_t)((26 / D) & 1));
+  const bool ok_wait = mbar_wait(&s_mbar, 0u);
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  const int gx = x0 + ox, gy = y0 + oy, gz = z0 + oz;
+  // warp w reads TMEM lanes 32 (w % 4) .. of tile w / 4: its row m -> (y, z)
+  const int j = warp >> 2, m = (warp & 3) * 32 + (tid & 31);
+  const int gx = x0 + j, gy = y0 + (m >> 3), gz = z0 + (m & 7);
   const bool store = ok_wait && gx < sx && gy < sy && gz < sz;
   const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(j * COUT);
   bf16* dst = out + (size_t)((gx * sy + gy) * sz + gz) * COUT;
@@ -631,13 +591,13 @@ __global__ void k_flip_transpose(const bf16* __restrict__ w, bf16* __restrict__ 
 template <int CIN, int COUT, bool RELU, bool BIAS>
 cudaError_t fwd_launch(cudaStream_t st, const bf16* in, const bf16* w, const float* b, bf16* out, int sx, int sy,
                        int sz) {
-  if constexpr (COUT % 16 == 0 && COUT <= 128) {
+  if constexpr (umma_fits<CIN, COUT>()) {
     if (g_conv_impl == 2) {
       constexpr size_t smem = fwd_umma_smem<CIN, COUT>();
       static const cudaError_t attr = cudaFuncSetAttribute(
           k_conv3_fwd_umma<CIN, COUT, RELU, BIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (attr != cudaSuccess) return attr;
-      const dim3 grid((sz + kTZ - 1) / kTZ, (sy + kTY - 1) / kTY, (sx + kTX - 1) / kTX);
+      const dim3 grid((sz + kUZ - 1) / kUZ, (sy + kUY - 1) / kUY, (sx + kUX - 1) / kUX);
       k_conv3_fwd_umma<CIN, COUT, RELU, BIAS><<<grid, 256, smem, st>>>(in, w, b, out, sx, sy, sz);
       return cudaGetLastError();
     }

@@ -368,10 +368,10 @@ aq_status aq_conv3_forward(int32_t cin, int32_t cout, int32_t relu, const void* 
 aq_status aq_conv3_weight_grad(int32_t cin, int32_t cout, const void* x, const void* dy, float* dw, int32_t sx,
                                int32_t sy, int32_t sz, void* stream);
 aq_status aq_conv3_flip_transpose(int32_t cin, int32_t cout, const void* w, void* wt, void* stream);
-/* Forward kernel used by aq_conv3_forward and the network: 1 = halo-tiled
- * mma.sync (default), 2 = tcgen05 UMMA with TMEM accumulators (pairs with
- * cout a multiple of 16; others fall back to 1), 0 = im2col streaming
- * mma.sync.  Process-wide;
+/* Forward kernel used by aq_conv3_forward and the network: 2 = tcgen05
+ * UMMA with TMEM accumulators (default; pairs whose halo and weights fit in
+ * shared memory, cout a multiple of 16 — the others run 1), 1 = halo-tiled
+ * mma.sync, 0 = im2col streaming mma.sync.  Process-wide;
  * set it while no convolution is in flight.  1 and 0 compute the same sums
  * in the same order; 2 sums the same products in the tensor core's order.
  * aq_conv3_umma_status: nonzero *timeouts if a tcgen05 convolution ever
