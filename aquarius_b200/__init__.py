@@ -284,9 +284,6 @@ class Fluid:
         """Fluid::simulationStep (Fluid/Fluid_3D_FLIP.cu:316-352), asynchronous."""
         _check(self._lib.aq_fluid_step(self._h, 1))
 
-    def draw(self, drawCommand=None):
-        """Rendering is not part of this library (headless)."""
-
     @property
     def physicalTime(self) -> float:
         t = ct.c_double()
@@ -416,13 +413,24 @@ class Fluid:
         """updatePositionsAndPhasesVBO: 7 floats per particle into a device buffer."""
         _check(self._lib.aq_fluid_points_vbo(self._h, ct.c_void_p(device_ptr)))
 
-    def draw(self, renderer: "Renderer", command: _abi.DrawCommand, device_ptr: Optional[int] = None):
-        """Fluid::draw(drawCommand): mesh (mesh modes), point VBO and one
-        frame; into device_ptr (W*H*4 bytes) or, when None, the renderer's own
-        image (renderer.image() downloads it)."""
-        _check(self._lib.aq_fluid_draw(self._h, renderer._h, ct.byref(command),
+    def draw(self, drawCommand: Optional[_abi.DrawCommand] = None, renderer: Optional["Renderer"] = None,
+             device_ptr: Optional[int] = None):
+        """Fluid::draw(drawCommand) (Fluid/Fluid_3D_FLIP.cu:396-430), headless:
+        mesh (mesh modes), point VBO and one frame, into device_ptr (W*H*4
+        bytes) or, when None, the renderer's own image (renderer.image()
+        downloads it).  Without a renderer the fluid's own is used (made on
+        first use); without a draw command nothing is drawn.  Returns the
+        renderer."""
+        if drawCommand is None:
+            return renderer
+        if renderer is None:
+            if getattr(self, "_renderer", None) is None:
+                self._renderer = Renderer(int(self._cfg_c.device))
+            renderer = self._renderer
+        _check(self._lib.aq_fluid_draw(self._h, renderer._h, ct.byref(drawCommand),
                                        None if device_ptr is None else ct.c_void_p(device_ptr)))
-        renderer._last = (command.window_height, command.window_width)
+        renderer._last = (drawCommand.window_height, drawCommand.window_width)
+        return renderer
 
     def download_sdf(self) -> np.ndarray:
         """The last mesh's SDF grid, [sdf_x, sdf_y, sdf_z]."""
@@ -488,6 +496,10 @@ class Fluid:
         return {"ms": ms.value, "launches": nl.value, "cells_per_sweep": cells.value}
 
     def close(self):
+        r = getattr(self, "_renderer", None)
+        if r is not None:
+            r.close()
+            self._renderer = None
         if getattr(self, "_h", None) and self._h.value:
             self._lib.aq_fluid_destroy(self._h)
             self._h = ct.c_void_p()

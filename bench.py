@@ -454,7 +454,7 @@ def render_timing(f, size: int, reps: int = 10, width: int = 1728, height: int =
             ts.append(time.perf_counter() - t0)
         return 1e3 * float(np.median(ts))
 
-    full_ms = best(lambda: f.draw(r, dc, img.data_ptr()))
+    full_ms = best(lambda: f.draw(dc, r, img.data_ptr()))
     recs = f.download_mesh()
     mesh = torch.from_numpy(np.ascontiguousarray(recs.reshape(-1, 6))).cuda()
     pts = torch.empty((f.particleCount * 7,), dtype=torch.float32, device="cuda")
@@ -858,7 +858,7 @@ def run_profile_case(case: str):
         r.set_skybox(np.random.default_rng(11).integers(0, 256, (6, 256, 256, 3), dtype=np.uint8))
         dc = aq.draw_command_default(1728, 864, f.getContainerSize(), 128)
         for _ in range(2):
-            f.draw(r, dc)
+            f.draw(dc, r)
         r.synchronize()
         print("render ok", r.launches())
         r.close()

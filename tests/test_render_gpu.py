@@ -97,7 +97,7 @@ def test_frame_matches_oracle(small, mode, env):
 def test_fluid_draw_equals_explicit_vbos(small):
     cfg, f = small["cfg"], small["f"]
     dc = aq.draw_command_default(256, 128, cfg.domain_size, cfg.size_y)
-    f.draw(small["r"], dc)
+    f.draw(dc, small["r"])
     a = small["r"].image()
     b, _ = _draw(small["r"], dc, small["pts"], small["mesh"])
     np.testing.assert_array_equal(a, b)
