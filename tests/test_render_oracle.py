@@ -141,3 +141,57 @@ def test_every_mode_draws(cpu_scene, mode, env):
     assert bool(ph.any()) == multiphase
     if multiphase:  # the two phases' fractions sum to 1 per particle: thickness = coverage count
         assert np.isclose(ph.sum(), ph[..., :2].sum())
+
+
+def _window(dc, p):
+    """Window coordinates of world point p (float64)."""
+    P = np.array(dc.projection, np.float64).reshape(4, 4).T
+    V = np.array(dc.view, np.float64).reshape(4, 4).T
+    c = P @ V @ np.array([p[0], p[1], p[2], 1.0])
+    ndc = c[:3] / c[3]
+    return np.array([(ndc[0] + 1) * dc.window_width / 2, (ndc[1] + 1) * dc.window_height / 2])
+
+
+def _quad_mesh(corners, normal):
+    a, b, c, d = corners
+    verts = [a, b, c, a, c, d]
+    return np.array([list(v) + list(normal) for v in verts], np.float32)
+
+
+def test_shared_edge_leaves_no_gap():
+    """A quad drawn as two triangles sharing a diagonal: every pixel whose
+    centre lies inside the quad is drawn (the top-left rule gives shared-edge
+    pixels to exactly one triangle, none to neither)."""
+    dc = _dc(400, 200)
+    dc.render_mode = _abi.RENDER_FLAT_MESH
+    corners = [(3.0, 6.0, 5.0), (7.0, 6.0, 5.0), (7.0, 9.0, 5.0), (3.0, 9.0, 5.0)]
+    img, _ = RenderOracle().frame(dc, None, _quad_mesh(corners, (0.0, 0.0, -1.0)))
+    bg, _ = RenderOracle().frame(dc, None, None)
+    drawn = (img != bg).any(-1)
+    w = np.array([_window(dc, c) for c in corners])
+    ys, xs = np.mgrid[0:dc.window_height, 0:dc.window_width]
+    px, py = xs + 0.5, ys + 0.5
+    inside = np.ones_like(drawn)
+    for k in range(4):  # a convex quad: inside every edge by a margin of 0.05 px
+        a, b = w[k], w[(k + 1) % 4]
+        e = (b[0] - a[0]) * (py - a[1]) - (b[1] - a[1]) * (px - a[0])
+        sgn = np.sign((w[(k + 2) % 4][1] - a[1]) * (b[0] - a[0]) - (w[(k + 2) % 4][0] - a[0]) * (b[1] - a[1]))
+        inside &= sgn * e > 0.05 * np.hypot(*(b - a))
+    assert inside.sum() > 500
+    assert drawn[inside].all(), int((~drawn[inside]).sum())
+
+
+def test_triangle_through_the_near_plane_is_dropped():
+    """A triangle with a vertex behind the eye is dropped whole (no
+    clipping), as the frame rules say."""
+    dc = _dc(160, 80)
+    dc.render_mode = _abi.RENDER_FLAT_MESH
+    eye = np.array(dc.camera_position, np.float64)
+    behind = eye + (eye - np.array([5.0, 5.0, 5.0])) * 0.5
+    tri = np.array([list(behind) + [0, 1, 0], [2.0, 5.0, 5.0, 0, 1, 0], [8.0, 5.0, 5.0, 0, 1, 0]], np.float32)
+    img, _ = RenderOracle().frame(dc, None, tri)
+    bg, _ = RenderOracle().frame(dc, None, None)
+    np.testing.assert_array_equal(img, bg)
+    tri[0, :3] = [5.0, 8.0, 5.0]  # the same triangle in front of the camera is drawn
+    img2, _ = RenderOracle().frame(dc, None, tri)
+    assert (img2 != bg).any()
