@@ -443,8 +443,8 @@ __global__ void __launch_bounds__(256) k_sprite_setup(RenderParams P, const floa
 }
 
 __global__ void __launch_bounds__(256) k_sprite_emit(RenderParams P, const float4* __restrict__ spr,
-                                                     const int* __restrict__ cnt_unused, const int* __restrict__ off,
-                                                     int n, unsigned* __restrict__ keys, int* __restrict__ vals) {
+                                                     const int* __restrict__ off, int n, unsigned* __restrict__ keys,
+                                                     int* __restrict__ vals) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int base = off[i], c = off[i + 1] - base;
@@ -739,7 +739,7 @@ cudaError_t launch_sprite_setup(cudaStream_t st, const RenderParams& P, const fl
 cudaError_t launch_sprite_emit(cudaStream_t st, const RenderParams& P, const float4* spr, const int* off, int n,
                                unsigned* keys, int* vals) {
   if (n <= 0) return cudaSuccess;
-  k_sprite_emit<<<(n + 255) / 256, 256, 0, st>>>(P, spr, nullptr, off, n, keys, vals);
+  k_sprite_emit<<<(n + 255) / 256, 256, 0, st>>>(P, spr, off, n, keys, vals);
   return cudaGetLastError();
 }
 

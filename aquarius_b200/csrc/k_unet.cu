@@ -330,7 +330,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
   return false;
 }
 
-template <int N>
+// 16 consecutive f32 columns of this thread's TMEM lane (32x32b shape).
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
   asm volatile(
@@ -449,7 +449,7 @@ __global__ void __launch_bounds__(256) k_conv3_fwd_umma(const bf16* __restrict__
 #pragma unroll
   for (int c0 = 0; c0 < COUT; c0 += 16) {
     float v[16];
-    tmem_ld16<16>(trow + (uint32_t)c0, v);
+    tmem_ld16(trow + (uint32_t)c0, v);
     if (store) {
       __align__(16) __nv_bfloat162 pk[8];
 #pragma unroll
