@@ -77,6 +77,8 @@ def load_library() -> ct.CDLL:
         "aq_fluid_download_state": (ct.c_int, [P, ct.POINTER(_abi.HostState)]),
         "aq_fluid_upload_state": (ct.c_int, [P, ct.POINTER(_abi.HostState)]),
         "aq_fluid_solve_stats": (ct.c_int, [P, ct.POINTER(_abi.SolveStats)]),
+        "aq_fluid_test_barrier_timeout": (ct.c_int, [P, ct.c_int32, ct.c_uint32]),
+        "aq_selfcheck_division": (ct.c_int, [ct.c_int32, ct.POINTER(ct.c_uint64)]),
         "aq_fluid_pcg_reference": (ct.c_int, [P, ct.c_double, ct.c_int32, P, ct.POINTER(ct.c_double),
                                               ct.POINTER(ct.c_int32), ct.POINTER(ct.c_double)]),
         "aq_fluid_profile_step": (ct.c_int, [P, ct.POINTER(ct.c_float)]),
@@ -342,9 +344,21 @@ class Fluid:
         _check(self._lib.aq_fluid_upload_state(self._h, ct.byref(st)))
 
     def solve_stats(self) -> dict:
+        """Statistics of the last pressure solve.  "status" is the call's
+        aq_status name: AQ_ERR_NOT_CONVERGED (residual mode stopped at its cap)
+        and AQ_ERR_NONFINITE are reported there, other errors raise."""
         s = _abi.SolveStats()
-        _check(self._lib.aq_fluid_solve_stats(self._h, ct.byref(s)))
-        return _solve_stats_dict(s)
+        rc = self._lib.aq_fluid_solve_stats(self._h, ct.byref(s))
+        if rc not in (_abi.AQ_OK, _abi.AQ_ERR_NOT_CONVERGED, _abi.AQ_ERR_NONFINITE):
+            _check(rc)
+        d = _solve_stats_dict(s)
+        d["status"] = _abi.STATUS_NAMES.get(rc, str(rc))
+        return d
+
+    def test_barrier_timeout(self, withhold_cta: int = -1, spin_limit: int = 0):
+        """Test hook of the bounded grid-barrier waits of the persistent
+        solves (aq_fluid_test_barrier_timeout); (-1, 0) switches it off."""
+        _check(self._lib.aq_fluid_test_barrier_timeout(self._h, withhold_cta, spin_limit))
 
     def phase_mass(self) -> list:
         """Sum over particles of the volume fractions of each of the 4 phases."""

@@ -9,6 +9,10 @@ AQ_MAX_VOLUMES = 16
 AQ_MAX_PHASES = 4
 
 AQ_OK = 0
+AQ_ERR_INVALID_ARGUMENT = 2
+AQ_ERR_NOT_CONVERGED = 5
+AQ_ERR_NONFINITE = 6
+AQ_ERR_TIMEOUT = 8
 STATUS_NAMES = {
     0: "AQ_OK",
     1: "AQ_ERR_INVALID_CONFIG",

@@ -9,6 +9,7 @@
 // the staggering of Fluid/MAC_Grid_3D.cuh:100-130 in the reference.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -107,6 +108,13 @@ __device__ __forceinline__ int find_scene(const int* __restrict__ pre, int ns, i
 }
 
 // Device-side record of the pressure solve; read back on demand.
+// ||b - A p|| / ||b|| from the squared norms; 0 for an empty system, NaN
+// when either norm is not finite (a NaN or Inf in the right-hand side).
+__host__ __device__ __forceinline__ double rel_residual_of(double r2, double b2) {
+  if (!isfinite(b2) || !isfinite(r2)) return (b2 - b2) + (r2 - r2);  // NaN
+  return b2 > 0.0 ? sqrt(r2) / sqrt(b2) : 0.0;
+}
+
 struct SolveState {
   int iterations;       // sweeps done in the current/last solve
   int bodies;           // residual-check blocks done
@@ -122,6 +130,9 @@ struct SolveState {
   int warm;                // learned warm start: 1 prediction kept, 2 zero-init fallback, 0 none
   double warm_rel;         // relative residuals after the first 20 sweeps of each start
   double zero_rel;
+  // Sticky: a divergence norm or residual of some step since creation (or
+  // since the last state upload) was not finite.
+  int nonfinite_seen;
 };
 
 }  // namespace aqb

@@ -148,10 +148,41 @@ int persist_ctas(int device);  // co-resident CTAs of the cooperative launch
 // Builds the ordered list of active items and clears the barrier counter.
 cudaError_t launch_items_compact(cudaStream_t st, const Dims& d, const uint8_t* brick_active, int* items,
                                  int* n_items, unsigned int* bar);
+// Polls of a bounded grid-barrier wait before it gives up (with 32 ns sleeps
+// between polls, about a second).
+constexpr unsigned kSpinLimit = 1u << 25;
+// Test hook of the persistent solves' bounded waits: CTA withhold_cta (-1:
+// none) leaves without arriving at any barrier, and the others give up after
+// spin_limit polls (0: kSpinLimit).  Either way the solve ends with
+// SolveState::sync_timeout set and no CTA left waiting.
+struct BarrierTest {
+  int withhold_cta;
+  unsigned spin_limit;
+};
+// ---- resident solve (k_resident.cu) ------------------------------------------
+// Plan rows = 4: the whole solve in one cooperative launch, one CTA per SM;
+// a CTA keeps a tile (plan.xc selects the TX x TY x TZ shape) plus a K-cell
+// halo (K = plan.levels, 2 or 4) in shared memory for the whole solve and
+// exchanges halos through L2 every K sweeps.  Bit for bit the flat sweep.
+bool resident_plan_ok(int shape, int k);
+int resident_tile_capacity(const Dims& d);        // tile-list entries any shape needs
+int resident_ctas(int device, int shape, int k);  // CTAs of the launch (0: shape unusable)
+long long resident_cells_updated(const Dims& d, int shape, const uint8_t* bact_host);
+// Builds the tile list (and clears the barrier counter), then solves:
+// fixed_sweeps > 0: that many sweeps then one residual; else residual mode
+// (check every `check` sweeps, stop at tol or max_iters).  Result in pa.
+cudaError_t launch_resident_solve(cudaStream_t st, const Dims& d, int shape, int k, int ctas, float* pa, float* pb,
+                                  const float* rhs, const int8_t* type, const uint8_t* bact, int* tiles,
+                                  int* n_tiles, unsigned int* bar, double* part, SolveState* ss, int fixed_sweeps,
+                                  int check, int max_iters, double tol, BarrierTest bt);
+// Counts the float bit patterns where the resident sweep's division by 6
+// differs from the IEEE divide (*bad must start at 0).
+cudaError_t launch_div6_check(cudaStream_t st, unsigned long long* bad);
 // fixed_sweeps > 0: that many sweeps then one residual; else residual mode.
 cudaError_t launch_persist_solve(cudaStream_t st, const Dims& d, int ctas, float* pa, float* pb, const float* rhs,
                                  const int8_t* type, const int* items, const int* n_items, unsigned int* bar,
-                                 double* part, SolveState* ss, int fixed_sweeps, int check, int max_iters, double tol);
+                                 double* part, SolveState* ss, int fixed_sweeps, int check, int max_iters, double tol,
+                                 BarrierTest bt);
 // Temporally blocked Jacobi: `levels` sweeps from pin to pout; with resid it
 // also writes per-CTA FP64 partial sums of ||b - A p_out||^2 to part.
 cudaError_t launch_jacobi(cudaStream_t st, const Dims& d, const JacobiPlan& plan, bool resid,

@@ -71,8 +71,7 @@ __global__ void __launch_bounds__(1024) k_pick_start(const double* __restrict__ 
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    const double bn = ss->b2 > 0.0 ? sqrt(ss->b2) : 0.0;
-    const double rl = bn > 0.0 ? sqrt(sa[0]) / bn : 0.0, rz = bn > 0.0 ? sqrt(sb[0]) / bn : 0.0;
+    const double rl = rel_residual_of(sa[0], ss->b2), rz = rel_residual_of(sb[0], ss->b2);
     const bool zero_wins = !(rl <= rz);
     *pick = zero_wins ? 1 : 0;
     ss->warm = zero_wins ? 2 : 1;
@@ -83,7 +82,7 @@ __global__ void __launch_bounds__(1024) k_pick_start(const double* __restrict__ 
     ss->total_sweeps += 2 * kWarmSweeps;
     ss->r2 = zero_wins ? sb[0] : sa[0];
     ss->rel_residual = rel;
-    if (!isfinite(rel)) ss->nonfinite = 1;
+    if (!isfinite(rel)) ss->nonfinite = ss->nonfinite_seen = 1;
     ss->converged = (isfinite(rel) && rel <= tol) ? 1 : 0;
   }
 }
@@ -231,6 +230,11 @@ aq_status aqb::set_last_error(aq_status st, const std::string& msg) {
   return st;
 }
 
+// Plans whose residual is a separate pass over the final iterate (flat, cube
+// and list); the x-streaming tiled plans (rows 8/16/32) fuse it into their
+// last launch as an extra level.
+static bool separate_residual(const aqb::JacobiPlan& p) { return p.by == 0 || p.by == 2 || p.by == 3; }
+
 // =================================================================== fluid
 // ------------------------------------------------------------- allocation
 aq_status aq_fluid::allocate() {
@@ -265,12 +269,17 @@ aq_status aq_fluid::allocate() {
   AQ_TRY(alloc(&jpart, (size_t)jpart_cap));
   AQ_TRY(alloc(&ss, 1));
   AQ_CUDA(cudaMallocHost(&ss_host, sizeof(SolveState)));
+  int sms = 0;
+  AQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  AQ_TRY(alloc(&bar, 1));
+  AQ_TRY(alloc(&tiles, (size_t)resident_tile_capacity(d)));
+  AQ_TRY(alloc(&n_tiles, 1));
+  if (d.sz % 4 == 0) ctas = persist_ctas(device);
+  // partials of the persistent and resident solves: one per CTA (at most one per SM)
+  AQ_TRY(alloc(&ppart, (size_t)std::max({ctas, sms, 1})));
   if (d.sz % 4 == 0) {
-    ctas = persist_ctas(device);
     AQ_TRY(alloc(&items, (size_t)persist_items(d)));
     AQ_TRY(alloc(&n_items, 1));
-    AQ_TRY(alloc(&bar, 1));
-    AQ_TRY(alloc(&ppart, (size_t)std::max(ctas, 1)));
     AQ_TRY(alloc(&row_items, (size_t)row_items_capacity(d)));
     AQ_TRY(alloc(&n_row_items, 1));
     AQ_TRY(alloc(&resid_ticket, 1));
@@ -279,8 +288,16 @@ aq_status aq_fluid::allocate() {
   // active warp rows where z allows it, otherwise the tiled kernel with two
   // sweeps per launch
   plan = d.sz % 4 == 0 ? JacobiPlan{1, 3, 1} : JacobiPlan{2, 16, 16};
-  if (d.sz % 4 == 0 && resid_flat_parts(d) > jpart_cap) {
-    jpart_cap = resid_flat_parts(d);
+  // room for the default plan's residual partials: the flat pass, or the
+  // fused residual level of every launch size split_sweeps can produce
+  int need = d.sz % 4 == 0 ? resid_flat_parts(d) : 0;
+  for (int l = plan.levels; l >= 1 && !separate_residual(plan); l >>= 1) {
+    JacobiPlan q = plan;
+    q.levels = l;
+    need = std::max(need, jacobi_parts(d, q, true));
+  }
+  if (need > jpart_cap) {
+    jpart_cap = need;
     AQ_TRY(alloc(&jpart, (size_t)jpart_cap));
   }
   memset(ss_host, 0, sizeof(SolveState));
@@ -328,11 +345,14 @@ static std::vector<int> split_sweeps(int sweeps, int levels) {
   return out;
 }
 
-int aq_fluid::count_jacobi_launches(int sweeps) const {
+static int jacobi_launches(const JacobiPlan& plan, int sweeps) {
+  if (plan.by == 1 || plan.by == 4) return 2;  // work list + the cooperative solve
   const int k = (int)split_sweeps(sweeps, plan.levels).size();
   // sweeps, parity copy, finalize, separate residual pass (flat, cube and list plans)
-  return k + (k % 2) + 1 + (plan.by == 0 || plan.by >= 2 ? 1 : 0);
+  return k + (k % 2) + 1 + (separate_residual(plan) ? 1 : 0);
 }
+
+int aq_fluid::count_jacobi_launches(int sweeps) const { return jacobi_launches(plan, sweeps); }
 
 // `sweeps` Jacobi sweeps from pa; the last launch also writes the residual
 // partials of its output; the result ends in pa.
@@ -345,7 +365,7 @@ int aq_fluid::count_jacobi_launches(int sweeps) const {
 static aq_status enqueue_sweeps_on(aq_fluid* f, const JacobiPlan& plan, float* a, float* b, int sweeps,
                                    bool with_residual, double* part) {
   const std::vector<int> parts = split_sweeps(sweeps, plan.levels);
-  const bool flat = plan.by == 0 || plan.by >= 2;  // residual in a separate pass
+  const bool flat = separate_residual(plan);
   float* bufs[2] = {a, b};
   for (size_t k = 0; k < parts.size(); ++k) {
     if (plan.by == 3) {
@@ -376,7 +396,7 @@ static aq_status enqueue_sweeps(aq_fluid* f, int sweeps, bool with_residual = tr
 static int last_parts_of(const aq_fluid* f, const JacobiPlan& plan, int sweeps) {
   const std::vector<int> parts = split_sweeps(sweeps, plan.levels);
   if (parts.empty()) return 0;
-  if (plan.by == 0 || plan.by >= 2) return resid_flat_parts(f->d);
+  if (separate_residual(plan)) return resid_flat_parts(f->d);
   JacobiPlan p = plan;
   p.levels = parts.back();
   return jacobi_parts(f->d, p, true);
@@ -385,7 +405,9 @@ static int last_parts_of(const aq_fluid* f, const JacobiPlan& plan, int sweeps) 
 static int last_parts(const aq_fluid* f, int sweeps) { return last_parts_of(f, f->plan, sweeps); }
 
 aq_status aq_fluid::enq_row_items() {
-  if (plan.by != 3) return AQ_OK;
+  // the list plan's rows; the resident plan's learned start sweeps them too
+  const bool warm_rows = plan.by == 4 && cfg.pressure_init == AQ_PRESSURE_LEARNED && d.sz % 4 == 0;
+  if (plan.by != 3 && !warm_rows) return AQ_OK;
   AQ_CUDA(launch_row_items(stream, d, bact, row_items, n_row_items));
   return AQ_OK;
 }
@@ -397,11 +419,14 @@ int aq_fluid::solve_sweeps_done() const { return cfg.pressure_init == AQ_PRESSUR
 aq_status aq_fluid::enq_learned_start() {
   if (!net || !net_acts) return fail(AQ_ERR_INVALID_CONFIG, "AQ_PRESSURE_LEARNED needs a network (aq_fluid_set_warm_start)");
   AQ_TRY(unet_predict(net, stream, net_acts, rhs, type, pa));
-  AQ_TRY(enqueue_sweeps_on(this, plan, pa, pb, kWarmSweeps, true, jpart));
+  // the two short starts run one sweep per launch (the list plan) when the
+  // solve itself is the resident plan
+  const JacobiPlan wp = plan.by == 4 ? JacobiPlan{1, 3, 1} : plan;
+  AQ_TRY(enqueue_sweeps_on(this, wp, pa, pb, kWarmSweeps, true, jpart));
   AQ_CUDA(cudaMemsetAsync(za, 0, sizeof(float) * d.C, stream));
   AQ_CUDA(cudaMemsetAsync(zb, 0, sizeof(float) * d.C, stream));
-  AQ_TRY(enqueue_sweeps_on(this, plan, za, zb, kWarmSweeps, true, jpart2));
-  k_pick_start<<<1, 1024, 0, stream>>>(jpart, jpart2, last_parts(this, kWarmSweeps), ss, pick,
+  AQ_TRY(enqueue_sweeps_on(this, wp, za, zb, kWarmSweeps, true, jpart2));
+  k_pick_start<<<1, 1024, 0, stream>>>(jpart, jpart2, last_parts_of(this, wp, kWarmSweeps), ss, pick,
                                        cfg.solve_mode == AQ_SOLVE_RESIDUAL ? (double)cfg.rel_residual : 0.0);
   AQ_CUDA(cudaGetLastError());
   k_copy_if<<<std::min((d.C + 255) / 256, 148 * 8), 256, 0, stream>>>(pick, za, pa, d.C);
@@ -414,13 +439,23 @@ static aq_status enqueue_persistent(aq_fluid* f, int fixed_sweeps) {
   AQ_CUDA(launch_items_compact(f->stream, f->d, f->bact, f->items, f->n_items, f->bar));
   AQ_CUDA(launch_persist_solve(f->stream, f->d, f->ctas, f->pa, f->pb, f->rhs, f->type, f->items, f->n_items, f->bar,
                                f->ppart, f->ss, fixed_sweeps, f->cfg.check_interval, f->cfg.max_iterations,
-                               (double)f->cfg.rel_residual));
+                               (double)f->cfg.rel_residual, f->barrier_test));
+  return AQ_OK;
+}
+
+// The whole solve as one cooperative launch of resident tiles (plan.by == 4).
+static aq_status enqueue_resident(aq_fluid* f, int fixed_sweeps) {
+  AQ_CUDA(launch_resident_solve(f->stream, f->d, f->plan.xc, f->plan.levels, f->res_ctas, f->pa, f->pb, f->rhs,
+                                f->type, f->bact, f->tiles, f->n_tiles, f->bar, f->ppart, f->ss, fixed_sweeps,
+                                f->cfg.check_interval, f->cfg.max_iterations, (double)f->cfg.rel_residual,
+                                f->barrier_test));
   return AQ_OK;
 }
 
 aq_status aq_fluid::enq_solve_fixed(int sweeps) {
   if (sweeps <= 0) return AQ_OK;
   if (plan.by == 1) return enqueue_persistent(this, sweeps);
+  if (plan.by == 4) return enqueue_resident(this, sweeps);
   AQ_TRY(enqueue_sweeps(this, sweeps));
   AQ_CUDA(launch_resid_finalize(stream, jpart, last_parts(this, sweeps), ss, sweeps, 0.0, 0, false, 0));
   return AQ_OK;
@@ -428,7 +463,7 @@ aq_status aq_fluid::enq_solve_fixed(int sweeps) {
 
 aq_status aq_fluid::enq_solve_body(bool set_cond, unsigned long long handle, int* launches) {
   const int m = cfg.check_interval;
-  if ((plan.by == 0 || plan.by >= 2) && d.sz % 4 == 0) {
+  if (separate_residual(plan) && d.sz % 4 == 0) {
     // plans whose residual is a separate pass: pass and check in one launch
     AQ_TRY(enqueue_sweeps(this, m, false));
     if (plan.by == 3)
@@ -450,6 +485,7 @@ aq_status aq_fluid::enq_solve_body(bool set_cond, unsigned long long handle, int
 // Residual mode without a graph: the host reads the solve state after each block.
 aq_status aq_fluid::enq_solve_residual_eager() {
   if (plan.by == 1) return enqueue_persistent(this, 0);
+  if (plan.by == 4) return enqueue_resident(this, 0);
   for (int guard = 0; guard < 1000000; ++guard) {
     AQ_TRY(enq_solve_body(false, 0, nullptr));
     AQ_CUDA(cudaMemcpyAsync(ss_host, ss, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
@@ -632,11 +668,11 @@ aq_status aq_fluid::build_graph() {
   };
   aq_status st = AQ_OK;
   launches += (n > 0 ? 6 : 3) + 2 + 2;  // particles (+3 scan kernels), p2g, slayer, divergence, b2
-  if (cfg.solve_mode == AQ_SOLVE_RESIDUAL && plan.by == 1) {
+  if (cfg.solve_mode == AQ_SOLVE_RESIDUAL && (plan.by == 1 || plan.by == 4)) {
     st = capture(g, nullptr, 0, [&]() {
       aq_status s2 = enq_pre_solve();
       if (s2 != AQ_OK) return s2;
-      s2 = enqueue_persistent(this, 0);
+      s2 = plan.by == 1 ? enqueue_persistent(this, 0) : enqueue_resident(this, 0);
       if (s2 != AQ_OK) return s2;
       return enq_post_solve();
     });
@@ -681,7 +717,8 @@ aq_status aq_fluid::build_graph() {
   }
   if (st != AQ_OK) { cudaGraphDestroy(g); return st; }
   if (cfg.pressure_init == AQ_PRESSURE_LEARNED)  // network, two 20-sweep starts, pick, copy
-    launches += kUNetForwardLaunches + 2 * (count_jacobi_launches(kWarmSweeps) - 1) + 2;
+    launches += kUNetForwardLaunches +
+                2 * (jacobi_launches(plan.by == 4 ? JacobiPlan{1, 3, 1} : plan, kWarmSweeps) - 1) + 2;
   launches += 1 + 3 + (multiphase ? cfg.diffusion_iterations : 0) + (ink_on && n_ink > 0 ? 1 : 0);
   graph_launches = launches;
   cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
@@ -920,6 +957,9 @@ aq_status aq_fluid::upload(const aq_host_state* s) {
   if (s->size_x != d.sx || s->size_y != d.sy || s->size_z != d.sz || s->particle_count != n)
     return fail(AQ_ERR_INVALID_ARGUMENT, "state dimensions do not match the fluid");
   AQ_CUDA(cudaStreamSynchronize(stream));
+  // a new state: the sticky health flags start over
+  AQ_CUDA(cudaMemsetAsync(&ss->nonfinite_seen, 0, sizeof(int), stream));
+  AQ_CUDA(cudaMemsetAsync(&ss->sync_timeout, 0, sizeof(int), stream));
   const size_t N = (size_t)n, C = (size_t)d.C, F = (size_t)d.F;
   if (s->position) {
     const float lim[3] = {d.sx * d.h, d.sy * d.h, d.sz * d.h};
@@ -1243,8 +1283,7 @@ aq_status aq_fluid_step_host(aq_fluid* f, int32_t n_steps, const float* pin, con
       AQ_CUDA(cudaMemcpyAsync(vout + 2 * N, f->cur.vz, 4 * N, cudaMemcpyDeviceToHost, s));
     }
   }
-  AQ_CUDA(cudaStreamSynchronize(s));
-  return AQ_OK;
+  return f->health();
 }
 
 aq_status aq_fluid_set_graph_mode(aq_fluid* f, int32_t use_graph) {
@@ -1261,7 +1300,44 @@ aq_status aq_fluid_run_stage(aq_fluid* f, int32_t stage) {
 
 aq_status aq_fluid_synchronize(aq_fluid* f) {
   if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
-  AQ_CUDA(cudaStreamSynchronize(f->stream));
+  cudaSetDevice(f->device);
+  return f->health();
+}
+
+// Waits for the fluid's work, then reports what the device recorded: a
+// bounded wait that gave up (AQ_ERR_TIMEOUT), or a non-finite divergence
+// norm or pressure residual in any step since creation or the last upload
+// (AQ_ERR_NONFINITE).  The reference has no such check: a NaN there simply
+// propagates (Common/GpuCommons.h:118-142 only catches CUDA errors).
+aq_status aq_fluid::health() {
+  AQ_CUDA(cudaMemcpyAsync(ss_host, ss, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+  AQ_CUDA(cudaStreamSynchronize(stream));
+  const SolveState& s = *ss_host;
+  if (s.sync_timeout) return fail(AQ_ERR_TIMEOUT, "a persistent pressure solve gave up waiting at a grid barrier");
+  if (s.nonfinite_seen) return fail(AQ_ERR_NONFINITE, "a step produced a non-finite divergence norm or pressure residual");
+  return AQ_OK;
+}
+
+aq_status aq_selfcheck_division(int32_t device, uint64_t* mismatches) {
+  if (!mismatches) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
+  AQ_CUDA(cudaSetDevice(device));
+  unsigned long long* bad = nullptr;
+  AQ_CUDA(cudaMalloc(&bad, sizeof(unsigned long long)));
+  cudaError_t e = cudaMemset(bad, 0, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = launch_div6_check(nullptr, bad);
+  unsigned long long h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, bad, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(bad);
+  if (e != cudaSuccess) return fail(AQ_ERR_CUDA, cudaGetErrorString(e));
+  *mismatches = h;
+  return AQ_OK;
+}
+
+aq_status aq_fluid_test_barrier_timeout(aq_fluid* f, int32_t withhold_cta, uint32_t spin_limit) {
+  if (!f) return fail(AQ_ERR_INVALID_ARGUMENT, "fluid is NULL");
+  f->barrier_test.withhold_cta = withhold_cta;
+  f->barrier_test.spin_limit = spin_limit;
+  f->invalidate_graph();  // the step graph holds the solve's launch parameters
   return AQ_OK;
 }
 
@@ -1316,13 +1392,16 @@ aq_status aq_fluid_solve_stats(const aq_fluid* f, aq_solve_stats* st) {
   st->b_norm = s.b2 >= 0 ? sqrt(s.b2) : -1.0;
   st->fluid_cells = s.fluid_cells;
   st->converged = s.converged;
-  if (s.sync_timeout) return fail(AQ_ERR_TIMEOUT, "persistent pressure solve timed out at a grid barrier");
   st->blocks = s.bodies;
   st->total_sweeps = s.total_sweeps;
   st->total_blocks = s.total_bodies;
   st->warm_start = s.warm;
   st->warm_rel_residual = s.warm_rel;
   st->zero_rel_residual = s.zero_rel;
+  if (s.sync_timeout) return fail(AQ_ERR_TIMEOUT, "persistent pressure solve timed out at a grid barrier");
+  if (s.nonfinite) return fail(AQ_ERR_NONFINITE, "the last pressure solve's residual is not finite");
+  if (f->cfg.solve_mode == AQ_SOLVE_RESIDUAL && !s.converged && s.rel_residual >= 0.0)
+    return fail(AQ_ERR_NOT_CONVERGED, "the last pressure solve stopped at max_iterations above rel_residual");
   return AQ_OK;
 }
 
@@ -1454,6 +1533,20 @@ aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, in
     f->invalidate_graph();
     return AQ_OK;
   }
+  if (rows == 4) {  // resident tiles: levels = sweeps per halo exchange, x_planes = tile shape
+    cudaSetDevice(f->device);
+    const int c = resident_ctas(f->device, x_planes, levels);
+    if (c <= 0) return fail(AQ_ERR_INVALID_ARGUMENT, "unsupported resident plan (levels 2 or 4, shape 0-5)");
+    if (f->cfg.pressure_init == AQ_PRESSURE_LEARNED && f->d.sz % 4 != 0)
+      return fail(AQ_ERR_INVALID_ARGUMENT, "the learned warm start needs sz % 4 == 0");
+    AQ_CUDA(cudaStreamSynchronize(f->stream));
+    f->res_ctas = c;
+    f->plan = JacobiPlan{levels, 4, x_planes};
+    AQ_TRY(f->enq_row_items());  // the learned start's rows, if any
+    AQ_CUDA(cudaStreamSynchronize(f->stream));
+    f->invalidate_graph();
+    return AQ_OK;
+  }
   if (rows == 3) {  // list of active warp rows, one sweep per launch
     if (f->d.sz % 4 != 0 || levels != 1 || x_planes != 1)
       return fail(AQ_ERR_INVALID_ARGUMENT, "the list plan is (1, 3, 1) and needs sz % 4 == 0");
@@ -1535,7 +1628,9 @@ aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, in
   // The sweeps are captured into a graph and replayed, as inside a step.
   cudaGraph_t g = nullptr;
   AQ_CUDA(cudaStreamBeginCapture(f->stream, cudaStreamCaptureModeThreadLocal));
-  aq_status st = f->plan.by == 1 ? enqueue_persistent(f, sweeps) : enqueue_sweeps(f, sweeps, false);
+  aq_status st = f->plan.by == 1   ? enqueue_persistent(f, sweeps)
+                 : f->plan.by == 4 ? enqueue_resident(f, sweeps)
+                                   : enqueue_sweeps(f, sweeps, false);
   cudaGraph_t got = nullptr;
   cudaError_t ce = cudaStreamEndCapture(f->stream, &got);
   if (st != AQ_OK) { if (got) cudaGraphDestroy(got); return st; }
@@ -1560,12 +1655,15 @@ aq_status aq_fluid_benchmark_pressure(aq_fluid* f, int32_t sweeps, float* ms, in
   cudaEventDestroy(b);
   const std::vector<int> parts = split_sweeps(sweeps, f->plan.levels);
   if (ms) *ms = t;
-  if (launches) *launches = f->plan.by == 1 ? 2 : (int32_t)(parts.size() + parts.size() % 2);
+  if (launches)
+    *launches = f->plan.by == 1 || f->plan.by == 4 ? 2 : (int32_t)(parts.size() + parts.size() % 2);
   if (cells_per_sweep) {
     std::vector<uint8_t> act((size_t)f->nbricks);
     AQ_CUDA(cudaMemcpy(act.data(), f->bact, act.size(), cudaMemcpyDeviceToHost));
     *cells_per_sweep =
-        jacobi_cells_updated(f->d, f->plan.by == 1 || f->plan.by == 3 ? JacobiPlan{1, 0, 1} : f->plan, act.data());
+        f->plan.by == 4 ? resident_cells_updated(f->d, f->plan.xc, act.data())
+                        : jacobi_cells_updated(f->d, f->plan.by == 1 || f->plan.by == 3 ? JacobiPlan{1, 0, 1} : f->plan,
+                                               act.data());
   }
   return AQ_OK;
 }
@@ -1637,8 +1735,9 @@ aq_status aq_fluid_autotune(aq_fluid* f, int32_t sweeps_per_trial, const char* c
     if (out) *out = r;
     return AQ_OK;
   }
-  const int cands[][3] = {{1, 0, 1}, {1, 0, 2}, {1, 1, 1}, {1, 16, 8}, {2, 16, 16}, {2, 32, 16}, {4, 32, 16},
-                          {2, 2, 8},  {3, 2, 8},  {4, 2, 8}, {2, 2, 16}, {4, 2, 16}, {1, 3, 1}};
+  const int cands[][3] = {{1, 0, 1}, {1, 0, 2}, {1, 1, 1},  {1, 16, 8}, {2, 16, 16}, {2, 32, 16}, {4, 32, 16},
+                          {2, 2, 8},  {3, 2, 8},  {4, 2, 8},  {2, 2, 16}, {4, 2, 16},  {1, 3, 1},   {4, 4, 0},
+                          {4, 4, 1},  {4, 4, 2},  {4, 4, 3},  {4, 4, 4},  {4, 4, 5},   {2, 4, 0},   {2, 4, 2}};
   float best = 1e30f;
   int bestp[3] = {f->plan.levels, f->plan.by, f->plan.xc};
   for (const auto& c : cands) {

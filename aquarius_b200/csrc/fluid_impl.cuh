@@ -89,6 +89,11 @@ struct aq_fluid {
   unsigned int* bar = nullptr;
   double* ppart = nullptr;
   int ctas = 0;
+  aqb::BarrierTest barrier_test{-1, 0};  // aq_fluid_test_barrier_timeout
+  // resident solve (plan rows 4): tile list and CTAs of its launch
+  int* tiles = nullptr;
+  int* n_tiles = nullptr;
+  int res_ctas = 0;
 
   JacobiPlan plan{4, 16, 32};
   // learned warm start (AQ_PRESSURE_LEARNED)
@@ -171,6 +176,7 @@ struct aq_fluid {
   aq_status build_graph();
   aq_status step(int nsteps);
   aq_status upload(const aq_host_state* s);
+  aq_status health();  // synchronises; AQ_ERR_TIMEOUT / AQ_ERR_NONFINITE from the device's records
   aq_status download(aq_host_state* s);
   aq_status derive_from_state(const std::vector<int>& content, const std::vector<float>& divv,
                               const std::vector<float>& dens);

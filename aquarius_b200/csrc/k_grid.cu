@@ -286,6 +286,7 @@ __device__ __forceinline__ void b2_finalize_body(const double* __restrict__ part
   }
   if (threadIdx.x == 0) {
     ss->b2 = sb[0];
+    if (!isfinite(sb[0])) ss->nonfinite_seen = 1;
     ss->fluid_cells = sn[0];
     ss->iterations = 0;
     ss->bodies = 0;

@@ -744,12 +744,11 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned int* p) {
   return v;
 }
 
-constexpr unsigned kSpinLimit = 1u << 25;  // with 32 ns sleeps: ~1 s before giving up
-
 // Grid barrier on a counter that only grows: arrival e of every CTA waits for
-// e * gridDim.x arrivals.  Bounded: on timeout it sets *fail and returns
-// false; after any failure every barrier returns false at once.
-__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned target, int* fail) {
+// e * gridDim.x arrivals.  Bounded: after spin_limit polls (kSpinLimit, about
+// a second, unless a test shortens it) it sets *fail and returns false; after
+// any failure every barrier returns false at once.
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned target, int* fail, unsigned spin_limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -761,7 +760,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned target,
       atomicAdd(bar, 1u);
       unsigned spins = 0;
       while (ld_acquire(bar) < target) {
-        if (++spins > kSpinLimit || *reinterpret_cast<volatile int*>(fail)) {
+        if (++spins > spin_limit || *reinterpret_cast<volatile int*>(fail)) {
           atomicExch(fail, 1);
           ok = 0;
           break;
@@ -827,11 +826,15 @@ __global__ void __launch_bounds__(1024) k_persist_solve(Dims d, float* __restric
                                                       const int* __restrict__ items, const int* __restrict__ n_items,
                                                       unsigned int* __restrict__ bar, double* __restrict__ part,
                                                       SolveState* __restrict__ ss, int fixed_sweeps, int check,
-                                                      int max_iters, double tol) {
+                                                      int max_iters, double tol, BarrierTest bt) {
   __shared__ double s_red[32];
   __shared__ double s_r2;
   // one CTA per SM; four groups of 256 threads each sweep one item at a time
   const int P = gridDim.x, cta = blockIdx.x;
+  // test hook: this CTA never arrives (a participant that does not join), so
+  // the others' bounded barrier waits run out
+  if (cta == bt.withhold_cta) return;
+  const unsigned spin_limit = bt.spin_limit ? bt.spin_limit : kSpinLimit;
   const int G = 4, grp = threadIdx.x >> 8;
   const int first = cta * G + grp, stride = P * G;
   const int n = *n_items;
@@ -847,7 +850,7 @@ __global__ void __launch_bounds__(1024) k_persist_solve(Dims d, float* __restric
     for (int i = first; i < n; i += stride) sweep_item(d, items[i], bufs[cur], bufs[cur ^ 1], rhs, type);
     cur ^= 1;
     ++epoch;
-    ok = ok && grid_barrier(bar, epoch * (unsigned)P, fail);
+    ok = ok && grid_barrier(bar, epoch * (unsigned)P, fail, spin_limit);
   };
   // residual of the current iterate; every CTA ends with the same r2
   auto residual = [&]() {
@@ -863,7 +866,7 @@ __global__ void __launch_bounds__(1024) k_persist_solve(Dims d, float* __restric
       part[cta] = t;
     }
     ++epoch;
-    ok = ok && grid_barrier(bar, epoch * (unsigned)P, fail);
+    ok = ok && grid_barrier(bar, epoch * (unsigned)P, fail, spin_limit);
     if (threadIdx.x < 32) {
       double t = 0.0;
       for (int k = threadIdx.x; k < P; k += 32) t += *reinterpret_cast<volatile double*>(part + k);
@@ -873,7 +876,7 @@ __global__ void __launch_bounds__(1024) k_persist_solve(Dims d, float* __restric
     }
     __syncthreads();
     r2 = s_r2;
-    rel = ss->b2 > 0.0 ? sqrt(r2) / sqrt(ss->b2) : 0.0;
+    rel = rel_residual_of(r2, ss->b2);
     ++checks;
   };
 
@@ -911,7 +914,7 @@ __global__ void __launch_bounds__(1024) k_persist_solve(Dims d, float* __restric
     ss->r2 = r2;
     ss->rel_residual = rel;
     const bool finite = isfinite(rel);
-    if (!finite) ss->nonfinite = 1;
+    if (!finite) ss->nonfinite = ss->nonfinite_seen = 1;
     ss->converged = (ok && finite && rel >= 0.0 && rel <= tol) ? 1 : 0;
   }
 }
@@ -944,10 +947,10 @@ __device__ __forceinline__ bool finalize_state(double r2, SolveState* __restrict
   ss->total_sweeps += sweeps;
   ss->total_bodies += 1;
   ss->r2 = r2;
-  const double rel = ss->b2 > 0.0 ? sqrt(r2) / sqrt(ss->b2) : 0.0;
+  const double rel = rel_residual_of(r2, ss->b2);
   ss->rel_residual = rel;
   const bool finite = isfinite(rel);
-  if (!finite) ss->nonfinite = 1;
+  if (!finite) ss->nonfinite = ss->nonfinite_seen = 1;
   const bool conv = finite && rel <= tol;
   ss->converged = conv ? 1 : 0;
   return finite && !conv && ss->iterations < max_iters;
@@ -1540,7 +1543,8 @@ cudaError_t launch_items_compact(cudaStream_t st, const Dims& d, const uint8_t* 
 
 cudaError_t launch_persist_solve(cudaStream_t st, const Dims& d, int ctas, float* pa, float* pb, const float* rhs,
                                  const int8_t* type, const int* items, const int* n_items, unsigned int* bar,
-                                 double* part, SolveState* ss, int fixed_sweeps, int check, int max_iters, double tol) {
+                                 double* part, SolveState* ss, int fixed_sweeps, int check, int max_iters, double tol,
+                                 BarrierTest bt) {
   if (d.sz % 4 != 0 || ctas <= 0) return cudaErrorInvalidValue;
   cudaLaunchConfig_t lc = {};
   lc.gridDim = dim3(ctas);
@@ -1552,7 +1556,7 @@ cudaError_t launch_persist_solve(cudaStream_t st, const Dims& d, int ctas, float
   lc.attrs = at;
   lc.numAttrs = 1;
   return cudaLaunchKernelEx(&lc, k_persist_solve, d, pa, pb, rhs, type, items, n_items, bar, part, ss, fixed_sweeps,
-                            check, max_iters, tol);
+                            check, max_iters, tol, bt);
 }
 
 int resid_flat_parts(const Dims& d) { return ((d.sz / 4 + 31) / 32) * ((d.sy + 7) / 8) * d.sx; }
