@@ -205,7 +205,8 @@ aq_status aq_fluid_step(aq_fluid* f, int32_t n_steps);
 /* Host-buffer step, for callers that keep the particle state in host memory:
  * uploads position_in/velocity_in ([3][N] each, may be NULL to keep the device
  * copy), runs n_steps, downloads position_out/velocity_out ([3][N], may be
- * NULL) and synchronizes.  Pinned buffers make the copies asynchronous. */
+ * NULL) and synchronizes.  Pinned buffers make the copies asynchronous.
+ * Returns what aq_fluid_synchronize returns after the steps. */
 aq_status aq_fluid_step_host(aq_fluid* f, int32_t n_steps,
                              const float* position_in, const float* velocity_in,
                              float* position_out, float* velocity_out);
@@ -221,7 +222,15 @@ aq_status aq_fluid_set_graph_mode(aq_fluid* f, int32_t use_graph);
  * statement of simulationStep does. */
 aq_status aq_fluid_run_stage(aq_fluid* f, int32_t stage);
 
-/* Waits for all work of the fluid. */
+/* Waits for all work of the fluid, then reports what the device recorded
+ * while stepping (a step itself is asynchronous and returns before its
+ * kernels run):
+ *   AQ_ERR_TIMEOUT    a bounded device wait of a persistent pressure solve
+ *                     gave up (its grid barrier);
+ *   AQ_ERR_NONFINITE  some step since creation or the last
+ *                     aq_fluid_upload_state had a non-finite divergence norm
+ *                     ||b|| or pressure residual (a NaN or Inf in the state).
+ * Both are sticky until the next aq_fluid_upload_state. */
 aq_status aq_fluid_synchronize(aq_fluid* f);
 
 aq_status aq_fluid_time(const aq_fluid* f, double* physical_time);
@@ -234,12 +243,38 @@ aq_status aq_fluid_stream(const aq_fluid* f, void** stream);
 aq_status aq_fluid_download_state(aq_fluid* f, aq_host_state* s);
 aq_status aq_fluid_upload_state(aq_fluid* f, const aq_host_state* s);
 
+/* Fills *st (synchronising), then returns AQ_ERR_TIMEOUT if the last solve's
+ * grid barrier gave up, AQ_ERR_NONFINITE if its residual is not finite, and
+ * AQ_ERR_NOT_CONVERGED in AQ_SOLVE_RESIDUAL mode when it stopped at
+ * max_iterations above rel_residual (st then holds the achieved residual);
+ * otherwise AQ_OK. */
 aq_status aq_fluid_solve_stats(const aq_fluid* f, aq_solve_stats* st);
+
+/* Test hook of the bounded device waits (no counterpart in the reference):
+ * from the next step on, the persistent pressure solves (Jacobi plans rows 1
+ * and 4) run with CTA withhold_cta (-1: none) leaving without ever arriving
+ * at a grid barrier, and the other CTAs giving up after spin_limit polls
+ * (0: the default, about a second).  The solve then ends early with
+ * aq_fluid_synchronize returning AQ_ERR_TIMEOUT, and the device stays usable.
+ * Call with (-1, 0) to switch it off. */
+aq_status aq_fluid_test_barrier_timeout(aq_fluid* f, int32_t withhold_cta, uint32_t spin_limit);
+
+/* Self-check of the resident solve's division by 6 (an FMA-corrected
+ * reciprocal product on normal quotients) against the IEEE divide over all
+ * 2^32 float bit patterns on `device`; *mismatches receives the count of
+ * differing results (NaN equal to NaN).  No counterpart in the reference. */
+aq_status aq_selfcheck_division(int32_t device, uint64_t* mismatches);
 
 /* Plan of the Jacobi kernels.  rows = 0: one vectorised sweep per launch
  * (levels 1, x_planes in {1,2,4,8} planes per block; sz % 4 == 0).
  * rows = 1: the whole solve in one persistent cooperative launch with a
- * grid barrier between sweeps (levels 1; sz % 4 == 0).  rows = 8, 16, 32:
+ * grid barrier between sweeps (levels 1; sz % 4 == 0).  rows = 3: one sweep
+ * per launch over a list of the warp rows that hold fluid (levels 1,
+ * x_planes 1; sz % 4 == 0).  rows = 4: the whole solve in one cooperative
+ * launch of resident tiles: each CTA keeps a tile of the grid (x_planes
+ * selects the shape: 0 8x40x16, 1 8x32x16, 2 16x16x16, 3 8x24x16, 4 8x16x16,
+ * 5 16x24x16 cells) with a `levels`-cell halo (2 or 4) in shared memory for
+ * the whole solve and exchanges halos every `levels` sweeps.  rows = 8, 16, 32:
  * the temporally blocked kernel with `levels` sweeps (1, 2, 4, 8) per launch
  * over tiles of that many rows and x_planes planes.  Chosen per grid by the
  * tuner; invalid plans are rejected. */
@@ -521,9 +556,11 @@ aq_status aq_fluid_set_warm_start(aq_fluid* f, aq_unet* net);
  * handed over by a host application, a memory-budgeted frame loop, a plugin
  * that must not touch its host process's allocator).
  *
- * cell_type [C] (0 air, 1 fluid), rhs [C] (-divergence*density on fluid
- * cells) and pressure [C] (initial guess in, result out) are device buffers
- * in the cell layout of aq_host_state; `sweeps` Jacobi sweeps are run on
+ * cell_type [C] (1 fluid; any other value, such as 0 air or 2 solid, is
+ * not fluid and its pressure is set to 0, as the pressure stage does), rhs
+ * [C] (-divergence*density on fluid cells) and pressure [C] (initial guess
+ * in, result out) are device buffers in the cell layout of aq_host_state;
+ * `sweeps` Jacobi sweeps are run on
  * `stream` (NULL = the legacy default stream) exactly as the pressure stage
  * of aq_fluid_step does in AQ_SOLVE_FIXED mode, including clearing air
  * pressure first.  The second Jacobi buffer and the activity flags are a
