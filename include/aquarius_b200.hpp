@@ -15,12 +15,23 @@
 //                                                    step (the reference's
 //                                                    commented-out :349-350)
 //
+//   DrawCommand (Rendering/DrawCommand.h:37-59)       aquarius_b200::DrawCommand
+//   ::draw(const DrawCommand&)                       same name: the headless
+//     (Fluid/Fluid_3D_FLIP.cu:396-430)                 frame (aq_fluid_draw) into
+//                                                    an RGBA8 image owned by a
+//                                                    Renderer instead of a GL
+//                                                    framebuffer
+//
 // Differences: errors throw aquarius_b200::Error (the reference prints and
-// exits); draw() is a no-op (rendering is not part of this library); the
-// centre is returned as std::array<float,3> instead of glm::vec3.
+// exits); draw() renders into a device image (row 0 at the bottom, as
+// glReadPixels returns it) that Renderer::downloadImage copies out, since no
+// graphics API is used; the centre is returned as std::array<float,3>
+// instead of glm::vec3.
 #pragma once
 
 #include <array>
+#include <cstdint>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -129,6 +140,45 @@ struct FluidConfig {  // Fluid/FluidConfig.cuh:68-97
   }
 };
 
+using DrawCommand = aq_draw_command;
+
+// The frame target of draw(): the reference draws into the window's GL
+// framebuffer; here an RGBA8 device image owned by the renderer, with the
+// skybox and logo textures the reference loads from files set by the caller.
+class Renderer {
+ public:
+  explicit Renderer(int device = 0, void* stream = nullptr) {
+    check(aq_renderer_create(device, stream, &r_), "aq_renderer_create");
+  }
+  Renderer(const Renderer&) = delete;
+  Renderer& operator=(const Renderer&) = delete;
+  ~Renderer() {
+    if (r_) aq_renderer_destroy(r_);
+  }
+  // Six face_size^2 RGB8 faces, posx negx posy negy posz negz (Skybox.cu:24-44).
+  void setSkybox(const uint8_t* faces_rgb, int face_size) {
+    check(aq_renderer_set_skybox(r_, faces_rgb, face_size), "aq_renderer_set_skybox");
+  }
+  void setLogo(const uint8_t* rgb, int width, int height) {
+    check(aq_renderer_set_logo(r_, rgb, width, height), "aq_renderer_set_logo");
+  }
+  void synchronize() { check(aq_renderer_synchronize(r_), "aq_renderer_synchronize"); }
+  // The last frame, W*H*4 bytes into host memory, row 0 at the bottom.
+  void downloadImage(uint8_t* host) { check(aq_renderer_download_image(r_, host), "aq_renderer_download_image"); }
+  aq_renderer* handle() const { return r_; }
+
+ private:
+  aq_renderer* r_ = nullptr;
+};
+
+// DrawCommand of main.cu's first frame for a fluid (camera, projection,
+// light, container, render and environment modes).
+inline DrawCommand defaultDrawCommand(int width, int height, float containerSize, int sizeY) {
+  DrawCommand dc{};
+  check(aq_draw_command_default(&dc, width, height, containerSize, sizeY), "aq_draw_command_default");
+  return dc;
+}
+
 namespace Fluid_3D_FLIP {
 
 class Fluid {
@@ -154,8 +204,24 @@ class Fluid {
     check(aq_fluid_time(f_, &t), "aq_fluid_time");
     physicalTime = (float)t;
   }
-  template <typename DrawCommand>
-  void draw(const DrawCommand&) {}  // headless
+  // Fluid::draw (Fluid/Fluid_3D_FLIP.cu:396-430), headless: meshes the
+  // particles (mesh modes), fills the point-sprite VBO and draws the frame
+  // into the renderer's image, or into rgba (a device buffer of W*H*4 bytes).
+  void draw(const DrawCommand& drawCommand, Renderer& renderer, uint8_t* rgba = nullptr) {
+    check(aq_fluid_draw(f_, renderer.handle(), &drawCommand, rgba), "aq_fluid_draw");
+  }
+  // The reference's one-argument form: draws with a renderer the fluid owns
+  // (created on the fluid's device and stream at the first draw).
+  void draw(const DrawCommand& drawCommand) {
+    if (!renderer_) {
+      void* stream = nullptr;
+      check(aq_fluid_stream(f_, &stream), "aq_fluid_stream");
+      renderer_.reset(new Renderer(config_.device, stream));
+    }
+    draw(drawCommand, *renderer_);
+  }
+  // The renderer of the one-argument draw (nullptr before the first draw).
+  Renderer* renderer() const { return renderer_.get(); }
   std::array<float, 3> getCenter() const {
     std::array<float, 3> c{};
     check(aq_fluid_container(f_, c.data(), nullptr), "aq_fluid_container");
@@ -195,11 +261,13 @@ class Fluid {
 
  private:
   void release() {
+    renderer_.reset();
     if (f_) aq_fluid_destroy(f_);
     f_ = nullptr;
   }
   aq_fluid* f_ = nullptr;
   FluidConfig config_;
+  std::unique_ptr<Renderer> renderer_;
 };
 
 }  // namespace Fluid_3D_FLIP

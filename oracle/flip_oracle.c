@@ -55,6 +55,10 @@ struct orc_fluid {
   orc_rng rng;
   int n_ink;
   float *ink_pos, *ink_vel; /* [3][n_ink] */
+  /* 0: race-free reading of the reference's in-place stages (default);
+   * 1: those stages in place, in a serial schedule of the reference's launch
+   *    (orc_set_schedule) */
+  int schedule;
 };
 
 /* ---------------------------------------------------------------- helpers */
@@ -891,6 +895,8 @@ static void residual_sums(const orc_fluid* o, const float* p, double* rr, double
   *rr = a; *bb = b; *nf = k;
 }
 
+void orc_set_schedule(orc_fluid* o, int schedule) { o->schedule = schedule == 1 ? 1 : 0; }
+
 double orc_pressure_residual(const orc_fluid* o) {
   double rr, bb;
   int nf;
@@ -909,6 +915,46 @@ static void jacobi_sweep(orc_fluid* o, const float* pin, float* pout) {
         float rhs = -o->divergence[ci] * o->density[ci];
         pout[ci] = jacobi_cell(o, pin, x, y, z, rhs);
       }
+}
+
+/* The reference's launch of its grid kernels (MAC_Grid_3D.cu:48): blocks of
+ * 8^3 threads, threadIdx.x along x, a grid of divUp(s+1, 8) blocks per axis.
+ * A warp is 32 consecutive threads: 8 x by 4 y of one z.  Serial schedule:
+ * blocks in launch order (x fastest), a block's 16 warps in order, each warp
+ * doing every read before any write (lockstep).  It is one of the outcomes
+ * the reference's in-place stencils allow when a launch's threads read cells
+ * other threads write (jacobiImpl, extrapolateVelocityByOne): each read sees
+ * every update of the warps before it, the opposite extreme of the race-free
+ * reading in which no read sees an update of its own launch.
+ * Calls f(o, x, y, z, k) for the 32 threads of each warp with k = 0..31 in
+ * the read phase, then w(o, x, y, z, k) in the write phase. */
+typedef void (*serial_read_fn)(orc_fluid* o, int x, int y, int z, int k, void* scratch);
+typedef void (*serial_write_fn)(orc_fluid* o, int x, int y, int z, int k, void* scratch);
+static void serial_launch(orc_fluid* o, serial_read_fn rd, serial_write_fn wr, void* scratch) {
+  const int gx = divUp(o->sx + 1, 8), gy = divUp(o->sy + 1, 8), gz = divUp(o->sz + 1, 8);
+  for (int bz = 0; bz < gz; ++bz)
+    for (int by = 0; by < gy; ++by)
+      for (int bx = 0; bx < gx; ++bx)
+        for (int w = 0; w < 16; ++w) {
+          const int tz = w >> 1, ty0 = (w & 1) * 4;
+          for (int phase = 0; phase < 2; ++phase)
+            for (int k = 0; k < 32; ++k) {
+              const int x = bx * 8 + (k & 7), y = by * 8 + ty0 + (k >> 3), z = bz * 8 + tz;
+              if (x >= o->sx || y >= o->sy || z >= o->sz) continue;
+              if (phase == 0) rd(o, x, y, z, k, scratch);
+              else wr(o, x, y, z, k, scratch);
+            }
+        }
+}
+
+static void jacobi_serial_read(orc_fluid* o, int x, int y, int z, int k, void* scratch) {
+  float* v = (float*)scratch;
+  const int ci = cidx(o, x, y, z);
+  if (content_cell(o, x, y, z) == AIR) { v[k] = 0.f; return; }
+  v[k] = jacobi_cell(o, o->pressure, x, y, z, -o->divergence[ci] * o->density[ci]);
+}
+static void jacobi_serial_write(orc_fluid* o, int x, int y, int z, int k, void* scratch) {
+  o->pressure[cidx(o, x, y, z)] = ((float*)scratch)[k];
 }
 
 /* solvePressureJacobi (Fluid_3D_common.cu:48-55), ping-pong.  RESIDUAL mode
@@ -941,6 +987,11 @@ static void stage_pressure(orc_fluid* o) {
     o->rel_res = rel;
   } else {
     for (int k = 0; k < o->cfg.pressure_iterations; ++k) {
+      if (o->schedule == 1) {
+        float v[32];
+        serial_launch(o, jacobi_serial_read, jacobi_serial_write, v);
+        continue;
+      }
       jacobi_sweep(o, o->pressure, o->p_tmp);
       float* t = o->pressure; o->pressure = o->p_tmp; o->p_tmp = t;
     }
@@ -1003,11 +1054,75 @@ static void stage_project(orc_fluid* o) {
       }
 }
 
+/* One cell of extrapolateVelocityByOne (Fluid_3D_kernels.cu:210-422) read
+ * from nv/hs: the extrapolated components (has_out[c] = 1, nv_out[c]) and
+ * the unchanged ones as they are. */
+static void extrapolate_cell(const orc_fluid* o, const float* nv, const int* hs, int x, int y, int z, float nv_out[3],
+                             int has_out[3]) {
+  const int sx = o->sx, sy = o->sy, sz = o->sz, C = o->C, F = o->F;
+  const float eps = (float)(-1 + 1e-6);
+  const int ci = cidx(o, x, y, z), ni = nidx(o, x, y, z);
+  for (int comp = 0; comp < 3; ++comp) {
+    has_out[comp] = hs[comp * C + ci];
+    nv_out[comp] = nv[comp * F + ni];
+    if (has_out[comp]) continue;
+    float sum = 0;
+    int cnt = 0;
+    if (x > 0) {
+      int nc = cidx(o, x - 1, y, z), nn = nidx(o, x - 1, y, z);
+      if (hs[comp * C + nc] && nv[nn] > eps) { sum += nv[comp * F + nn]; cnt++; }
+    }
+    if (y > 0) {
+      int nc = cidx(o, x, y - 1, z), nn = nidx(o, x, y - 1, z);
+      if (hs[comp * C + nc] && nv[F + nn] > eps) { sum += nv[comp * F + nn]; cnt++; }
+    }
+    if (z > 0) {
+      int nc = cidx(o, x, y, z - 1), nn = nidx(o, x, y, z - 1);
+      if (hs[comp * C + nc] && nv[2 * F + nn] > eps) { sum += nv[comp * F + nn]; cnt++; }
+    }
+    if (x < sx - 1) {
+      int nc = cidx(o, x + 1, y, z), nn = nidx(o, x + 1, y, z);
+      if (hs[comp * C + nc] && nv[nn] < -eps) { sum += nv[comp * F + nn]; cnt++; }
+    }
+    if (y < sy - 1) {
+      int nc = cidx(o, x, y + 1, z), nn = nidx(o, x, y + 1, z);
+      if (hs[comp * C + nc] && nv[F + nn] < -eps) { sum += nv[comp * F + nn]; cnt++; }
+    }
+    if (z < sz - 1) {
+      int nc = cidx(o, x, y, z + 1), nn = nidx(o, x, y, z + 1);
+      if (hs[comp * C + nc] && nv[2 * F + nn] < -eps) { sum += nv[comp * F + nn]; cnt++; }
+    }
+    if (cnt > 0) {
+      nv_out[comp] = sum / (float)cnt;
+      has_out[comp] = 1;
+    }
+  }
+}
+
+typedef struct { float nv[32][3]; int has[32][3]; } extrap_scratch;
+static void extrap_serial_read(orc_fluid* o, int x, int y, int z, int k, void* scratch) {
+  extrap_scratch* s = (extrap_scratch*)scratch;
+  extrapolate_cell(o, o->new_velocity, o->has, x, y, z, s->nv[k], s->has[k]);
+}
+static void extrap_serial_write(orc_fluid* o, int x, int y, int z, int k, void* scratch) {
+  extrap_scratch* s = (extrap_scratch*)scratch;
+  const int ci = cidx(o, x, y, z), ni = nidx(o, x, y, z);
+  for (int comp = 0; comp < 3; ++comp) {
+    o->new_velocity[comp * o->F + ni] = s->nv[k][comp];
+    o->has[comp * o->C + ci] = s->has[k][comp];
+  }
+}
+
 /* extrapolateVelocityByOne (Fluid_3D_kernels.cu:210-422), 3 passes
  * (Fluid_3D_common.cu:65-82); each pass reads the previous pass's values. */
 static void stage_extrapolate(orc_fluid* o) {
   const int sx = o->sx, sy = o->sy, sz = o->sz, C = o->C, F = o->F;
   const float eps = (float)(-1 + 1e-6);
+  if (o->schedule == 1) {
+    extrap_scratch s;
+    for (int pass = 0; pass < 3; ++pass) serial_launch(o, extrap_serial_read, extrap_serial_write, &s);
+    return;
+  }
   for (int pass = 0; pass < 3; ++pass) {
     const float* nv = o->new_velocity;
     const int* hs = o->has;

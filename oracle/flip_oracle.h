@@ -48,6 +48,13 @@ void orc_solve_stats(const orc_fluid* o, int* iters, double* rel_res, double* b_
 /* Relative residual of the current pressure for the current system. */
 double orc_pressure_residual(const orc_fluid* o);
 
+/* 0 (default): the race-free reading of the reference's in-place Jacobi and
+ * extrapolation.  1: those two stages in place in a serial schedule of the
+ * reference's launch (blocks in launch order, warps in order, each warp
+ * reading before it writes), another outcome the racy kernels allow; used by
+ * the tests to bound how far the race can move the reference's result. */
+void orc_set_schedule(orc_fluid* o, int schedule);
+
 /* Fills a default config (same values as aq_config_default). */
 void orc_config_default(aq_config* cfg);
 

@@ -192,6 +192,29 @@ int aqref_step(void* h, int n) {
   return (int)aqref_first_error;
 }
 
+/* Times n simulationStep()s with CUDA events on the legacy default stream,
+ * the stream every reference kernel is launched on.  The reference
+ * synchronises the device inside a step (HANDLE_ERROR / CHECK_CUDA_ERROR,
+ * Common/GpuCommons.h:118-142); those waits are part of its behaviour and of
+ * the measured time. */
+int aqref_time_steps(void* h, int n, float* ms) {
+  RefFluid* r = (RefFluid*)h;
+  cudaEvent_t a, b;
+  aqref_record(cudaEventCreate(&a), "event", __FILE__, __LINE__);
+  aqref_record(cudaEventCreate(&b), "event", __FILE__, __LINE__);
+  cudaDeviceSynchronize();
+  cudaEventRecord(a, 0);
+  for (int i = 0; i < n; ++i) r->f->simulationStep();
+  cudaEventRecord(b, 0);
+  cudaEventSynchronize(b);
+  float t = 0.f;
+  aqref_record(cudaEventElapsedTime(&t, a, b), "elapsed", __FILE__, __LINE__);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (ms) *ms = t;
+  return (int)aqref_first_error;
+}
+
 /* One sub-stage, with the exact calls simulationStep / transferToGrid make. */
 int aqref_stage(void* h, int stage) {
   Fluid_3D_FLIP::Fluid* f = ((RefFluid*)h)->f;

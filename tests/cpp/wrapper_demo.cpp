@@ -23,7 +23,16 @@ int main() {
   fluid.synchronize();
   std::vector<float> ink(3 * (size_t)fluid.inkParticleCount);
   fluid.downloadInk(ink.data(), nullptr);
-  std::printf("particles %d ink %d time %.3f center %.1f size %.1f\n", fluid.particleCount(),
-              fluid.inkParticleCount, fluid.physicalTime, fluid.getCenter()[0], fluid.getContainerSize());
-  return fluid.physicalTime > 0 && fluid.inkParticleCount > 0 ? 0 : 4;
+  // Fluid::draw with main.cu's first-frame command, into the fluid's renderer
+  const int W = 96, H = 64;
+  DrawCommand dc = defaultDrawCommand(W, H, fluid.getContainerSize(), config.FLIP.sizeY);
+  dc.environment_mode = AQ_ENV_CHESS_BOARD;  // procedural floor: lit without loaded textures
+  fluid.draw(dc);
+  std::vector<uint8_t> image((size_t)W * H * 4);
+  fluid.renderer()->downloadImage(image.data());
+  long lit = 0;
+  for (size_t i = 0; i < image.size(); i += 4) lit += (image[i] | image[i + 1] | image[i + 2]) != 0;
+  std::printf("particles %d ink %d time %.3f center %.1f size %.1f lit %ld\n", fluid.particleCount(),
+              fluid.inkParticleCount, fluid.physicalTime, fluid.getCenter()[0], fluid.getContainerSize(), lit);
+  return fluid.physicalTime > 0 && fluid.inkParticleCount > 0 && lit > 0 ? 0 : 4;
 }

@@ -51,6 +51,7 @@ def _load_oracle():
         lib.orc_set_state.argtypes = [ct.c_void_p, ct.POINTER(_abi.HostState)]
         lib.orc_solve_stats.argtypes = [ct.c_void_p, ct.POINTER(ct.c_int), ct.POINTER(ct.c_double),
                                         ct.POINTER(ct.c_double), ct.POINTER(ct.c_int)]
+        lib.orc_set_schedule.argtypes = [ct.c_void_p, ct.c_int]
         lib.orc_pressure_residual.restype = ct.c_double
         lib.orc_pressure_residual.argtypes = [ct.c_void_p]
         lib.orc_threads.restype = ct.c_int
@@ -103,6 +104,8 @@ def _load_ref():
         lib.aqref_particle_count.argtypes = [ct.c_void_p]
         lib.aqref_step.restype = ct.c_int
         lib.aqref_step.argtypes = [ct.c_void_p, ct.c_int]
+        lib.aqref_time_steps.restype = ct.c_int
+        lib.aqref_time_steps.argtypes = [ct.c_void_p, ct.c_int, ct.POINTER(ct.c_float)]
         lib.aqref_stage.restype = ct.c_int
         lib.aqref_stage.argtypes = [ct.c_void_p, ct.c_int]
         lib.aqref_get_state.restype = ct.c_int
@@ -299,6 +302,11 @@ class Oracle(_StateIO):
     def pressure_residual(self) -> float:
         return self.lib.orc_pressure_residual(self.h)
 
+    def set_schedule(self, serial: bool):
+        """serial: the in-place Jacobi / extrapolation in a serial schedule of
+        the reference's launch instead of the race-free reading."""
+        self.lib.orc_set_schedule(self.h, 1 if serial else 0)
+
     def mesh_dims(self) -> dict:
         buf = (ct.c_byte * 64)()  # orc_mesh_dims: int sdf[3], mesh[3]; float h_sdf, h_mesh, radius
         self.lib.orc_mesh_dims_of(self.h, buf)
@@ -371,6 +379,15 @@ class RefFluid(_StateIO):
         rc = self.lib.aqref_step(self.h, n)
         if rc != 0:
             raise RuntimeError(f"reference step failed: {rc}")
+
+    def time_steps(self, n: int) -> float:
+        """Milliseconds of n simulationStep()s, CUDA events on the legacy
+        default stream (the reference's own device syncs included)."""
+        ms = ct.c_float()
+        rc = self.lib.aqref_time_steps(self.h, n, ct.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"reference step failed: {rc}")
+        return float(ms.value)
 
     def enable_ink(self) -> int:
         n = self.lib.aqref_ink_init(self.h)
