@@ -162,7 +162,7 @@ struct BarrierTest {
 // ---- resident solve (k_resident.cu) ------------------------------------------
 // Plan rows = 4: the whole solve in one cooperative launch, one CTA per SM;
 // a CTA keeps a tile (plan.xc selects the TX x TY x TZ shape) plus a K-cell
-// halo (K = plan.levels, 2 or 4) in shared memory for the whole solve and
+// halo (K = plan.levels, 4) in shared memory for the whole solve and
 // exchanges halos through L2 every K sweeps.  Bit for bit the flat sweep.
 bool resident_plan_ok(int shape, int k);
 int resident_tile_capacity(const Dims& d);        // tile-list entries any shape needs

@@ -1535,8 +1535,8 @@ aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, in
   }
   if (rows == 4) {  // resident tiles: levels = sweeps per halo exchange, x_planes = tile shape
     cudaSetDevice(f->device);
-    const int c = resident_ctas(f->device, x_planes, levels);
-    if (c <= 0) return fail(AQ_ERR_INVALID_ARGUMENT, "unsupported resident plan (levels 2 or 4, shape 0-5)");
+    const int c = f->d.sz % 4 == 0 ? resident_ctas(f->device, x_planes, levels) : 0;
+    if (c <= 0) return fail(AQ_ERR_INVALID_ARGUMENT, "unsupported resident plan (levels 4, shape 0-7, sz % 4 == 0)");
     if (f->cfg.pressure_init == AQ_PRESSURE_LEARNED && f->d.sz % 4 != 0)
       return fail(AQ_ERR_INVALID_ARGUMENT, "the learned warm start needs sz % 4 == 0");
     AQ_CUDA(cudaStreamSynchronize(f->stream));
@@ -1737,7 +1737,7 @@ aq_status aq_fluid_autotune(aq_fluid* f, int32_t sweeps_per_trial, const char* c
   }
   const int cands[][3] = {{1, 0, 1}, {1, 0, 2}, {1, 1, 1},  {1, 16, 8}, {2, 16, 16}, {2, 32, 16}, {4, 32, 16},
                           {2, 2, 8},  {3, 2, 8},  {4, 2, 8},  {2, 2, 16}, {4, 2, 16},  {1, 3, 1},   {4, 4, 0},
-                          {4, 4, 1},  {4, 4, 2},  {4, 4, 3},  {4, 4, 4},  {4, 4, 5},   {2, 4, 0},   {2, 4, 2}};
+                          {4, 4, 1},  {4, 4, 2},  {4, 4, 3},  {4, 4, 4},  {4, 4, 5},   {4, 4, 6}};
   float best = 1e30f;
   int bestp[3] = {f->plan.levels, f->plan.by, f->plan.xc};
   for (const auto& c : cands) {

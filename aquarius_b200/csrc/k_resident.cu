@@ -26,12 +26,14 @@
 // the CTAs, each CTA walks its tiles one after another per block and
 // reloads each whole box from L2 (same results, not resident).
 //
-// Threads.  One per (x, z) column of the box: a thread keeps its column's
-// pressure and rhs in registers, so y neighbours are its own, and reads the
-// x and z neighbours from the other shared buffer (ping-pong per sweep).
-// The x stride of the shared arrays is padded to EZ mod 32, so the 32 lanes
-// of a warp, consecutive columns of one or two x rows, load one y level from
-// 32 distinct banks.
+// Threads.  One per (8-level y segment, x, z-quad) of the box: a thread
+// keeps its segment's pressure quads in registers (y neighbours inside the
+// segment are its own), takes the z neighbours from the lanes holding the
+// adjacent quads (shuffles), and reads x neighbours, segment-end y
+// neighbours and the rhs from shared memory; the new iterate goes to the
+// other shared buffer (ping-pong per sweep).  The x stride of the shared
+// arrays is padded to EZ mod 32, so the lanes of a warp, consecutive quads of
+// one or two x rows, read 16-byte quads from distinct banks.
 //
 // Residual checks (RESIDUAL mode, every `check` sweeps; once at the end in
 // FIXED mode): FP64 ||b - A p||^2 over the tiles' fluid cells, per thread in
@@ -43,39 +45,46 @@
 
 namespace aqb {
 
-// RN(s / 6) for every float s.  On the fast path q0 = RN(s * RN(1/6)) is
-// within an ulp of s/6, the FMA remainder s - 6 q0 is exact, and the FMA
-// correction q0 + rem * RN(1/6) rounds to the correctly rounded quotient
-// (the correction step of Markstein's division); checked exhaustively
-// against IEEE division for every float whose quotient is a normal number
-// (|s| >= 6 * 2^-126, finite: 4,219,469,824 values, no difference).  Zeros,
-// subnormal quotients, infinities and NaN take the IEEE divide.
-__device__ __forceinline__ float div6(float s) {
-  const float a = fabsf(s);
-  if (a >= 0x1.8p-124f && a <= 0x1.fffffep127f) {
-    const float r = 0x1.555556p-3f;  // RN(1/6)
-    const float q0 = __fmul_rn(s, r);
-    const float rem = __fmaf_rn(-q0, 6.0f, s);
-    return __fmaf_rn(rem, r, q0);
-  }
-  return __fdiv_rn(s, 6.f);
+// RN(s / 6).  On the fast path q0 = RN(s * RN(1/6)) is within an ulp of
+// s/6, the FMA remainder s - 6 q0 is exact, and the FMA correction
+// q0 + rem * RN(1/6) rounds to the correctly rounded quotient (the
+// correction step of Markstein's division).  Checked exhaustively against
+// IEEE division: equal for +0 and for every finite s whose quotient is a
+// normal number (|s| >= 6 * 2^-126; 4,219,469,824 values, no difference).
+// div6_fast_ok(s) accepts +0 and finite s with |s| >= 2^-123, a subset;
+// everything else (-0, tiny, Inf, NaN) takes the IEEE divide.
+__device__ __forceinline__ float div6_fast(float s) {
+  const float r = 0x1.555556p-3f;  // RN(1/6)
+  const float q0 = __fmul_rn(s, r);
+  const float rem = __fmaf_rn(-q0, 6.0f, s);
+  return __fmaf_rn(rem, r, q0);
 }
+__device__ __forceinline__ bool div6_fast_ok(float s) {
+  const unsigned b = __float_as_uint(s);
+  return b == 0u || ((b >> 23) & 0xffu) - 4u <= 250u;  // biased exponent in [4, 254]
+}
+__device__ __forceinline__ float div6(float s) { return div6_fast_ok(s) ? div6_fast(s) : __fdiv_rn(s, 6.f); }
 
 namespace {
 
-template <int TX, int TY, int TZ, int K>
+template <int TX, int TY, int TZ, int K, int SEG_>
 struct Res {
   static constexpr int EX = TX + 2 * K, EY = TY + 2 * K, EZ = TZ + 2 * K;
-  static constexpr int NT = EX * EZ;                  // one thread per (x, z) column
+  static constexpr int EQ = EZ / 4;                   // z-quads per box row
+  static constexpr int SEG = SEG_;                    // y levels per thread
+  static constexpr int NSEG = (EY + SEG - 1) / SEG;
+  static constexpr int NT = NSEG * EX * EQ;           // one thread per (y segment, x, z-quad)
   static constexpr int THREADS = (NT + 31) / 32 * 32;
   static constexpr int XS0 = EY * EZ;
   static constexpr int XS = XS0 + ((EZ % 32) - (XS0 % 32) + 64) % 32;  // x stride = EZ (mod 32)
   static constexpr int BUF = EX * XS;                 // floats per shared buffer
-  static constexpr int SMEM = 2 * BUF * (int)sizeof(float);
-  static_assert(THREADS <= 1024, "too many columns for one CTA");
-  static_assert(EY <= 64, "the fluid mask holds 64 levels");
+  // two pressure buffers (ping-pong) and the right-hand side
+  static constexpr int SMEM = 3 * BUF * (int)sizeof(float);
+  static_assert(K % 4 == 0 && TZ % 4 == 0, "z-quads stay aligned to the grid");
+  static_assert(THREADS <= 1024, "too many threads for one CTA");
   static_assert(TX % kBrick == 0 && TY % kBrick == 0 && TZ % kBrick == 0, "tiles are whole bricks");
-  static_assert(XS % 32 == EZ % 32, "padding");
+  static_assert(XS % 32 == EZ % 32 && XS % 4 == 0, "padding");
+  static_assert(4 * SEG <= 64, "the fluid mask holds 16 levels of quads");
 };
 
 // A tile's box: origin (ex, ey, ez) and extent n* (clipped to the domain),
@@ -119,9 +128,16 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned int* p) {
   return v;
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Bounded grid barrier on a counter that only grows (arrival e waits for
-// e * gridDim.x arrivals); on timeout it sets *fail and returns false, and
-// after any failure every barrier returns false at once.
+// e * gridDim.x arrivals).  Gives up after spin_limit polls or one second,
+// whichever comes first: it then sets *fail and returns false, and after any
+// failure every barrier returns false at once.
 __device__ __forceinline__ bool res_barrier(unsigned int* bar, unsigned target, int* fail, unsigned spin_limit) {
   __shared__ int s_ok;
   __syncthreads();
@@ -133,13 +149,14 @@ __device__ __forceinline__ bool res_barrier(unsigned int* bar, unsigned target, 
       __threadfence();
       atomicAdd(bar, 1u);
       unsigned spins = 0;
+      const unsigned long long t0 = global_ns();
       while (ld_acquire_u32(bar) < target) {
-        if (++spins > spin_limit || *reinterpret_cast<volatile int*>(fail)) {
+        if (++spins > spin_limit || *reinterpret_cast<volatile int*>(fail) ||
+            ((spins & 255u) == 0u && global_ns() - t0 > 1000000000ull)) {
           atomicExch(fail, 1);
           ok = 0;
           break;
         }
-        __nanosleep(32);
       }
       __threadfence();
     }
@@ -163,15 +180,78 @@ __device__ __forceinline__ double cta_sum(double v, double* s_red) {
   return t;  // valid in thread 0
 }
 
-template <int TX, int TY, int TZ, int K>
-__global__ void __launch_bounds__(Res<TX, TY, TZ, K>::THREADS, 1)
+// The quotients of a quad whose sums leave the fast path: IEEE divides, out
+// of line so the common path carries no predicated copy of them.
+__device__ __noinline__ float4 div6_quad_slow(float4 s, unsigned f) {
+  return make_float4((f & 1u) ? __fdiv_rn(s.x, 6.f) : 0.f, (f & 2u) ? __fdiv_rn(s.y, 6.f) : 0.f,
+                     (f & 4u) ? __fdiv_rn(s.z, 6.f) : 0.f, (f & 8u) ? __fdiv_rn(s.w, 6.f) : 0.f);
+}
+
+// The rhs of a non-fluid cell in the resident solve's shared copy: a NaN
+// payload no arithmetic produces (the GPU's NaN results are the canonical
+// 0x7fffffff, and the rhs comes from the divergence stage's arithmetic).
+constexpr unsigned kNotFluidBits = 0x7fc0a11au;
+#define kNotFluid __uint_as_float(kNotFluidBits)
+__device__ __forceinline__ unsigned fluid_bits(const float4& b) {
+  return (__float_as_uint(b.x) != kNotFluidBits ? 1u : 0u) | (__float_as_uint(b.y) != kNotFluidBits ? 2u : 0u) |
+         (__float_as_uint(b.z) != kNotFluidBits ? 4u : 0u) | (__float_as_uint(b.w) != kNotFluidBits ? 8u : 0u);
+}
+
+// One Jacobi update of a z-quad: p' = (x+1, x-1, y+1, y-1, z+1, z-1 summed in
+// that order, + rhs) / 6 on fluid cells (bits 0-3 of f), 0 elsewhere.
+__device__ __forceinline__ float4 quad_update(const float4& xp, const float4& xm, const float4& yp, const float4& ym,
+                                              const float4& pc, float zl, float zh, const float4& b, unsigned f) {
+  float4 s;
+  s.x = xp.x + xm.x; s.x += yp.x; s.x += ym.x; s.x += pc.y; s.x += zl; s.x += b.x;
+  s.y = xp.y + xm.y; s.y += yp.y; s.y += ym.y; s.y += pc.z; s.y += pc.x; s.y += b.y;
+  s.z = xp.z + xm.z; s.z += yp.z; s.z += ym.z; s.z += pc.w; s.z += pc.y; s.z += b.z;
+  s.w = xp.w + xm.w; s.w += yp.w; s.w += ym.w; s.w += zh; s.w += pc.z; s.w += b.w;
+  // one warp-uniform test: the rare quads leaving the fast path take the IEEE divides
+  const bool slow = ((f & 1u) && !div6_fast_ok(s.x)) || ((f & 2u) && !div6_fast_ok(s.y)) ||
+                    ((f & 4u) && !div6_fast_ok(s.z)) || ((f & 8u) && !div6_fast_ok(s.w));
+  if (__any_sync(__activemask(), slow)) {
+    if (slow) return div6_quad_slow(s, f);
+  }
+  return make_float4((f & 1u) ? div6_fast(s.x) : 0.f, (f & 2u) ? div6_fast(s.y) : 0.f,
+                     (f & 4u) ? div6_fast(s.z) : 0.f, (f & 8u) ? div6_fast(s.w) : 0.f);
+}
+
+// FP64 ||b - A p||^2 of the fluid cells (bits 0-3 of f) of a z-quad, in cell
+// order, each as b + (x+1 + x-1 + y+1 + y-1 + z+1 + z-1) - 6 p.
+__device__ __forceinline__ double quad_residual(const float4& xp, const float4& xm, const float4& yp,
+                                                const float4& ym, const float4& pc, float zl, float zh,
+                                                const float4& b, unsigned f) {
+  const float self[4] = {pc.x, pc.y, pc.z, pc.w};
+  const float zp[4] = {pc.y, pc.z, pc.w, zh};
+  const float zm[4] = {zl, pc.x, pc.y, pc.z};
+  const float vxp[4] = {xp.x, xp.y, xp.z, xp.w}, vxm[4] = {xm.x, xm.y, xm.z, xm.w};
+  const float vyp[4] = {yp.x, yp.y, yp.z, yp.w}, vym[4] = {ym.x, ym.y, ym.z, ym.w};
+  const float vb[4] = {b.x, b.y, b.z, b.w};
+  double acc = 0.0;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    if (!((f >> c) & 1u)) continue;
+    double s = (double)vxp[c];
+    s += (double)vxm[c];
+    s += (double)vyp[c];
+    s += (double)vym[c];
+    s += (double)zp[c];
+    s += (double)zm[c];
+    const double r = (double)vb[c] + s - 6.0 * (double)self[c];
+    acc += r * r;
+  }
+  return acc;
+}
+
+template <int TX, int TY, int TZ, int K, int SEG_>
+__global__ void __launch_bounds__(Res<TX, TY, TZ, K, SEG_>::THREADS, 1)
     k_resident_solve(Dims d, float* __restrict__ pa, float* __restrict__ pb, const float* __restrict__ rhs,
                      const int8_t* __restrict__ type, const int* __restrict__ tiles, const int* __restrict__ n_tiles,
                      unsigned int* __restrict__ bar, double* __restrict__ part, SolveState* __restrict__ ss,
                      int fixed_sweeps, int check, int max_iters, double tol, BarrierTest bt) {
-  using R = Res<TX, TY, TZ, K>;
-  constexpr int EY = R::EY, EZ = R::EZ, XS = R::XS;
-  extern __shared__ float smem[];  // [2][EX][XS]: buffer, x, y * EZ + z
+  using R = Res<TX, TY, TZ, K, SEG_>;
+  constexpr int SEG = R::SEG, EQ = R::EQ, XS4 = R::XS / 4;
+  extern __shared__ float4 smem4[];  // [3][EX][XS / 4]: p, p, rhs; x; (y * EZ + z) / 4
   __shared__ double s_red[32];
   __shared__ double s_r2;
 
@@ -185,128 +265,129 @@ __global__ void __launch_bounds__(Res<TX, TY, TZ, K>::THREADS, 1)
   const bool resident = n <= G;
   const int tid = threadIdx.x;
   const bool thr = tid < R::NT;
-  const int cx = tid / EZ, cz = tid % EZ;  // this thread's column in the box
-  const int it0 = ss->iterations;          // sweeps a warm start already did
+  // this thread: z-quad q of box row cx, levels [y0, y0 + SEG) of the box
+  const int q = tid % EQ, cx = (tid / EQ) % R::EX, y0 = (tid / (EQ * R::EX)) * SEG;
+  const int it0 = ss->iterations;  // sweeps a warm start already did
 
-  float p[EY], b[EY];
-  unsigned long long fl = 0ull;  // bit ly: cell (cx, ly, cz) is fluid
-#pragma unroll
-  for (int ly = 0; ly < EY; ++ly) p[ly] = b[ly] = 0.f;
+  unsigned long long fl = 0ull;  // bit 4(ly - y0) + c: cell c of the quad at level ly is fluid
+  float4* RB = smem4 + 2 * (R::BUF / 4);  // the rhs of the box
   float* g[2] = {pa, pb};
   int cur = 0;  // global buffer of the current iterate
   int par = 0;  // shared buffer of the current iterate
+  const int col_i = cx * XS4 + q;  // shared index of level 0 of this thread's quad column
 
-  // This thread's column of box t from global buffer src into p (every level
-  // when `full`, with rhs and fluid mask; else the levels outside the tile's
-  // own cells), then the whole column into shared buffer par.
+  // This thread's quads of box t from global buffer src into shared buffer
+  // par (all of them, with rhs and fluid bits, when `full`; else those
+  // outside the tile's own cells, whose current values are already there).
   auto load = [&](const Box& t, const float* __restrict__ src, bool full) {
-    const bool col = thr && cx < t.nx && cz < t.nz;
-    const bool own = col && cx >= t.cx0 && cx < t.cx1 && cz >= t.cz0 && cz < t.cz1;
+    const bool col = thr && cx < t.nx && 4 * q < t.nz;
+    const bool ownq = col && cx >= t.cx0 && cx < t.cx1 && 4 * q >= t.cz0 && 4 * q < t.cz1;
     if (full) fl = 0ull;
     if (col) {
-      const int base = ((t.ex + cx) * d.sy + t.ey) * d.sz + t.ez + cz;
+      const int base = ((t.ex + cx) * d.sy + t.ey + y0) * d.sz + t.ez + 4 * q;
+      float4* S = smem4 + par * (R::BUF / 4) + col_i;
 #pragma unroll
-      for (int ly = 0; ly < EY; ++ly) {
+      for (int j = 0; j < SEG; ++j) {
+        const int ly = y0 + j;
         if (ly < t.ny) {
-          const int c = base + ly * d.sz;
-          if (full || !own || ly < t.cy0 || ly >= t.cy1) p[ly] = __ldcg(src + c);
+          const int c = base + j * d.sz;
+          if (full || !ownq || ly < t.cy0 || ly >= t.cy1) S[ly * EQ] = __ldcg(reinterpret_cast<const float4*>(src + c));
           if (full) {
-            b[ly] = __ldg(rhs + c);
-            if (type[c] == kFluid) fl |= 1ull << ly;
+            // non-fluid cells carry a NaN sentinel instead of their rhs (which
+            // they never use): the sweep reads the fluid mark with the rhs
+            float4 rb = __ldg(reinterpret_cast<const float4*>(rhs + c));
+            const char4 ty = *reinterpret_cast<const char4*>(type + c);
+            if (ty.x != kFluid) rb.x = kNotFluid;
+            if (ty.y != kFluid) rb.y = kNotFluid;
+            if (ty.z != kFluid) rb.z = kNotFluid;
+            if (ty.w != kFluid) rb.w = kNotFluid;
+            RB[col_i + ly * EQ] = rb;
+            fl |= (unsigned long long)((ty.x == kFluid ? 1u : 0u) | (ty.y == kFluid ? 2u : 0u) |
+                                       (ty.z == kFluid ? 4u : 0u) | (ty.w == kFluid ? 8u : 0u))
+                  << (4 * j);
           }
         }
       }
-      float* S = smem + par * R::BUF + cx * XS + cz;
-#pragma unroll
-      for (int ly = 0; ly < EY; ++ly)
-        if (ly < t.ny) S[ly * EZ] = p[ly];
     }
     __syncthreads();
   };
 
-  // Sweep s of a block (1-based) on box t: shared buffer par -> par ^ 1.
+  // Sweep s (1-based) of a block on box t: shared buffer par -> par ^ 1.  The
+  // sweep's region (every cell at least s cells inside each cut face) is cut
+  // into rows of z-quads; the CTA's lanes take consecutive quads of
+  // consecutive rows, so every lane has work and a warp's loads of a level
+  // are contiguous.  A wall neighbour is the cell itself (offset 0).
   auto sweep = [&](const Box& t, int s) {
     const int xlo = (t.cut & 1) ? s : 0, xhi = t.nx - ((t.cut & 2) ? s : 0);
     const int ylo = (t.cut & 4) ? s : 0, yhi = t.ny - ((t.cut & 8) ? s : 0);
     const int zlo = (t.cut & 16) ? s : 0, zhi = t.nz - ((t.cut & 32) ? s : 0);
-    const bool act = thr && cx >= xlo && cx < xhi && cz >= zlo && cz < zhi;
-    if (act) {
-      const int gx = t.ex + cx, gz = t.ez + cz;
-      const int oxm = gx == 0 ? 0 : -XS, oxp = gx == d.sx - 1 ? 0 : XS;
-      const int ozm = gz == 0 ? 0 : -1, ozp = gz == d.sz - 1 ? 0 : 1;
-      const float* S = smem + par * R::BUF + cx * XS + cz;
-      float* D = smem + (par ^ 1) * R::BUF + cx * XS + cz;
-      const bool ywall_lo = t.ey == 0, ywall_hi = t.ey + t.ny == d.sy;
-      float last = 0.f;  // level ly - 1 before this sweep
-#pragma unroll
-      for (int ly = 0; ly < EY; ++ly) {
-        const float old = p[ly];
-        if (ly >= ylo && ly < yhi) {
-          const int i = ly * EZ;
-          const float xm = S[i + oxm], xp = S[i + oxp], zm = S[i + ozm], zp = S[i + ozp];
-          const float ym = (ly == 0 && ywall_lo) ? old : last;
-          const float yp = (ly + 1 < EY && !(ly == t.ny - 1 && ywall_hi)) ? p[ly + 1 < EY ? ly + 1 : ly] : old;
-          float sum = xp + xm;
-          sum += yp;
-          sum += ym;
-          sum += zp;
-          sum += zm;
-          sum += b[ly];
-          const float nv = ((fl >> ly) & 1ull) ? div6(sum) : 0.f;
-          p[ly] = nv;
-          D[i] = nv;
-        }
-        last = old;
-        // the levels are independent; without this fence the compiler hoists
-        // every level's shared loads at once and runs out of registers
-        if ((ly & 7) == 7) asm volatile("" ::: "memory");
-      }
+    // quads holding a cell of [zlo, zhi); their other cells are invalid and never read by valid ones
+    const int qlo = zlo / 4, qhi = (zhi + 3) / 4;
+    const int nq = qhi - qlo, ny = yhi - ylo;
+    const int total = (xhi - xlo) * ny * nq;
+    const float inv_nq = 1.f / (float)nq, inv_ny = 1.f / (float)ny;
+    const bool ywall_lo = t.ey == 0, ywall_hi = t.ey + t.ny == d.sy;
+    const float4* S = smem4 + par * (R::BUF / 4);
+    float4* D = smem4 + (par ^ 1) * (R::BUF / 4);
+    for (int it = tid; it < total; it += R::THREADS) {
+      // it = (xr * ny + yr) * nq + qr; small integers, so the float quotients are exact
+      const int rq = __float2int_rz(((float)it + 0.5f) * inv_nq);
+      const int qr = it - rq * nq;
+      const int xr = __float2int_rz(((float)rq + 0.5f) * inv_ny);
+      const int yr = rq - xr * ny;
+      const int x = xlo + xr, ly = ylo + yr, qq = qlo + qr;
+      const int i = x * XS4 + ly * EQ + qq;
+      const int gx = t.ex + x, gz = t.ez + 4 * qq;
+      const float4 pc = S[i];
+      const float4 xm = S[i + (gx == 0 ? 0 : -XS4)];
+      const float4 xp = S[i + (gx == d.sx - 1 ? 0 : XS4)];
+      const float4 ym = (ly == 0 && ywall_lo) ? pc : S[i - (ly > 0 ? EQ : 0)];
+      const float4 yp = (ly == t.ny - 1 && ywall_hi) ? pc : S[i + EQ];
+      const float* Sf = reinterpret_cast<const float*>(S + i);
+      const float zl = Sf[(gz == 0 || qq == 0) ? 0 : -1];
+      const float zh = Sf[(gz + 4 == d.sz || qq == EQ - 1) ? 3 : 4];
+      const float4 b = RB[i];
+      D[i] = quad_update(xp, xm, yp, ym, pc, zl, zh, b, fluid_bits(b));
     }
     __syncthreads();
     par ^= 1;
   };
 
   // ||b - A p||^2 over this thread's own fluid cells of box t (shared buffer
-  // par and p current), FP64, in y order; summed over the CTA.
+  // par current), FP64, in level order; summed over the CTA in a fixed order.
   auto residual = [&](const Box& t) -> double {
     double acc = 0.0;
-    const bool own = thr && cx >= t.cx0 && cx < t.cx1 && cz >= t.cz0 && cz < t.cz1;
-    if (own) {
-      const int gx = t.ex + cx, gz = t.ez + cz;
-      const int oxm = gx == 0 ? 0 : -XS, oxp = gx == d.sx - 1 ? 0 : XS;
-      const int ozm = gz == 0 ? 0 : -1, ozp = gz == d.sz - 1 ? 0 : 1;
-      const float* S = smem + par * R::BUF + cx * XS + cz;
-#pragma unroll
-      for (int ly = 0; ly < EY; ++ly) {
-        if (ly >= t.cy0 && ly < t.cy1 && ((fl >> ly) & 1ull)) {
-          const int gy = t.ey + ly;
-          const int i = ly * EZ;
-          const float self = p[ly];
-          const float ym = (gy == 0 || ly == 0) ? self : p[ly > 0 ? ly - 1 : 0];
-          const float yp = (gy == d.sy - 1 || ly + 1 >= EY) ? self : p[ly + 1 < EY ? ly + 1 : ly];
-          double s = (double)S[i + oxp];
-          s += (double)S[i + oxm];
-          s += (double)yp;
-          s += (double)ym;
-          s += (double)S[i + ozp];
-          s += (double)S[i + ozm];
-          const double r = (double)b[ly] + s - 6.0 * (double)self;
-          acc += r * r;
-        }
-        if ((ly & 7) == 7) asm volatile("" ::: "memory");
+    const bool ownq = thr && cx >= t.cx0 && cx < t.cx1 && 4 * q >= t.cz0 && 4 * q < t.cz1;
+    const int lo = max(t.cy0, y0), hi = min(t.cy1, y0 + SEG);
+    if (ownq && lo < hi) {
+      const int gx = t.ex + cx, gz = t.ez + 4 * q;
+      const int oxm = gx == 0 ? 0 : -XS4, oxp = gx == d.sx - 1 ? 0 : XS4;
+      const int ozl = (gz == 0 || q == 0) ? 0 : -1, ozh = (gz + 4 == d.sz || q == EQ - 1) ? 3 : 4;
+      const float4* S = smem4 + par * (R::BUF / 4) + col_i;
+      const float4* Rb = RB + col_i;
+      for (int ly = lo; ly < hi; ++ly) {
+        const unsigned f = (unsigned)(fl >> (4 * (ly - y0))) & 15u;
+        if (!f) continue;
+        const int i = ly * EQ, gy = t.ey + ly;
+        const float4 pc = S[i];
+        const float4 ym = gy == 0 ? pc : S[i - EQ];
+        const float4 yp = gy == d.sy - 1 ? pc : S[i + EQ];
+        const float zl = reinterpret_cast<const float*>(S + i)[ozl];
+        const float zh = reinterpret_cast<const float*>(S + i)[ozh];
+        acc += quad_residual(S[i + oxp], S[i + oxm], yp, ym, pc, zl, zh, Rb[i], f);
       }
     }
     return cta_sum<R::THREADS>(acc, s_red);
   };
 
-  // This thread's own cells of box t from p into dst.
+  // This thread's own cells of box t from shared buffer par into dst.
   auto store = [&](const Box& t, float* __restrict__ dst) {
-    const bool own = thr && cx >= t.cx0 && cx < t.cx1 && cz >= t.cz0 && cz < t.cz1;
-    if (own) {
-      const int base = ((t.ex + cx) * d.sy + t.ey) * d.sz + t.ez + cz;
-#pragma unroll
-      for (int ly = 0; ly < EY; ++ly)
-        if (ly >= t.cy0 && ly < t.cy1) dst[base + ly * d.sz] = p[ly];
+    const bool ownq = thr && cx >= t.cx0 && cx < t.cx1 && 4 * q >= t.cz0 && 4 * q < t.cz1;
+    const int lo = max(t.cy0, y0), hi = min(t.cy1, y0 + SEG);
+    if (ownq) {
+      const float4* S = smem4 + par * (R::BUF / 4) + col_i;
+      const int base = ((t.ex + cx) * d.sy + t.ey) * d.sz + t.ez + 4 * q;
+      for (int ly = lo; ly < hi; ++ly) *reinterpret_cast<float4*>(dst + base + ly * d.sz) = S[ly * EQ];
     }
   };
 
@@ -379,10 +460,15 @@ __global__ void __launch_bounds__(Res<TX, TY, TZ, K>::THREADS, 1)
     } else {
       for (int j = cta; j < n; j += G) {
         const Box t = box_of<TX, TY, TZ, K>(d, tiles[j]);
-        const bool own = thr && cx >= t.cx0 && cx < t.cx1 && cz >= t.cz0 && cz < t.cz1;
-        if (own) {
-          const int base = ((t.ex + cx) * d.sy + t.ey) * d.sz + t.ez + cz;
-          for (int ly = t.cy0; ly < t.cy1; ++ly) pa[base + ly * d.sz] = __ldcg(pb + base + ly * d.sz);
+        const bool ownq = thr && cx >= t.cx0 && cx < t.cx1 && 4 * q >= t.cz0 && 4 * q < t.cz1;
+        if (ownq) {
+          const int base = ((t.ex + cx) * d.sy + t.ey + y0) * d.sz + t.ez + 4 * q;
+          for (int jj = 0; jj < SEG; ++jj) {
+            const int ly = y0 + jj;
+            if (ly >= t.cy0 && ly < t.cy1)
+              *reinterpret_cast<float4*>(pa + base + jj * d.sz) =
+                  __ldcg(reinterpret_cast<const float4*>(pb + base + jj * d.sz));
+          }
         }
       }
     }
@@ -453,15 +539,17 @@ struct ShapeInfo {
   int tx, ty, tz;
 };
 // Tile shapes of the resident plan (plan.xc indexes this table).
-constexpr ShapeInfo kShapes[] = {{8, 40, 16}, {8, 32, 16}, {16, 16, 16}, {8, 24, 16}, {8, 16, 16}, {16, 24, 16}};
+// (6, 7: shape 0 with 8- and 5-level y segments: 576 and 960 threads)
+constexpr ShapeInfo kShapes[] = {{8, 40, 16}, {8, 32, 16}, {16, 16, 16}, {8, 24, 16}, {8, 16, 16},
+                                 {16, 24, 16}, {8, 40, 16}, {8, 40, 16}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
-template <int TX, int TY, int TZ, int K>
+template <int TX, int TY, int TZ, int K, int SEG>
 cudaError_t launch_res(cudaStream_t st, const Dims& d, int ctas, float* pa, float* pb, const float* rhs,
                        const int8_t* type, const int* tiles, const int* n_tiles, unsigned int* bar, double* part,
                        SolveState* ss, int fixed_sweeps, int check, int max_iters, double tol, BarrierTest bt) {
-  using R = Res<TX, TY, TZ, K>;
-  auto fn = &k_resident_solve<TX, TY, TZ, K>;
+  using R = Res<TX, TY, TZ, K, SEG>;
+  auto fn = &k_resident_solve<TX, TY, TZ, K, SEG>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, R::SMEM);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t lc = {};
@@ -478,10 +566,10 @@ cudaError_t launch_res(cudaStream_t st, const Dims& d, int ctas, float* pa, floa
                             max_iters, tol, bt);
 }
 
-template <int TX, int TY, int TZ, int K>
+template <int TX, int TY, int TZ, int K, int SEG>
 int occupancy_of(int device) {
-  using R = Res<TX, TY, TZ, K>;
-  auto fn = &k_resident_solve<TX, TY, TZ, K>;
+  using R = Res<TX, TY, TZ, K, SEG>;
+  auto fn = &k_resident_solve<TX, TY, TZ, K, SEG>;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, R::SMEM) != cudaSuccess) return 0;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, R::THREADS, R::SMEM) != cudaSuccess) return 0;
@@ -490,26 +578,27 @@ int occupancy_of(int device) {
   return per_sm >= 1 ? sms : 0;  // one CTA per SM
 }
 
-// Dispatch over (shape, K): calls f.template operator()<TX, TY, TZ, K>().
+// Dispatch over (shape, K): calls f.template operator()<TX, TY, TZ, K, SEG>().
 template <typename F>
-auto dispatch(int shape, int k, const F& f) -> decltype(f.template operator()<8, 40, 16, 4>()) {
-#define AQ_RES_CASE(S, A, B, C)                                   \
-  if (shape == S && k == 4) return f.template operator()<A, B, C, 4>(); \
-  if (shape == S && k == 2) return f.template operator()<A, B, C, 2>();
-  AQ_RES_CASE(0, 8, 40, 16)
-  AQ_RES_CASE(1, 8, 32, 16)
-  AQ_RES_CASE(2, 16, 16, 16)
-  AQ_RES_CASE(3, 8, 24, 16)
-  AQ_RES_CASE(4, 8, 16, 16)
-  AQ_RES_CASE(5, 16, 24, 16)
+auto dispatch(int shape, int k, const F& f) -> decltype(f.template operator()<8, 40, 16, 4, 12>()) {
+#define AQ_RES_CASE(S, A, B, C, G) \
+  if (shape == S && k == 4) return f.template operator()<A, B, C, 4, G>();
+  AQ_RES_CASE(0, 8, 40, 16, 12)
+  AQ_RES_CASE(1, 8, 32, 16, 12)
+  AQ_RES_CASE(2, 16, 16, 16, 8)
+  AQ_RES_CASE(3, 8, 24, 16, 8)
+  AQ_RES_CASE(4, 8, 16, 16, 8)
+  AQ_RES_CASE(5, 16, 24, 16, 12)
+  AQ_RES_CASE(6, 8, 40, 16, 8)
+  AQ_RES_CASE(7, 8, 40, 16, 5)
 #undef AQ_RES_CASE
-  return decltype(f.template operator()<8, 40, 16, 4>())();
+  return decltype(f.template operator()<8, 40, 16, 4, 12>())();
 }
 
 struct OccupancyOf {
   int device;
-  template <int A, int B, int C, int D>
-  int operator()() const { return occupancy_of<A, B, C, D>(device); }
+  template <int A, int B, int C, int D, int E>
+  int operator()() const { return occupancy_of<A, B, C, D, E>(device); }
 };
 
 struct LaunchRes {
@@ -527,16 +616,16 @@ struct LaunchRes {
   int fixed_sweeps, check, max_iters;
   double tol;
   BarrierTest bt;
-  template <int A, int B, int C, int D>
+  template <int A, int B, int C, int D, int E>
   cudaError_t operator()() const {
-    return launch_res<A, B, C, D>(st, d, ctas, pa, pb, rhs, type, tiles, n_tiles, bar, part, ss, fixed_sweeps, check,
+    return launch_res<A, B, C, D, E>(st, d, ctas, pa, pb, rhs, type, tiles, n_tiles, bar, part, ss, fixed_sweeps, check,
                                   max_iters, tol, bt);
   }
 };
 
 }  // namespace
 
-bool resident_plan_ok(int shape, int k) { return shape >= 0 && shape < kNumShapes && (k == 2 || k == 4); }
+bool resident_plan_ok(int shape, int k) { return shape >= 0 && shape < kNumShapes && k == 4; }
 
 int resident_tile_capacity(const Dims& d) {
   int cap = 1;

@@ -59,6 +59,17 @@ def workload_config(size=128, pressure_init="zero"):
         solve_mode=_abi.SOLVE_RESIDUAL, rel_residual=1e-4, max_iterations=2000, check_interval=40)
 
 
+def config1_config():
+    """50^3 ball drop, pool y < 0.2 plus a sphere r 0.15 at
+    (0.5, 0.65, 0.5), 8 particles per cell, dt 0.01, FLIP 0.95, 100 Jacobi
+    sweeps per step with the pressure carried as the reference does."""
+    from aquarius_b200 import _abi
+    vols = [dict(shape="box", min=(0, 0, 0), max=(1, 0.2, 1), phase=0),
+            dict(shape="sphere", center=(0.5, 0.65, 0.5), radius=0.15, phase=0)]
+    return _abi.make_config((50, 50, 50), vols, timestep=0.01, flip_coeff=0.95, particle_jitter=0.05,
+                            pressure_init=_abi.PRESSURE_CARRY, solve_mode=_abi.SOLVE_FIXED, pressure_iterations=100)
+
+
 def config_desc(size, pressure_init):
     return {"workload": f"ball drop {size}^3 x 8ppc (pool y<0.3 + sphere r=0.12), dt=0.005, "
                         f"Jacobi to rel-res 1e-4 cap 2000, {pressure_init}-init pressure",
@@ -134,13 +145,21 @@ def weak_scaling_value(steps_per_rank: int, world: int, max_ms: float) -> float:
 
 
 def jacobi_kernel_name(f) -> str:
-    levels, rows, xplanes = f.jacobi_plan()
+    return jacobi_kernel_name_of(f.jacobi_plan())
+
+
+def jacobi_kernel_name_of(plan) -> str:
+    levels, rows, xplanes = plan
     if rows == 1:
         return "k_persist_solve (whole solve in one cooperative launch)"
     if rows == 0:
         return f"k_jacobi_flat<{xplanes}> (1 sweep/launch, float4 z-quads)"
     if rows == 3:
         return "k_jacobi_list (1 sweep/launch over the listed active warp rows, one resident wave)"
+    if rows == 4:
+        shapes = ["8x40x16", "8x32x16", "16x16x16", "8x24x16", "8x16x16", "16x24x16", "8x40x16 (576 threads)"]
+        return (f"k_resident_solve<tiles {shapes[xplanes]}, halo {levels}> (whole solve in one cooperative launch, "
+                f"tiles resident in shared memory, halos exchanged every {levels} sweeps)")
     if rows == 2:
         return f"k_jacobi_cube<{levels} sweeps/launch, {xplanes}x{xplanes}x{32 - 2 * levels} tiles> (shared-memory cubes)"
     return f"k_jacobi<{levels} sweeps/launch, {rows} rows, {xplanes} x-planes> (temporally blocked)"
@@ -153,6 +172,8 @@ def measured_traffic(f):
         d = json.loads((ROOT / "profiles" / "roofline_traffic.json").read_text())
         levels, rows, xplanes = f.jacobi_plan()
         key = {(0, 1): "k_jacobi_flat", (3, 1): "k_jacobi_list"}.get((rows, xplanes))
+        if rows == 4:
+            key = f"k_resident_solve/{levels}/{xplanes}"
         if key in d:
             return d[key]["bytes_per_launch"]
     except Exception:
@@ -245,7 +266,7 @@ def run_reference(args, rank: int, world: int):
     import oracle_binding
     cfg = workload_config(args.size, args.pressure_init)
     o = oracle_binding.Oracle(cfg)
-    o.step(min(args.warmup, 1))
+    o.step(min(args.warmup, 10))
     budget_s = 150.0
     done, t0 = 0, time.perf_counter()
     while done < args.steps:
@@ -256,7 +277,7 @@ def run_reference(args, rank: int, world: int):
     dt = time.perf_counter() - t0
     v = done / dt
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": done,
-            "warmup": min(args.warmup, 1), "ms_per_step": 1000 * dt / done, "higher_is_better": True,
+            "warmup": min(args.warmup, 10), "ms_per_step": 1000 * dt / done, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_desc(args.size, args.pressure_init),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": oracle_binding.oracle_threads(), "kind": "port",
@@ -385,6 +406,8 @@ def run_ours(args, rank: int, world: int, dist):
     plain_rel = [st1["rel_residual"], pstats["rel_residual"]]
     plan = f.jacobi_plan()
     f.close()
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_comparator(args, dev, plan)
     if not args.no_learned:
         line["learned"] = learned_arm(args, dev, stream, max(plain_rel), ms_max / args.steps, dist, plan)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -471,6 +494,80 @@ def render_timing(f, size: int, reps: int = 10, width: int = 1728, height: int =
     return out
 
 
+def reference_gpu_step_ms(size: int, steps: int = 5, workload: str = "ball128") -> dict:
+    """Milliseconds per simulationStep of the reference's own kernels on the
+    fixed-sweep comparator workload.  Runs in a process of its own: the
+    reference's init sets the device's printf FIFO size
+    (Fluid/Fluid_3D_FLIP.cu:489), which CUDA refuses once other kernels ran
+    in the context."""
+    from aquarius_b200 import _abi
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_binding
+    if workload == "ball50":
+        cfg = config1_config()
+    else:
+        cfg = workload_config(size, "carry")
+        cfg.solve_mode = _abi.SOLVE_FIXED
+        cfg.pressure_iterations = 2000
+    ref = oracle_binding.RefFluid(cfg)
+    ref.step(2)
+    ms = min(ref.time_steps(steps) for _ in range(3)) / steps
+    ref.close()
+    return {"reference_ms_per_step": ms}
+
+
+def reference_gpu_comparator(args, dev, plan, steps: int = 5) -> dict:
+    """The reference's own FLIP kernels (Fluid_3D_FLIP::Fluid compiled headless
+    from its sources into oracle/_ref/libaqref.so, Fluid/Fluid_3D_FLIP.cu:316-352)
+    on this workload with the reference's fixed-iteration Jacobi (2000
+    sweeps; pressure carried across steps as the reference does,
+    Fluid/Fluid_3D_common.cu:48-55), timed with CUDA events on the legacy
+    default stream it launches on (its own device synchronisations inside a
+    step included), beside this library on the same scene, the same 2000
+    sweeps (AQ_SOLVE_FIXED, carried pressure) and the tuned Jacobi plan, timed
+    on the fluid's stream.  Not the product path: the comparator the plain
+    step is measured against."""
+    import torch
+
+    import aquarius_b200 as aq
+    from aquarius_b200 import _abi
+    if not (ROOT / "oracle" / "_ref" / "libaqref.so").exists():
+        return {"unavailable": "the headless reference build (oracle/_ref/libaqref.so) is not present"}
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)))
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--reference-gpu-only", "--size", str(args.size)],
+                       capture_output=True, text=True, env=env, timeout=600)
+    try:
+        ref = json.loads(r.stdout.strip().splitlines()[-1])
+    except Exception:
+        return {"unavailable": f"reference run failed: {(r.stderr or r.stdout)[-300:]}"}
+    cfg = workload_config(args.size, "carry")
+    cfg.solve_mode = _abi.SOLVE_FIXED
+    cfg.pressure_iterations = 2000
+    cfg.device = dev
+    f = aq.Fluid(cfg)
+    if plan[1] != 1:
+        f.set_jacobi_plan(*plan)
+    f.step(3)
+    f.synchronize()
+    st = torch.cuda.ExternalStream(f.stream(), device=dev)
+    lib = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        f.step(steps)
+        e1.record(st)
+        e1.synchronize()
+        lib.append(e0.elapsed_time(e1) / steps)
+    sweeps = f.solve_stats()["iterations"]
+    f.close()
+    lib_ms = min(lib)
+    ref_ms = ref["reference_ms_per_step"]
+    return {"workload": f"{args.size}^3 ball drop, 2000 fixed Jacobi sweeps per step, carried pressure",
+            "reference_ms_per_step": ref_ms, "library_ms_per_step": lib_ms, "library_sweeps_per_step": sweeps,
+            "speedup": ref_ms / lib_ms, "library_jacobi_plan": list(plan),
+            "reference_build": "Fluid/*.cu compiled headless with the reference's flags (-use_fast_math) for sm_100a"}
+
+
 def learned_arm(args, dev, stream, plain_residual: float, plain_ms: float, dist, plan) -> dict:
     """The same workload with the learned warm start (AQ_PRESSURE_LEARNED) and
     the plain step's Jacobi plan: (a) to the same target 1e-4 (cap 2000), (b)
@@ -520,6 +617,96 @@ def learned_arm(args, dev, stream, plain_residual: float, plain_ms: float, dist,
         f.close()
     net.close()
     return out
+
+
+def run_config1(args, rank: int, world: int, dist):
+    """BASELINE config 1 (the reference's own scale: 50^3, 100 Jacobi sweeps):
+    steps/s of this library (graph), end to end through the host-buffer
+    C-ABI step, of the reference's own kernels on the same GPU (child
+    process, CUDA events) and of the CPU oracle.  50 is not a multiple of 4,
+    so the library runs its tiled sweep kernels here."""
+    import torch
+
+    import aquarius_b200 as aq
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    cfg = config1_config()
+    cfg.device = dev
+    f = aq.Fluid(cfg)
+    stream = torch.cuda.ExternalStream(f.stream(), device=dev)
+    f.step(args.warmup)
+    f.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    f.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = reduce_max(e0.elapsed_time(e1), dist, f"cuda:{dev}")
+    value = weak_scaling_value(args.steps, world, ms)
+    n = f.particleCount
+    pin_pos = torch.empty((3, n), dtype=torch.float32).pin_memory().numpy()
+    pin_vel = torch.empty((3, n), dtype=torch.float32).pin_memory().numpy()
+    f.step_host(0, None, None, pin_pos, pin_vel)
+    e0.record(stream)
+    for _ in range(args.steps):
+        f.step_host(1, pin_pos, pin_vel, pin_pos, pin_vel)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = reduce_max(e0.elapsed_time(e1), dist, f"cuda:{dev}")
+    hbm_peak, peak_kind = measured_hbm_peak()
+    jb = f.benchmark_pressure(400)
+    sweep_ms = jb["ms"] / 400
+    cells = jb["cells_per_sweep"]
+    achieved = JACOBI_BYTES_PER_CELL * cells / (sweep_ms / 1000.0) / 1e9
+    plan = f.jacobi_plan()
+    f.close()
+    line = {"metric": "FLIP steps/s at 50^3 x 8ppc, 100 Jacobi sweeps per step (BASELINE config 1)",
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "ball drop 50^3 x 8ppc (pool y<0.2 + sphere r=0.15), dt=0.01, 100 Jacobi "
+                                   "sweeps, carried pressure", "grid": [50, 50, 50], "particles_per_cell": 8,
+                       "l2": "working set < L2 (the reference's own scale); no flush"},
+            "e2e": {"value": weak_scaling_value(args.steps, world, e2e_ms), "unit": UNIT,
+                    "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n,
+                    "path": "aq_fluid_step_host (C ABI), pinned host particle state in and out every step"},
+            "roofline": {"bound": "hbm", "kernel": jacobi_kernel_name_of(plan), "achieved": achieved,
+                         "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "traffic": None, "sweep_us": sweep_ms * 1000.0,
+                         "algorithmic_bytes": f"{JACOBI_BYTES_PER_CELL} B per updated cell per sweep x {cells} cells"},
+            "clocks": clk, "particles": n}
+    if rank == 0 and world == 1:
+        env = dict(os.environ)
+        r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--reference-gpu-only", "--workload", "ball50"],
+                           capture_output=True, text=True, env=env, timeout=600)
+        try:
+            ref_ms = json.loads(r.stdout.strip().splitlines()[-1])["reference_ms_per_step"]
+            line["reference_gpu"] = {"reference_ms_per_step": ref_ms, "library_ms_per_step": ms / args.steps,
+                                     "speedup": ref_ms / (ms / args.steps)}
+        except Exception:
+            line["reference_gpu"] = {"unavailable": (r.stderr or r.stdout)[-300:]}
+        if not args.no_cpu_baseline:
+            sys.path.insert(0, str(ROOT / "tests"))
+            import oracle_binding
+            o = oracle_binding.Oracle(config1_config())
+            o.step(1)
+            t0 = time.perf_counter()
+            k = 0
+            while k < 20 and time.perf_counter() - t0 < 15.0:
+                o.step(1)
+                k += 1
+            dt = time.perf_counter() - t0
+            o.close()
+            line["cpu_baseline"] = {"value": k / dt, "unit": UNIT, "cores": oracle_binding.oracle_threads(),
+                                    "kind": "port", "sample": f"{k} steps of the same scene on the OpenMP oracle"}
+        print(json.dumps(line), flush=True)
 
 
 def run_batch(args, rank: int, world: int, dist):
@@ -813,7 +1000,8 @@ def run_multiphase(args, rank: int, world: int, dist):
 def run_profile_case(case: str):
     """Small, fixed cases for single-kernel ncu captures (no JSON line):
     jacobi: the 128^3 workload's system after 3 steps, 6 sweeps of the
-    default plan; batch-rows: 32 scenes of the batch set, 6 batched sweeps;
+    default plan; resident: the same system, 40 sweeps of the resident plan
+    (one cooperative launch, 8x40x16 tiles, 960 threads); batch-rows: 32 scenes of the batch set, 6 batched sweeps;
     conv: two U-Net inferences at 128^3 on seeded random inputs; mesh: two
     surface meshes of the 128^3 workload's initial particles; pbf / pcisph:
     one step of the solver at particle budget 3e6 (593k particles); render:
@@ -828,6 +1016,13 @@ def run_profile_case(case: str):
         f.step(3)
         f.synchronize()
         print(f.jacobi_plan(), f.benchmark_pressure(6))
+        f.close()
+    elif case == "resident":
+        f = aq.Fluid(workload_config(128, "zero"))
+        f.step(3)
+        f.synchronize()
+        f.set_jacobi_plan(4, 4, 7)
+        print(f.jacobi_plan(), f.benchmark_pressure(40))
         f.close()
     elif case == "batch-rows":
         from aquarius_b200.scenes import batch_configs
@@ -889,11 +1084,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default Jacobi plan")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
-    ap.add_argument("--profile-case", choices=["jacobi", "batch-rows", "conv", "mesh", "pbf", "pcisph", "render"],
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own kernels (the plain-step comparator)")
+    ap.add_argument("--reference-gpu-only", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--profile-case", choices=["jacobi", "resident", "batch-rows", "conv", "mesh", "pbf", "pcisph",
+                                               "render"],
                     default=None,
                     help="run one small fixed case for an ncu capture and exit")
-    ap.add_argument("--workload", default="ball128", choices=["ball128", "batch", "multiphase256", "pbf", "pcisph"],
-                    help="ball128: the 128^3 scene; batch: 256 independent scenes of uneven sizes; "
+    ap.add_argument("--workload", default="ball128",
+                    choices=["ball128", "ball50", "batch", "multiphase256", "pbf", "pcisph"],
+                    help="ball128: the 128^3 scene; ball50: BASELINE config 1 (50^3, 100 sweeps); "
+                         "batch: 256 independent scenes of uneven sizes; "
                          "multiphase256: two phases with diffusion at 256^3; pbf / pcisph: the "
                          "particle-only solvers")
     ap.add_argument("--particles", type=float, default=3e7, help="particle budget of the pbf / pcisph workloads")
@@ -905,6 +1106,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     if args.profile_case:
         run_profile_case(args.profile_case)
+        return
+    if args.reference_gpu_only:
+        print(json.dumps(reference_gpu_step_ms(args.size, steps=20 if args.workload == "ball50" else 5,
+                                               workload=args.workload)), flush=True)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)
@@ -925,6 +1130,8 @@ def main():
             run_multiphase(args, rank, world, dist)
         elif args.workload in ("pbf", "pcisph"):
             run_sph(args, rank, world, dist)
+        elif args.workload == "ball50":
+            run_config1(args, rank, world, dist)
         else:
             run_ours(args, rank, world, dist)
     finally:

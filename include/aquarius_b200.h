@@ -273,8 +273,8 @@ aq_status aq_selfcheck_division(int32_t device, uint64_t* mismatches);
  * x_planes 1; sz % 4 == 0).  rows = 4: the whole solve in one cooperative
  * launch of resident tiles: each CTA keeps a tile of the grid (x_planes
  * selects the shape: 0 8x40x16, 1 8x32x16, 2 16x16x16, 3 8x24x16, 4 8x16x16,
- * 5 16x24x16 cells) with a `levels`-cell halo (2 or 4) in shared memory for
- * the whole solve and exchanges halos every `levels` sweeps.  rows = 8, 16, 32:
+ * 5 16x24x16 cells, 6 8x40x16 with twice the threads) with a `levels`-cell halo (4) in shared memory for the
+ * whole solve and exchanges halos every `levels` sweeps (sz % 4 == 0).  rows = 8, 16, 32:
  * the temporally blocked kernel with `levels` sweeps (1, 2, 4, 8) per launch
  * over tiles of that many rows and x_planes planes.  Chosen per grid by the
  * tuner; invalid plans are rejected. */

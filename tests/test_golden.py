@@ -8,7 +8,8 @@ import json
 import numpy as np
 import pytest
 
-from golden_check import FLOAT_TOL, GOLDEN, INK_SCENES, judge, load, load_ink, replay, replay_ink, replay_special
+from golden_check import (FLOAT_TOL, GOLDEN, INK_SCENES, judge, load, load_ink, replay, replay_ink, replay_special,
+                          spreads)
 from oracle_binding import Oracle, oracle_tex_linear
 
 SCENES_STEPS = [("cfg1_16", 2), ("aniso", 1), ("multi_16", 1)]
@@ -29,7 +30,7 @@ def test_oracle_against_reference_fixtures(scene, steps):
         pytest.skip("fixture missing")
     directional = []
     res = replay(data, Oracle, steps, directional=directional)
-    assert judge(res) == []
+    assert judge(res, spreads().get(scene, {})) == []
     # exactness where the reference does not race
     for (s, k, f, kind, v) in res:
         if kind == "int_mismatch" and not (k == 7 and f == "has_velocity"):

@@ -2,7 +2,7 @@
 reference's own kernels (no reference build needed at test time)."""
 import pytest
 
-from golden_check import judge, load, replay, replay_special
+from golden_check import judge, load, replay, replay_special, spreads
 from lib_checker import LibChecker
 
 pytestmark = pytest.mark.gpu
@@ -15,7 +15,7 @@ def test_library_against_reference_fixtures(scene, steps):
         pytest.skip("fixture missing")
     directional = []
     res = replay(data, LibChecker, steps, directional=directional)
-    assert judge(res) == []
+    assert judge(res, spreads().get(scene, {})) == []
     for (s, k, f, kind, v) in res:
         if kind == "int_mismatch" and not (k == 7 and f == "has_velocity"):
             assert v == 0, (s, k, f)

@@ -71,12 +71,21 @@ def test_matches_reference_per_stage(checker, scene, steps):
 
 def test_library_step_tracks_reference_step():
     """Whole steps teacher-forced from the reference's state: the non-racing
-    fields match; pressure within the racy-Jacobi bound."""
+    fields match; pressure no farther from the reference than the two legal
+    schedules of its racing Jacobi are from each other on the same step (the
+    oracle's race-free reading and its serial launch-order schedule)."""
     cfg = SCENES["cfg1_24"]()
     ref = RefFluid(cfg)
     f = aq.Fluid(cfg)
+    race_free, serial = Oracle(cfg), Oracle(cfg)
+    serial.set_schedule(True)
     for step in range(4):
-        f.upload_state(ref.get_state())
+        st = ref.get_state()
+        f.upload_state(st)
+        for o in (race_free, serial):
+            o.set_state(st)
+            o.step(1)
+        env = rel_l2(serial.get_state(["pressure"])["pressure"], race_free.get_state(["pressure"])["pressure"])
         ref.step(1)
         f.step(1)
         a, b = f.download_state(), ref.get_state()
@@ -85,4 +94,4 @@ def test_library_step_tracks_reference_step():
         # particle within an ulp of a cell face may hash differently
         assert (a["cell_start"] != b["cell_start"]).mean() < 1e-3
         assert rel_l2(a["divergence"], b["divergence"]) <= 1e-5
-        assert rel_l2(a["pressure"], b["pressure"]) <= 3e-3
+        assert rel_l2(a["pressure"], b["pressure"]) <= max(1e-5, env), (step, env)
