@@ -79,6 +79,7 @@ def load_library() -> ct.CDLL:
         "aq_fluid_solve_stats": (ct.c_int, [P, ct.POINTER(_abi.SolveStats)]),
         "aq_fluid_test_barrier_timeout": (ct.c_int, [P, ct.c_int32, ct.c_uint32]),
         "aq_selfcheck_division": (ct.c_int, [ct.c_int32, ct.POINTER(ct.c_uint64)]),
+        "aq_p2g_set_variant": (ct.c_int, [ct.c_int32]),
         "aq_fluid_pcg_reference": (ct.c_int, [P, ct.c_double, ct.c_int32, P, ct.POINTER(ct.c_double),
                                               ct.POINTER(ct.c_int32), ct.POINTER(ct.c_double)]),
         "aq_fluid_profile_step": (ct.c_int, [P, ct.POINTER(ct.c_float)]),

@@ -93,6 +93,10 @@ cudaError_t launch_rank_gather(cudaStream_t st, bool multiphase, const int* key,
 // Stage (b): particle-to-grid gather onto the staggered faces, weight
 // normalisation, fluid marking, density/fractions and (forces=true) gravity
 // and the wall clamps of fixBoundary for nodes in [0,s)^3.
+// P2G kernel: 1 (default) stages each CTA's particles in shared memory, 0 is
+// one thread per node reading particles through L1.  Same sums, same order.
+void set_p2g_variant(int v);
+int p2g_variant();
 cudaError_t launch_p2g(cudaStream_t st, const Dims& d, const StepParams& sp, bool forces, Particles cur,
                        const int* off, int n, float* u0, float* v0, float* w0, float* un, float* vn,
                        float* wn, int8_t* type, float* density, float4* vf, float4* nvf);

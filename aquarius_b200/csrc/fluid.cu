@@ -1318,6 +1318,12 @@ aq_status aq_fluid::health() {
   return AQ_OK;
 }
 
+aq_status aq_p2g_set_variant(int32_t variant) {
+  if (variant != 0 && variant != 1) return fail(AQ_ERR_INVALID_ARGUMENT, "P2G variant must be 0 or 1");
+  set_p2g_variant(variant);
+  return AQ_OK;
+}
+
 aq_status aq_selfcheck_division(int32_t device, uint64_t* mismatches) {
   if (!mismatches) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
   AQ_CUDA(cudaSetDevice(device));

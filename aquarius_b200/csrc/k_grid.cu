@@ -10,7 +10,44 @@
 namespace aqb {
 namespace {
 
-__device__ __forceinline__ float hat1(float r) { return fmaxf(0.f, 1.f - fabsf(r)); }
+__device__ __forceinline__ float hat1(float r) { return fmaxf(0.f, __fsub_rn(1.f, fabsf(r))); }
+
+// One particle's contributions to node (fx, fy, fz) from the cell at offset
+// (DX, DY, DZ) (transferToCellAccumPhase, Fluid/Fluid_3D_FLIP.cu:29-64): hat
+// weights of the u, v, w faces in cell units, each sum rounded as written
+// (explicit intrinsics, so every P2G kernel produces the same bits).
+// dx, dy, dz are constants wherever this is inlined (unrolled loops).
+__device__ __forceinline__ void p2g_particle(int DX, int DY, int DZ, float qx, float qy, float qz, float vx, float vy,
+                                             float vz, float fx,
+                                             float fy, float fz, float fxh, float fyh, float fzh, float& su,
+                                             float& sv, float& sw, float& wu, float& wv, float& ww, float& bxyz) {
+  const float bx = hat1(__fsub_rn(qx, fxh)), by = hat1(__fsub_rn(qy, fyh)), bz = hat1(__fsub_rn(qz, fzh));
+  if (DX < 1) {  // a cell at dx = +1 cannot touch the u face (weight exactly 0)
+    const float w = __fmul_rn(__fmul_rn(hat1(__fsub_rn(qx, fx)), by), bz);
+    su = __fmaf_rn(w, vx, su);
+    wu = __fadd_rn(wu, w);
+  }
+  if (DY < 1) {
+    const float w = __fmul_rn(__fmul_rn(bx, hat1(__fsub_rn(qy, fy))), bz);
+    sv = __fmaf_rn(w, vy, sv);
+    wv = __fadd_rn(wv, w);
+  }
+  if (DZ < 1) {
+    const float w = __fmul_rn(__fmul_rn(bx, by), hat1(__fsub_rn(qz, fz)));
+    sw = __fmaf_rn(w, vz, sw);
+    ww = __fadd_rn(ww, w);
+  }
+  bxyz = __fmul_rn(__fmul_rn(bx, by), bz);
+}
+
+// The fractions' weighted sum of the node's own cell (transferVolumeFractionsToCell).
+__device__ __forceinline__ void p2g_fractions(float w, const float4& f, float4& fs, float& fw) {
+  fs.x = __fmaf_rn(w, f.x, fs.x);
+  fs.y = __fmaf_rn(w, f.y, fs.y);
+  fs.z = __fmaf_rn(w, f.z, fs.z);
+  fs.w = __fmaf_rn(w, f.w, fs.w);
+  fw = __fadd_rn(fw, w);
+}
 
 // P2G gather for node (x,y,z) in [0,s)^3.  The reference loops over the 27
 // neighbour cells by a flat index with only a [0,C) range check, so rows at
@@ -20,72 +57,26 @@ __device__ __forceinline__ float hat1(float r) { return fmaxf(0.f, 1.f - fabsf(r
 // u-face at x (weight exactly 0 there), likewise dy=+1 for v and dz=+1 for w.
 // Weights use positions in cell units, q = p/h; the reference evaluates
 // (p - face*h)/h with approximate division (-use_fast_math).
+// Accumulated P2G sums of one node.
+struct P2gAcc {
+  float su, sv, sw, wu, wv, ww;
+  float4 fs;
+  float fw;
+  int own, left, down, back;  // particles in the node's cell and its -x, -y, -z neighbours
+};
+
+// transferToCellDividePhase + transferVolumeFractionsToCell + applyGravity +
+// fixBoundary (low walls) for node (x, y, z) from its accumulated sums.
 template <bool FORCES, bool MULTI>
-__device__ __forceinline__ void p2g_body(const Dims& d, const StepParams& sp, const Particles& cur,
-                                         const int* __restrict__ off, float* __restrict__ u0, float* __restrict__ v0,
-                                         float* __restrict__ w0, float* __restrict__ un, float* __restrict__ vn,
-                                         float* __restrict__ wn, int8_t* __restrict__ type,
-                                         float* __restrict__ density, float4* __restrict__ vf,
-                                         float4* __restrict__ nvf, int bx, int by, int bz) {
-  const int z = bx * 32 + threadIdx.x;
-  const int y = by * 8 + threadIdx.y;
-  const int x = bz;
-  if (z >= d.sz || y >= d.sy) return;
-  const float fx = (float)x, fy = (float)y, fz = (float)z;
-  const float fxh = fx + 0.5f, fyh = fy + 0.5f, fzh = fz + 0.5f;
-  const float inv_h = d.inv_h;
-  float su = 0.f, sv = 0.f, sw = 0.f, wu = 0.f, wv = 0.f, ww = 0.f;
-  float4 fs = make_float4(0.f, 0.f, 0.f, 0.f);
-  float fw = 0.f;
-  int own = 0, left = 0, down = 0, back = 0;
-#pragma unroll
-  for (int dx = -1; dx <= 1; ++dx) {
-    const int X = x + dx;
-    if (X < 0 || X >= d.sx) continue;
-#pragma unroll
-    for (int dy = -1; dy <= 1; ++dy) {
-      const int Y = y + dy;
-      if (Y < 0 || Y >= d.sy) continue;
-#pragma unroll
-      for (int dz = -1; dz <= 1; ++dz) {
-        const int Z = z + dz;
-        if (Z < 0 || Z >= d.sz) continue;
-        const int c = (X * d.sy + Y) * d.sz + Z;
-        const int b = __ldg(off + c), e = __ldg(off + c + 1);
-        if (dx == 0 && dy == 0 && dz == 0) own = e - b;
-        if (dx == -1 && dy == 0 && dz == 0) left = e - b;
-        if (dx == 0 && dy == -1 && dz == 0) down = e - b;
-        if (dx == 0 && dy == 0 && dz == -1) back = e - b;
-        for (int j = b; j < e; ++j) {
-          const float qx = __ldg(cur.px + j) * inv_h;
-          const float qy = __ldg(cur.py + j) * inv_h;
-          const float qz = __ldg(cur.pz + j) * inv_h;
-          const float bx = hat1(qx - fxh), by = hat1(qy - fyh), bz = hat1(qz - fzh);
-          if (dx < 1) {
-            const float w = hat1(qx - fx) * by * bz;
-            su += w * __ldg(cur.vx + j);
-            wu += w;
-          }
-          if (dy < 1) {
-            const float w = bx * hat1(qy - fy) * bz;
-            sv += w * __ldg(cur.vy + j);
-            wv += w;
-          }
-          if (dz < 1) {
-            const float w = bx * by * hat1(qz - fz);
-            sw += w * __ldg(cur.vz + j);
-            ww += w;
-          }
-          if (MULTI && dx == 0 && dy == 0 && dz == 0) {
-            const float w = bx * by * bz;
-            const float4 f = cur.frac[j];
-            fs.x += w * f.x; fs.y += w * f.y; fs.z += w * f.z; fs.w += w * f.w;
-            fw += w;
-          }
-        }
-      }
-    }
-  }
+__device__ __forceinline__ void p2g_finish(const Dims& d, const StepParams& sp, int x, int y, int z, const P2gAcc& a,
+                                           float* __restrict__ u0, float* __restrict__ v0, float* __restrict__ w0,
+                                           float* __restrict__ un, float* __restrict__ vn, float* __restrict__ wn,
+                                           int8_t* __restrict__ type, float* __restrict__ density,
+                                           float4* __restrict__ vf, float4* __restrict__ nvf) {
+  const float su = a.su, sv = a.sv, sw = a.sw, wu = a.wu, wv = a.wv, ww = a.ww;
+  const float4 fs = a.fs;
+  const float fw = a.fw;
+  const int own = a.own, left = a.left, down = a.down, back = a.back;
   // transferToCellDividePhase
   const float u = wu > 0.f ? __fdiv_rn(su, wu) : 0.f;
   const float v = wv > 0.f ? __fdiv_rn(sv, wv) : 0.f;
@@ -128,6 +119,64 @@ __device__ __forceinline__ void p2g_body(const Dims& d, const StepParams& sp, co
   un[ni] = nu; vn[ni] = nv; wn[ni] = nw;
 }
 
+
+template <bool FORCES, bool MULTI>
+__device__ __forceinline__ void p2g_body(const Dims& d, const StepParams& sp, const Particles& cur,
+                                         const int* __restrict__ off, float* __restrict__ u0, float* __restrict__ v0,
+                                         float* __restrict__ w0, float* __restrict__ un, float* __restrict__ vn,
+                                         float* __restrict__ wn, int8_t* __restrict__ type,
+                                         float* __restrict__ density, float4* __restrict__ vf,
+                                         float4* __restrict__ nvf, int bx, int by, int bz) {
+  const int z = bx * 32 + threadIdx.x;
+  const int y = by * 8 + threadIdx.y;
+  const int x = bz;
+  if (z >= d.sz || y >= d.sy) return;
+  const float fx = (float)x, fy = (float)y, fz = (float)z;
+  const float fxh = fx + 0.5f, fyh = fy + 0.5f, fzh = fz + 0.5f;
+  const float inv_h = d.inv_h;
+  float su = 0.f, sv = 0.f, sw = 0.f, wu = 0.f, wv = 0.f, ww = 0.f;
+  float4 fs = make_float4(0.f, 0.f, 0.f, 0.f);
+  float fw = 0.f;
+  int own = 0, left = 0, down = 0, back = 0;
+#pragma unroll
+  for (int dx = -1; dx <= 1; ++dx) {
+    const int X = x + dx;
+    if (X < 0 || X >= d.sx) continue;
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int Y = y + dy;
+      if (Y < 0 || Y >= d.sy) continue;
+#pragma unroll
+      for (int dz = -1; dz <= 1; ++dz) {
+        const int Z = z + dz;
+        if (Z < 0 || Z >= d.sz) continue;
+        const int c = (X * d.sy + Y) * d.sz + Z;
+        const int b = __ldg(off + c), e = __ldg(off + c + 1);
+        if (dx == 0 && dy == 0 && dz == 0) own = e - b;
+        if (dx == -1 && dy == 0 && dz == 0) left = e - b;
+        if (dx == 0 && dy == -1 && dz == 0) down = e - b;
+        if (dx == 0 && dy == 0 && dz == -1) back = e - b;
+        for (int j = b; j < e; ++j) {
+          const float qx = __fmul_rn(__ldg(cur.px + j), inv_h);
+          const float qy = __fmul_rn(__ldg(cur.py + j), inv_h);
+          const float qz = __fmul_rn(__ldg(cur.pz + j), inv_h);
+          const float vx = dx < 1 ? __ldg(cur.vx + j) : 0.f;
+          const float vy = dy < 1 ? __ldg(cur.vy + j) : 0.f;
+          const float vz = dz < 1 ? __ldg(cur.vz + j) : 0.f;
+          float bxyz;
+          p2g_particle(dx, dy, dz, qx, qy, qz, vx, vy, vz, fx, fy, fz, fxh, fyh, fzh, su, sv, sw, wu, wv, ww, bxyz);
+          if (MULTI && dx == 0 && dy == 0 && dz == 0) p2g_fractions(bxyz, cur.frac[j], fs, fw);
+        }
+      }
+    }
+  }
+  P2gAcc a;
+  a.su = su; a.sv = sv; a.sw = sw; a.wu = wu; a.wv = wv; a.ww = ww;
+  a.fs = fs; a.fw = fw;
+  a.own = own; a.left = left; a.down = down; a.back = back;
+  p2g_finish<FORCES, MULTI>(d, sp, x, y, z, a, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+}
+
 template <bool FORCES, bool MULTI>
 __global__ void __launch_bounds__(256) k_p2g(Dims d, StepParams sp, Particles cur, const int* __restrict__ off,
                                             float* __restrict__ u0, float* __restrict__ v0,
@@ -137,6 +186,119 @@ __global__ void __launch_bounds__(256) k_p2g(Dims d, StepParams sp, Particles cu
                                             float4* __restrict__ vf, float4* __restrict__ nvf) {
   p2g_body<FORCES, MULTI>(d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf, blockIdx.x, blockIdx.y,
                           blockIdx.z);
+}
+
+// ------------------------------------------------------- shared-memory P2G
+// The gather of p2g_body (same arithmetic, same (dx, dy, dz, j) order, same
+// epilogue) with the particles staged in shared memory.  A CTA owns the
+// nodes of one x plane, 8 y rows and 32 z columns, one per thread.  For each
+// dx it stages, once and coalesced, the particles of the cells it reads in
+// plane x + dx (10 rows of 34 cells: its own rows and columns and a one-cell
+// rim), in positions scaled to cell units, into cell-major slots: slot k of
+// cell c sits at k * kP2gCells + c.  The 32 lanes of a warp read the k-th
+// particle of 32 consecutive cells, i.e. 32 consecutive words and 32
+// distinct banks, where the one-thread-per-node kernel's lanes gathered from
+// scattered addresses through L1.  A cell holding more than kP2gSlots
+// particles reads the rest from global memory.
+constexpr int kP2gSlots = 12;
+constexpr int kP2gCols = 34, kP2gRows = 10, kP2gCells = kP2gCols * kP2gRows;
+constexpr int kP2gSmem = 6 * kP2gSlots * kP2gCells * (int)sizeof(float);
+
+template <bool FORCES, bool MULTI>
+__global__ void __launch_bounds__(256, 2) k_p2g_tiled(Dims d, StepParams sp, Particles cur, const int* __restrict__ off,
+                                                     float* __restrict__ u0, float* __restrict__ v0,
+                                                     float* __restrict__ w0, float* __restrict__ un,
+                                                     float* __restrict__ vn, float* __restrict__ wn,
+                                                     int8_t* __restrict__ type, float* __restrict__ density,
+                                                     float4* __restrict__ vf, float4* __restrict__ nvf) {
+  extern __shared__ float p2g_sm[];  // qx, qy, qz, vx, vy, vz: [kP2gSlots][kP2gCells] each
+  __shared__ int s_beg[kP2gCells], s_cnt[kP2gCells];
+  constexpr int A = kP2gSlots * kP2gCells;
+  float* const sqx = p2g_sm;
+  float* const sqy = sqx + A;
+  float* const sqz = sqy + A;
+  float* const svx = sqz + A;
+  float* const svy = svx + A;
+  float* const svz = svy + A;
+  const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
+  const int z0 = blockIdx.x * 32, y0 = blockIdx.y * 8, x = blockIdx.z;
+  const int z = z0 + lane, y = y0 + wy;
+  const bool node = z < d.sz && y < d.sy;
+  const float fx = (float)x, fy = (float)y, fz = (float)z;
+  const float fxh = fx + 0.5f, fyh = fy + 0.5f, fzh = fz + 0.5f;
+  const float inv_h = d.inv_h;
+  float su = 0.f, sv = 0.f, sw = 0.f, wu = 0.f, wv = 0.f, ww = 0.f;
+  float4 fs = make_float4(0.f, 0.f, 0.f, 0.f);
+  float fw = 0.f;
+  int own = 0, left = 0, down = 0, back = 0;
+#pragma unroll
+  for (int dx = -1; dx <= 1; ++dx) {
+    const int X = x + dx;
+    if (X < 0 || X >= d.sx) continue;  // the same for the whole CTA
+    __syncthreads();                   // the previous plane's slots are consumed
+    for (int lc = tid; lc < kP2gCells; lc += 256) {
+      const int Y = y0 - 1 + lc / kP2gCols, Z = z0 - 1 + lc % kP2gCols;
+      int b = 0, n = 0;
+      if (Y >= 0 && Y < d.sy && Z >= 0 && Z < d.sz) {
+        const int c = (X * d.sy + Y) * d.sz + Z;
+        b = __ldg(off + c);
+        n = __ldg(off + c + 1) - b;
+      }
+      s_beg[lc] = b;
+      s_cnt[lc] = n;
+      const int m = min(n, kP2gSlots);
+      for (int k = 0; k < m; ++k) {
+        const int j = b + k, sl = k * kP2gCells + lc;
+        sqx[sl] = __fmul_rn(__ldg(cur.px + j), inv_h);
+        sqy[sl] = __fmul_rn(__ldg(cur.py + j), inv_h);
+        sqz[sl] = __fmul_rn(__ldg(cur.pz + j), inv_h);
+        svx[sl] = __ldg(cur.vx + j);
+        svy[sl] = __ldg(cur.vy + j);
+        svz[sl] = __ldg(cur.vz + j);
+      }
+    }
+    __syncthreads();
+    if (!node) continue;
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int Y = y + dy;
+      if (Y < 0 || Y >= d.sy) continue;
+#pragma unroll
+      for (int dz = -1; dz <= 1; ++dz) {
+        const int Z = z + dz;
+        if (Z < 0 || Z >= d.sz) continue;
+        const int lc = (wy + 1 + dy) * kP2gCols + lane + 1 + dz;
+        const int b = s_beg[lc], n = s_cnt[lc];
+        if (dx == 0 && dy == 0 && dz == 0) own = n;
+        if (dx == -1 && dy == 0 && dz == 0) left = n;
+        if (dx == 0 && dy == -1 && dz == 0) down = n;
+        if (dx == 0 && dy == 0 && dz == -1) back = n;
+        const int m = min(n, kP2gSlots);
+        for (int k = 0; k < m; ++k) {  // the staged slots
+          const int sl = k * kP2gCells + lc;
+          float bxyz;
+          p2g_particle(dx, dy, dz, sqx[sl], sqy[sl], sqz[sl], dx < 1 ? svx[sl] : 0.f, dy < 1 ? svy[sl] : 0.f,
+                       dz < 1 ? svz[sl] : 0.f, fx, fy, fz, fxh, fyh, fzh, su, sv, sw, wu, wv, ww, bxyz);
+          if (MULTI && dx == 0 && dy == 0 && dz == 0) p2g_fractions(bxyz, cur.frac[b + k], fs, fw);
+        }
+        for (int k = m; k < n; ++k) {  // a crowded cell's particles beyond the slots
+          const int j = b + k;
+          float bxyz;
+          p2g_particle(dx, dy, dz, __fmul_rn(__ldg(cur.px + j), inv_h), __fmul_rn(__ldg(cur.py + j), inv_h),
+                       __fmul_rn(__ldg(cur.pz + j), inv_h), dx < 1 ? __ldg(cur.vx + j) : 0.f,
+                       dy < 1 ? __ldg(cur.vy + j) : 0.f, dz < 1 ? __ldg(cur.vz + j) : 0.f, fx, fy, fz, fxh, fyh, fzh,
+                       su, sv, sw, wu, wv, ww, bxyz);
+          if (MULTI && dx == 0 && dy == 0 && dz == 0) p2g_fractions(bxyz, cur.frac[j], fs, fw);
+        }
+      }
+    }
+  }
+  if (!node) return;
+  P2gAcc a;
+  a.su = su; a.sv = sv; a.sw = sw; a.wu = wu; a.wv = wv; a.ww = ww;
+  a.fs = fs; a.fw = fw;
+  a.own = own; a.left = left; a.down = down; a.back = back;
+  p2g_finish<FORCES, MULTI>(d, sp, x, y, z, a, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
 }
 
 // node-grid virtual block -> (z block, y block, x plane) of one scene
@@ -600,12 +762,36 @@ cudaError_t launch_batch_extrapolate(cudaStream_t st, const BatchIndex& bi, int 
   return cudaGetLastError();
 }
 
+static int g_p2g_variant = 1;  // 1: shared-memory staged (default), 0: one thread per node through L1
+void set_p2g_variant(int v) { g_p2g_variant = v; }
+int p2g_variant() { return g_p2g_variant; }
+
+template <bool F, bool M>
+static cudaError_t launch_p2g_tiled(cudaStream_t st, const Dims& d, const StepParams& sp, Particles cur,
+                                    const int* off, float* u0, float* v0, float* w0, float* un, float* vn,
+                                    float* wn, int8_t* type, float* density, float4* vf, float4* nvf) {
+  cudaError_t e = cudaFuncSetAttribute(k_p2g_tiled<F, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, kP2gSmem);
+  if (e != cudaSuccess) return e;
+  k_p2g_tiled<F, M><<<node_grid(d), dim3(32, 8), kP2gSmem, st>>>(d, sp, cur, off, u0, v0, w0, un, vn, wn, type,
+                                                                  density, vf, nvf);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_p2g(cudaStream_t st, const Dims& d, const StepParams& sp, bool forces, Particles cur,
                        const int* off, int n, float* u0, float* v0, float* w0, float* un, float* vn,
                        float* wn, int8_t* type, float* density, float4* vf, float4* nvf) {
   (void)n;
   const dim3 g = node_grid(d), b(32, 8);
   const bool multi = sp.multiphase != 0;
+  if (g_p2g_variant == 1) {
+    if (forces && multi)
+      return launch_p2g_tiled<true, true>(st, d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+    if (forces)
+      return launch_p2g_tiled<true, false>(st, d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+    if (multi)
+      return launch_p2g_tiled<false, true>(st, d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+    return launch_p2g_tiled<false, false>(st, d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+  }
   if (forces && multi)
     k_p2g<true, true><<<g, b, 0, st>>>(d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
   else if (forces)
