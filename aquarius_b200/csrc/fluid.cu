@@ -1319,7 +1319,7 @@ aq_status aq_fluid::health() {
 }
 
 aq_status aq_p2g_set_variant(int32_t variant) {
-  if (variant != 0 && variant != 1) return fail(AQ_ERR_INVALID_ARGUMENT, "P2G variant must be 0 or 1");
+  if (variant < 0 || variant > 3) return fail(AQ_ERR_INVALID_ARGUMENT, "P2G variant must be 0-3");
   set_p2g_variant(variant);
   return AQ_OK;
 }

@@ -40,6 +40,31 @@ __device__ __forceinline__ void p2g_particle(int DX, int DY, int DZ, float qx, f
   bxyz = __fmul_rn(__fmul_rn(bx, by), bz);
 }
 
+// p2g_particle with the x factors already evaluated: ax = hat1(qx - fx) and
+// bx = hat1(qx - fxh), the same values (a staged plane shares the node x).
+__device__ __forceinline__ void p2g_particle_x(int DX, int DY, int DZ, float ax, float bx, float qy, float qz,
+                                               float vx, float vy, float vz, float fy, float fz, float fyh,
+                                               float fzh, float& su, float& sv, float& sw, float& wu, float& wv,
+                                               float& ww, float& bxyz) {
+  const float by = hat1(__fsub_rn(qy, fyh)), bz = hat1(__fsub_rn(qz, fzh));
+  if (DX < 1) {
+    const float w = __fmul_rn(__fmul_rn(ax, by), bz);
+    su = __fmaf_rn(w, vx, su);
+    wu = __fadd_rn(wu, w);
+  }
+  if (DY < 1) {
+    const float w = __fmul_rn(__fmul_rn(bx, hat1(__fsub_rn(qy, fy))), bz);
+    sv = __fmaf_rn(w, vy, sv);
+    wv = __fadd_rn(wv, w);
+  }
+  if (DZ < 1) {
+    const float w = __fmul_rn(__fmul_rn(bx, by), hat1(__fsub_rn(qz, fz)));
+    sw = __fmaf_rn(w, vz, sw);
+    ww = __fadd_rn(ww, w);
+  }
+  bxyz = __fmul_rn(__fmul_rn(bx, by), bz);
+}
+
 // The fractions' weighted sum of the node's own cell (transferVolumeFractionsToCell).
 __device__ __forceinline__ void p2g_fractions(float w, const float4& f, float4& fs, float& fw) {
   fs.x = __fmaf_rn(w, f.x, fs.x);
@@ -194,28 +219,32 @@ __global__ void __launch_bounds__(256) k_p2g(Dims d, StepParams sp, Particles cu
 // nodes of one x plane, 8 y rows and 32 z columns, one per thread.  For each
 // dx it stages, once and coalesced, the particles of the cells it reads in
 // plane x + dx (10 rows of 34 cells: its own rows and columns and a one-cell
-// rim), in positions scaled to cell units, into cell-major slots: slot k of
-// cell c sits at k * kP2gCells + c.  The 32 lanes of a warp read the k-th
+// rim), into cell-major slots: slot k of cell c sits at k * kP2gCells + c.
+// A slot holds the particle's two x hat factors (the CTA's nodes share one
+// x, so they are the particle's for the whole plane), its y and z in cell
+// units and its velocity.  The 32 lanes of a warp read the k-th
 // particle of 32 consecutive cells, i.e. 32 consecutive words and 32
 // distinct banks, where the one-thread-per-node kernel's lanes gathered from
 // scattered addresses through L1.  A cell holding more than kP2gSlots
 // particles reads the rest from global memory.
-constexpr int kP2gSlots = 12;
 constexpr int kP2gCols = 34, kP2gRows = 10, kP2gCells = kP2gCols * kP2gRows;
-constexpr int kP2gSmem = 6 * kP2gSlots * kP2gCells * (int)sizeof(float);
+constexpr int p2g_smem(int slots) { return 7 * slots * kP2gCells * (int)sizeof(float); }
 
-template <bool FORCES, bool MULTI>
-__global__ void __launch_bounds__(256, 2) k_p2g_tiled(Dims d, StepParams sp, Particles cur, const int* __restrict__ off,
+template <bool FORCES, bool MULTI, int kP2gSlots>
+__global__ void __launch_bounds__(256, kP2gSlots <= 7 ? 3 : (kP2gSlots <= 11 ? 2 : 1)) k_p2g_tiled(Dims d, StepParams sp, Particles cur, const int* __restrict__ off,
                                                      float* __restrict__ u0, float* __restrict__ v0,
                                                      float* __restrict__ w0, float* __restrict__ un,
                                                      float* __restrict__ vn, float* __restrict__ wn,
                                                      int8_t* __restrict__ type, float* __restrict__ density,
                                                      float4* __restrict__ vf, float4* __restrict__ nvf) {
-  extern __shared__ float p2g_sm[];  // qx, qy, qz, vx, vy, vz: [kP2gSlots][kP2gCells] each
+  // hat1(qx - fx), hat1(qx - fxh), qy, qz, vx, vy, vz: [kP2gSlots][kP2gCells] each (the x
+  // factors are per particle: the CTA's nodes share one x)
+  extern __shared__ float p2g_sm[];
   __shared__ int s_beg[kP2gCells], s_cnt[kP2gCells];
   constexpr int A = kP2gSlots * kP2gCells;
-  float* const sqx = p2g_sm;
-  float* const sqy = sqx + A;
+  float* const sax = p2g_sm;
+  float* const sbx = sax + A;
+  float* const sqy = sbx + A;
   float* const sqz = sqy + A;
   float* const svx = sqz + A;
   float* const svy = svx + A;
@@ -249,7 +278,9 @@ __global__ void __launch_bounds__(256, 2) k_p2g_tiled(Dims d, StepParams sp, Par
       const int m = min(n, kP2gSlots);
       for (int k = 0; k < m; ++k) {
         const int j = b + k, sl = k * kP2gCells + lc;
-        sqx[sl] = __fmul_rn(__ldg(cur.px + j), inv_h);
+        const float qx = __fmul_rn(__ldg(cur.px + j), inv_h);
+        sax[sl] = hat1(__fsub_rn(qx, fx));
+        sbx[sl] = hat1(__fsub_rn(qx, fxh));
         sqy[sl] = __fmul_rn(__ldg(cur.py + j), inv_h);
         sqz[sl] = __fmul_rn(__ldg(cur.pz + j), inv_h);
         svx[sl] = __ldg(cur.vx + j);
@@ -259,11 +290,14 @@ __global__ void __launch_bounds__(256, 2) k_p2g_tiled(Dims d, StepParams sp, Par
     }
     __syncthreads();
     if (!node) continue;
-#pragma unroll
+    // dy and dz stay loops (the branches on them are uniform across the
+    // warp): 27 unrolled copies of the particle loop overflow the
+    // instruction cache
+#pragma unroll 1
     for (int dy = -1; dy <= 1; ++dy) {
       const int Y = y + dy;
       if (Y < 0 || Y >= d.sy) continue;
-#pragma unroll
+#pragma unroll 1
       for (int dz = -1; dz <= 1; ++dz) {
         const int Z = z + dz;
         if (Z < 0 || Z >= d.sz) continue;
@@ -277,8 +311,9 @@ __global__ void __launch_bounds__(256, 2) k_p2g_tiled(Dims d, StepParams sp, Par
         for (int k = 0; k < m; ++k) {  // the staged slots
           const int sl = k * kP2gCells + lc;
           float bxyz;
-          p2g_particle(dx, dy, dz, sqx[sl], sqy[sl], sqz[sl], dx < 1 ? svx[sl] : 0.f, dy < 1 ? svy[sl] : 0.f,
-                       dz < 1 ? svz[sl] : 0.f, fx, fy, fz, fxh, fyh, fzh, su, sv, sw, wu, wv, ww, bxyz);
+          p2g_particle_x(dx, dy, dz, sax[sl], sbx[sl], sqy[sl], sqz[sl], dx < 1 ? svx[sl] : 0.f,
+                         dy < 1 ? svy[sl] : 0.f, dz < 1 ? svz[sl] : 0.f, fy, fz, fyh, fzh, su, sv, sw, wu, wv, ww,
+                         bxyz);
           if (MULTI && dx == 0 && dy == 0 && dz == 0) p2g_fractions(bxyz, cur.frac[b + k], fs, fw);
         }
         for (int k = m; k < n; ++k) {  // a crowded cell's particles beyond the slots
@@ -762,19 +797,34 @@ cudaError_t launch_batch_extrapolate(cudaStream_t st, const BatchIndex& bi, int 
   return cudaGetLastError();
 }
 
-static int g_p2g_variant = 1;  // 1: shared-memory staged (default), 0: one thread per node through L1
+// 0: one thread per node through L1; 1, 2, 3: shared-memory staged with
+// 11, 7 or 16 slots per cell (2, 3 or 1 CTAs per SM; with fewer slots more
+// crowded cells read partly from global memory)
+static int g_p2g_variant = 1;
 void set_p2g_variant(int v) { g_p2g_variant = v; }
 int p2g_variant() { return g_p2g_variant; }
+
+template <bool F, bool M, int SLOTS>
+static cudaError_t launch_p2g_slots(cudaStream_t st, const Dims& d, const StepParams& sp, Particles cur,
+                                    const int* off, float* u0, float* v0, float* w0, float* un, float* vn,
+                                    float* wn, int8_t* type, float* density, float4* vf, float4* nvf) {
+  constexpr int smem = p2g_smem(SLOTS);
+  cudaError_t e = cudaFuncSetAttribute(k_p2g_tiled<F, M, SLOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  k_p2g_tiled<F, M, SLOTS><<<node_grid(d), dim3(32, 8), smem, st>>>(d, sp, cur, off, u0, v0, w0, un, vn, wn, type,
+                                                                     density, vf, nvf);
+  return cudaGetLastError();
+}
 
 template <bool F, bool M>
 static cudaError_t launch_p2g_tiled(cudaStream_t st, const Dims& d, const StepParams& sp, Particles cur,
                                     const int* off, float* u0, float* v0, float* w0, float* un, float* vn,
                                     float* wn, int8_t* type, float* density, float4* vf, float4* nvf) {
-  cudaError_t e = cudaFuncSetAttribute(k_p2g_tiled<F, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, kP2gSmem);
-  if (e != cudaSuccess) return e;
-  k_p2g_tiled<F, M><<<node_grid(d), dim3(32, 8), kP2gSmem, st>>>(d, sp, cur, off, u0, v0, w0, un, vn, wn, type,
-                                                                  density, vf, nvf);
-  return cudaGetLastError();
+  if (g_p2g_variant == 2)
+    return launch_p2g_slots<F, M, 7>(st, d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+  if (g_p2g_variant == 3)
+    return launch_p2g_slots<F, M, 16>(st, d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
+  return launch_p2g_slots<F, M, 11>(st, d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
 }
 
 cudaError_t launch_p2g(cudaStream_t st, const Dims& d, const StepParams& sp, bool forces, Particles cur,
@@ -783,7 +833,7 @@ cudaError_t launch_p2g(cudaStream_t st, const Dims& d, const StepParams& sp, boo
   (void)n;
   const dim3 g = node_grid(d), b(32, 8);
   const bool multi = sp.multiphase != 0;
-  if (g_p2g_variant == 1) {
+  if (g_p2g_variant >= 1) {
     if (forces && multi)
       return launch_p2g_tiled<true, true>(st, d, sp, cur, off, u0, v0, w0, un, vn, wn, type, density, vf, nvf);
     if (forces)

@@ -1001,7 +1001,8 @@ def run_profile_case(case: str):
     """Small, fixed cases for single-kernel ncu captures (no JSON line):
     jacobi: the 128^3 workload's system after 3 steps, 6 sweeps of the
     default plan; resident: the same system, 40 sweeps of the resident plan
-    (one cooperative launch, 8x40x16 tiles, 960 threads); batch-rows: 32 scenes of the batch set, 6 batched sweeps;
+    (one cooperative launch, 8x40x16 tiles, 960 threads); p2g: the same
+    state, the particle-to-grid stage twice; batch-rows: 32 scenes of the batch set, 6 batched sweeps;
     conv: two U-Net inferences at 128^3 on seeded random inputs; mesh: two
     surface meshes of the 128^3 workload's initial particles; pbf / pcisph:
     one step of the solver at particle budget 3e6 (593k particles); render:
@@ -1016,6 +1017,16 @@ def run_profile_case(case: str):
         f.step(3)
         f.synchronize()
         print(f.jacobi_plan(), f.benchmark_pressure(6))
+        f.close()
+    elif case == "p2g":
+        from aquarius_b200 import _abi
+        f = aq.Fluid(workload_config(128, "zero"))
+        f.step(3)
+        f.synchronize()
+        for _ in range(2):
+            f.run_stage(_abi.STAGE_P2G)
+        f.synchronize()
+        print("p2g ok")
         f.close()
     elif case == "resident":
         f = aq.Fluid(workload_config(128, "zero"))
@@ -1087,8 +1098,8 @@ def main():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own kernels (the plain-step comparator)")
     ap.add_argument("--reference-gpu-only", action="store_true", help=argparse.SUPPRESS)
-    ap.add_argument("--profile-case", choices=["jacobi", "resident", "batch-rows", "conv", "mesh", "pbf", "pcisph",
-                                               "render"],
+    ap.add_argument("--profile-case", choices=["jacobi", "resident", "p2g", "batch-rows", "conv", "mesh", "pbf",
+                                               "pcisph", "render"],
                     default=None,
                     help="run one small fixed case for an ncu capture and exit")
     ap.add_argument("--workload", default="ball128",

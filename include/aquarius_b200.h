@@ -260,9 +260,10 @@ aq_status aq_fluid_solve_stats(const aq_fluid* f, aq_solve_stats* st);
 aq_status aq_fluid_test_barrier_timeout(aq_fluid* f, int32_t withhold_cta, uint32_t spin_limit);
 
 /* Particle-to-grid kernel, process-wide (set it while no step is in flight):
- * 1 (default) stages each CTA's particles in shared memory (cell-major
- * slots, conflict-free gathers), 0 gathers through L1 with one thread per
- * node.  Both sum the same terms in the reference's (dx, dy, dz, j) order
+ * 1 (default), 2, 3 stage each CTA's particles in shared memory (cell-major
+ * slots, conflict-free gathers) with 11, 7 or 16 slots per cell (particles
+ * beyond them are read from global memory); 0 gathers through L1 with one
+ * thread per node.  Both sum the same terms in the reference's (dx, dy, dz, j) order
  * (transferToCellAccumPhase, Fluid/Fluid_3D_FLIP.cu:8-70). */
 aq_status aq_p2g_set_variant(int32_t variant);
 
