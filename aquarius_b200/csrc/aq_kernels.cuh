@@ -305,6 +305,10 @@ size_t conv3_wgrad_part_floats(int cin, int cout, int voxels);
 void set_conv_impl(int impl);
 // Nonzero if a tcgen05 convolution ever gave up waiting on its mbarriers.
 int conv_umma_timeouts();
+// Test hook: skip != 0 makes every tcgen05 convolution issue no MMA, so its
+// bounded wait runs out after wait_ns (0 = the default second); also clears
+// the timeout record.
+cudaError_t conv_umma_test_hook(int skip, unsigned long long wait_ns);
 // wt[t][ci][co] = w[26-t][co][ci] (weights of the data gradient).
 cudaError_t launch_flip_transpose(cudaStream_t st, const void* w, void* wt, int cin, int cout);
 

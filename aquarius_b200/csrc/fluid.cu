@@ -1542,7 +1542,7 @@ aq_status aq_fluid_set_jacobi_plan(aq_fluid* f, int32_t levels, int32_t rows, in
   if (rows == 4) {  // resident tiles: levels = sweeps per halo exchange, x_planes = tile shape
     cudaSetDevice(f->device);
     const int c = f->d.sz % 4 == 0 ? resident_ctas(f->device, x_planes, levels) : 0;
-    if (c <= 0) return fail(AQ_ERR_INVALID_ARGUMENT, "unsupported resident plan (levels 4, shape 0-7, sz % 4 == 0)");
+    if (c <= 0) return fail(AQ_ERR_INVALID_ARGUMENT, "unsupported resident plan (levels 4, shape 0-6, sz % 4 == 0)");
     if (f->cfg.pressure_init == AQ_PRESSURE_LEARNED && f->d.sz % 4 != 0)
       return fail(AQ_ERR_INVALID_ARGUMENT, "the learned warm start needs sz % 4 == 0");
     AQ_CUDA(cudaStreamSynchronize(f->stream));

@@ -309,7 +309,7 @@ __device__ __forceinline__ void jacobi_row_pre(const Dims& d, const float* __res
 // fluid, from a list built once per solve (k_row_items).  A resident wave of
 // CTAs walks the list, so no CTA is scheduled only to find its rows empty.
 // Same arithmetic as the flat sweep (jacobi_quad).
-__global__ void __launch_bounds__(256) k_jacobi_list(Dims d, const float* __restrict__ pin, float* __restrict__ pout,
+__global__ void __launch_bounds__(256, 6) k_jacobi_list(Dims d, const float* __restrict__ pin, float* __restrict__ pout,
                                                     const float* __restrict__ rhs, const int8_t* __restrict__ type,
                                                     const int* __restrict__ items, const int* __restrict__ n_items,
                                                     int early) {
@@ -1711,7 +1711,10 @@ cudaError_t launch_jacobi_list(cudaStream_t st, const Dims& d, const float* pin,
                                const int8_t* type, const int* items, const int* n_items, bool early) {
   if (d.sz % 4 != 0) return cudaErrorInvalidValue;
   // 8 warps per CTA, one resident wave (4 to 32 warps per CTA and fewer,
-  // fatter waves measured the same or slower at 128^3)
+  // fatter waves measured the same or slower at 128^3); the kernel is held
+  // to 40 registers so 6 CTAs fit per SM (888 CTAs, 7104 warps): every warp
+  // of a 128^3 pool's ~6300 rows then has at most one row, and none waits
+  // on a second row's loads after the first (3.02 against 3.29 us a sweep)
   const int wy = 8;
   const int need = (row_items_capacity(d) + wy - 1) / wy;
   cudaLaunchConfig_t lc = {};

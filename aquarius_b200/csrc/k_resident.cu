@@ -1,7 +1,7 @@
 // Resident Jacobi pressure solve (stage (c), hot loop #1): the whole solve in
 // one cooperative launch whose CTAs keep their tiles' pressure in shared
 // memory and right-hand side in registers from the first sweep to the last,
-// and exchange only tile halos through L2, once every K sweeps.
+// and exchange only tile halos through L2, once every K = 4 sweeps.
 //
 // Reference: jacobiImpl (Fluid/Fluid_3D_kernels.cu:460-505), launched
 // pressureIterations times by solvePressureJacobi (Fluid/Fluid_3D_common.cu:48-55).
@@ -11,34 +11,38 @@
 // clamped to the cell itself: the arithmetic of every other sweep kernel of
 // the library (jacobi_quad), so the iterates are bit for bit the flat sweep's.
 //
-// Decomposition.  The grid is cut into tiles of TX x TY x TZ cells (whole 8^3
+// Decomposition.  The grid is cut into tiles of TX x TY x 24 cells (whole 8^3
 // activity bricks); a tile takes part when one of its bricks holds fluid
 // (cells outside every such tile are non-fluid, 0 in both global buffers,
-// and stay 0).  A CTA owns one tile and holds its box, the tile plus a K-cell
-// halo clipped to the domain, in shared memory.  A block of K sweeps runs on
-// the box with redundant halo work: sweep s updates the cells at least s
-// cells inside every face of the box that is not a domain wall, so after K
-// sweeps the tile's own cells hold exactly what K global sweeps give.  The
-// tile then writes its cells to the global buffer of the block, every CTA
-// meets at a bounded grid barrier, and each reloads only its halo.  The two
-// global buffers alternate between blocks, so a CTA never overwrites cells a
-// slower neighbour may still be reading.  When the active tiles outnumber
-// the CTAs, each CTA walks its tiles one after another per block and
-// reloads each whole box from L2 (same results, not resident).
+// and stay 0).  A CTA owns one tile and holds its box, the tile plus a 4-cell
+// halo clipped to the domain (at most (TX+8) x (TY+8) x 32 cells), in two
+// shared-memory pressure buffers (ping-pong per sweep).  A block of 4 sweeps
+// runs on the box with redundant halo work: sweep s updates the cells at
+// least s cells inside every face of the box that is not a domain wall, so
+// after 4 sweeps the tile's own cells hold exactly what 4 global sweeps give.
+// The tile then writes its cells to the global buffer of the block, every
+// CTA meets at a bounded grid barrier, and each reloads its box with one TMA
+// tensor copy (cp.async.bulk.tensor, the tile's own cells come back
+// unchanged; a bounded mbarrier wait).  The
+// two global buffers alternate between blocks, so a CTA never overwrites
+// cells a slower neighbour may still be reading.  When the active tiles
+// outnumber the CTAs, each CTA walks its tiles one after another per block
+// and reloads each whole box from L2 (same results, not resident).
 //
-// Threads.  One per (8-level y segment, x, z-quad) of the box: a thread
-// keeps its segment's pressure quads in registers (y neighbours inside the
-// segment are its own), takes the z neighbours from the lanes holding the
-// adjacent quads (shuffles), and reads x neighbours, segment-end y
-// neighbours and the rhs from shared memory; the new iterate goes to the
-// other shared buffer (ping-pong per sweep).  The x stride of the shared
-// arrays is padded to EZ mod 32, so the lanes of a warp, consecutive quads of
-// one or two x rows, read 16-byte quads from distinct banks.
+// Threads.  One per (8-level x segment, y row, z-quad) of the box; a warp is
+// 4 whole y rows of 8 quads.  A thread keeps the rhs and fluid marks of its
+// 8 quads in registers and walks its segment in x with a 3-quad window
+// (x-1, x, x+1), so a quad costs one shared load for x+1, one each for y+1
+// and y-1 (consecutive quads of consecutive rows: conflict-free 16-byte
+// loads), and two shuffles for z+1 and z-1.
 //
 // Residual checks (RESIDUAL mode, every `check` sweeps; once at the end in
 // FIXED mode): FP64 ||b - A p||^2 over the tiles' fluid cells, per thread in
-// y order, per CTA by a fixed tree, then summed over the CTAs' partials in
+// x order, per CTA by a fixed tree, then summed over the CTAs' partials in
 // index order by every CTA, so all make the same stop decision.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 
 #include "aq_kernels.cuh"
@@ -65,30 +69,35 @@ __device__ __forceinline__ bool div6_fast_ok(float s) {
 }
 __device__ __forceinline__ float div6(float s) { return div6_fast_ok(s) ? div6_fast(s) : __fdiv_rn(s, 6.f); }
 
+// div6_fast_ok for all four sums of a quad: +0 (every non-fluid cell away
+// from the fluid sums to +0 each sweep) or 2^-123 <= |s| <= FLT_MAX (false
+// for NaN), as float compares.
+__device__ __forceinline__ bool div6_fast_ok_f(float s) {
+  constexpr float lo = 0x1p-123f, hi = 0x1.fffffep127f;
+  return (fabsf(s) >= lo && fabsf(s) <= hi) || __float_as_uint(s) == 0u;
+}
+__device__ __forceinline__ bool div6_quad_fast_ok(const float4& s) {
+  return div6_fast_ok_f(s.x) && div6_fast_ok_f(s.y) && div6_fast_ok_f(s.z) && div6_fast_ok_f(s.w);
+}
+
 namespace {
 
-template <int TX, int TY, int TZ, int K, int SEG_>
+template <int TX, int TY>
 struct Res {
+  static constexpr int K = 4, TZ = 24;
   static constexpr int EX = TX + 2 * K, EY = TY + 2 * K, EZ = TZ + 2 * K;
-  static constexpr int EQ = EZ / 4;                   // z-quads per box row
-  static constexpr int SEG = SEG_;                    // y levels per thread
-  static constexpr int NSEG = (EY + SEG - 1) / SEG;
-  static constexpr int NT = NSEG * EX * EQ;           // one thread per (y segment, x, z-quad)
-  static constexpr int THREADS = (NT + 31) / 32 * 32;
-  static constexpr int XS0 = EY * EZ;
-  static constexpr int XS = XS0 + ((EZ % 32) - (XS0 % 32) + 64) % 32;  // x stride = EZ (mod 32)
-  static constexpr int BUF = EX * XS;                 // floats per shared buffer
-  // two pressure buffers (ping-pong) and the right-hand side
-  static constexpr int SMEM = 3 * BUF * (int)sizeof(float);
-  static_assert(K % 4 == 0 && TZ % 4 == 0, "z-quads stay aligned to the grid");
+  static constexpr int EQ = EZ / 4;        // 8 z-quads per box row
+  static constexpr int XSEG = 8;           // x levels per thread
+  static constexpr int NXS = EX / XSEG;    // x segments
+  static constexpr int THREADS = NXS * EY * EQ;
+  static constexpr int PL4 = EY * EQ;      // float4 per x plane of a buffer
+  static constexpr int BUF4 = EX * PL4;    // float4 per buffer
+  static constexpr int SMEM = 2 * BUF4 * (int)sizeof(float4);
+  static_assert(EQ == 8 && EX % XSEG == 0 && EY % 4 == 0, "a warp is 4 whole rows of one x segment");
   static_assert(THREADS <= 1024, "too many threads for one CTA");
+  static_assert(SMEM <= 232448, "two buffers must fit in shared memory");
   static_assert(TX % kBrick == 0 && TY % kBrick == 0 && TZ % kBrick == 0, "tiles are whole bricks");
-  static_assert(XS % 32 == EZ % 32 && XS % 4 == 0, "padding");
-  static_assert(4 * SEG <= 64, "the fluid mask holds 16 levels of quads");
 };
-
-// A tile's box: origin (ex, ey, ez) and extent n* (clipped to the domain),
-// the tile's own cells [c*0, c*1) in box coordinates, and which faces are
 // cut (halo inside the domain) rather than domain walls.
 struct Box {
   int ex, ey, ez;
@@ -134,8 +143,44 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// One TMA tensor copy of a (32, EY, EX) box of a pressure buffer at (z, y, x)
+// into shared memory, completing on the mbarrier (expected bytes armed by the
+// same thread just before).
+__device__ __forceinline__ void tma_box_load(uint32_t dst, const CUtensorMap* map, int z, int y, int x,
+                                             uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(z), "r"(y), "r"(x), "r"(mbar)
+      : "memory");
+}
+
+// Bounded wait for phase `parity` of an mbarrier: false after spin_limit
+// polls or one second.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity, unsigned spin_limit) {
+  const unsigned long long t0 = global_ns();
+  for (unsigned i = 0;; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (i > spin_limit || ((i & 255u) == 0u && global_ns() - t0 > 1000000000ull)) return false;
+  }
+}
+
 // Bounded grid barrier on a counter that only grows (arrival e waits for
-// e * gridDim.x arrivals).  Gives up after spin_limit polls or one second,
+// e * gridDim.x arrivals): the CTA's writes are published by thread 0's
+// release add after the CTA barrier (release is cumulative over what the CTA
+// barrier ordered before it) and the others' are seen through the acquire
+// poll.  Gives up after spin_limit polls or one second,
 // whichever comes first: it then sets *fail and returns false, and after any
 // failure every barrier returns false at once.
 __device__ __forceinline__ bool res_barrier(unsigned int* bar, unsigned target, int* fail, unsigned spin_limit) {
@@ -146,8 +191,7 @@ __device__ __forceinline__ bool res_barrier(unsigned int* bar, unsigned target, 
     if (*reinterpret_cast<volatile int*>(fail)) {
       ok = 0;
     } else {
-      __threadfence();
-      atomicAdd(bar, 1u);
+      asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
       unsigned spins = 0;
       const unsigned long long t0 = global_ns();
       while (ld_acquire_u32(bar) < target) {
@@ -158,7 +202,6 @@ __device__ __forceinline__ bool res_barrier(unsigned int* bar, unsigned target, 
           break;
         }
       }
-      __threadfence();
     }
     s_ok = ok;
   }
@@ -180,40 +223,11 @@ __device__ __forceinline__ double cta_sum(double v, double* s_red) {
   return t;  // valid in thread 0
 }
 
+
 // The quotients of a quad whose sums leave the fast path: IEEE divides, out
 // of line so the common path carries no predicated copy of them.
-__device__ __noinline__ float4 div6_quad_slow(float4 s, unsigned f) {
-  return make_float4((f & 1u) ? __fdiv_rn(s.x, 6.f) : 0.f, (f & 2u) ? __fdiv_rn(s.y, 6.f) : 0.f,
-                     (f & 4u) ? __fdiv_rn(s.z, 6.f) : 0.f, (f & 8u) ? __fdiv_rn(s.w, 6.f) : 0.f);
-}
-
-// The rhs of a non-fluid cell in the resident solve's shared copy: a NaN
-// payload no arithmetic produces (the GPU's NaN results are the canonical
-// 0x7fffffff, and the rhs comes from the divergence stage's arithmetic).
-constexpr unsigned kNotFluidBits = 0x7fc0a11au;
-#define kNotFluid __uint_as_float(kNotFluidBits)
-__device__ __forceinline__ unsigned fluid_bits(const float4& b) {
-  return (__float_as_uint(b.x) != kNotFluidBits ? 1u : 0u) | (__float_as_uint(b.y) != kNotFluidBits ? 2u : 0u) |
-         (__float_as_uint(b.z) != kNotFluidBits ? 4u : 0u) | (__float_as_uint(b.w) != kNotFluidBits ? 8u : 0u);
-}
-
-// One Jacobi update of a z-quad: p' = (x+1, x-1, y+1, y-1, z+1, z-1 summed in
-// that order, + rhs) / 6 on fluid cells (bits 0-3 of f), 0 elsewhere.
-__device__ __forceinline__ float4 quad_update(const float4& xp, const float4& xm, const float4& yp, const float4& ym,
-                                              const float4& pc, float zl, float zh, const float4& b, unsigned f) {
-  float4 s;
-  s.x = xp.x + xm.x; s.x += yp.x; s.x += ym.x; s.x += pc.y; s.x += zl; s.x += b.x;
-  s.y = xp.y + xm.y; s.y += yp.y; s.y += ym.y; s.y += pc.z; s.y += pc.x; s.y += b.y;
-  s.z = xp.z + xm.z; s.z += yp.z; s.z += ym.z; s.z += pc.w; s.z += pc.y; s.z += b.z;
-  s.w = xp.w + xm.w; s.w += yp.w; s.w += ym.w; s.w += zh; s.w += pc.z; s.w += b.w;
-  // one warp-uniform test: the rare quads leaving the fast path take the IEEE divides
-  const bool slow = ((f & 1u) && !div6_fast_ok(s.x)) || ((f & 2u) && !div6_fast_ok(s.y)) ||
-                    ((f & 4u) && !div6_fast_ok(s.z)) || ((f & 8u) && !div6_fast_ok(s.w));
-  if (__any_sync(__activemask(), slow)) {
-    if (slow) return div6_quad_slow(s, f);
-  }
-  return make_float4((f & 1u) ? div6_fast(s.x) : 0.f, (f & 2u) ? div6_fast(s.y) : 0.f,
-                     (f & 4u) ? div6_fast(s.z) : 0.f, (f & 8u) ? div6_fast(s.w) : 0.f);
+__device__ __noinline__ float4 div6_quad_slow(float4 s) {
+  return make_float4(__fdiv_rn(s.x, 6.f), __fdiv_rn(s.y, 6.f), __fdiv_rn(s.z, 6.f), __fdiv_rn(s.w, 6.f));
 }
 
 // FP64 ||b - A p||^2 of the fluid cells (bits 0-3 of f) of a z-quad, in cell
@@ -243,17 +257,22 @@ __device__ __forceinline__ double quad_residual(const float4& xp, const float4& 
   return acc;
 }
 
-template <int TX, int TY, int TZ, int K, int SEG_>
-__global__ void __launch_bounds__(Res<TX, TY, TZ, K, SEG_>::THREADS, 1)
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(Res<TX, TY>::THREADS, 1)
     k_resident_solve(Dims d, float* __restrict__ pa, float* __restrict__ pb, const float* __restrict__ rhs,
                      const int8_t* __restrict__ type, const int* __restrict__ tiles, const int* __restrict__ n_tiles,
                      unsigned int* __restrict__ bar, double* __restrict__ part, SolveState* __restrict__ ss,
-                     int fixed_sweeps, int check, int max_iters, double tol, BarrierTest bt) {
-  using R = Res<TX, TY, TZ, K, SEG_>;
-  constexpr int SEG = R::SEG, EQ = R::EQ, XS4 = R::XS / 4;
-  extern __shared__ float4 smem4[];  // [3][EX][XS / 4]: p, p, rhs; x; (y * EZ + z) / 4
+                     int fixed_sweeps, int check, int max_iters, double tol, BarrierTest bt,
+                     const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b) {
+  using R = Res<TX, TY>;
+  constexpr int EQ = R::EQ, PL4 = R::PL4, XSEG = R::XSEG, K = R::K;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(128) float4 smem4[];  // [2][EX][EY][EQ]; TMA destinations are 128-byte aligned
   __shared__ double s_red[32];
   __shared__ double s_r2;
+  __shared__ Box s_box;  // the resident tile's box (read where used: no registers held across the solve)
+  __shared__ __align__(8) uint64_t s_mbar;  // completion of the box's TMA copy
 
   const int G = gridDim.x, cta = blockIdx.x;
   // test hook: this CTA never arrives at a barrier (a participant that does
@@ -264,117 +283,147 @@ __global__ void __launch_bounds__(Res<TX, TY, TZ, K, SEG_>::THREADS, 1)
   const int n = *n_tiles;
   const bool resident = n <= G;
   const int tid = threadIdx.x;
-  const bool thr = tid < R::NT;
-  // this thread: z-quad q of box row cx, levels [y0, y0 + SEG) of the box
-  const int q = tid % EQ, cx = (tid / EQ) % R::EX, y0 = (tid / (EQ * R::EX)) * SEG;
+  // this thread: z-quad qq of box row ly, x levels [xa, xa + XSEG)
+  const int qq = tid % EQ, ly = (tid / EQ) % R::EY, xa = (tid / (EQ * R::EY)) * XSEG;
+  const int col = ly * EQ + qq;
   const int it0 = ss->iterations;  // sweeps a warm start already did
 
-  unsigned long long fl = 0ull;  // bit 4(ly - y0) + c: cell c of the quad at level ly is fluid
-  float4* RB = smem4 + 2 * (R::BUF / 4);  // the rhs of the box
-  float* g[2] = {pa, pb};
-  int cur = 0;  // global buffer of the current iterate
+  float4 rb[XSEG];  // rhs of this thread's quads (0 on non-fluid cells)
+  unsigned fl = 0u;  // bit 4 j + c: cell c of the quad at level xa + j is fluid
+  int cur = 0;  // global buffer of the current iterate (0: pa, 1: pb)
   int par = 0;  // shared buffer of the current iterate
-  const int col_i = cx * XS4 + q;  // shared index of level 0 of this thread's quad column
 
-  // This thread's quads of box t from global buffer src into shared buffer
-  // par (all of them, with rhs and fluid bits, when `full`; else those
-  // outside the tile's own cells, whose current values are already there).
-  auto load = [&](const Box& t, const float* __restrict__ src, bool full) {
-    const bool col = thr && cx < t.nx && 4 * q < t.nz;
-    const bool ownq = col && cx >= t.cx0 && cx < t.cx1 && 4 * q >= t.cz0 && 4 * q < t.cz1;
-    if (full) fl = 0ull;
-    if (col) {
-      const int base = ((t.ex + cx) * d.sy + t.ey + y0) * d.sz + t.ez + 4 * q;
-      float4* S = smem4 + par * (R::BUF / 4) + col_i;
+  // both buffers zero once: cells no box covers stay finite
+  for (int i = tid; i < 2 * R::BUF4; i += R::THREADS) smem4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t mbar = smem_addr(&s_mbar);
+  uint32_t tma_phase = 0;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+
+  // Box t of global buffer `which` (0: pa, 1: pb) into shared buffer par by
+  // one TMA copy of the whole (32, EY, EX) box (the tile's own cells come
+  // back as the block stored them; cells past the domain read 0), and with
+  // `full` this thread's rhs and fluid marks into registers.  Returns false,
+  // CTA-uniformly, if the copy did not complete within the bounded wait.
+  auto load = [&](const Box& t, int which, bool full) -> bool {
+    if (tid == 0) {
+      // order this CTA's earlier shared accesses and the other CTAs' global
+      // stores (acquired at the grid barrier) before the async-proxy copy
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      tma_box_load(smem_addr(smem4 + par * R::BUF4), which ? &map_b : &map_a, t.ez, t.ey, t.ex, mbar,
+                   (uint32_t)R::BUF4 * 16u);
+    }
+    if (full) {
+      const bool colin = ly < t.ny && 4 * qq < t.nz;
+      const int base = (t.ex * d.sy + t.ey + ly) * d.sz + t.ez + 4 * qq;
+      fl = 0u;
 #pragma unroll
-      for (int j = 0; j < SEG; ++j) {
-        const int ly = y0 + j;
-        if (ly < t.ny) {
-          const int c = base + j * d.sz;
-          if (full || !ownq || ly < t.cy0 || ly >= t.cy1) S[ly * EQ] = __ldcg(reinterpret_cast<const float4*>(src + c));
-          if (full) {
-            // non-fluid cells carry a NaN sentinel instead of their rhs (which
-            // they never use): the sweep reads the fluid mark with the rhs
-            float4 rb = __ldg(reinterpret_cast<const float4*>(rhs + c));
-            const char4 ty = *reinterpret_cast<const char4*>(type + c);
-            if (ty.x != kFluid) rb.x = kNotFluid;
-            if (ty.y != kFluid) rb.y = kNotFluid;
-            if (ty.z != kFluid) rb.z = kNotFluid;
-            if (ty.w != kFluid) rb.w = kNotFluid;
-            RB[col_i + ly * EQ] = rb;
-            fl |= (unsigned long long)((ty.x == kFluid ? 1u : 0u) | (ty.y == kFluid ? 2u : 0u) |
-                                       (ty.z == kFluid ? 4u : 0u) | (ty.w == kFluid ? 8u : 0u))
-                  << (4 * j);
-          }
+      for (int j = 0; j < XSEG; ++j) {
+        const int x = xa + j;
+        rb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (colin && x < t.nx) {
+          const int c = base + x * d.sy * d.sz;
+          const char4 ty = *reinterpret_cast<const char4*>(type + c);
+          const unsigned f = (ty.x == kFluid ? 1u : 0u) | (ty.y == kFluid ? 2u : 0u) | (ty.z == kFluid ? 4u : 0u) |
+                             (ty.w == kFluid ? 8u : 0u);
+          fl |= f << (4 * j);
+          if (f) rb[j] = __ldg(reinterpret_cast<const float4*>(rhs + c));
         }
       }
     }
-    __syncthreads();
+    bool done = mbar_wait_bounded(mbar, tma_phase, spin_limit);
+    if (!done) {
+      atomicExch(fail, 1);
+      done = mbar_wait_bounded(mbar, tma_phase, spin_limit);  // the copy in flight, bounded again
+    }
+    tma_phase ^= 1u;
+    return __syncthreads_and(done) != 0;
   };
 
-  // Sweep s (1-based) of a block on box t: shared buffer par -> par ^ 1.  The
-  // sweep's region (every cell at least s cells inside each cut face) is cut
-  // into rows of z-quads; the CTA's lanes take consecutive quads of
-  // consecutive rows, so every lane has work and a warp's loads of a level
-  // are contiguous.  A wall neighbour is the cell itself (offset 0).
+  // Sweep s (1-based) of a block on box t: shared buffer par -> par ^ 1, over
+  // the region of cells at least s cells inside each cut face (whole quads:
+  // a quad's cells outside the region are never read by cells inside it).
+  // Wall neighbours are the cell itself.
   auto sweep = [&](const Box& t, int s) {
     const int xlo = (t.cut & 1) ? s : 0, xhi = t.nx - ((t.cut & 2) ? s : 0);
     const int ylo = (t.cut & 4) ? s : 0, yhi = t.ny - ((t.cut & 8) ? s : 0);
     const int zlo = (t.cut & 16) ? s : 0, zhi = t.nz - ((t.cut & 32) ? s : 0);
-    // quads holding a cell of [zlo, zhi); their other cells are invalid and never read by valid ones
-    const int qlo = zlo / 4, qhi = (zhi + 3) / 4;
-    const int nq = qhi - qlo, ny = yhi - ylo;
-    const int total = (xhi - xlo) * ny * nq;
-    const float inv_nq = 1.f / (float)nq, inv_ny = 1.f / (float)ny;
-    const bool ywall_lo = t.ey == 0, ywall_hi = t.ey + t.ny == d.sy;
-    const float4* S = smem4 + par * (R::BUF / 4);
-    float4* D = smem4 + (par ^ 1) * (R::BUF / 4);
-    for (int it = tid; it < total; it += R::THREADS) {
-      // it = (xr * ny + yr) * nq + qr; small integers, so the float quotients are exact
-      const int rq = __float2int_rz(((float)it + 0.5f) * inv_nq);
-      const int qr = it - rq * nq;
-      const int xr = __float2int_rz(((float)rq + 0.5f) * inv_ny);
-      const int yr = rq - xr * ny;
-      const int x = xlo + xr, ly = ylo + yr, qq = qlo + qr;
-      const int i = x * XS4 + ly * EQ + qq;
-      const int gx = t.ex + x, gz = t.ez + 4 * qq;
-      const float4 pc = S[i];
-      const float4 xm = S[i + (gx == 0 ? 0 : -XS4)];
-      const float4 xp = S[i + (gx == d.sx - 1 ? 0 : XS4)];
-      const float4 ym = (ly == 0 && ywall_lo) ? pc : S[i - (ly > 0 ? EQ : 0)];
-      const float4 yp = (ly == t.ny - 1 && ywall_hi) ? pc : S[i + EQ];
-      const float* Sf = reinterpret_cast<const float*>(S + i);
-      const float zl = Sf[(gz == 0 || qq == 0) ? 0 : -1];
-      const float zh = Sf[(gz + 4 == d.sz || qq == EQ - 1) ? 3 : 4];
-      const float4 b = RB[i];
-      D[i] = quad_update(xp, xm, yp, ym, pc, zl, zh, b, fluid_bits(b));
+    const bool act = ly >= ylo && ly < yhi && 4 * qq + 4 > zlo && 4 * qq < zhi;
+    const bool zl_self = qq == 0, zh_self = 4 * qq + 4 >= t.nz;
+    const float4* S = smem4 + par * R::BUF4 + col;
+    // ly == 0 and ly == ny - 1 are in the region only at walls; rows past the
+    // box (clipped boxes) read their own column, so no read leaves the buffer
+    const float4* Sym = S - (ly == 0 ? 0 : EQ);
+    const float4* Syp = S + (ly >= t.ny - 1 ? 0 : EQ);
+    float4* D = smem4 + (par ^ 1) * R::BUF4 + col;
+    if (xa < xhi && xa + XSEG > xlo) {  // warp-uniform
+      float4 pc = S[xa * PL4];
+      float4 pm = xa > 0 ? S[(xa - 1) * PL4] : pc;  // x == 0 in the region only at a wall
+#pragma unroll
+      for (int j = 0; j < XSEG; ++j) {
+        const int x = xa + j;
+        const float4 pn = x + 1 < t.nx ? S[(x + 1) * PL4] : pc;
+        if (x >= xlo && x < xhi) {
+          float zl = __shfl_up_sync(FULL, pc.w, 1), zh = __shfl_down_sync(FULL, pc.x, 1);
+          if (zl_self) zl = pc.x;  // box z face: a wall, or a cell outside the region
+          if (zh_self) zh = pc.w;
+          const float4 ym = Sym[x * PL4], yp = Syp[x * PL4];
+          const float4 b = rb[j];
+          float4 sm;
+          sm.x = pn.x + pm.x; sm.x += yp.x; sm.x += ym.x; sm.x += pc.y; sm.x += zl; sm.x += b.x;
+          sm.y = pn.y + pm.y; sm.y += yp.y; sm.y += ym.y; sm.y += pc.z; sm.y += pc.x; sm.y += b.y;
+          sm.z = pn.z + pm.z; sm.z += yp.z; sm.z += ym.z; sm.z += pc.w; sm.z += pc.y; sm.z += b.z;
+          sm.w = pn.w + pm.w; sm.w += yp.w; sm.w += ym.w; sm.w += zh; sm.w += pc.z; sm.w += b.w;
+          const bool ok = !act || div6_quad_fast_ok(sm);
+          float4 qv;
+          if (ok) {
+            qv = make_float4(div6_fast(sm.x), div6_fast(sm.y), div6_fast(sm.z), div6_fast(sm.w));
+          } else {
+            qv = div6_quad_slow(sm);
+          }
+          const unsigned f = (fl >> (4 * j)) & 15u;
+          qv.x = (f & 1u) ? qv.x : 0.f;
+          qv.y = (f & 2u) ? qv.y : 0.f;
+          qv.z = (f & 4u) ? qv.z : 0.f;
+          qv.w = (f & 8u) ? qv.w : 0.f;
+          if (act) D[x * PL4] = qv;
+        }
+        pm = pc;
+        pc = pn;
+      }
     }
     __syncthreads();
     par ^= 1;
   };
 
   // ||b - A p||^2 over this thread's own fluid cells of box t (shared buffer
-  // par current), FP64, in level order; summed over the CTA in a fixed order.
+  // par current), FP64, in x order; summed over the CTA in a fixed order.
   auto residual = [&](const Box& t) -> double {
     double acc = 0.0;
-    const bool ownq = thr && cx >= t.cx0 && cx < t.cx1 && 4 * q >= t.cz0 && 4 * q < t.cz1;
-    const int lo = max(t.cy0, y0), hi = min(t.cy1, y0 + SEG);
-    if (ownq && lo < hi) {
-      const int gx = t.ex + cx, gz = t.ez + 4 * q;
-      const int oxm = gx == 0 ? 0 : -XS4, oxp = gx == d.sx - 1 ? 0 : XS4;
-      const int ozl = (gz == 0 || q == 0) ? 0 : -1, ozh = (gz + 4 == d.sz || q == EQ - 1) ? 3 : 4;
-      const float4* S = smem4 + par * (R::BUF / 4) + col_i;
-      const float4* Rb = RB + col_i;
-      for (int ly = lo; ly < hi; ++ly) {
-        const unsigned f = (unsigned)(fl >> (4 * (ly - y0))) & 15u;
-        if (!f) continue;
-        const int i = ly * EQ, gy = t.ey + ly;
-        const float4 pc = S[i];
-        const float4 ym = gy == 0 ? pc : S[i - EQ];
-        const float4 yp = gy == d.sy - 1 ? pc : S[i + EQ];
-        const float zl = reinterpret_cast<const float*>(S + i)[ozl];
-        const float zh = reinterpret_cast<const float*>(S + i)[ozh];
-        acc += quad_residual(S[i + oxp], S[i + oxm], yp, ym, pc, zl, zh, Rb[i], f);
+    const bool owncol = ly < t.ny && 4 * qq < t.nz && ly >= t.cy0 && ly < t.cy1 && 4 * qq >= t.cz0 && 4 * qq < t.cz1;
+    const bool zl_self = qq == 0, zh_self = 4 * qq + 4 >= t.nz;
+    const float4* S = smem4 + par * R::BUF4 + col;
+    const float4* Sym = S - (ly == 0 ? 0 : EQ);
+    const float4* Syp = S + (ly >= t.ny - 1 ? 0 : EQ);
+    if (xa < t.cx1 && xa + XSEG > t.cx0) {
+      float4 pc = S[xa * PL4];
+      float4 pm = xa > 0 ? S[(xa - 1) * PL4] : pc;
+#pragma unroll
+      for (int j = 0; j < XSEG; ++j) {
+        const int x = xa + j;
+        const float4 pn = x + 1 < t.nx ? S[(x + 1) * PL4] : pc;
+        if (x >= t.cx0 && x < t.cx1) {
+          float zl = __shfl_up_sync(FULL, pc.w, 1), zh = __shfl_down_sync(FULL, pc.x, 1);
+          if (zl_self) zl = pc.x;
+          if (zh_self) zh = pc.w;
+          const unsigned f = owncol ? (fl >> (4 * j)) & 15u : 0u;
+          if (f) acc += quad_residual(pn, pm, Syp[x * PL4], Sym[x * PL4], pc, zl, zh, rb[j], f);
+        }
+        pm = pc;
+        pc = pn;
       }
     }
     return cta_sum<R::THREADS>(acc, s_red);
@@ -382,37 +431,40 @@ __global__ void __launch_bounds__(Res<TX, TY, TZ, K, SEG_>::THREADS, 1)
 
   // This thread's own cells of box t from shared buffer par into dst.
   auto store = [&](const Box& t, float* __restrict__ dst) {
-    const bool ownq = thr && cx >= t.cx0 && cx < t.cx1 && 4 * q >= t.cz0 && 4 * q < t.cz1;
-    const int lo = max(t.cy0, y0), hi = min(t.cy1, y0 + SEG);
-    if (ownq) {
-      const float4* S = smem4 + par * (R::BUF / 4) + col_i;
-      const int base = ((t.ex + cx) * d.sy + t.ey) * d.sz + t.ez + 4 * q;
-      for (int ly = lo; ly < hi; ++ly) *reinterpret_cast<float4*>(dst + base + ly * d.sz) = S[ly * EQ];
+    const bool owncol = ly < t.ny && 4 * qq < t.nz && ly >= t.cy0 && ly < t.cy1 && 4 * qq >= t.cz0 && 4 * qq < t.cz1;
+    if (owncol) {
+      const float4* S = smem4 + par * R::BUF4 + col;
+      const int base = (t.ex * d.sy + t.ey + ly) * d.sz + t.ez + 4 * qq;
+#pragma unroll
+      for (int j = 0; j < XSEG; ++j) {
+        const int x = xa + j;
+        if (x >= t.cx0 && x < t.cx1) *reinterpret_cast<float4*>(dst + base + x * d.sy * d.sz) = S[x * PL4];
+      }
     }
   };
 
-  Box T{};
   const bool have = resident && cta < n;
-  if (have) {
-    T = box_of<TX, TY, TZ, K>(d, tiles[cta]);
-    load(T, g[cur], true);
-  }
+  if (have && tid == 0) s_box = box_of<TX, TY, R::TZ, K>(d, tiles[cta]);
+  __syncthreads();
+  const Box& T = s_box;
+  bool ok = true;
+  if (have) ok = load(T, 0, true);
   unsigned epoch = 0;
   int done = 0, checks = 0;
-  bool ok = true;
   double r2 = -1.0, rel = -1.0;
-  for (;;) {
+  while (ok) {
     const bool due = fixed_sweeps > 0 ? done >= fixed_sweeps : (done > 0 && done % check == 0);
     if (due) {
       double acc = 0.0;
       if (resident) {
         if (have) acc = residual(T);
       } else {
-        for (int j = cta; j < n; j += G) {
-          const Box t = box_of<TX, TY, TZ, K>(d, tiles[j]);
-          load(t, g[cur], true);
-          acc += residual(t);  // thread 0's running sum, tiles in order
+        for (int j = cta; j < n && ok; j += G) {
+          const Box t = box_of<TX, TY, R::TZ, K>(d, tiles[j]);
+          ok = load(t, cur, true);
+          if (ok) acc += residual(t);  // thread 0's running sum, tiles in order
         }
+        if (!ok) break;
       }
       if (tid == 0) part[cta] = acc;
       ok = ok && res_barrier(bar, ++epoch * (unsigned)G, fail, spin_limit);
@@ -436,21 +488,23 @@ __global__ void __launch_bounds__(Res<TX, TY, TZ, K, SEG_>::THREADS, 1)
     if (resident) {
       if (have) {
         for (int s = 1; s <= nsw; ++s) sweep(T, s);
-        store(T, g[cur ^ 1]);
+        store(T, cur ? pa : pb);
       }
     } else {
-      for (int j = cta; j < n; j += G) {
-        const Box t = box_of<TX, TY, TZ, K>(d, tiles[j]);
-        load(t, g[cur], true);
+      for (int j = cta; j < n && ok; j += G) {
+        const Box t = box_of<TX, TY, R::TZ, K>(d, tiles[j]);
+        ok = load(t, cur, true);
+        if (!ok) break;
         for (int s = 1; s <= nsw; ++s) sweep(t, s);
-        store(t, g[cur ^ 1]);
+        store(t, cur ? pa : pb);
       }
+      if (!ok) break;
     }
     done += nsw;
     ok = ok && res_barrier(bar, ++epoch * (unsigned)G, fail, spin_limit);
     if (!ok) break;
     cur ^= 1;
-    if (have) load(T, g[cur], false);  // the halo of the new iterate
+    if (have) ok = load(T, cur, false);  // the box of the new iterate
   }
 
   // the result belongs in pa
@@ -459,15 +513,16 @@ __global__ void __launch_bounds__(Res<TX, TY, TZ, K, SEG_>::THREADS, 1)
       if (have) store(T, pa);
     } else {
       for (int j = cta; j < n; j += G) {
-        const Box t = box_of<TX, TY, TZ, K>(d, tiles[j]);
-        const bool ownq = thr && cx >= t.cx0 && cx < t.cx1 && 4 * q >= t.cz0 && 4 * q < t.cz1;
-        if (ownq) {
-          const int base = ((t.ex + cx) * d.sy + t.ey + y0) * d.sz + t.ez + 4 * q;
-          for (int jj = 0; jj < SEG; ++jj) {
-            const int ly = y0 + jj;
-            if (ly >= t.cy0 && ly < t.cy1)
-              *reinterpret_cast<float4*>(pa + base + jj * d.sz) =
-                  __ldcg(reinterpret_cast<const float4*>(pb + base + jj * d.sz));
+        const Box t = box_of<TX, TY, R::TZ, K>(d, tiles[j]);
+        const bool owncol =
+            ly < t.ny && 4 * qq < t.nz && ly >= t.cy0 && ly < t.cy1 && 4 * qq >= t.cz0 && 4 * qq < t.cz1;
+        if (owncol) {
+          const int base = (t.ex * d.sy + t.ey + ly) * d.sz + t.ez + 4 * qq;
+          for (int jj = 0; jj < XSEG; ++jj) {
+            const int x = xa + jj;
+            if (x >= t.cx0 && x < t.cx1)
+              *reinterpret_cast<float4*>(pa + base + x * d.sy * d.sz) =
+                  __ldcg(reinterpret_cast<const float4*>(pb + base + x * d.sy * d.sz));
           }
         }
       }
@@ -538,19 +593,51 @@ __global__ void __launch_bounds__(1024) k_tile_list(Dims d, int tbx, int tby, in
 struct ShapeInfo {
   int tx, ty, tz;
 };
-// Tile shapes of the resident plan (plan.xc indexes this table).
-// (6, 7: shape 0 with 8- and 5-level y segments: 576 and 960 threads)
-constexpr ShapeInfo kShapes[] = {{8, 40, 16}, {8, 32, 16}, {16, 16, 16}, {8, 24, 16}, {8, 16, 16},
-                                 {16, 24, 16}, {8, 40, 16}, {8, 40, 16}};
+// Tile shapes of the resident plan (plan.xc indexes this table); z is 24
+// cells (a 32-cell box) for all.
+constexpr ShapeInfo kShapes[] = {{8, 40, 24}, {16, 24, 24}, {8, 32, 24}, {16, 16, 24},
+                                 {8, 16, 24}, {24, 16, 24}, {8, 48, 24}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
-template <int TX, int TY, int TZ, int K, int SEG>
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// Tensor map of a pressure buffer: 3D (z, y, x), fp32, boxes of (32, EY, EX)
+// cells, zero fill past the domain.
+template <int TX, int TY>
+cudaError_t box_map(CUtensorMap* m, const Dims& d, float* p) {
+  using R = Res<TX, TY>;
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || reinterpret_cast<uintptr_t>(p) % 16 != 0 || d.sz % 4 != 0) return cudaErrorInvalidValue;
+  const cuuint64_t dims[3] = {(cuuint64_t)d.sz, (cuuint64_t)d.sy, (cuuint64_t)d.sx};
+  const cuuint64_t strides[2] = {(cuuint64_t)d.sz * 4, (cuuint64_t)d.sy * d.sz * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)R::EZ, (cuuint32_t)R::EY, (cuuint32_t)R::EX};
+  const cuuint32_t es[3] = {1, 1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, p, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <int TX, int TY>
 cudaError_t launch_res(cudaStream_t st, const Dims& d, int ctas, float* pa, float* pb, const float* rhs,
                        const int8_t* type, const int* tiles, const int* n_tiles, unsigned int* bar, double* part,
                        SolveState* ss, int fixed_sweeps, int check, int max_iters, double tol, BarrierTest bt) {
-  using R = Res<TX, TY, TZ, K, SEG>;
-  auto fn = &k_resident_solve<TX, TY, TZ, K, SEG>;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, R::SMEM);
+  using R = Res<TX, TY>;
+  auto fn = &k_resident_solve<TX, TY>;
+  CUtensorMap ma, mb;
+  cudaError_t e = box_map<TX, TY>(&ma, d, pa);
+  if (e == cudaSuccess) e = box_map<TX, TY>(&mb, d, pb);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, R::SMEM);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t lc = {};
   lc.gridDim = dim3(ctas);
@@ -563,13 +650,13 @@ cudaError_t launch_res(cudaStream_t st, const Dims& d, int ctas, float* pa, floa
   lc.attrs = at;
   lc.numAttrs = 1;
   return cudaLaunchKernelEx(&lc, fn, d, pa, pb, rhs, type, tiles, n_tiles, bar, part, ss, fixed_sweeps, check,
-                            max_iters, tol, bt);
+                            max_iters, tol, bt, ma, mb);
 }
 
-template <int TX, int TY, int TZ, int K, int SEG>
+template <int TX, int TY>
 int occupancy_of(int device) {
-  using R = Res<TX, TY, TZ, K, SEG>;
-  auto fn = &k_resident_solve<TX, TY, TZ, K, SEG>;
+  using R = Res<TX, TY>;
+  auto fn = &k_resident_solve<TX, TY>;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, R::SMEM) != cudaSuccess) return 0;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, R::THREADS, R::SMEM) != cudaSuccess) return 0;
@@ -578,27 +665,26 @@ int occupancy_of(int device) {
   return per_sm >= 1 ? sms : 0;  // one CTA per SM
 }
 
-// Dispatch over (shape, K): calls f.template operator()<TX, TY, TZ, K, SEG>().
+// Dispatch over the shape: calls f.template operator()<TX, TY>().
 template <typename F>
-auto dispatch(int shape, int k, const F& f) -> decltype(f.template operator()<8, 40, 16, 4, 12>()) {
-#define AQ_RES_CASE(S, A, B, C, G) \
-  if (shape == S && k == 4) return f.template operator()<A, B, C, 4, G>();
-  AQ_RES_CASE(0, 8, 40, 16, 12)
-  AQ_RES_CASE(1, 8, 32, 16, 12)
-  AQ_RES_CASE(2, 16, 16, 16, 8)
-  AQ_RES_CASE(3, 8, 24, 16, 8)
-  AQ_RES_CASE(4, 8, 16, 16, 8)
-  AQ_RES_CASE(5, 16, 24, 16, 12)
-  AQ_RES_CASE(6, 8, 40, 16, 8)
-  AQ_RES_CASE(7, 8, 40, 16, 5)
+auto dispatch(int shape, const F& f) -> decltype(f.template operator()<8, 40>()) {
+#define AQ_RES_CASE(S, A, B) \
+  if (shape == S) return f.template operator()<A, B>();
+  AQ_RES_CASE(0, 8, 40)
+  AQ_RES_CASE(1, 16, 24)
+  AQ_RES_CASE(2, 8, 32)
+  AQ_RES_CASE(3, 16, 16)
+  AQ_RES_CASE(4, 8, 16)
+  AQ_RES_CASE(5, 24, 16)
+  AQ_RES_CASE(6, 8, 48)
 #undef AQ_RES_CASE
-  return decltype(f.template operator()<8, 40, 16, 4, 12>())();
+  return decltype(f.template operator()<8, 40>())();
 }
 
 struct OccupancyOf {
   int device;
-  template <int A, int B, int C, int D, int E>
-  int operator()() const { return occupancy_of<A, B, C, D, E>(device); }
+  template <int A, int B>
+  int operator()() const { return occupancy_of<A, B>(device); }
 };
 
 struct LaunchRes {
@@ -616,10 +702,10 @@ struct LaunchRes {
   int fixed_sweeps, check, max_iters;
   double tol;
   BarrierTest bt;
-  template <int A, int B, int C, int D, int E>
+  template <int A, int B>
   cudaError_t operator()() const {
-    return launch_res<A, B, C, D, E>(st, d, ctas, pa, pb, rhs, type, tiles, n_tiles, bar, part, ss, fixed_sweeps, check,
-                                  max_iters, tol, bt);
+    return launch_res<A, B>(st, d, ctas, pa, pb, rhs, type, tiles, n_tiles, bar, part, ss, fixed_sweeps, check,
+                            max_iters, tol, bt);
   }
 };
 
@@ -638,7 +724,7 @@ int resident_tile_capacity(const Dims& d) {
 
 int resident_ctas(int device, int shape, int k) {
   if (!resident_plan_ok(shape, k)) return 0;
-  return dispatch(shape, k, OccupancyOf{device});
+  return dispatch(shape, OccupancyOf{device});
 }
 
 long long resident_cells_updated(const Dims& d, int shape, const uint8_t* bact_host) {
@@ -671,7 +757,7 @@ cudaError_t launch_resident_solve(cudaStream_t st, const Dims& d, int shape, int
   k_tile_list<<<1, 1024, 0, st>>>(d, s.tx / kBrick, s.ty / kBrick, s.tz / kBrick, bact, tiles, n_tiles, bar);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  return dispatch(shape, k,
+  return dispatch(shape,
                   LaunchRes{st, d, ctas, pa, pb, rhs, type, tiles, n_tiles, bar, part, ss, fixed_sweeps, check,
                             max_iters, tol, bt});
 }

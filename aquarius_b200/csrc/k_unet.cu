@@ -284,6 +284,11 @@ __global__ void __launch_bounds__(256) k_conv3_fwd_tile(const bf16* __restrict__
 // bounded (a timeout is recorded in g_umma_timeout; the kernel then frees its
 // TMEM without storing), results read back with tcgen05.ld.
 __device__ int g_umma_timeout;
+// Test hook of the bounded wait: when set, the issuing thread neither issues
+// the MMAs nor commits (nothing is left in flight), so every thread's wait
+// runs out; g_umma_wait_ns bounds the wait (default one second).
+__device__ int g_umma_test_skip;
+__device__ unsigned long long g_umma_wait_ns = 1000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -321,11 +326,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
   return done != 0;
 }
 
+__device__ __forceinline__ unsigned long long umma_now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Bounded wait on an mbarrier phase; false (and the timeout recorded) if it
-// does not complete within the limit.
+// does not complete within g_umma_wait_ns or 2^22 polls, whichever is first.
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
-  for (int i = 0; i < (1 << 22); ++i)
+  const unsigned long long t0 = umma_now_ns(), limit = g_umma_wait_ns;
+  for (int i = 0; i < (1 << 22); ++i) {
     if (mbar_try_wait(mbar, parity)) return true;
+    if ((i & 255) == 255 && umma_now_ns() - t0 > limit) break;
+  }
   atomicExch(&g_umma_timeout, 1);
   return false;
 }
@@ -419,7 +433,7 @@ __global__ void __launch_bounds__(256) k_conv3_fwd_umma(const bf16* __restrict__
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = s_tmem;
-  if (tid == 0) {
+  if (tid == 0 && !g_umma_test_skip) {
     const uint32_t h0 = smem_u32(sH), b0 = smem_u32(sB);
     for (int tap = 0; tap < 27; ++tap) {
       int dx, dy, dz;
@@ -962,6 +976,15 @@ int conv_umma_timeouts() {
   int v = 0;
   cudaMemcpyFromSymbol(&v, g_umma_timeout, sizeof(int));
   return v;
+}
+
+cudaError_t conv_umma_test_hook(int skip, unsigned long long wait_ns) {
+  const int zero = 0;
+  const unsigned long long ns = wait_ns ? wait_ns : 1000000000ull;
+  cudaError_t e = cudaMemcpyToSymbol(g_umma_test_skip, &skip, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_umma_wait_ns, &ns, sizeof(ns));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_umma_timeout, &zero, sizeof(int));
+  return e;
 }
 
 int unet_wgrad_chunk(int voxels) {

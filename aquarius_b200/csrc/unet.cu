@@ -286,6 +286,13 @@ aq_status aq_conv3_umma_status(int32_t* timeouts) {
   return AQ_OK;
 }
 
+aq_status aq_conv3_test_wait_timeout(int32_t skip_mma, uint64_t wait_ns) {
+  if (skip_mma != 0 && skip_mma != 1) return fail(AQ_ERR_INVALID_ARGUMENT, "skip_mma must be 0 or 1");
+  UN_CUDA(cudaDeviceSynchronize());
+  UN_CUDA(conv_umma_test_hook(skip_mma, (unsigned long long)wait_ns));
+  return AQ_OK;
+}
+
 aq_status aq_conv3_flip_transpose(int32_t cin, int32_t cout, const void* w, void* wt, void* stream) {
   if (!w || !wt) return fail(AQ_ERR_INVALID_ARGUMENT, "bad argument");
   UN_CUDA(launch_flip_transpose((cudaStream_t)stream, w, wt, cin, cout));

@@ -157,7 +157,7 @@ def jacobi_kernel_name_of(plan) -> str:
     if rows == 3:
         return "k_jacobi_list (1 sweep/launch over the listed active warp rows, one resident wave)"
     if rows == 4:
-        shapes = ["8x40x16", "8x32x16", "16x16x16", "8x24x16", "8x16x16", "16x24x16", "8x40x16 (576 threads)"]
+        shapes = ["8x40x24", "16x24x24", "8x32x24", "16x16x24", "8x16x24", "24x16x24", "8x48x24"]
         return (f"k_resident_solve<tiles {shapes[xplanes]}, halo {levels}> (whole solve in one cooperative launch, "
                 f"tiles resident in shared memory, halos exchanged every {levels} sweeps)")
     if rows == 2:
@@ -1032,7 +1032,7 @@ def run_profile_case(case: str):
         f = aq.Fluid(workload_config(128, "zero"))
         f.step(3)
         f.synchronize()
-        f.set_jacobi_plan(4, 4, 7)
+        f.set_jacobi_plan(4, 4, 0)
         print(f.jacobi_plan(), f.benchmark_pressure(40))
         f.close()
     elif case == "batch-rows":

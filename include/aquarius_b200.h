@@ -280,9 +280,10 @@ aq_status aq_selfcheck_division(int32_t device, uint64_t* mismatches);
  * per launch over a list of the warp rows that hold fluid (levels 1,
  * x_planes 1; sz % 4 == 0).  rows = 4: the whole solve in one cooperative
  * launch of resident tiles: each CTA keeps a tile of the grid (x_planes
- * selects the shape: 0 8x40x16, 1 8x32x16, 2 16x16x16, 3 8x24x16, 4 8x16x16,
- * 5 16x24x16 cells, 6 8x40x16 with twice the threads) with a `levels`-cell halo (4) in shared memory for the
- * whole solve and exchanges halos every `levels` sweeps (sz % 4 == 0).  rows = 8, 16, 32:
+ * selects the shape: 0 8x40x24, 1 16x24x24, 2 8x32x24, 3 16x16x24,
+ * 4 8x16x24, 5 24x16x24, 6 8x48x24 cells) with a `levels`-cell halo (4) in
+ * shared memory for the whole solve and exchanges halos every `levels`
+ * sweeps (sz % 4 == 0).  rows = 8, 16, 32:
  * the temporally blocked kernel with `levels` sweeps (1, 2, 4, 8) per launch
  * over tiles of that many rows and x_planes planes.  Chosen per grid by the
  * tuner; invalid plans are rejected. */
@@ -421,6 +422,14 @@ aq_status aq_conv3_flip_transpose(int32_t cin, int32_t cout, const void* w, void
  * gave up waiting for its MMAs (its output is then not written). */
 aq_status aq_conv3_set_tiled(int32_t tiled);
 aq_status aq_conv3_umma_status(int32_t* timeouts);
+/* Test hook of the tcgen05 convolution's bounded mbarrier wait.  skip_mma = 1
+ * makes every later tcgen05 convolution issue no MMA and no commit (nothing is
+ * in flight), so each thread's wait gives up after wait_ns nanoseconds (0 = the
+ * default of one second): no output is written, TMEM is freed and
+ * aq_conv3_umma_status reports the timeout.  skip_mma = 0 restores normal
+ * operation with the default wait.  Either call synchronizes the device and
+ * clears the timeout record.  Test use only. */
+aq_status aq_conv3_test_wait_timeout(int32_t skip_mma, uint64_t wait_ns);
 
 /* ---- Learned pressure warm start: network, dataset, training ---------------
  * No counterpart in the reference.  A 3-level 3D U-Net (16/32/64 channels,

@@ -49,4 +49,20 @@ inline void aqref_record(cudaError_t err, const char* what, const char* file, in
 
 inline void printGLError() {}
 
+// The reference sizes the device printf FIFO when a Fluid is built
+// (Fluid/Fluid_3D_FLIP.cu:489).  CUDA refuses that call once any kernel with
+// printf has run in the process, which happens when a test builds a second
+// reference Fluid after stepping a first one.  The FIFO only bounds buffered
+// device printf output, never the simulation, so that refusal is not an
+// error here; every other limit and error passes through.
+inline cudaError_t aqref_device_set_limit(cudaLimit limit, size_t value) {
+  const cudaError_t e = cudaDeviceSetLimit(limit, value);
+  if (e == cudaErrorInvalidValue && limit == cudaLimitPrintfFifoSize) {
+    (void)cudaGetLastError();
+    return cudaSuccess;
+  }
+  return e;
+}
+#define cudaDeviceSetLimit aqref_device_set_limit
+
 #endif

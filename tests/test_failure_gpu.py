@@ -11,7 +11,12 @@ solve that stops short).
   test hook, a short poll limit) gives up: AQ_ERR_TIMEOUT, and the device
   keeps answering (the same fluid after an upload, and a new fluid checked
   against the oracle).
+* A tcgen05 convolution whose MMAs are never issued (test hook) gives up its
+  bounded mbarrier wait: nothing is written, aq_conv3_umma_status reports the
+  timeout, and with the hook off the same call matches PyTorch again.
 """
+import ctypes as ct
+
 import numpy as np
 import pytest
 
@@ -99,3 +104,46 @@ def test_persistent_barrier_timeout_leaves_device_usable(mode):
     assert rel_l2(a["pressure"], b["pressure"]) <= 1e-5
     g.close()
     o.close()
+
+
+def test_umma_wait_timeout_writes_nothing_and_recovers():
+    import torch
+    lib = aq.load_library()
+    P, I = ct.c_void_p, ct.c_int32
+    lib.aq_conv3_forward.restype = ct.c_int
+    lib.aq_conv3_forward.argtypes = [I, I, I, P, P, P, P, I, I, I, P]
+    lib.aq_conv3_set_tiled.argtypes = [I]
+    lib.aq_conv3_umma_status.restype = ct.c_int
+    lib.aq_conv3_umma_status.argtypes = [ct.POINTER(I)]
+    lib.aq_conv3_test_wait_timeout.restype = ct.c_int
+    lib.aq_conv3_test_wait_timeout.argtypes = [I, ct.c_uint64]
+    shape, cin, cout = (5, 6, 7), 16, 16
+    V = shape[0] * shape[1] * shape[2]
+    g = torch.Generator(device="cuda").manual_seed(11)
+    x = torch.randn(V, cin, device="cuda", generator=g).to(torch.bfloat16)
+    w = (torch.randn(27, cout, cin, device="cuda", generator=g) * 0.1).to(torch.bfloat16)
+    b = torch.randn(cout, device="cuda", generator=g)
+    sentinel = torch.full((V, cout), 7.0, device="cuda", dtype=torch.bfloat16)
+    out = sentinel.clone()
+    status = ct.c_int32(-1)
+    assert lib.aq_conv3_set_tiled(2) == 0
+    assert lib.aq_conv3_test_wait_timeout(1, 20_000_000) == 0  # 20 ms wait
+    try:
+        assert lib.aq_conv3_forward(cin, cout, 0, x.data_ptr(), w.data_ptr(), b.data_ptr(), out.data_ptr(),
+                                    *shape, None) == 0
+        torch.cuda.synchronize()
+        assert lib.aq_conv3_umma_status(ct.byref(status)) == 0
+        assert status.value != 0
+        assert torch.equal(out, sentinel)
+    finally:
+        assert lib.aq_conv3_test_wait_timeout(0, 0) == 0
+    assert lib.aq_conv3_umma_status(ct.byref(status)) == 0 and status.value == 0
+    assert lib.aq_conv3_forward(cin, cout, 0, x.data_ptr(), w.data_ptr(), b.data_ptr(), out.data_ptr(),
+                                *shape, None) == 0
+    torch.cuda.synchronize()
+    ref = torch.nn.functional.conv3d(
+        x.float().reshape(*shape, cin).permute(3, 0, 1, 2)[None],
+        w.float().reshape(3, 3, 3, cout, cin).permute(3, 4, 0, 1, 2), b, padding=1)
+    got = out.float().reshape(*shape, cout).permute(3, 0, 1, 2)[None]
+    assert float((got - ref).norm() / ref.norm()) < 8e-3
+    assert lib.aq_conv3_umma_status(ct.byref(status)) == 0 and status.value == 0
