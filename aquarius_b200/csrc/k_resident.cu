@@ -29,12 +29,17 @@
 // outnumber the CTAs, each CTA walks its tiles one after another per block
 // and reloads each whole box from L2 (same results, not resident).
 //
-// Threads.  One per (8-level x segment, y row, z-quad) of the box; a warp is
-// 4 whole y rows of 8 quads.  A thread keeps the rhs and fluid marks of its
-// 8 quads in registers and walks its segment in x with a 3-quad window
-// (x-1, x, x+1), so a quad costs one shared load for x+1, one each for y+1
-// and y-1 (consecutive quads of consecutive rows: conflict-free 16-byte
-// loads), and two shuffles for z+1 and z-1.
+// Threads.  One per (XS-level x segment, y row, z-quad) of the box (XS = 8,
+// 12 or 16 per shape: fewer threads with more registers each, so the rhs of
+// every level stays in registers without spills); a warp is 4 whole y rows
+// of 8 quads.  A thread keeps the rhs and fluid marks of its XS quads in
+// registers and walks its segment in x with a 3-quad window (x-1, x, x+1),
+// so a quad costs one shared load for x+1, one each for y+1 and y-1
+// (consecutive quads of consecutive rows: conflict-free 16-byte loads), and
+// two shuffles for z+1 and z-1.  Levels without fluid in the whole warp are
+// skipped (their cells stay 0 in both buffers).  The division by 6 is the
+// FMA-corrected reciprocal product; a sweep in which some sum leaves its
+// exact range is repeated by the CTA with IEEE divides.
 //
 // Residual checks (RESIDUAL mode, every `check` sweeps; once at the end in
 // FIXED mode): FP64 ||b - A p||^2 over the tiles' fluid cells, per thread in
@@ -69,25 +74,14 @@ __device__ __forceinline__ bool div6_fast_ok(float s) {
 }
 __device__ __forceinline__ float div6(float s) { return div6_fast_ok(s) ? div6_fast(s) : __fdiv_rn(s, 6.f); }
 
-// div6_fast_ok for all four sums of a quad: +0 (every non-fluid cell away
-// from the fluid sums to +0 each sweep) or 2^-123 <= |s| <= FLT_MAX (false
-// for NaN), as float compares.
-__device__ __forceinline__ bool div6_fast_ok_f(float s) {
-  constexpr float lo = 0x1p-123f, hi = 0x1.fffffep127f;
-  return (fabsf(s) >= lo && fabsf(s) <= hi) || __float_as_uint(s) == 0u;
-}
-__device__ __forceinline__ bool div6_quad_fast_ok(const float4& s) {
-  return div6_fast_ok_f(s.x) && div6_fast_ok_f(s.y) && div6_fast_ok_f(s.z) && div6_fast_ok_f(s.w);
-}
-
 namespace {
 
-template <int TX, int TY>
+template <int TX, int TY, int XS>
 struct Res {
   static constexpr int K = 4, TZ = 24;
   static constexpr int EX = TX + 2 * K, EY = TY + 2 * K, EZ = TZ + 2 * K;
   static constexpr int EQ = EZ / 4;        // 8 z-quads per box row
-  static constexpr int XSEG = 8;           // x levels per thread
+  static constexpr int XSEG = XS;          // x levels per thread
   static constexpr int NXS = EX / XSEG;    // x segments
   static constexpr int THREADS = NXS * EY * EQ;
   static constexpr int PL4 = EY * EQ;      // float4 per x plane of a buffer
@@ -182,25 +176,25 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity
 // barrier ordered before it) and the others' are seen through the acquire
 // poll.  Gives up after spin_limit polls or one second,
 // whichever comes first: it then sets *fail and returns false, and after any
-// failure every barrier returns false at once.
+// failure every later barrier returns false within 64 polls.
 __device__ __forceinline__ bool res_barrier(unsigned int* bar, unsigned target, int* fail, unsigned spin_limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
+    // arrive at once (a failure elsewhere shows in the poll below); the
+    // failure flag is read every 64 polls only, as a read after an acquire
+    // waits for it
     int ok = 1;
-    if (*reinterpret_cast<volatile int*>(fail)) {
-      ok = 0;
-    } else {
-      asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
-      unsigned spins = 0;
-      const unsigned long long t0 = global_ns();
-      while (ld_acquire_u32(bar) < target) {
-        if (++spins > spin_limit || *reinterpret_cast<volatile int*>(fail) ||
-            ((spins & 255u) == 0u && global_ns() - t0 > 1000000000ull)) {
-          atomicExch(fail, 1);
-          ok = 0;
-          break;
-        }
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+    unsigned spins = 0;
+    const unsigned long long t0 = global_ns();
+    while (ld_acquire_u32(bar) < target) {
+      ++spins;
+      if (spins > spin_limit ||
+          ((spins & 63u) == 0u && (*reinterpret_cast<volatile int*>(fail) || global_ns() - t0 > 1000000000ull))) {
+        atomicExch(fail, 1);
+        ok = 0;
+        break;
       }
     }
     s_ok = ok;
@@ -223,12 +217,6 @@ __device__ __forceinline__ double cta_sum(double v, double* s_red) {
   return t;  // valid in thread 0
 }
 
-
-// The quotients of a quad whose sums leave the fast path: IEEE divides, out
-// of line so the common path carries no predicated copy of them.
-__device__ __noinline__ float4 div6_quad_slow(float4 s) {
-  return make_float4(__fdiv_rn(s.x, 6.f), __fdiv_rn(s.y, 6.f), __fdiv_rn(s.z, 6.f), __fdiv_rn(s.w, 6.f));
-}
 
 // FP64 ||b - A p||^2 of the fluid cells (bits 0-3 of f) of a z-quad, in cell
 // order, each as b + (x+1 + x-1 + y+1 + y-1 + z+1 + z-1) - 6 p.
@@ -258,14 +246,75 @@ __device__ __forceinline__ double quad_residual(const float4& xp, const float4& 
 }
 
 
-template <int TX, int TY>
-__global__ void __launch_bounds__(Res<TX, TY>::THREADS, 1)
+// One sweep of one thread's x segment: the XSEG z-quads at S, S + PL4, ...
+// (levels of jmask only) into D.  Levels are compile-time (registers only);
+// x neighbours from a 3-quad window, the x + 1 neighbour clamped to level
+// jlast (the box's last level, where the x+1 face is a wall: the cell
+// itself), x - 1 of level 0 the cell itself at an x = 0 wall (xm_self);
+// y neighbours at offsets ymo and ypo; z neighbours by shuffle (the cell
+// itself at the box's z faces).  Non-fluid cells carry rhs 1 and are written
+// as 0; lanes outside the region (act false) write nothing.  Without IEEE the quotient
+// is the FMA-corrected reciprocal product, exact while every |sum| of a quad
+// is in [2^-123, FLT_MAX]; the return value says that some sum of a lane in
+// the region was not (min/max skip a NaN sum, whose quotient is NaN either
+// way).
+template <int XSEG, int PL4, bool IEEE>
+__device__ __forceinline__ bool res_sweep(const float4* __restrict__ S, float4* __restrict__ D, int ymo, int ypo,
+                                          const float4 (&rb)[XSEG], unsigned long long fl, unsigned jmask, int jlast,
+                                          bool xm_self, bool act, bool zl_self, bool zh_self) {
+  constexpr unsigned FULL = 0xffffffffu;
+  bool bad = false;
+  float4 pc = S[0];
+  float4 pm = S[xm_self ? 0 : -PL4];
+#pragma unroll
+  for (int j = 0; j < XSEG; ++j) {
+    const float4 pn = S[min(j + 1, jlast) * PL4];
+    if ((jmask >> j) & 1u) {
+      float zl = __shfl_up_sync(FULL, pc.w, 1), zh = __shfl_down_sync(FULL, pc.x, 1);
+      zl = zl_self ? pc.x : zl;
+      zh = zh_self ? pc.w : zh;
+      const float4 ym = S[j * PL4 + ymo], yp = S[j * PL4 + ypo];
+      const float4 b = rb[j];
+      // per cell: x+1, x-1, y+1, y-1, z+1, z-1, rhs, summed in that order
+      float s0 = pn.x + pm.x, s1 = pn.y + pm.y, s2 = pn.z + pm.z, s3 = pn.w + pm.w;
+      s0 += yp.x; s1 += yp.y; s2 += yp.z; s3 += yp.w;
+      s0 += ym.x; s1 += ym.y; s2 += ym.z; s3 += ym.w;
+      s0 += pc.y; s1 += pc.z; s2 += pc.w; s3 += zh;
+      s0 += zl;   s1 += pc.x; s2 += pc.y; s3 += pc.z;
+      s0 += b.x;  s1 += b.y;  s2 += b.z;  s3 += b.w;
+      float q0, q1, q2, q3;
+      if (IEEE) {
+        q0 = __fdiv_rn(s0, 6.f);
+        q1 = __fdiv_rn(s1, 6.f);
+        q2 = __fdiv_rn(s2, 6.f);
+        q3 = __fdiv_rn(s3, 6.f);
+      } else {
+        const float mn = fminf(fminf(fabsf(s0), fabsf(s1)), fminf(fabsf(s2), fabsf(s3)));
+        const float mx = fmaxf(fmaxf(fabsf(s0), fabsf(s1)), fmaxf(fabsf(s2), fabsf(s3)));
+        bad |= !(mn >= 0x1p-123f && mx <= 0x1.fffffep127f);
+        q0 = div6_fast(s0);
+        q1 = div6_fast(s1);
+        q2 = div6_fast(s2);
+        q3 = div6_fast(s3);
+      }
+      const unsigned f = (unsigned)(fl >> (4 * j));
+      if (act) D[j * PL4] = make_float4((f & 1u) ? q0 : 0.f, (f & 2u) ? q1 : 0.f, (f & 4u) ? q2 : 0.f,
+                                        (f & 8u) ? q3 : 0.f);
+    }
+    pm = pc;
+    pc = pn;
+  }
+  return bad && act;
+}
+
+template <int TX, int TY, int XS>
+__global__ void __launch_bounds__(Res<TX, TY, XS>::THREADS, 1)
     k_resident_solve(Dims d, float* __restrict__ pa, float* __restrict__ pb, const float* __restrict__ rhs,
                      const int8_t* __restrict__ type, const int* __restrict__ tiles, const int* __restrict__ n_tiles,
                      unsigned int* __restrict__ bar, double* __restrict__ part, SolveState* __restrict__ ss,
                      int fixed_sweeps, int check, int max_iters, double tol, BarrierTest bt,
                      const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b) {
-  using R = Res<TX, TY>;
+  using R = Res<TX, TY, XS>;
   constexpr int EQ = R::EQ, PL4 = R::PL4, XSEG = R::XSEG, K = R::K;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(128) float4 smem4[];  // [2][EX][EY][EQ]; TMA destinations are 128-byte aligned
@@ -289,7 +338,11 @@ __global__ void __launch_bounds__(Res<TX, TY>::THREADS, 1)
   const int it0 = ss->iterations;  // sweeps a warm start already did
 
   float4 rb[XSEG];  // rhs of this thread's quads (0 on non-fluid cells)
-  unsigned fl = 0u;  // bit 4 j + c: cell c of the quad at level xa + j is fluid
+  unsigned long long fl = 0ull;  // bit 4 j + c: cell c of the quad at level xa + j is fluid
+  // bit j: some lane of the warp holds fluid at level xa + j.  Resident tiles
+  // skip the other levels (their cells are 0 in both shared buffers for the
+  // whole solve); tiles that take turns in one CTA sweep every level.
+  unsigned wmask = (1u << XSEG) - 1u;
   int cur = 0;  // global buffer of the current iterate (0: pa, 1: pb)
   int par = 0;  // shared buffer of the current iterate
 
@@ -319,19 +372,27 @@ __global__ void __launch_bounds__(Res<TX, TY>::THREADS, 1)
     if (full) {
       const bool colin = ly < t.ny && 4 * qq < t.nz;
       const int base = (t.ex * d.sy + t.ey + ly) * d.sz + t.ez + 4 * qq;
-      fl = 0u;
+      fl = 0ull;
 #pragma unroll
       for (int j = 0; j < XSEG; ++j) {
         const int x = xa + j;
-        rb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        rb[j] = make_float4(1.f, 1.f, 1.f, 1.f);
         if (colin && x < t.nx) {
           const int c = base + x * d.sy * d.sz;
           const char4 ty = *reinterpret_cast<const char4*>(type + c);
           const unsigned f = (ty.x == kFluid ? 1u : 0u) | (ty.y == kFluid ? 2u : 0u) | (ty.z == kFluid ? 4u : 0u) |
                              (ty.w == kFluid ? 8u : 0u);
-          fl |= f << (4 * j);
-          if (f) rb[j] = __ldg(reinterpret_cast<const float4*>(rhs + c));
+          fl |= (unsigned long long)f << (4 * j);
+          if (f) {
+            const float4 b = __ldg(reinterpret_cast<const float4*>(rhs + c));
+            rb[j] = make_float4((f & 1u) ? b.x : 1.f, (f & 2u) ? b.y : 1.f, (f & 4u) ? b.z : 1.f, (f & 8u) ? b.w : 1.f);
+          }
         }
+      }
+      if (resident) {
+        wmask = 0u;
+#pragma unroll
+        for (int j = 0; j < XSEG; ++j) wmask |= (__any_sync(FULL, (fl >> (4 * j)) & 15u) ? 1u : 0u) << j;
       }
     }
     bool done = mbar_wait_bounded(mbar, tma_phase, spin_limit);
@@ -352,50 +413,26 @@ __global__ void __launch_bounds__(Res<TX, TY>::THREADS, 1)
     const int ylo = (t.cut & 4) ? s : 0, yhi = t.ny - ((t.cut & 8) ? s : 0);
     const int zlo = (t.cut & 16) ? s : 0, zhi = t.nz - ((t.cut & 32) ? s : 0);
     const bool act = ly >= ylo && ly < yhi && 4 * qq + 4 > zlo && 4 * qq < zhi;
-    const bool zl_self = qq == 0, zh_self = 4 * qq + 4 >= t.nz;
-    const float4* S = smem4 + par * R::BUF4 + col;
+    // levels of this segment inside the region (and, resident, holding fluid)
+    const int jl = max(xlo - xa, 0), jh = min(xhi - xa, XSEG);
+    const unsigned jmask = jh > jl ? (((1u << jh) - 1u) & ~((1u << jl) - 1u)) & wmask : 0u;
+    const float4* S = smem4 + par * R::BUF4 + col + xa * PL4;
+    float4* D = smem4 + (par ^ 1) * R::BUF4 + col + xa * PL4;
     // ly == 0 and ly == ny - 1 are in the region only at walls; rows past the
     // box (clipped boxes) read their own column, so no read leaves the buffer
-    const float4* Sym = S - (ly == 0 ? 0 : EQ);
-    const float4* Syp = S + (ly >= t.ny - 1 ? 0 : EQ);
-    float4* D = smem4 + (par ^ 1) * R::BUF4 + col;
-    if (xa < xhi && xa + XSEG > xlo) {  // warp-uniform
-      float4 pc = S[xa * PL4];
-      float4 pm = xa > 0 ? S[(xa - 1) * PL4] : pc;  // x == 0 in the region only at a wall
-#pragma unroll
-      for (int j = 0; j < XSEG; ++j) {
-        const int x = xa + j;
-        const float4 pn = x + 1 < t.nx ? S[(x + 1) * PL4] : pc;
-        if (x >= xlo && x < xhi) {
-          float zl = __shfl_up_sync(FULL, pc.w, 1), zh = __shfl_down_sync(FULL, pc.x, 1);
-          if (zl_self) zl = pc.x;  // box z face: a wall, or a cell outside the region
-          if (zh_self) zh = pc.w;
-          const float4 ym = Sym[x * PL4], yp = Syp[x * PL4];
-          const float4 b = rb[j];
-          float4 sm;
-          sm.x = pn.x + pm.x; sm.x += yp.x; sm.x += ym.x; sm.x += pc.y; sm.x += zl; sm.x += b.x;
-          sm.y = pn.y + pm.y; sm.y += yp.y; sm.y += ym.y; sm.y += pc.z; sm.y += pc.x; sm.y += b.y;
-          sm.z = pn.z + pm.z; sm.z += yp.z; sm.z += ym.z; sm.z += pc.w; sm.z += pc.y; sm.z += b.z;
-          sm.w = pn.w + pm.w; sm.w += yp.w; sm.w += ym.w; sm.w += zh; sm.w += pc.z; sm.w += b.w;
-          const bool ok = !act || div6_quad_fast_ok(sm);
-          float4 qv;
-          if (ok) {
-            qv = make_float4(div6_fast(sm.x), div6_fast(sm.y), div6_fast(sm.z), div6_fast(sm.w));
-          } else {
-            qv = div6_quad_slow(sm);
-          }
-          const unsigned f = (fl >> (4 * j)) & 15u;
-          qv.x = (f & 1u) ? qv.x : 0.f;
-          qv.y = (f & 2u) ? qv.y : 0.f;
-          qv.z = (f & 4u) ? qv.z : 0.f;
-          qv.w = (f & 8u) ? qv.w : 0.f;
-          if (act) D[x * PL4] = qv;
-        }
-        pm = pc;
-        pc = pn;
-      }
+    const int ymo = ly == 0 ? 0 : -EQ, ypo = ly >= t.ny - 1 ? 0 : EQ;
+    const bool zl_self = qq == 0, zh_self = 4 * qq + 4 >= t.nz;
+    const int jlast = t.nx - 1 - xa;  // x + 1 of level jlast is outside the box (a wall)
+    bool bad = false;
+    if (jmask)  // warp-uniform
+      bad = res_sweep<XSEG, PL4, false>(S, D, ymo, ypo, rb, fl, jmask, jlast, xa == 0, act, zl_self, zh_self);
+    // a sum outside the fast quotient's range anywhere in the CTA's region:
+    // the sweep again with IEEE divides (it reads only buffer par, so it can
+    // repeat)
+    if (__syncthreads_or(bad)) {
+      if (jmask) res_sweep<XSEG, PL4, true>(S, D, ymo, ypo, rb, fl, jmask, jlast, xa == 0, act, zl_self, zh_self);
+      __syncthreads();
     }
-    __syncthreads();
     par ^= 1;
   };
 
@@ -593,10 +630,11 @@ __global__ void __launch_bounds__(1024) k_tile_list(Dims d, int tbx, int tby, in
 struct ShapeInfo {
   int tx, ty, tz;
 };
-// Tile shapes of the resident plan (plan.xc indexes this table); z is 24
-// cells (a 32-cell box) for all.
+// Tile shapes of the resident plan (plan.xc indexes this table; the x levels
+// per thread of each are in dispatch below); z is 24 cells (a 32-cell box)
+// for all.
 constexpr ShapeInfo kShapes[] = {{8, 40, 24}, {16, 24, 24}, {8, 32, 24}, {16, 16, 24},
-                                 {8, 16, 24}, {24, 16, 24}, {8, 48, 24}};
+                                 {8, 16, 24}, {24, 16, 24}, {8, 40, 24}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -613,9 +651,9 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 // Tensor map of a pressure buffer: 3D (z, y, x), fp32, boxes of (32, EY, EX)
 // cells, zero fill past the domain.
-template <int TX, int TY>
+template <int TX, int TY, int XS>
 cudaError_t box_map(CUtensorMap* m, const Dims& d, float* p) {
-  using R = Res<TX, TY>;
+  using R = Res<TX, TY, XS>;
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   if (!enc || reinterpret_cast<uintptr_t>(p) % 16 != 0 || d.sz % 4 != 0) return cudaErrorInvalidValue;
   const cuuint64_t dims[3] = {(cuuint64_t)d.sz, (cuuint64_t)d.sy, (cuuint64_t)d.sx};
@@ -628,15 +666,15 @@ cudaError_t box_map(CUtensorMap* m, const Dims& d, float* p) {
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-template <int TX, int TY>
+template <int TX, int TY, int XS>
 cudaError_t launch_res(cudaStream_t st, const Dims& d, int ctas, float* pa, float* pb, const float* rhs,
                        const int8_t* type, const int* tiles, const int* n_tiles, unsigned int* bar, double* part,
                        SolveState* ss, int fixed_sweeps, int check, int max_iters, double tol, BarrierTest bt) {
-  using R = Res<TX, TY>;
-  auto fn = &k_resident_solve<TX, TY>;
+  using R = Res<TX, TY, XS>;
+  auto fn = &k_resident_solve<TX, TY, XS>;
   CUtensorMap ma, mb;
-  cudaError_t e = box_map<TX, TY>(&ma, d, pa);
-  if (e == cudaSuccess) e = box_map<TX, TY>(&mb, d, pb);
+  cudaError_t e = box_map<TX, TY, XS>(&ma, d, pa);
+  if (e == cudaSuccess) e = box_map<TX, TY, XS>(&mb, d, pb);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, R::SMEM);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t lc = {};
@@ -653,10 +691,10 @@ cudaError_t launch_res(cudaStream_t st, const Dims& d, int ctas, float* pa, floa
                             max_iters, tol, bt, ma, mb);
 }
 
-template <int TX, int TY>
+template <int TX, int TY, int XS>
 int occupancy_of(int device) {
-  using R = Res<TX, TY>;
-  auto fn = &k_resident_solve<TX, TY>;
+  using R = Res<TX, TY, XS>;
+  auto fn = &k_resident_solve<TX, TY, XS>;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, R::SMEM) != cudaSuccess) return 0;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, R::THREADS, R::SMEM) != cudaSuccess) return 0;
@@ -665,26 +703,26 @@ int occupancy_of(int device) {
   return per_sm >= 1 ? sms : 0;  // one CTA per SM
 }
 
-// Dispatch over the shape: calls f.template operator()<TX, TY>().
+// Dispatch over the shape: calls f.template operator()<TX, TY, XS>().
 template <typename F>
-auto dispatch(int shape, const F& f) -> decltype(f.template operator()<8, 40>()) {
-#define AQ_RES_CASE(S, A, B) \
-  if (shape == S) return f.template operator()<A, B>();
-  AQ_RES_CASE(0, 8, 40)
-  AQ_RES_CASE(1, 16, 24)
-  AQ_RES_CASE(2, 8, 32)
-  AQ_RES_CASE(3, 16, 16)
-  AQ_RES_CASE(4, 8, 16)
-  AQ_RES_CASE(5, 24, 16)
-  AQ_RES_CASE(6, 8, 48)
+auto dispatch(int shape, const F& f) -> decltype(f.template operator()<8, 40, 16>()) {
+#define AQ_RES_CASE(S, A, B, X) \
+  if (shape == S) return f.template operator()<A, B, X>();
+  AQ_RES_CASE(0, 8, 40, 16)
+  AQ_RES_CASE(1, 16, 24, 12)
+  AQ_RES_CASE(2, 8, 32, 16)
+  AQ_RES_CASE(3, 16, 16, 12)
+  AQ_RES_CASE(4, 8, 16, 8)
+  AQ_RES_CASE(5, 24, 16, 16)
+  AQ_RES_CASE(6, 8, 40, 8)
 #undef AQ_RES_CASE
-  return decltype(f.template operator()<8, 40>())();
+  return decltype(f.template operator()<8, 40, 16>())();
 }
 
 struct OccupancyOf {
   int device;
-  template <int A, int B>
-  int operator()() const { return occupancy_of<A, B>(device); }
+  template <int A, int B, int X>
+  int operator()() const { return occupancy_of<A, B, X>(device); }
 };
 
 struct LaunchRes {
@@ -702,9 +740,9 @@ struct LaunchRes {
   int fixed_sweeps, check, max_iters;
   double tol;
   BarrierTest bt;
-  template <int A, int B>
+  template <int A, int B, int X>
   cudaError_t operator()() const {
-    return launch_res<A, B>(st, d, ctas, pa, pb, rhs, type, tiles, n_tiles, bar, part, ss, fixed_sweeps, check,
+    return launch_res<A, B, X>(st, d, ctas, pa, pb, rhs, type, tiles, n_tiles, bar, part, ss, fixed_sweeps, check,
                             max_iters, tol, bt);
   }
 };

@@ -1001,7 +1001,7 @@ def run_profile_case(case: str):
     """Small, fixed cases for single-kernel ncu captures (no JSON line):
     jacobi: the 128^3 workload's system after 3 steps, 6 sweeps of the
     default plan; resident: the same system, 40 sweeps of the resident plan
-    (one cooperative launch, 8x40x16 tiles, 960 threads); p2g: the same
+    (one cooperative launch, 8x40x24 tiles, 384 threads); p2g: the same
     state, the particle-to-grid stage twice; batch-rows: 32 scenes of the batch set, 6 batched sweeps;
     conv: two U-Net inferences at 128^3 on seeded random inputs; mesh: two
     surface meshes of the 128^3 workload's initial particles; pbf / pcisph:

@@ -281,7 +281,8 @@ aq_status aq_selfcheck_division(int32_t device, uint64_t* mismatches);
  * x_planes 1; sz % 4 == 0).  rows = 4: the whole solve in one cooperative
  * launch of resident tiles: each CTA keeps a tile of the grid (x_planes
  * selects the shape: 0 8x40x24, 1 16x24x24, 2 8x32x24, 3 16x16x24,
- * 4 8x16x24, 5 24x16x24, 6 8x48x24 cells) with a `levels`-cell halo (4) in
+ * 4 8x16x24, 5 24x16x24 cells, 6 8x40x24 with twice the threads) with a
+ * `levels`-cell halo (4) in
  * shared memory for the whole solve and exchanges halos every `levels`
  * sweeps (sz % 4 == 0).  rows = 8, 16, 32:
  * the temporally blocked kernel with `levels` sweeps (1, 2, 4, 8) per launch
