@@ -2,8 +2,12 @@
 
     python -m aquarius_b200.train_unet --size 64 --scenes 500 --train-steps 12000 --calibrate-scale \
         --out aquarius_b200/weights/unet_64.bin
-    python -m aquarius_b200.train_unet --size 128 --scenes 40 --adopt aquarius_b200/weights/unet_64.bin \
-        --calibrate-scale --out aquarius_b200/weights/unet_128.bin
+    python -m aquarius_b200.train_unet --size 128 --scenes 500 --init aquarius_b200/weights/unet_64.bin \
+        --train-steps 6000 --lr 2e-4 --residual-weight 1.0 --select-every 500 --calibrate-scale \
+        --out aquarius_b200/weights/unet_128.bin
+    python -m aquarius_b200.train_unet --size 256 --scenes 25 --init aquarius_b200/weights/unet_128.bin \
+        --train-steps 1500 --lr 1e-4 --residual-weight 1.0 --select-every 250 --calibrate-scale \
+        --out aquarius_b200/weights/unet_256.bin
 
 Training pairs: seeded ball-drop scenes (a pool of random depth 0.1-0.4 under
 1-3 spheres of radius 0.08-0.2 at random positions, 8 particles per cell),
@@ -15,6 +19,10 @@ trained by the library's own kernels (Adam, cosine learning rate) on 90% of
 the pairs and evaluated on the rest (mean relative L2 pressure error over
 fluid cells).  `--adopt` skips training and takes a trained network as it is
 (the fully convolutional network applies to any grid size divisible by 4).
+`--init` starts from a trained network (fine-tuning); `--select-every` then
+trains in chunks and keeps the chunk's weights, the starting ones included,
+whose held-out 20-sweep residual ratio (the fallback rule's quantity) is
+lowest.
 `--calibrate-scale` then picks the network's output scale, among multiples
 of its current one, that minimises the mean ratio of the residuals after 20
 Jacobi sweeps from the prediction and from zero on the held-out pairs (all
@@ -25,7 +33,9 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import pathlib
+import tempfile
 import time
 
 import numpy as np
@@ -110,6 +120,10 @@ def main():
     ap.add_argument("--adopt", type=str, default=None, help="weights file to use as it is (no training)")
     ap.add_argument("--calibrate-scale", action="store_true",
                     help="choose the output scale by the 20-sweep residual ratio on held-out pairs")
+    ap.add_argument("--select-every", type=int, default=0,
+                    help="train in chunks of this many steps (learning rate on one cosine over all steps) and "
+                         "keep the weights, the starting ones included, with the lowest held-out 20-sweep "
+                         "residual ratio")
     ap.add_argument("--out", type=str, default=None)
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args()
@@ -119,6 +133,7 @@ def main():
     n = len(ds)
     net = UNet(device=args.device, seed=args.seed)
     t0 = time.perf_counter()
+    selection = None
     if args.adopt:
         net.load(args.adopt)
         n_train, n_test = 0, n
@@ -131,9 +146,29 @@ def main():
             net.load(args.init)
         net.train(ds, 0, n_train, steps=1, lr=0.0)  # output scale from the training targets
         before = net.evaluate(ds, n_train, n_test) if n_test else None
-        loss = net.train(ds, 0, n_train, steps=args.train_steps, lr=args.lr, seed=args.seed,
-                         out_scale=net.output_scale(), residual_weight=args.residual_weight,
-                         residual_sweeps=args.residual_sweeps)
+        if args.select_every > 0 and n_test:
+            best_path = pathlib.Path(tempfile.mkdtemp()) / "best.bin"
+            net.save(best_path)
+            best = net.evaluate_warm(ds, n_train, n_test, args.residual_sweeps)
+            selection = [[0, best]]
+            done, loss = 0, None
+            while done < args.train_steps:
+                k = min(args.select_every, args.train_steps - done)
+                lr_k = args.lr * 0.5 * (1.0 + math.cos(math.pi * done / args.train_steps))
+                loss = net.train(ds, 0, n_train, steps=k, lr=lr_k, seed=args.seed + done,
+                                 out_scale=net.output_scale(), residual_weight=args.residual_weight,
+                                 residual_sweeps=args.residual_sweeps)
+                done += k
+                r = net.evaluate_warm(ds, n_train, n_test, args.residual_sweeps)
+                selection.append([done, r])
+                if r < best:
+                    best = r
+                    net.save(best_path)
+            net.load(best_path)
+        else:
+            loss = net.train(ds, 0, n_train, steps=args.train_steps, lr=args.lr, seed=args.seed,
+                             out_scale=net.output_scale(), residual_weight=args.residual_weight,
+                             residual_sweeps=args.residual_sweeps)
         after = net.evaluate(ds, n_train, n_test) if n_test else None
         train_err = net.evaluate(ds, 0, min(n_train, 64))
     train_s = time.perf_counter() - t0
@@ -151,7 +186,8 @@ def main():
     net.save(out)
     warm = check_warm(net, args.size, args.device) if args.check_warm else None
     print(json.dumps(dict(info, size=args.size, train_pairs=n_train, test_pairs=n_test, warm_check=warm,
-                          adopted=args.adopt, scale_calibration=calibration,
+                          adopted=args.adopt, init=args.init, scale_calibration=calibration,
+                          selection=selection,
                           residual_weight=args.residual_weight, residual_sweeps=args.residual_sweeps,
                           train_steps=args.train_steps, train_s=train_s, final_loss=loss,
                           test_rel_error_before=before, test_rel_error_after=after,

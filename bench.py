@@ -931,27 +931,23 @@ def run_sph(args, rank: int, world: int, dist):
     s.close()
 
 
-def run_multiphase(args, rank: int, world: int, dist):
-    """Multiphase FLIP with diffusion at 256^3: a phase-0 pool (concentration
-    c = 0) fills y < 0.35, a phase-1 sphere (c = 1) of radius 0.12 sits at
-    (0.5, 0.75, 0.5), 8 particles per fluid cell, D = 1e-4, dt = 0.0025,
-    zero-init Jacobi to relative residual 1e-4 (cap 2000), 100 diffusion
-    sweeps.  Reports steps/s, the concentration-mass conservation error (the
-    change of the phase-1 fraction sum over the run) and the pressure error
-    against the FP64 PCG."""
+def _multiphase_run(args, size: int, dev: int, dist, net=None) -> dict:
+    """One timed run of the multiphase workload; with `net` the pressure
+    solve starts from the learned warm start (zero-init Jacobi as its
+    fallback and judge), else from zero."""
     import torch
 
     import aquarius_b200 as aq
     from aquarius_b200 import _abi
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(dev)
-    size = args.size if args.size != 128 else 256
     vols = [dict(shape="box", min=(0, 0, 0), max=(1, 0.35, 1), phase=0),
             dict(shape="sphere", center=(0.5, 0.75, 0.5), radius=0.12, phase=1)]
     cfg = _abi.make_config((size, size, size), vols, timestep=0.0025, diffusion_coeff=1e-4, phase_count=2,
-                           pressure_init=_abi.PRESSURE_ZERO, solve_mode=_abi.SOLVE_RESIDUAL, rel_residual=1e-4,
-                           max_iterations=2000, check_interval=40, device=dev)
+                           pressure_init=_abi.PRESSURE_LEARNED if net is not None else _abi.PRESSURE_ZERO,
+                           solve_mode=_abi.SOLVE_RESIDUAL, rel_residual=1e-4, max_iterations=2000,
+                           check_interval=40, device=dev)
     f = aq.Fluid(cfg)
+    if net is not None:
+        f.set_warm_start(net)
     m0 = f.phase_mass()
     stream = torch.cuda.ExternalStream(f.stream(), device=dev)
     f.step(args.warmup)
@@ -975,26 +971,67 @@ def run_multiphase(args, rank: int, world: int, dist):
     s1 = f.solve_stats()
     m1 = f.phase_mass()
     pcg = f.pcg_reference(rel_tol=1e-12, max_iter=400000)
-    launches = args.steps * per_step + (s1["total_blocks"] - s0["total_blocks"]) * per_block
+    out = {"ms": ms, "clocks": clk, "particles": f.particleCount,
+           "launches": args.steps * per_step + (s1["total_blocks"] - s0["total_blocks"]) * per_block,
+           "concentration_mass": {"phase1_initial": m0[1], "phase1_final": m1[1],
+                                  "rel_error": abs(m1[1] - m0[1]) / m0[1] if m0[1] else None,
+                                  "total_rel_error": abs(sum(m1) - sum(m0)) / sum(m0),
+                                  "steps": args.warmup + args.steps},
+           "solver": {"sweeps_per_step": (s1["total_sweeps"] - s0["total_sweeps"]) / args.steps,
+                      "last_rel_residual": s1["rel_residual"], "converged": s1["converged"],
+                      "pressure_rel_error_vs_fp64_pcg": pcg["rel_error"], "pcg_iterations": pcg["iterations"]}}
+    if net is not None:
+        out["solver"]["warm_start_kept"] = s1["warm_start"] == 1
+        out["solver"]["residual_after_20_sweeps"] = {"learned": s1["warm_rel_residual"],
+                                                     "zero_init": s1["zero_rel_residual"]}
+    f.close()
+    return out
+
+
+def run_multiphase(args, rank: int, world: int, dist):
+    """Multiphase FLIP with diffusion at 256^3: a phase-0 pool (concentration
+    c = 0) fills y < 0.35, a phase-1 sphere (c = 1) of radius 0.12 sits at
+    (0.5, 0.75, 0.5), 8 particles per fluid cell, D = 1e-4, dt = 0.0025,
+    Jacobi to relative residual 1e-4 (cap 2000) started from the learned warm
+    start (the network fine-tuned on 256^3 pairs, weights/unet_256.bin), 100
+    diffusion sweeps; the same run from zero-init pressure is reported beside
+    it.  Reports steps/s, the concentration-mass conservation error (the
+    change of the phase-1 fraction sum over the run) and the pressure error
+    against the FP64 PCG."""
+    import torch
+
+    import aquarius_b200 as aq
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    size = args.size if args.size != 128 else 256
+    wpath = ROOT / "aquarius_b200" / "weights" / f"unet_{size}.bin"
+    plain = _multiphase_run(args, size, dev, dist)
+    learned = None
+    if wpath.exists() and not args.no_learned:
+        net = aq.UNet(device=dev, weights=wpath)
+        learned = _multiphase_run(args, size, dev, dist, net)
+        learned["weights"] = wpath.name
+        learned["time_vs_plain"] = learned["ms"] / plain["ms"]
+        net.close()
+    main = learned if learned is not None else plain
+    init = "learned warm start (weights/" + wpath.name + ")" if learned is not None else "zero-init"
     line = {"metric": "multiphase FLIP steps/s at 256^3 x 8ppc with diffusion, Jacobi to relative residual 1e-4",
-            "value": weak_scaling_value(args.steps, world, ms), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "value": weak_scaling_value(args.steps, world, main["ms"]), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": main["ms"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"multiphase {size}^3 x 8ppc: phase-0 pool y<0.35 + phase-1 sphere r=0.12 at "
-                                   "(0.5,0.75,0.5), D=1e-4, dt=0.0025, 100 diffusion sweeps, zero-init Jacobi to "
-                                   "rel-res 1e-4 cap 2000 (the learned warm start has no 256^3 network here)",
-                       "particles": f.particleCount, "l2": "working set > 126 MB L2"},
-            "gpu_launches": int(launches), "clocks": clk,
-            "concentration_mass": {"phase1_initial": m0[1], "phase1_final": m1[1],
-                                   "rel_error": abs(m1[1] - m0[1]) / m0[1] if m0[1] else None,
-                                   "total_rel_error": abs(sum(m1) - sum(m0)) / sum(m0),
-                                   "steps": args.warmup + args.steps},
-            "solver": {"sweeps_per_step": (s1["total_sweeps"] - s0["total_sweeps"]) / args.steps,
-                       "last_rel_residual": s1["rel_residual"],
-                       "pressure_rel_error_vs_fp64_pcg": pcg["rel_error"], "pcg_iterations": pcg["iterations"]}}
+                                   f"(0.5,0.75,0.5), D=1e-4, dt=0.0025, 100 diffusion sweeps, {init} Jacobi to "
+                                   "rel-res 1e-4 cap 2000",
+                       "particles": main["particles"], "l2": "working set > 126 MB L2"},
+            "gpu_launches": int(main["launches"]), "clocks": main["clocks"],
+            "concentration_mass": main["concentration_mass"], "solver": main["solver"],
+            "plain": {"steps_per_s": weak_scaling_value(args.steps, world, plain["ms"]),
+                      "ms_per_step": plain["ms"] / args.steps, "solver": plain["solver"],
+                      "concentration_mass": plain["concentration_mass"]}}
+    if learned is not None:
+        line["learned"] = {"weights": learned["weights"], "time_vs_plain": learned["time_vs_plain"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    f.close()
 
 
 def run_profile_case(case: str):
