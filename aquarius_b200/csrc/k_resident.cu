@@ -246,63 +246,85 @@ __device__ __forceinline__ double quad_residual(const float4& xp, const float4& 
 }
 
 
+// The Jacobi update of one z-quad (cells c..c+3 along z): pn / pm the x + 1
+// / x - 1 quads, yp / ym the y neighbours, pc the quad itself, zl / zh the
+// z - 1 neighbour of cell 0 and z + 1 of cell 3, b the rhs; f its fluid
+// marks (bits 0-3).  Non-fluid cells give 0.  Without IEEE, bad is set when
+// some sum leaves the fast quotient's exact range.
+template <bool IEEE>
+__device__ __forceinline__ float4 quad_update(const float4& pn, const float4& pm, const float4& yp, const float4& ym,
+                                              const float4& pc, float zl, float zh, const float4& b, unsigned f,
+                                              bool& bad) {
+  // per cell: x+1, x-1, y+1, y-1, z+1, z-1, rhs, summed in that order
+  float s0 = pn.x + pm.x, s1 = pn.y + pm.y, s2 = pn.z + pm.z, s3 = pn.w + pm.w;
+  s0 += yp.x; s1 += yp.y; s2 += yp.z; s3 += yp.w;
+  s0 += ym.x; s1 += ym.y; s2 += ym.z; s3 += ym.w;
+  s0 += pc.y; s1 += pc.z; s2 += pc.w; s3 += zh;
+  s0 += zl;   s1 += pc.x; s2 += pc.y; s3 += pc.z;
+  s0 += b.x;  s1 += b.y;  s2 += b.z;  s3 += b.w;
+  float q0, q1, q2, q3;
+  if (IEEE) {
+    q0 = __fdiv_rn(s0, 6.f);
+    q1 = __fdiv_rn(s1, 6.f);
+    q2 = __fdiv_rn(s2, 6.f);
+    q3 = __fdiv_rn(s3, 6.f);
+  } else {
+    const float mn = fminf(fminf(fabsf(s0), fabsf(s1)), fminf(fabsf(s2), fabsf(s3)));
+    const float mx = fmaxf(fmaxf(fabsf(s0), fabsf(s1)), fmaxf(fabsf(s2), fabsf(s3)));
+    bad |= !(mn >= 0x1p-123f && mx <= 0x1.fffffep127f);
+    q0 = div6_fast(s0);
+    q1 = div6_fast(s1);
+    q2 = div6_fast(s2);
+    q3 = div6_fast(s3);
+  }
+  return make_float4((f & 1u) ? q0 : 0.f, (f & 2u) ? q1 : 0.f, (f & 4u) ? q2 : 0.f, (f & 8u) ? q3 : 0.f);
+}
+
 // One sweep of one thread's x segment: the XSEG z-quads at S, S + PL4, ...
-// (levels of jmask only) into D.  Levels are compile-time (registers only);
-// x neighbours from a 3-quad window, the x + 1 neighbour clamped to level
-// jlast (the box's last level, where the x+1 face is a wall: the cell
-// itself), x - 1 of level 0 the cell itself at an x = 0 wall (xm_self);
-// y neighbours at offsets ymo and ypo; z neighbours by shuffle (the cell
-// itself at the box's z faces).  Non-fluid cells carry rhs 1 and are written
-// as 0; lanes outside the region (act false) write nothing.  Without IEEE the quotient
-// is the FMA-corrected reciprocal product, exact while every |sum| of a quad
-// is in [2^-123, FLT_MAX]; the return value says that some sum of a lane in
-// the region was not (min/max skip a NaN sum, whose quotient is NaN either
-// way).
+// (levels of jmask only) into D, two levels per step so that their loads and
+// sums overlap.  Levels are compile-time (registers only); x neighbours from
+// a sliding window, the x + 1 neighbour clamped to level jlast (the box's
+// last level, where the x+1 face is a wall: the cell itself), x - 1 of level
+// 0 the cell itself at an x = 0 wall (xm_self); y neighbours at offsets ymo
+// and ypo; z neighbours by shuffle (the cell itself at the box's z faces).
+// Non-fluid cells carry rhs 1 and are written as 0; lanes outside the region
+// (act false) write nothing.  Without IEEE the quotient is the FMA-corrected
+// reciprocal product, exact while every |sum| of a quad is in [2^-123,
+// FLT_MAX]; the return value says that some sum of a lane in the region was
+// not (min/max skip a NaN sum, whose quotient is NaN either way).
 template <int XSEG, int PL4, bool IEEE>
 __device__ __forceinline__ bool res_sweep(const float4* __restrict__ S, float4* __restrict__ D, int ymo, int ypo,
                                           const float4 (&rb)[XSEG], unsigned long long fl, unsigned jmask, int jlast,
                                           bool xm_self, bool act, bool zl_self, bool zh_self) {
+  static_assert(XSEG % 2 == 0, "levels go in pairs");
   constexpr unsigned FULL = 0xffffffffu;
   bool bad = false;
   float4 pc = S[0];
   float4 pm = S[xm_self ? 0 : -PL4];
 #pragma unroll
-  for (int j = 0; j < XSEG; ++j) {
-    const float4 pn = S[min(j + 1, jlast) * PL4];
-    if ((jmask >> j) & 1u) {
-      float zl = __shfl_up_sync(FULL, pc.w, 1), zh = __shfl_down_sync(FULL, pc.x, 1);
-      zl = zl_self ? pc.x : zl;
-      zh = zh_self ? pc.w : zh;
-      const float4 ym = S[j * PL4 + ymo], yp = S[j * PL4 + ypo];
-      const float4 b = rb[j];
-      // per cell: x+1, x-1, y+1, y-1, z+1, z-1, rhs, summed in that order
-      float s0 = pn.x + pm.x, s1 = pn.y + pm.y, s2 = pn.z + pm.z, s3 = pn.w + pm.w;
-      s0 += yp.x; s1 += yp.y; s2 += yp.z; s3 += yp.w;
-      s0 += ym.x; s1 += ym.y; s2 += ym.z; s3 += ym.w;
-      s0 += pc.y; s1 += pc.z; s2 += pc.w; s3 += zh;
-      s0 += zl;   s1 += pc.x; s2 += pc.y; s3 += pc.z;
-      s0 += b.x;  s1 += b.y;  s2 += b.z;  s3 += b.w;
-      float q0, q1, q2, q3;
-      if (IEEE) {
-        q0 = __fdiv_rn(s0, 6.f);
-        q1 = __fdiv_rn(s1, 6.f);
-        q2 = __fdiv_rn(s2, 6.f);
-        q3 = __fdiv_rn(s3, 6.f);
-      } else {
-        const float mn = fminf(fminf(fabsf(s0), fabsf(s1)), fminf(fabsf(s2), fabsf(s3)));
-        const float mx = fmaxf(fmaxf(fabsf(s0), fabsf(s1)), fmaxf(fabsf(s2), fabsf(s3)));
-        bad |= !(mn >= 0x1p-123f && mx <= 0x1.fffffep127f);
-        q0 = div6_fast(s0);
-        q1 = div6_fast(s1);
-        q2 = div6_fast(s2);
-        q3 = div6_fast(s3);
-      }
-      const unsigned f = (unsigned)(fl >> (4 * j));
-      if (act) D[j * PL4] = make_float4((f & 1u) ? q0 : 0.f, (f & 2u) ? q1 : 0.f, (f & 4u) ? q2 : 0.f,
-                                        (f & 8u) ? q3 : 0.f);
+  for (int j = 0; j < XSEG; j += 2) {
+    const float4 p1 = S[min(j + 1, jlast) * PL4];  // level j + 1 (x + 1 of level j)
+    const float4 p2 = S[min(j + 2, jlast) * PL4];  // x + 1 of level j + 1
+    const unsigned pair = (jmask >> j) & 3u;
+    if (pair) {
+      float zl0 = __shfl_up_sync(FULL, pc.w, 1), zh0 = __shfl_down_sync(FULL, pc.x, 1);
+      float zl1 = __shfl_up_sync(FULL, p1.w, 1), zh1 = __shfl_down_sync(FULL, p1.x, 1);
+      zl0 = zl_self ? pc.x : zl0;
+      zh0 = zh_self ? pc.w : zh0;
+      zl1 = zl_self ? p1.x : zl1;
+      zh1 = zh_self ? p1.w : zh1;
+      const float4 ym0 = S[j * PL4 + ymo], yp0 = S[j * PL4 + ypo];
+      const float4 ym1 = S[(j + 1) * PL4 + ymo], yp1 = S[(j + 1) * PL4 + ypo];
+      bool bad0 = false, bad1 = false;
+      const float4 q0 = quad_update<IEEE>(p1, pm, yp0, ym0, pc, zl0, zh0, rb[j], (unsigned)(fl >> (4 * j)), bad0);
+      const float4 q1 = quad_update<IEEE>(p2, pc, yp1, ym1, p1, zl1, zh1, rb[j + 1],
+                                          (unsigned)(fl >> (4 * (j + 1))), bad1);
+      if (act && (pair & 1u)) D[j * PL4] = q0;
+      if (act && (pair & 2u)) D[(j + 1) * PL4] = q1;
+      bad |= ((pair & 1u) && bad0) || ((pair & 2u) && bad1);
     }
-    pm = pc;
-    pc = pn;
+    pm = p1;
+    pc = p2;
   }
   return bad && act;
 }
