@@ -404,6 +404,12 @@ cudaError_t launch_tri_setup(cudaStream_t st, const RenderParams& P, const float
 cudaError_t launch_tri_emit(cudaStream_t st, const RenderParams& P, const RenderTri* tris, const int* off, int ntri,
                             unsigned* keys, int* vals);
 cudaError_t launch_container_setup(cudaStream_t st, const RenderParams& P, RenderTri* tris, int* live);
+// Stable LSD radix sort (k_sort.cu) of n (key, value) pairs by the low `bits`
+// bits of the keys, ascending (or descending) into (k1, v1); (k0, v0) is left
+// as it was.  tmp: radix_sort_temp_ints(n) ints of scratch.
+size_t radix_sort_temp_ints(int n);
+cudaError_t radix_sort_pairs(cudaStream_t st, const unsigned* k0, const int* v0, unsigned* k1, int* v1, int n,
+                             int bits, bool descending, int* tmp);
 // range[key] = [first, last+1) of each key's run in sorted keys[0..n)
 cudaError_t launch_tile_ranges(cudaStream_t st, const unsigned* keys, int n, int2* range);
 // The phase-thickness pass over the 8x8 sprite tiles, in the given order.

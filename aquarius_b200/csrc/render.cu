@@ -9,7 +9,6 @@
 // FluidMeshRenderer.  The GL draw calls become: per-primitive setup kernels,
 // a stable sort of (tile, primitive) pairs by tile, and two per-tile kernels
 // (phase thickness, then the frame).
-#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <climits>
@@ -122,7 +121,7 @@ struct aq_renderer {
   DevBuf<unsigned> tload, tload2;  // sprite-tile list lengths (longest-first order)
   DevBuf<int> tids, torder;
   DevBuf<unsigned long long> totals;
-  DevBuf<unsigned char> cub_tmp;
+  DevBuf<int> sort_tmp;
   DevBuf<uchar4> image;          // the image when the caller passes none
   DevBuf<float> points_vbo, mesh_vbo;  // aq_fluid_draw's VBOs
   const uint8_t* last_image = nullptr;
@@ -138,7 +137,7 @@ struct aq_renderer {
     tris.release();
     ctris.release();
     skeys.release(); skeys2.release(); tkeys.release(); tkeys2.release();
-    srange.release(); trange.release(); totals.release(); cub_tmp.release();
+    srange.release(); trange.release(); totals.release(); sort_tmp.release();
     image.release(); points_vbo.release(); mesh_vbo.release();
     tload.release(); tload2.release(); tids.release(); torder.release();
     if (sky) cudaFree(sky);
@@ -152,10 +151,8 @@ struct aq_renderer {
   aq_status sort_pairs(DevBuf<unsigned>& keys, DevBuf<unsigned>& keys2, DevBuf<int>& vals, DevBuf<int>& vals2,
                        int n, int ntiles, DevBuf<int2>& range) {
     const int bits = key_bits(ntiles);
-    size_t bytes = 0;
-    AQR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.p, keys2.p, vals.p, vals2.p, n, 0, bits, stream));
-    AQR_TRY(cub_tmp.ensure(bytes));
-    AQR_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp.p, bytes, keys.p, keys2.p, vals.p, vals2.p, n, 0, bits, stream));
+    AQR_TRY(sort_tmp.ensure(radix_sort_temp_ints(n)));
+    AQR_CUDA(radix_sort_pairs(stream, keys.p, vals.p, keys2.p, vals2.p, n, bits, false, sort_tmp.p));
     AQR_CUDA(launch_tile_ranges(stream, keys2.p, n, range.p));
     ++launches;
     return AQ_OK;
@@ -419,12 +416,8 @@ aq_status aq_renderer_draw(aq_renderer* r, const aq_draw_command* dc, const floa
     AQR_TRY(r->tload.ensure(nstiles)); AQR_TRY(r->tload2.ensure(nstiles));
     AQR_TRY(r->tids.ensure(nstiles)); AQR_TRY(r->torder.ensure(nstiles));
     AQR_CUDA(launch_tile_load(st, r->srange.p, nstiles, r->tload.p, r->tids.p));
-    size_t bytes = 0;
-    AQR_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, r->tload.p, r->tload2.p, r->tids.p,
-                                                       r->torder.p, nstiles, 0, 32, st));
-    AQR_TRY(r->cub_tmp.ensure(bytes));
-    AQR_CUDA(cub::DeviceRadixSort::SortPairsDescending(r->cub_tmp.p, bytes, r->tload.p, r->tload2.p, r->tids.p,
-                                                       r->torder.p, nstiles, 0, 32, st));
+    AQR_TRY(r->sort_tmp.ensure(radix_sort_temp_ints(nstiles)));
+    AQR_CUDA(radix_sort_pairs(st, r->tload.p, r->tids.p, r->tload2.p, r->torder.p, nstiles, 32, true, r->sort_tmp.p));
     AQR_CUDA(launch_phase(st, P, r->srange.p, r->torder.p, r->svals2.p, r->spr.p, r->frac.p, r->phase.p));
     r->launches += 2;
   } else {

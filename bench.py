@@ -410,6 +410,10 @@ def run_ours(args, rank: int, world: int, dist):
         line["reference_gpu"] = reference_gpu_comparator(args, dev, plan)
     if not args.no_learned:
         line["learned"] = learned_arm(args, dev, stream, max(plain_rel), ms_max / args.steps, dist, plan)
+        alt = ROOT / "aquarius_b200" / "weights" / f"unet_{args.size}_from64.bin"
+        if alt.exists():  # the 64^3 network with a recalibrated output scale, no training at this size
+            line["learned_from64"] = learned_arm(args, dev, stream, max(plain_rel), ms_max / args.steps, dist,
+                                                 plan, wpath=alt)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(args.size, args.pressure_init, steps=1)
     if rank == 0:
@@ -568,16 +572,17 @@ def reference_gpu_comparator(args, dev, plan, steps: int = 5) -> dict:
             "reference_build": "Fluid/*.cu compiled headless with the reference's flags (-use_fast_math) for sm_100a"}
 
 
-def learned_arm(args, dev, stream, plain_residual: float, plain_ms: float, dist, plan) -> dict:
+def learned_arm(args, dev, stream, plain_residual: float, plain_ms: float, dist, plan, wpath=None) -> dict:
     """The same workload with the learned warm start (AQ_PRESSURE_LEARNED) and
     the plain step's Jacobi plan: (a) to the same target 1e-4 (cap 2000), (b)
     to the residual the plain step reached at its cap, i.e. at equal achieved
-    residual."""
+    residual.  wpath: the network (default weights/unet_<size>.bin)."""
     import torch
 
     import aquarius_b200 as aq
     from aquarius_b200 import _abi
-    wpath = ROOT / "aquarius_b200" / "weights" / f"unet_{args.size}.bin"
+    if wpath is None:
+        wpath = ROOT / "aquarius_b200" / "weights" / f"unet_{args.size}.bin"
     if not wpath.exists():
         return {"unavailable": f"no trained weights for {args.size}^3 ({wpath.name})"}
     net = aq.UNet(device=dev, weights=wpath)
