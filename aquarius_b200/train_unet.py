@@ -8,6 +8,9 @@
     python -m aquarius_b200.train_unet --size 256 --scenes 25 --init aquarius_b200/weights/unet_128.bin \
         --train-steps 1500 --lr 1e-4 --residual-weight 1.0 --select-every 250 --calibrate-scale \
         --out aquarius_b200/weights/unet_256.bin
+    python -m aquarius_b200.train_unet --size 128 --scenes 250 --every 5 --init aquarius_b200/weights/unet_128.bin \
+        --train-steps 4000 --lr 1e-4 --residual-weight 1.0 --select-every 500 --calibrate-scale \
+        --out aquarius_b200/weights/unet_128.bin
 
 Training pairs: seeded ball-drop scenes (a pool of random depth 0.1-0.4 under
 1-3 spheres of radius 0.08-0.2 at random positions, 8 particles per cell),
