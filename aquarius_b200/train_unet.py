@@ -150,24 +150,25 @@ def main():
         net.train(ds, 0, n_train, steps=1, lr=0.0)  # output scale from the training targets
         before = net.evaluate(ds, n_train, n_test) if n_test else None
         if args.select_every > 0 and n_test:
-            best_path = pathlib.Path(tempfile.mkdtemp()) / "best.bin"
-            net.save(best_path)
-            best = net.evaluate_warm(ds, n_train, n_test, args.residual_sweeps)
-            selection = [[0, best]]
-            done, loss = 0, None
-            while done < args.train_steps:
-                k = min(args.select_every, args.train_steps - done)
-                lr_k = args.lr * 0.5 * (1.0 + math.cos(math.pi * done / args.train_steps))
-                loss = net.train(ds, 0, n_train, steps=k, lr=lr_k, seed=args.seed + done,
-                                 out_scale=net.output_scale(), residual_weight=args.residual_weight,
-                                 residual_sweeps=args.residual_sweeps)
-                done += k
-                r = net.evaluate_warm(ds, n_train, n_test, args.residual_sweeps)
-                selection.append([done, r])
-                if r < best:
-                    best = r
-                    net.save(best_path)
-            net.load(best_path)
+            with tempfile.TemporaryDirectory() as tmp:
+                best_path = pathlib.Path(tmp) / "best.bin"
+                net.save(best_path)
+                best = net.evaluate_warm(ds, n_train, n_test, args.residual_sweeps)
+                selection = [[0, best]]
+                done, loss = 0, None
+                while done < args.train_steps:
+                    k = min(args.select_every, args.train_steps - done)
+                    lr_k = args.lr * 0.5 * (1.0 + math.cos(math.pi * done / args.train_steps))
+                    loss = net.train(ds, 0, n_train, steps=k, lr=lr_k, seed=args.seed + done,
+                                     out_scale=net.output_scale(), residual_weight=args.residual_weight,
+                                     residual_sweeps=args.residual_sweeps)
+                    done += k
+                    r = net.evaluate_warm(ds, n_train, n_test, args.residual_sweeps)
+                    selection.append([done, r])
+                    if r < best:
+                        best = r
+                        net.save(best_path)
+                net.load(best_path)
         else:
             loss = net.train(ds, 0, n_train, steps=args.train_steps, lr=args.lr, seed=args.seed,
                              out_scale=net.output_scale(), residual_weight=args.residual_weight,
